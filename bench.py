@@ -1,0 +1,350 @@
+"""Benchmark: Richardson-Lucy Gvox-iter/s on the 3-D bead volume (headline)
+and Gaussian GPix/s on the 2048^2 blob image (secondary), on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one richardson_lucy call (50 iterations) on the 64 x 512 x 512 f32
+bead volume (PSF 31 x 15 x 15, eps 1e-6, zero padding, FFT grid
+128 x 1024 x 1024), inputs resident in HBM.  Under torchrun every rank runs
+its own replica (one volume does not shard); value = all ranks' voxel
+iterations / max-over-ranks time.  One JSON line is printed by rank 0.
+
+--impl reference times the reference's algorithm (direct spatial
+correlation, the oracle's restatement of crates/lucem-ops/src/restore/
+deconvolve.rs:45-149) on the host cores, on a bounded sample of the same
+workload per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SHAPE = (64, 512, 512)
+PSF_SHAPE = (31, 15, 15)
+GRID = (128, 1024, 1024)
+ITERS = 50
+EPS = 1e-6
+METRIC = "RL Gvox-iter/s (3-D Richardson-Lucy, 64x512x512 bead volume, 50 iterations)"
+UNIT = "Gvox-iter/s"
+WORKLOAD = ("rl3d: 64x512x512 f32 bead volume (3000 beads U[1e3,1e4], Gaussian PSF 31x15x15 "
+            "sigma_xy 1.5 sigma_z 3, background 10, Poisson), 50 iterations, eps 1e-6, clip off, "
+            "zero padding, FFT grid 128x1024x1024")
+# CPU sample of the reference algorithm: one iteration on a sub-volume.
+CPU_SAMPLE = (16, 128, 128)
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(kind):
+    """DRAM bytes per launch of `kind` from the committed ncu summary (or None)."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        v = d.get(kind)
+        return None if v is None else float(v)
+    return None
+
+
+# ---------------------------------------------------------------------------
+# clocks
+
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_id: str):
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", device_id], stdout=self.file,
+                                         stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.4)
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        self.file.flush()
+        with open(self.file.name) as f:
+            rows = [r.strip().split(", ") for r in f if r.strip()]
+        os.unlink(self.file.name)
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows if len(r) >= 9 for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(sm)}
+
+
+def nvsmi_id(dev):
+    import torch
+
+    props = torch.cuda.get_device_properties(dev)
+    uuid = getattr(props, "uuid", None)
+    if uuid is not None:
+        s = str(uuid)
+        return s if s.startswith("GPU-") else "GPU-" + s
+    return str(dev)
+
+
+# ---------------------------------------------------------------------------
+# algorithmic bytes per launch ("Measurement")
+
+
+def rl_kernel_bytes(shape, grid):
+    Z, Y, X = shape
+    Pz, Py, Px = grid
+    Hx = Px // 2 + 1
+    c = 8  # complex64
+    s1 = Z * Y * Hx * c
+    s2 = Z * Py * Hx * c
+    h = Pz * Py * Hx * c
+    v = Z * Y * X * 4
+    return {
+        "rl_col_full": s2 + h + s2,           # z pass: read S2, read H, write S2
+        "rl_col_forward": s1 + s2,            # y forward: read S1, write S2
+        "rl_col_inverse": s2 + s1,            # y inverse: read S2, write S1
+        "rl_row_pass": s1 + v + s1,           # ratio pass: read S1 + obs, write S1 (update: + est)
+    }
+
+
+# ---------------------------------------------------------------------------
+
+
+def cpu_sample_rate(num_threads=0):
+    """Reference algorithm (direct correlation) on a sub-volume, 1 iteration:
+    returns (Gvox-iter/s, seconds, threads)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O  # the CPU restatement (baseline leg only)
+
+    from lucem_b200 import synth
+
+    if num_threads:
+        O.set_threads(num_threads)
+    obs, psf = synth.bead_volume(shape=CPU_SAMPLE, n_beads=max(1, 3000 * int(np.prod(CPU_SAMPLE)) // int(np.prod(SHAPE))),
+                                 seed=synth.SEED_BASE + 101)
+    t0 = time.perf_counter()
+    O.richardson_lucy(obs, psf, num_iter=1, clip=False, filter_epsilon=EPS, mode="constant")
+    dt = time.perf_counter() - t0
+    return int(np.prod(CPU_SAMPLE)) / dt / 1e9, dt, O.get_threads()
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    rates = []
+    for i in range(args.warmup + args.steps):
+        r, dt, threads = cpu_sample_rate()
+        if i >= args.warmup:
+            rates.append((r, dt))
+    value = float(np.median([r for r, _ in rates]))
+    ms = float(np.median([d for _, d in rates])) * 1e3
+    sample = (f"direct-correlation RL (reference algorithm, oracle restatement) on a "
+              f"{CPU_SAMPLE[0]}x{CPU_SAMPLE[1]}x{CPU_SAMPLE[2]} sub-volume of the workload, full 31x15x15 PSF, "
+              f"1 iteration per step")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "parallelism": "host cores"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def gaussian_secondary(dev, peak):
+    """The 2048^2 u16 blob image, sigma 2, reflect, f32 out: GPix/s with L2
+    flushed between calls (inputs + output are 25 MB < L2)."""
+    import torch
+
+    import lucem_b200 as lb
+
+    x = torch.from_numpy(lb.synth.blob_image()).to(dev)
+    out = torch.empty(x.shape, dtype=torch.float32, device=dev)
+    ws = lb.Workspace(dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    s = torch.cuda.current_stream(dev)
+    for _ in range(5):
+        lb.gaussian_blur(x, 2.0, out=out, workspace=ws)
+    n = 50
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
+    torch.cuda.synchronize(dev)
+    for a, b in evs:
+        flush.fill_(1.0)
+        a.record(s)
+        lb.gaussian_blur(x, 2.0, out=out, workspace=ws)
+        b.record(s)
+    torch.cuda.synchronize(dev)
+    ms = float(np.mean([a.elapsed_time(b) for a, b in evs]))
+    px = x.numel()
+    bytes_ = px * (2 + 4)
+    achieved = bytes_ / (ms * 1e-3) / 1e9
+    return {"metric": "Gaussian GPix/s (2048x2048 u16 blob image, sigma 2, 17 taps, reflect, f32 out)",
+            "value": px / (ms * 1e-3) / 1e9, "unit": "GPix/s", "ms_per_call": ms, "l2": "flushed between calls",
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": profile_traffic("gaussian_family_2048")}}
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+
+    import lucem_b200 as lb
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    peak, peak_kind = measured_peaks()
+    obs_h, psf_h = lb.synth.bead_volume(shape=SHAPE, psf_shape=PSF_SHAPE)
+    obs = torch.from_numpy(obs_h).to(dev)
+    psf = torch.from_numpy(psf_h).to(dev)
+    out = torch.empty_like(obs)
+    ws = lb.Workspace(local_rank)
+    s = torch.cuda.current_stream(dev)
+
+    def step(o=obs, p=psf, r=out):
+        return lb.richardson_lucy(o, p, num_iter=ITERS, clip=False, filter_epsilon=EPS, mode="constant",
+                                  grid=GRID, out=r, workspace=ws)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+
+    # per-kernel device times of one step (for the roofline and launch count)
+    ws.set_timing(True)
+    step()
+    kinds = ws.timings()
+    ws.set_timing(False)
+    launches_per_step = sum(c for c, _ in kinds.values())
+
+    sampler = ClockSampler(nvsmi_id(local_rank)) if rank == 0 else None
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(args.steps):
+        step()
+    e1.record(s)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    ms = e0.elapsed_time(e1) / args.steps
+    clocks = sampler.stop() if sampler else None
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    units = int(np.prod(SHAPE)) * ITERS * world
+    value = units / (ms * 1e-3) / 1e9
+
+    # end to end through the public API with pinned host buffers
+    obs_pin = torch.from_numpy(obs_h).pin_memory()
+    psf_pin = torch.from_numpy(psf_h).pin_memory()
+    res_pin = torch.empty(obs_h.shape, dtype=torch.float32).pin_memory()
+    obs_d = torch.empty_like(obs)
+    psf_d = torch.empty_like(psf)
+    torch.cuda.synchronize(dev)
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(s)
+    for _ in range(args.steps):
+        obs_d.copy_(obs_pin, non_blocking=True)
+        psf_d.copy_(psf_pin, non_blocking=True)
+        step(obs_d, psf_d, out)
+        res_pin.copy_(out, non_blocking=True)
+    f1.record(s)
+    torch.cuda.synchronize(dev)
+    e2e_ms = f0.elapsed_time(f1) / args.steps
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = {"value": units / (e2e_ms * 1e-3) / 1e9, "unit": UNIT,
+           "h2d_bytes_per_step": int(obs_h.nbytes + psf_h.nbytes), "d2h_bytes_per_step": int(obs_h.nbytes)}
+
+    if rank != 0:
+        return
+    nbytes = rl_kernel_bytes(SHAPE, GRID)
+    dominant = max(kinds, key=lambda k: kinds[k][1])
+    cnt, tot = kinds[dominant]
+    per_launch_ms = tot / cnt
+    alg = nbytes.get(dominant)
+    achieved = alg / (per_launch_ms * 1e-3) / 1e9 if alg else None
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak if achieved else None, "traffic": profile_traffic(dominant),
+                "kernel": dominant, "launches_per_step": cnt, "us_per_launch": per_launch_ms * 1e3,
+                "algorithmic_bytes_per_launch": alg, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"}
+    step_kernels = {k: {"launches": c, "ms": t, "share": t / sum(v[1] for v in kinds.values())}
+                    for k, (c, t) in kinds.items()}
+    cpu = None
+    if world == 1:
+        r, dt, threads = cpu_sample_rate()
+        cpu = {"value": r, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"direct-correlation RL (reference algorithm) on a {CPU_SAMPLE[0]}x{CPU_SAMPLE[1]}x"
+                         f"{CPU_SAMPLE[2]} sub-volume, full PSF, 1 iteration ({dt:.2f} s)"}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "l2": "working set ~0.95 GB per step (spectra + transfer function) > 126 MB L2; no flush"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": launches_per_step * args.steps, "clocks": clocks, "step_kernels": step_kernels,
+            "secondary": {"gaussian_2048": gaussian_secondary(dev, peak)}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,266 @@
+/*
+ * lucem_b200.h -- C ABI of the B200 (sm_100a) implementation of lucem-ops'
+ * separable Gaussian family and Richardson-Lucy deconvolution.
+ *
+ * This is the layer a Rust `extern "C"` block in lucem-core binds in place of
+ * the CubeCL launches for these operations.  Every entry point cites the
+ * reference interface it replaces (paths inside neuro-kitchen/lucem).
+ *
+ * Conventions
+ *  - Tensors are C-contiguous device arrays described by lucem_tensor (data
+ *    pointer, element type, dims), as lucem-core's DeviceArray
+ *    (crates/lucem-core/src/memory/array.rs:21-27).  The caller owns them.
+ *  - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ *    Launches are asynchronous on it; only functions that say so synchronise.
+ *  - Scratch comes from a lucem_workspace: named slots that only grow, as
+ *    lucem-core's Workspace (crates/lucem-core/src/memory/workspace.rs:10-52).
+ *    A workspace serves one thread of work at a time.
+ *  - A context is bound to one device; constant data (Gaussian taps, PSF
+ *    transfer functions) lives in its mutex-guarded cache, as DeviceCache
+ *    (crates/lucem-core/src/memory/cache.rs:19-44).
+ *  - Return codes mirror OpsError / CoreError
+ *    (crates/lucem-ops/src/error.rs:9-59, crates/lucem-core/src/error.rs:8-38);
+ *    lucem_last_error_message() gives the text of the calling thread's last
+ *    error.  No C++ exception crosses this boundary.
+ *  - Element counts are capped at 2^32-1 per buffer, as
+ *    crates/lucem-core/src/compute/limits.rs:12.
+ *  - Empty inputs return LUCEM_OK with no work, as the reference does.
+ */
+#ifndef LUCEM_B200_H
+#define LUCEM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LUCEM_B200_ABI_VERSION 1
+#define LUCEM_MAX_DIMS 8
+
+typedef enum lucem_status {
+    LUCEM_OK = 0,
+    LUCEM_ERR_SHAPE_MISMATCH = 1,       /* OpsError::ShapeMismatch */
+    LUCEM_ERR_ALIASED_BUFFERS = 2,      /* OpsError::AliasedBuffers */
+    LUCEM_ERR_INVALID_DIMENSION = 3,    /* OpsError::InvalidDimension */
+    LUCEM_ERR_UNKNOWN_PAD_MODE = 4,     /* OpsError::UnknownPadMode */
+    LUCEM_ERR_INVALID_ORIGIN = 5,       /* OpsError::InvalidOrigin */
+    LUCEM_ERR_INVALID_WEIGHTS = 6,      /* OpsError::InvalidWeights */
+    LUCEM_ERR_INVALID_PARAMETER = 7,    /* OpsError::InvalidParameter */
+    LUCEM_ERR_EMPTY_INPUT = 8,          /* OpsError::EmptyInput */
+    LUCEM_ERR_AXIS_OUT_OF_BOUNDS = 9,   /* CoreError::AxisOutOfBounds */
+    LUCEM_ERR_REPEATED_AXIS = 10,       /* CoreError::RepeatedAxis */
+    LUCEM_ERR_TOO_MANY_ELEMENTS = 11,   /* CoreError::TooManyElements */
+    LUCEM_ERR_OUT_OF_DEVICE_MEMORY = 12,/* CoreError::OutOfDeviceMemory */
+    LUCEM_ERR_UNSUPPORTED_DTYPE = 13,   /* element type not accepted by the op */
+    LUCEM_ERR_CUDA = 14,                /* a CUDA runtime call failed */
+    LUCEM_ERR_DEVICE_TIMEOUT = 15,      /* a bounded device wait gave up */
+    LUCEM_ERR_INVALID_HANDLE = 16       /* NULL / foreign context or workspace */
+} lucem_status;
+
+typedef enum lucem_dtype { LUCEM_U8 = 1, LUCEM_U16 = 2, LUCEM_F32 = 3 } lucem_dtype;
+
+/* crates/lucem-ops/src/core/pad.rs:84-88 (same ids). */
+typedef enum lucem_pad_mode {
+    LUCEM_PAD_REFLECT = 0,  /* d c b a | a b c d | d c b a */
+    LUCEM_PAD_CONSTANT = 1, /* k k k k | a b c d | k k k k */
+    LUCEM_PAD_NEAREST = 2,  /* a a a a | a b c d | d d d d */
+    LUCEM_PAD_MIRROR = 3,   /*   d c b | a b c d | c b a   */
+    LUCEM_PAD_WRAP = 4      /* a b c d | a b c d | a b c d */
+} lucem_pad_mode;
+
+typedef struct lucem_tensor {
+    void *data;     /* device pointer, C-contiguous */
+    int32_t dtype;  /* lucem_dtype */
+    int32_t ndim;   /* 0..LUCEM_MAX_DIMS */
+    int64_t dims[LUCEM_MAX_DIMS];
+} lucem_tensor;
+
+typedef struct lucem_ctx lucem_ctx;
+typedef struct lucem_workspace lucem_workspace;
+
+/* ---- library, context, workspace ------------------------------------- */
+
+int32_t lucem_abi_version(void);
+/* Text of the calling thread's last error ("" if none). */
+const char *lucem_last_error_message(void);
+/* crates/lucem-core/src/device.rs:23-189 (ComputeTarget + client) reduced to
+ * "one CUDA device": binds `device`, reads its SM count. */
+lucem_status lucem_ctx_create(int32_t device, lucem_ctx **out);
+void lucem_ctx_destroy(lucem_ctx *ctx);
+/* crates/lucem-core/src/memory/workspace.rs:21-52. */
+lucem_status lucem_workspace_create(lucem_ctx *ctx, lucem_workspace **out);
+void lucem_workspace_destroy(lucem_workspace *ws);
+size_t lucem_workspace_capacity_bytes(const lucem_workspace *ws);
+/* Per-kernel device timing, the analogue of the pipeline's EvalTimings
+ * (engine/lucem-pipeline/src/eval.rs:59-71): while enabled, every kernel the
+ * workspace's calls launch is bracketed by CUDA events.  lucem_workspace_timings
+ * synchronises on those events and reports, per kernel kind, the launches and
+ * the summed device milliseconds since timing was (re)enabled; names are
+ * written as NUL-terminated strings of at most 31 chars in a [cap][32] array. */
+lucem_status lucem_workspace_set_timing(lucem_workspace *ws, int32_t enable);
+lucem_status lucem_workspace_timings(lucem_workspace *ws, char *names, double *ms, int64_t *launches,
+                                     int32_t cap, int32_t *n_out);
+/* Parses a pad-mode name with the reference's aliases
+ * (crates/lucem-ops/src/core/pad.rs:46-56); LUCEM_ERR_UNKNOWN_PAD_MODE else. */
+lucem_status lucem_pad_mode_parse(const char *name, int32_t *mode_out);
+
+/* ---- host-side helpers (no device work) ------------------------------ */
+
+/* crates/lucem-ops/src/filter/gaussian.rs:22-63: writes 2*radius+1 f64 taps. */
+lucem_status lucem_gaussian_kernel_1d(double sigma, uint32_t order, int64_t radius, double *out);
+/* crates/lucem-ops/src/filter/gaussian.rs:83-85: floor(truncate*sigma+0.5). */
+int64_t lucem_gaussian_radius(double truncate, double sigma);
+/* crates/lucem-ops/src/core/kernels/pad.rs:11-34 (-1 = constant fill). */
+int64_t lucem_pad_index(int64_t p, int64_t len, int32_t mode);
+
+/* ---- Gaussian family ------------------------------------------------- */
+
+/* crates/lucem-ops/src/filter/gaussian.rs:133-156 (GaussianBlur), plus the
+ * input scale of uint_to_unit_float (crates/lucem-ops/src/core/elementwise.rs
+ * :205-230) for integer inputs: value = (float)raw * input_scale. */
+typedef struct lucem_gaussian_settings {
+    const uint32_t *orders; int32_t n_orders;   /* broadcast per axis; {0} when n_orders == 0 */
+    int32_t mode;                               /* lucem_pad_mode */
+    double cval;
+    double truncate;                            /* 4.0 */
+    const int64_t *radii; int32_t n_radii;      /* None when n_radii == 0 */
+    const int64_t *axes; int32_t n_axes;        /* None (all axes) when axes == NULL */
+    int32_t has_channel_axis; int64_t channel_axis;
+    double input_scale;                         /* 1.0 */
+} lucem_gaussian_settings;
+void lucem_gaussian_settings_default(lucem_gaussian_settings *s);
+
+/* crates/lucem-ops/src/filter/gaussian.rs:176-237 gaussian_blur_into.
+ * in: u8 | u16 | f32 (the cast is fused into the load); out: f32, same dims. */
+lucem_status lucem_gaussian_blur(lucem_ctx *ctx, const lucem_tensor *in, const double *sigmas,
+                                 int32_t n_sigmas, const lucem_gaussian_settings *settings,
+                                 lucem_tensor *out, lucem_workspace *ws, void *stream);
+
+/* crates/lucem-ops/src/filter/gaussian.rs:66-118 (Gaussian1d, gaussian_1d_into).
+ * radius < 0 means None. */
+typedef struct lucem_gaussian_1d_settings {
+    int64_t axis; uint32_t order; int32_t mode; double cval; double truncate; int64_t radius;
+} lucem_gaussian_1d_settings;
+void lucem_gaussian_1d_settings_default(lucem_gaussian_1d_settings *s);
+lucem_status lucem_gaussian_1d(lucem_ctx *ctx, const lucem_tensor *in, double sigma,
+                               const lucem_gaussian_1d_settings *settings, lucem_tensor *out,
+                               void *stream);
+
+/* crates/lucem-ops/src/filter/convolve.rs:17-92 (Correlate1d, correlate_1d):
+ * host f64 weights, cast to f32 and cached per context. */
+typedef struct lucem_correlate_1d_settings {
+    int64_t axis; int32_t mode; double cval; int32_t origin;
+} lucem_correlate_1d_settings;
+lucem_status lucem_correlate_1d(lucem_ctx *ctx, const lucem_tensor *in, const double *weights,
+                                int64_t n_weights, const lucem_correlate_1d_settings *settings,
+                                lucem_tensor *out, void *stream);
+
+/* crates/lucem-ops/src/filter/gaussian.rs:374-390 difference_of_gaussians_into. */
+lucem_status lucem_difference_of_gaussians(lucem_ctx *ctx, const lucem_tensor *in,
+                                           const double *low_sigmas, int32_t n_low,
+                                           const double *high_sigmas, int32_t n_high,
+                                           const lucem_gaussian_settings *settings,
+                                           lucem_tensor *out, lucem_workspace *ws, void *stream);
+/* crates/lucem-ops/src/filter/gaussian.rs:255-288 gaussian_laplace_into. */
+lucem_status lucem_gaussian_laplace(lucem_ctx *ctx, const lucem_tensor *in, const double *sigmas,
+                                    int32_t n_sigmas, int32_t mode, double cval, double truncate,
+                                    lucem_tensor *out, lucem_workspace *ws, void *stream);
+/* crates/lucem-ops/src/filter/gaussian.rs:307-356 gaussian_grad_mag_into. */
+lucem_status lucem_gaussian_grad_mag(lucem_ctx *ctx, const lucem_tensor *in, const double *sigmas,
+                                     int32_t n_sigmas, int32_t mode, double cval, double truncate,
+                                     lucem_tensor *out, lucem_workspace *ws, void *stream);
+/* crates/lucem-ops/src/filter/gaussian.rs:407-421 unsharp_mask_into. */
+lucem_status lucem_unsharp_mask(lucem_ctx *ctx, const lucem_tensor *in, const double *sigmas,
+                                int32_t n_sigmas, double amount,
+                                const lucem_gaussian_settings *settings, lucem_tensor *out,
+                                lucem_workspace *ws, void *stream);
+
+/* Several Gaussian-family responses of one input in one fused pass: the input
+ * tile is read once and every response is written from shared memory.  Each
+ * response is what the named reference function returns for the same input:
+ *   LUCEM_RESP_GAUSSIAN   gaussian_blur(sigma)            (gaussian.rs:176)
+ *   LUCEM_RESP_DOG        difference_of_gaussians(sigma, sigma2) (:374)
+ *   LUCEM_RESP_LAPLACE    gaussian_laplace(sigma)         (:255)
+ *   LUCEM_RESP_GRAD_MAG   gaussian_grad_mag(sigma)        (:307)
+ *   LUCEM_RESP_UNSHARP    unsharp_mask(sigma, amount)     (:407)
+ * Sigmas are isotropic over the filtered axes (the last two).  This is the
+ * per-tile function a lucem-pipeline tile walk calls
+ * (engine/lucem-pipeline/src/custom.rs:233-251) when an Op list holds several
+ * Gaussian-family ops (engine/lucem-pipeline/src/ops.rs:795-800). */
+typedef enum lucem_response_kind {
+    LUCEM_RESP_GAUSSIAN = 0, LUCEM_RESP_DOG = 1, LUCEM_RESP_LAPLACE = 2,
+    LUCEM_RESP_GRAD_MAG = 3, LUCEM_RESP_UNSHARP = 4
+} lucem_response_kind;
+typedef struct lucem_response {
+    int32_t kind; double sigma; double sigma2; double amount; lucem_tensor out;
+} lucem_response;
+lucem_status lucem_gaussian_family(lucem_ctx *ctx, const lucem_tensor *in,
+                                   const lucem_response *responses, int32_t n_responses,
+                                   int32_t mode, double cval, double truncate, double input_scale,
+                                   lucem_workspace *ws, void *stream);
+
+/* ---- tiling and batched tiles ---------------------------------------- */
+
+/* crates/lucem-core/src/tiling.rs:13-49 Block ([z, y, x]). */
+typedef struct lucem_block {
+    int64_t index;
+    int64_t origin[3], size[3];
+    int64_t read_origin[3], read_size[3];
+} lucem_block;
+/* crates/lucem-core/src/tiling.rs:54-78 schedule: writes at most `cap` blocks,
+ * sets *n_out to the full count. */
+lucem_status lucem_schedule(const int64_t dims[3], const int64_t block[3], const int64_t halo[3],
+                            lucem_block *out, int64_t cap, int64_t *n_out);
+
+/* Runs lucem_gaussian_family on every block of every channel of a [C, H, W]
+ * slide, as the tile walk does (engine/lucem-pipeline/src/custom.rs:199-251):
+ * each block's read part is filtered with the pad mode applied at the read
+ * part's borders and only the owned part is written, into [C, H, W] outputs.
+ * blocks[] come from lucem_schedule over [1, H, W]; every channel is walked.
+ * persistent != 0: one persistent launch walks the whole work list (uneven
+ * edge tiles included); persistent == 0: one launch per block and channel (the
+ * plain per-tile drop-in). */
+lucem_status lucem_gaussian_family_tiles(lucem_ctx *ctx, const lucem_tensor *slide,
+                                         const lucem_block *blocks, int64_t n_blocks,
+                                         const lucem_response *responses, int32_t n_responses,
+                                         int32_t mode, double cval, double truncate,
+                                         double input_scale, int32_t persistent,
+                                         lucem_workspace *ws, void *stream);
+
+/* ---- Richardson-Lucy ------------------------------------------------- */
+
+/* crates/lucem-ops/src/restore/deconvolve.rs:19-41 (RichardsonLucy) plus the
+ * FFT grid.  grid[d] == 0 picks the smallest length with factors 2, 3, 5, 7
+ * (even along x) that holds the padded correlation: n + k/2 for
+ * LUCEM_PAD_CONSTANT, n + 2*(k/2) for the other modes. */
+typedef struct lucem_rl_settings {
+    int32_t num_iter;          /* 30 */
+    int32_t clip;              /* 1 */
+    int32_t has_filter_epsilon; double filter_epsilon; /* None -> 1e-12, floor 1e-15 */
+    int32_t mode;              /* LUCEM_PAD_REFLECT; LUCEM_PAD_CONSTANT = zero padding */
+    int64_t grid[3];           /* per axis of the input; 0 = automatic */
+} lucem_rl_settings;
+void lucem_rl_settings_default(lucem_rl_settings *s);
+
+/* crates/lucem-ops/src/restore/deconvolve.rs:45-162 richardson_lucy_into,
+ * computed with FFT convolution for 2-D and 3-D f32 inputs.  Every pad mode
+ * of the reference is honoured (the correlation input is extended by k/2
+ * samples per axis with the pad map; zero padding needs no extension).  The
+ * PSF is copied to the host once per call to normalise it (as the reference
+ * does at :77), so the call synchronises the stream once before the
+ * iterations are queued; its transfer function is cached in the workspace. */
+lucem_status lucem_richardson_lucy(lucem_ctx *ctx, const lucem_tensor *in, const lucem_tensor *psf,
+                                   const lucem_rl_settings *settings, lucem_tensor *out,
+                                   lucem_workspace *ws, void *stream);
+/* The grid lucem_richardson_lucy would use (host only). */
+lucem_status lucem_rl_grid(const int64_t *dims, const int64_t *kdims, int32_t ndim, int32_t mode,
+                           const int64_t *requested, int64_t *grid_out);
+/* Smallest length >= n that the FFT kernels support (host only). */
+int64_t lucem_fft_good_length(int64_t n, int32_t even);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,1674 @@
+// api.cpp -- the C ABI (include/lucem_b200.h): argument checks with the
+// reference's error semantics, pass planning, the workspace and constant
+// cache, and the host drivers of the filter and Richardson-Lucy kernels.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+
+using namespace lucem;
+
+// ---------------------------------------------------------------------------
+// Errors: thread-local message + status, as OpsError's Display text
+// (crates/lucem-ops/src/error.rs:9-59).
+
+namespace {
+
+thread_local std::string g_last_error;
+
+lucem_status fail(lucem_status st, const char *fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return st;
+}
+
+lucem_status ok() {
+    return LUCEM_OK;
+}
+
+lucem_status cuda_fail(int err, const char *what) {
+    return fail(LUCEM_ERR_CUDA, "%s: %s", what, cudaGetErrorString(static_cast<cudaError_t>(err)));
+}
+
+#define CUDA_TRY(expr, what)                                                  \
+    do {                                                                      \
+        int _e = static_cast<int>(expr);                                      \
+        if (_e != 0) return cuda_fail(_e, what);                              \
+    } while (0)
+
+std::string dims_str(const lucem_tensor *t) {
+    std::string s = "[";
+    for (int i = 0; i < t->ndim; ++i) {
+        if (i) s += ", ";
+        s += std::to_string(t->dims[i]);
+    }
+    return s + "]";
+}
+
+int64_t numel(const lucem_tensor *t) {
+    int64_t n = 1;
+    for (int i = 0; i < t->ndim; ++i) n *= t->dims[i];
+    return n;
+}
+
+size_t dtype_size(int dt) {
+    switch (dt) {
+    case LUCEM_U8: return 1;
+    case LUCEM_U16: return 2;
+    case LUCEM_F32: return 4;
+    default: return 0;
+    }
+}
+
+lucem_status check_tensor(const char *name, const lucem_tensor *t) {
+    if (!t) return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `%s`: null tensor", name);
+    if (t->ndim < 0 || t->ndim > LUCEM_MAX_DIMS)
+        return fail(LUCEM_ERR_INVALID_DIMENSION, "%s expects 0..%d-D array, got %d-D", name,
+                    LUCEM_MAX_DIMS, t->ndim);
+    if (dtype_size(t->dtype) == 0)
+        return fail(LUCEM_ERR_UNSUPPORTED_DTYPE, "%s: unsupported element type %d", name, t->dtype);
+    // crates/lucem-core/src/compute/limits.rs:16-22 (overflow refused too).
+    int64_t n = 1;
+    for (int i = 0; i < t->ndim; ++i) {
+        if (t->dims[i] < 0)
+            return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `%s`: negative dimension", name);
+        if (t->dims[i] != 0 && n > kMaxDeviceElements / t->dims[i])
+            return fail(LUCEM_ERR_TOO_MANY_ELEMENTS,
+                        "%s %s needs more than %lld elements in one device buffer (kernels use "
+                        "32-bit indices): use smaller tiles or batches",
+                        name, dims_str(t).c_str(), (long long)kMaxDeviceElements);
+        n *= t->dims[i];
+    }
+    if (n > 0 && !t->data)
+        return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `%s`: null data pointer", name);
+    return ok();
+}
+
+// crates/lucem-ops/src/core/check.rs:10-26.
+lucem_status same_shape(const char *a_name, const lucem_tensor *a, const char *b_name,
+                        const lucem_tensor *b) {
+    bool same = a->ndim == b->ndim;
+    for (int i = 0; same && i < a->ndim; ++i) same = a->dims[i] == b->dims[i];
+    if (same) return ok();
+    return fail(LUCEM_ERR_SHAPE_MISMATCH, "%s shape %s does not match %s shape %s", a_name,
+                dims_str(a).c_str(), b_name, dims_str(b).c_str());
+}
+
+// crates/lucem-ops/src/core/check.rs:47-57: byte ranges that overlap.
+lucem_status not_aliased(const lucem_tensor *a, const lucem_tensor *b) {
+    uintptr_t a0 = reinterpret_cast<uintptr_t>(a->data), b0 = reinterpret_cast<uintptr_t>(b->data);
+    uintptr_t a1 = a0 + (uintptr_t)(numel(a) * (int64_t)dtype_size(a->dtype));
+    uintptr_t b1 = b0 + (uintptr_t)(numel(b) * (int64_t)dtype_size(b->dtype));
+    if (numel(a) > 0 && numel(b) > 0 && a0 < b1 && b0 < a1)
+        return fail(LUCEM_ERR_ALIASED_BUFFERS,
+                    "input and output arrays must not share the same device buffer");
+    return ok();
+}
+
+lucem_status require_f32_out(const lucem_tensor *out) {
+    if (out->dtype != LUCEM_F32)
+        return fail(LUCEM_ERR_UNSUPPORTED_DTYPE, "output must be f32, got element type %d", out->dtype);
+    return ok();
+}
+
+lucem_status check_mode(int32_t mode) {
+    if (mode < 0 || mode > 4) return fail(LUCEM_ERR_UNKNOWN_PAD_MODE, "boundary pad mode '%d' is not supported (expected reflect, constant, nearest, mirror, or wrap)", mode);
+    return ok();
+}
+
+// numpy axis normalisation (crates/lucem-core/src/shape.rs:48-58).
+lucem_status norm_axis(int64_t axis, int ndim, int *out) {
+    int64_t a = axis < 0 ? axis + ndim : axis;
+    if (a < 0 || a >= ndim)
+        return fail(LUCEM_ERR_AXIS_OUT_OF_BOUNDS, "axis %lld is out of bounds for array of dimension %d",
+                    (long long)axis, ndim);
+    *out = (int)a;
+    return ok();
+}
+
+// crates/lucem-ops/src/core/check.rs:95-109.
+template <typename T>
+lucem_status broadcast(const char *name, const T *vals, int n_vals, int num_axes, std::vector<T> *out) {
+    out->clear();
+    if (num_axes == 0) return ok();
+    if (n_vals == 1) {
+        out->assign(num_axes, vals[0]);
+        return ok();
+    }
+    if (n_vals == num_axes) {
+        out->assign(vals, vals + n_vals);
+        return ok();
+    }
+    return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `%s`: expected 1 or %d values, got %d",
+                name, num_axes, n_vals);
+}
+
+double radius_of(double truncate, double sigma) {
+    double r = std::floor(truncate * sigma + 0.5);
+    return r > 0.0 ? r : 0.0;
+}
+
+// crates/lucem-ops/src/filter/gaussian.rs:22-63.
+void gaussian_taps(double sigma, uint32_t order, int64_t radius, double *out) {
+    if (radius == 0) {
+        out[0] = order == 0 ? 1.0 : 0.0;
+        return;
+    }
+    const double s2 = sigma * sigma;
+    const int64_t n = 2 * radius + 1;
+    double sum = 0.0;
+    for (int64_t i = 0; i < n; ++i) {
+        double x = (double)(i - radius);
+        out[i] = std::exp(-0.5 * (x * x) / s2);
+    }
+    for (int64_t i = 0; i < n; ++i) sum += out[i];
+    for (int64_t i = 0; i < n; ++i) out[i] /= sum;
+    if (order == 0) return;
+    for (int64_t i = 0; i < n; ++i) {
+        double x = (double)(i - radius), q;
+        if (order == 1) q = -x / s2;
+        else if (order == 2) q = (x * x - s2) / (s2 * s2);
+        else if (order == 3) q = -(x * x * x - 3.0 * x * s2) / (s2 * s2 * s2);
+        else {
+            double hp = 1.0, hc = -x / s2;
+            for (uint32_t k = 1; k < order; ++k) {
+                double hn = (-x / s2) * hc - ((double)k / s2) * hp;
+                hp = hc;
+                hc = hn;
+            }
+            q = hc;
+        }
+        out[i] = ((order % 2 == 1) ? -1.0 : 1.0) * q * out[i];
+    }
+}
+
+}  // namespace
+
+namespace lucem {
+const char *pass_name(int kind) {
+    static const char *names[kPassCount] = {"rl_row_pass", "rl_col_forward", "rl_col_full", "rl_col_inverse",
+                                            "rl_transfer_function", "gaussian_family", "correlate_1d",
+                                            "elementwise"};
+    return kind >= 0 && kind < kPassCount ? names[kind] : "?";
+}
+}  // namespace lucem
+
+// ---------------------------------------------------------------------------
+// Context and workspace.
+
+struct lucem_ctx {
+    int device = 0;
+    int sms = 148;
+    std::mutex mu;
+    // Constant cache: key -> device buffer (crates/lucem-core/src/memory/cache.rs:19-44).
+    std::map<std::string, void *> cache;
+    void *get_or_upload(const std::string &key, const void *host, size_t bytes, int *err) {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) return it->second;
+        void *d = nullptr;
+        int e = (int)cudaMalloc(&d, bytes > 0 ? bytes : 16);
+        if (e) { *err = e; return nullptr; }
+        e = (int)cudaMemcpy(d, host, bytes, cudaMemcpyHostToDevice);
+        if (e) { cudaFree(d); *err = e; return nullptr; }
+        cache[key] = d;
+        return d;
+    }
+};
+
+namespace {
+
+// CUDA events around each launch while a workspace's timing is on.
+struct EventTimer : PassTimer {
+    struct Rec {
+        int kind;
+        cudaEvent_t a, b;
+    };
+    std::vector<Rec> recs;
+    std::vector<cudaEvent_t> pool;
+    double total_ms[kPassCount] = {};
+    int64_t count[kPassCount] = {};
+    cudaEvent_t take() {
+        if (!pool.empty()) {
+            cudaEvent_t e = pool.back();
+            pool.pop_back();
+            return e;
+        }
+        cudaEvent_t e = nullptr;
+        cudaEventCreate(&e);
+        return e;
+    }
+    void begin(int kind, void *stream) override {
+        Rec r{kind, take(), nullptr};
+        cudaEventRecord(r.a, static_cast<cudaStream_t>(stream));
+        recs.push_back(r);
+    }
+    void end(int kind, void *stream) override {
+        if (recs.empty() || recs.back().kind != kind || recs.back().b) return;
+        recs.back().b = take();
+        cudaEventRecord(recs.back().b, static_cast<cudaStream_t>(stream));
+    }
+    int collect() {
+        int err = 0;
+        for (auto &r : recs) {
+            if (!r.b) continue;
+            int e = (int)cudaEventSynchronize(r.b);
+            float ms = 0.f;
+            if (!e) e = (int)cudaEventElapsedTime(&ms, r.a, r.b);
+            if (e && !err) err = e;
+            if (!e) {
+                total_ms[r.kind] += ms;
+                count[r.kind] += 1;
+            }
+        }
+        for (auto &r : recs) {
+            pool.push_back(r.a);
+            if (r.b) pool.push_back(r.b);
+        }
+        recs.clear();
+        return err;
+    }
+    void reset() {
+        collect();
+        for (int k = 0; k < kPassCount; ++k) {
+            total_ms[k] = 0.0;
+            count[k] = 0;
+        }
+    }
+    ~EventTimer() override {
+        for (auto &r : recs) {
+            pool.push_back(r.a);
+            if (r.b) pool.push_back(r.b);
+        }
+        for (auto e : pool) cudaEventDestroy(e);
+    }
+};
+
+struct Slot {
+    void *ptr = nullptr;
+    size_t cap = 0;
+    std::string key;  // what the slot's content was computed from (for caches)
+};
+}  // namespace
+
+namespace {
+// The timer of the workspace the current entry point runs with (if timing).
+thread_local PassTimer *g_timer = nullptr;
+template <typename F>
+int timed(int kind, void *stream, F &&f) {
+    if (g_timer) g_timer->begin(kind, stream);
+    int e = f();
+    if (g_timer) g_timer->end(kind, stream);
+    return e;
+}
+}  // namespace
+
+struct lucem_workspace {
+    lucem_ctx *ctx = nullptr;
+    std::map<std::string, Slot> slots;
+    std::unique_ptr<EventTimer> timer;  // set while timing is enabled
+    PassTimer *t() { return timer.get(); }
+    // crates/lucem-core/src/memory/workspace.rs:28-37: grow-only, budget checked.
+    lucem_status get(const char *name, size_t bytes, void **out, Slot **slot_out = nullptr) {
+        Slot &s = slots[name];
+        if (s.cap < bytes) {
+            if (s.ptr) {
+                cudaFree(s.ptr);
+                s.ptr = nullptr;
+                s.cap = 0;
+                s.key.clear();
+            }
+            size_t free_b = 0, total_b = 0;
+            cudaMemGetInfo(&free_b, &total_b);
+            void *p = nullptr;
+            cudaError_t e = cudaMalloc(&p, bytes);
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                return fail(LUCEM_ERR_OUT_OF_DEVICE_MEMORY,
+                            "%s needs %zu bytes of device memory; the budget leaves %zu (limit %zu)",
+                            name, bytes, free_b, total_b);
+            }
+            s.ptr = p;
+            s.cap = bytes;
+        }
+        *out = s.ptr;
+        if (slot_out) *slot_out = &s;
+        return ok();
+    }
+    ~lucem_workspace() {
+        for (auto &kv : slots)
+            if (kv.second.ptr) cudaFree(kv.second.ptr);
+    }
+};
+
+namespace {
+struct TimerScope {
+    PassTimer *prev;
+    explicit TimerScope(lucem_workspace *ws) : prev(g_timer) { g_timer = ws ? ws->t() : nullptr; }
+    ~TimerScope() { g_timer = prev; }
+};
+}  // namespace
+
+extern "C" {
+
+int32_t lucem_abi_version(void) { return LUCEM_B200_ABI_VERSION; }
+
+const char *lucem_last_error_message(void) { return g_last_error.c_str(); }
+
+lucem_status lucem_ctx_create(int32_t device, lucem_ctx **out) {
+    if (!out) return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `out`: null");
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return fail(LUCEM_ERR_CUDA, "no CUDA device available (%s)", cudaGetErrorString(e));
+    }
+    if (device < 0 || device >= count)
+        return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `device`: %d of %d", device, count);
+    CUDA_TRY(cudaSetDevice(device), "cudaSetDevice");
+    auto *c = new lucem_ctx();
+    c->device = device;
+    cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
+    *out = c;
+    return ok();
+}
+
+void lucem_ctx_destroy(lucem_ctx *ctx) {
+    if (!ctx) return;
+    for (auto &kv : ctx->cache) cudaFree(kv.second);
+    delete ctx;
+}
+
+lucem_status lucem_workspace_create(lucem_ctx *ctx, lucem_workspace **out) {
+    if (!ctx || !out) return fail(LUCEM_ERR_INVALID_HANDLE, "null context or output pointer");
+    auto *w = new lucem_workspace();
+    w->ctx = ctx;
+    *out = w;
+    return ok();
+}
+
+void lucem_workspace_destroy(lucem_workspace *ws) { delete ws; }
+
+lucem_status lucem_workspace_set_timing(lucem_workspace *ws, int32_t enable) {
+    if (!ws) return fail(LUCEM_ERR_INVALID_HANDLE, "null workspace");
+    if (enable) {
+        if (!ws->timer) ws->timer.reset(new EventTimer());
+        ws->timer->reset();
+    } else {
+        ws->timer.reset();
+    }
+    return ok();
+}
+
+lucem_status lucem_workspace_timings(lucem_workspace *ws, char *names, double *ms, int64_t *launches,
+                                     int32_t cap, int32_t *n_out) {
+    if (!ws || !n_out) return fail(LUCEM_ERR_INVALID_HANDLE, "null workspace or output");
+    *n_out = 0;
+    if (!ws->timer) return ok();
+    int e = ws->timer->collect();
+    if (e) return cuda_fail(e, "timing events");
+    int n = 0;
+    for (int k = 0; k < kPassCount; ++k) {
+        if (ws->timer->count[k] == 0) continue;
+        if (n < cap) {
+            if (names) {
+                std::strncpy(names + 32 * n, pass_name(k), 31);
+                names[32 * n + 31] = 0;
+            }
+            if (ms) ms[n] = ws->timer->total_ms[k];
+            if (launches) launches[n] = ws->timer->count[k];
+        }
+        ++n;
+    }
+    *n_out = n;
+    return ok();
+}
+
+size_t lucem_workspace_capacity_bytes(const lucem_workspace *ws) {
+    if (!ws) return 0;
+    size_t n = 0;
+    for (auto &kv : ws->slots) n += kv.second.cap;
+    return n;
+}
+
+lucem_status lucem_pad_mode_parse(const char *name, int32_t *mode_out) {
+    if (!name || !mode_out) return fail(LUCEM_ERR_INVALID_PARAMETER, "null argument");
+    std::string s(name);
+    size_t b = s.find_first_not_of(" \t\n\r"), e = s.find_last_not_of(" \t\n\r");
+    s = b == std::string::npos ? std::string() : s.substr(b, e - b + 1);
+    for (auto &ch : s) ch = (char)std::tolower((unsigned char)ch);
+    if (s == "reflect" || s == "symmetric" || s == "grid-mirror") *mode_out = LUCEM_PAD_REFLECT;
+    else if (s == "constant" || s == "grid-constant" || s == "zeros") *mode_out = LUCEM_PAD_CONSTANT;
+    else if (s == "nearest" || s == "edge" || s == "replicate") *mode_out = LUCEM_PAD_NEAREST;
+    else if (s == "mirror") *mode_out = LUCEM_PAD_MIRROR;
+    else if (s == "wrap" || s == "grid-wrap" || s == "periodic") *mode_out = LUCEM_PAD_WRAP;
+    else
+        return fail(LUCEM_ERR_UNKNOWN_PAD_MODE,
+                    "boundary pad mode '%s' is not supported (expected reflect, constant, nearest, "
+                    "mirror, or wrap)", s.c_str());
+    return ok();
+}
+
+lucem_status lucem_gaussian_kernel_1d(double sigma, uint32_t order, int64_t radius, double *out) {
+    if (!out || radius < 0) return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `radius`");
+    gaussian_taps(sigma, order, radius, out);
+    return ok();
+}
+
+int64_t lucem_gaussian_radius(double truncate, double sigma) {
+    return (int64_t)radius_of(truncate, sigma);
+}
+
+int64_t lucem_pad_index(int64_t p, int64_t len, int32_t mode) {
+    if (p >= 0 && p < len) return p;
+    switch (mode) {
+    case LUCEM_PAD_CONSTANT: return -1;
+    case LUCEM_PAD_NEAREST: return p < 0 ? 0 : len - 1;
+    case LUCEM_PAD_WRAP: return ((p % len) + len) % len;
+    case LUCEM_PAD_REFLECT: {
+        int64_t period = 2 * len, r = ((p % period) + period) % period;
+        return r < len ? r : period - 1 - r;
+    }
+    default: {
+        int64_t period = std::max<int64_t>(2 * len - 2, 1), r = ((p % period) + period) % period;
+        return r < len ? r : period - r;
+    }
+    }
+}
+
+void lucem_gaussian_settings_default(lucem_gaussian_settings *s) {
+    std::memset(s, 0, sizeof *s);
+    s->mode = LUCEM_PAD_REFLECT;
+    s->cval = 0.0;
+    s->truncate = 4.0;
+    s->input_scale = 1.0;
+}
+
+void lucem_gaussian_1d_settings_default(lucem_gaussian_1d_settings *s) {
+    std::memset(s, 0, sizeof *s);
+    s->axis = -1;
+    s->order = 0;
+    s->mode = LUCEM_PAD_REFLECT;
+    s->cval = 0.0;
+    s->truncate = 4.0;
+    s->radius = -1;
+}
+
+void lucem_rl_settings_default(lucem_rl_settings *s) {
+    std::memset(s, 0, sizeof *s);
+    s->num_iter = 30;
+    s->clip = 1;
+    s->has_filter_epsilon = 0;
+    s->filter_epsilon = 0.0;
+    s->mode = LUCEM_PAD_REFLECT;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Separable passes.
+
+namespace {
+
+struct Pass {
+    int axis;
+    double sigma;
+    uint32_t order;
+    int64_t radius;
+};
+
+// crates/lucem-ops/src/filter/gaussian.rs:184-219.
+lucem_status plan_passes(int ndim, const double *sigmas, int n_sigmas, const lucem_gaussian_settings *s,
+                         std::vector<Pass> *passes) {
+    std::vector<int> axes;
+    if (s->axes == nullptr) {
+        for (int d = 0; d < ndim; ++d) axes.push_back(d);
+    } else {
+        for (int i = 0; i < s->n_axes; ++i) {
+            int a;
+            lucem_status st = norm_axis(s->axes[i], ndim, &a);
+            if (st) return st;
+            if (std::find(axes.begin(), axes.end(), a) != axes.end())
+                return fail(LUCEM_ERR_REPEATED_AXIS, "repeated axis %lld", (long long)s->axes[i]);
+            axes.push_back(a);
+        }
+    }
+    if (s->has_channel_axis) {
+        int ch;
+        lucem_status st = norm_axis(s->channel_axis, ndim, &ch);
+        if (st) return st;
+        axes.erase(std::remove(axes.begin(), axes.end(), ch), axes.end());
+    }
+    const int na = (int)axes.size();
+    std::vector<double> sig;
+    lucem_status st = broadcast("sigmas", sigmas, n_sigmas, na, &sig);
+    if (st) return st;
+    for (double v : sig)
+        if (!std::isfinite(v) || v < 0.0)
+            return fail(LUCEM_ERR_INVALID_PARAMETER,
+                        "invalid parameter `sigmas`: sigma must be non-negative and finite, got %g", v);
+    static const uint32_t zero_order = 0;
+    std::vector<uint32_t> ords;
+    st = s->n_orders > 0 ? broadcast("orders", s->orders, s->n_orders, na, &ords)
+                         : broadcast("orders", &zero_order, 1, na, &ords);
+    if (st) return st;
+    std::vector<int64_t> rad;
+    bool has_r = s->n_radii > 0 && s->radii;
+    if (has_r) {
+        st = broadcast("radii", s->radii, s->n_radii, na, &rad);
+        if (st) return st;
+    }
+    passes->clear();
+    for (int i = 0; i < na; ++i) {
+        if (!(sig[i] > 0.0)) continue;
+        int64_t r = has_r ? rad[i] : (int64_t)radius_of(s->truncate, sig[i]);
+        if (r < 0) return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `radii`: negative radius");
+        passes->push_back(Pass{axes[i], sig[i], ords[i], r});
+    }
+    return ok();
+}
+
+// Device copy of f32 weights, cached per context under `key`.
+lucem_status cached_weights(lucem_ctx *ctx, const std::string &key, const std::vector<float> &w,
+                            const float **out) {
+    int err = 0;
+    void *d = ctx->get_or_upload(key, w.data(), w.size() * sizeof(float), &err);
+    if (!d) return cuda_fail(err, "uploading filter taps");
+    *out = static_cast<const float *>(d);
+    return ok();
+}
+
+std::string tap_key(double sigma, uint32_t order, int64_t radius) {
+    char buf[128];
+    // Same identity as GAUSSIAN_TAPS' key (crates/lucem-ops/src/filter/gaussian.rs:107).
+    snprintf(buf, sizeof buf, "f32-gauss1d-%.12f-o%u-r%lld", sigma, order, (long long)radius);
+    return buf;
+}
+
+std::vector<float> taps_f32(double sigma, uint32_t order, int64_t radius) {
+    std::vector<double> d((size_t)(2 * radius + 1));
+    gaussian_taps(sigma, order, radius, d.data());
+    return std::vector<float>(d.begin(), d.end());
+}
+
+void split_axis(const lucem_tensor *t, int axis, int64_t *outer, int64_t *len, int64_t *inner) {
+    *outer = 1;
+    *inner = 1;
+    for (int d = 0; d < axis; ++d) *outer *= t->dims[d];
+    for (int d = axis + 1; d < t->ndim; ++d) *inner *= t->dims[d];
+    *len = t->dims[axis];
+}
+
+// One generic pass: src (dtype, scale) -> dst f32 along `axis`.
+lucem_status generic_pass(lucem_ctx *ctx, const lucem_tensor *shape, const void *src, int src_dtype,
+                          float scale, float *dst, const Pass &p, int mode, double cval, void *stream) {
+    const float *w = nullptr;
+    lucem_status st = cached_weights(ctx, tap_key(p.sigma, p.order, p.radius),
+                                     taps_f32(p.sigma, p.order, p.radius), &w);
+    if (st) return st;
+    int64_t outer, len, inner;
+    split_axis(shape, p.axis, &outer, &len, &inner);
+    int size = (int)(2 * p.radius + 1);
+    int e = timed(kPassCorrelate, stream, [&] { return launch_correlate_1d(src, src_dtype, scale, dst, outer, len, inner, w, size, size / 2,
+                                mode, (float)cval, stream); });
+    if (e) return cuda_fail(e, "correlate_1d launch");
+    return ok();
+}
+
+void fill_filter_taps(FamParams *fp, int f, const Pass *p0, const Pass *p1) {
+    // p0: axis 0 (rows) pass or null (identity), p1: axis 1 (columns).
+    std::memset(fp->taps0[f], 0, sizeof fp->taps0[f]);
+    std::memset(fp->taps1[f], 0, sizeof fp->taps1[f]);
+    auto put = [](float *dst, const Pass *p) -> int {
+        if (!p) {
+            dst[0] = 1.0f;
+            return 0;
+        }
+        std::vector<float> t = taps_f32(p->sigma, p->order, p->radius);
+        for (size_t i = 0; i < t.size(); ++i) dst[i] = t[i];
+        return (int)p->radius;
+    };
+    fp->r0[f] = put(fp->taps0[f], p0);
+    fp->r1[f] = put(fp->taps1[f], p1);
+}
+
+void init_fam(FamParams *fp, const lucem_tensor *in, int mode, double cval, double scale) {
+    std::memset(fp, 0, sizeof *fp);
+    fp->in = in->data;
+    const int nd = in->ndim;
+    fp->H = (int32_t)in->dims[nd - 2];
+    fp->W = (int32_t)in->dims[nd - 1];
+    int64_t B = 1;
+    for (int d = 0; d < nd - 2; ++d) B *= in->dims[d];
+    fp->B = (int32_t)B;
+    fp->in_plane_stride = (int64_t)fp->H * fp->W;
+    fp->in_row_pitch = fp->W;
+    fp->mode = mode;
+    fp->cval = (float)cval;
+    fp->in_scale = (float)scale;
+}
+
+// Executes a pass list from `in` into `out` (f32): the reference's
+// separable::run (crates/lucem-ops/src/core/separable.rs:20-61), with the
+// last two passes fused into one launch when they are the two innermost axes
+// in ascending order.
+lucem_status run_passes(lucem_ctx *ctx, const lucem_tensor *in, const std::vector<Pass> &passes,
+                        int mode, double cval, double scale, float *out, lucem_workspace *ws,
+                        void *stream) {
+    const int64_t n = numel(in);
+    if (n == 0) return ok();
+    if (passes.empty()) {
+        int e = timed(kPassElementwise, stream, [&] { return launch_cast(in->data, in->dtype, (float)scale, out, n, stream); });
+        return e ? cuda_fail(e, "copy launch") : ok();
+    }
+    const int nd = in->ndim;
+    size_t np = passes.size();
+    bool fuse = np >= 2 && passes[np - 2].axis == nd - 2 && passes[np - 1].axis == nd - 1 &&
+                passes[np - 2].radius <= kFamMaxRadius && passes[np - 1].radius <= kFamMaxRadius &&
+                in->dims[nd - 2] < (1 << 30) && in->dims[nd - 1] < (1 << 30);
+    size_t n_generic = fuse ? np - 2 : np;
+    // Ping/pong slots as the reference's "sep_ping"/"sep_pong".
+    float *bufs[2] = {nullptr, nullptr};
+    size_t needed = n_generic + (fuse ? 1 : 0) > 1 ? std::min<size_t>(2, n_generic) : 0;
+    if (n_generic >= 1 && (fuse || n_generic >= 2)) needed = n_generic >= 2 ? 2 : 1;
+    for (size_t i = 0; i < needed; ++i) {
+        if (!ws) return fail(LUCEM_ERR_INVALID_HANDLE, "a workspace is required for multi-pass filters");
+        void *p = nullptr;
+        lucem_status st = ws->get(i == 0 ? "sep_ping" : "sep_pong", (size_t)n * sizeof(float), &p);
+        if (st) return st;
+        bufs[i] = static_cast<float *>(p);
+    }
+    const void *src = in->data;
+    int src_dtype = in->dtype;
+    float src_scale = (float)scale;
+    int ping = 0;
+    for (size_t i = 0; i < n_generic; ++i) {
+        bool last = !fuse && i + 1 == n_generic;
+        float *dst = last ? out : bufs[ping];
+        lucem_status st = generic_pass(ctx, in, src, src_dtype, src_scale, dst, passes[i], mode, cval, stream);
+        if (st) return st;
+        src = dst;
+        src_dtype = LUCEM_F32;
+        src_scale = 1.0f;
+        ping ^= 1;
+    }
+    if (fuse) {
+        FamParams fp;
+        lucem_tensor view = *in;
+        view.data = const_cast<void *>(src);
+        view.dtype = src_dtype;
+        init_fam(&fp, &view, mode, cval, src_scale);
+        fp.n_filters = 1;
+        fill_filter_taps(&fp, 0, &passes[np - 2], &passes[np - 1]);
+        fp.rmax0 = fp.r0[0];
+        fp.rmax1 = fp.r1[0];
+        fp.n_outputs = 1;
+        FamOutput &o = fp.outs[0];
+        o.out = out;
+        o.plane_stride = (int64_t)fp.H * fp.W;
+        o.row_pitch = fp.W;
+        o.combine = (int)Combine::kLinear;
+        o.fa = 0;
+        o.fb = -1;
+        o.alpha = 1.0f;
+        o.beta = 0.0f;
+        o.bias = 0.0f;
+        int e = timed(kPassFamily, stream, [&] { return launch_family_planes(fp, src_dtype, stream); });
+        if (e) return cuda_fail(e, "gaussian family launch");
+    }
+    return ok();
+}
+
+lucem_status check_in_out(const lucem_tensor *in, const lucem_tensor *out) {
+    lucem_status st;
+    if ((st = check_tensor("input", in))) return st;
+    if ((st = check_tensor("output", out))) return st;
+    if ((st = same_shape("input", in, "output", out))) return st;
+    if ((st = not_aliased(in, out))) return st;
+    return require_f32_out(out);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Gaussian family entry points.
+
+extern "C" {
+
+lucem_status lucem_gaussian_blur(lucem_ctx *ctx, const lucem_tensor *in, const double *sigmas,
+                                 int32_t n_sigmas, const lucem_gaussian_settings *settings,
+                                 lucem_tensor *out, lucem_workspace *ws, void *stream) {
+    TimerScope timer_scope(ws);
+    if (!ctx) return fail(LUCEM_ERR_INVALID_HANDLE, "null context");
+    lucem_gaussian_settings def;
+    lucem_gaussian_settings_default(&def);
+    const lucem_gaussian_settings *s = settings ? settings : &def;
+    lucem_status st;
+    if ((st = check_in_out(in, out))) return st;
+    if ((st = check_mode(s->mode))) return st;
+    std::vector<Pass> passes;
+    if ((st = plan_passes(in->ndim, sigmas, n_sigmas, s, &passes))) return st;
+    return run_passes(ctx, in, passes, s->mode, s->cval, s->input_scale, static_cast<float *>(out->data),
+                      ws, stream);
+}
+
+lucem_status lucem_gaussian_1d(lucem_ctx *ctx, const lucem_tensor *in, double sigma,
+                               const lucem_gaussian_1d_settings *settings, lucem_tensor *out,
+                               void *stream) {
+    if (!ctx) return fail(LUCEM_ERR_INVALID_HANDLE, "null context");
+    lucem_gaussian_1d_settings def;
+    lucem_gaussian_1d_settings_default(&def);
+    const lucem_gaussian_1d_settings *s = settings ? settings : &def;
+    lucem_status st;
+    // crates/lucem-ops/src/filter/gaussian.rs:96-104 (sigma checked first).
+    if (!std::isfinite(sigma) || sigma < 0.0)
+        return fail(LUCEM_ERR_INVALID_PARAMETER,
+                    "invalid parameter `sigma`: sigma must be non-negative and finite, got %g", sigma);
+    if ((st = check_in_out(in, out))) return st;
+    if ((st = check_mode(s->mode))) return st;
+    int axis;
+    if ((st = norm_axis(s->axis, in->ndim, &axis))) return st;
+    std::vector<Pass> passes;
+    if (sigma > 0.0) {
+        int64_t r = s->radius >= 0 ? s->radius : (int64_t)radius_of(s->truncate, sigma);
+        passes.push_back(Pass{axis, sigma, s->order, r});
+    }
+    return run_passes(ctx, in, passes, s->mode, s->cval, 1.0, static_cast<float *>(out->data), nullptr,
+                      stream);
+}
+
+lucem_status lucem_correlate_1d(lucem_ctx *ctx, const lucem_tensor *in, const double *weights,
+                                int64_t n_weights, const lucem_correlate_1d_settings *settings,
+                                lucem_tensor *out, void *stream) {
+    if (!ctx) return fail(LUCEM_ERR_INVALID_HANDLE, "null context");
+    if (!settings) return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `settings`: null");
+    lucem_status st;
+    // crates/lucem-ops/src/core/check.rs:74-82.
+    if (!weights || n_weights <= 0)
+        return fail(LUCEM_ERR_INVALID_WEIGHTS, "weights: filter weights cannot be empty");
+    for (int64_t i = 0; i < n_weights; ++i)
+        if (!std::isfinite(weights[i]))
+            return fail(LUCEM_ERR_INVALID_WEIGHTS, "weights: filter weights must be finite");
+    if ((st = check_in_out(in, out))) return st;
+    if ((st = check_mode(settings->mode))) return st;
+    // crates/lucem-ops/src/core/check.rs:60-71.
+    int32_t mn = -(int32_t)(n_weights / 2), mx = (int32_t)((n_weights - 1) / 2);
+    if (settings->origin < mn || settings->origin > mx)
+        return fail(LUCEM_ERR_INVALID_ORIGIN,
+                    "origin %d is out of bounds for window of size %lld (must be in %d..=%d)",
+                    settings->origin, (long long)n_weights, mn, mx);
+    int axis;
+    if ((st = norm_axis(settings->axis, in->ndim, &axis))) return st;
+    if (numel(in) == 0) return ok();
+    std::vector<float> w(weights, weights + n_weights);
+    std::string key = "f32-corr1d-";
+    key.append(reinterpret_cast<const char *>(weights), (size_t)n_weights * sizeof(double));
+    const float *wd = nullptr;
+    if ((st = cached_weights(ctx, key, w, &wd))) return st;
+    int64_t outer, len, inner;
+    split_axis(in, axis, &outer, &len, &inner);
+    int left = (int)(n_weights / 2) + settings->origin;
+    int e = timed(kPassCorrelate, stream, [&] { return launch_correlate_1d(in->data, in->dtype, 1.0f, static_cast<float *>(out->data), outer, len,
+                                inner, wd, (int)n_weights, left, settings->mode,
+                                (float)settings->cval, stream); });
+    return e ? cuda_fail(e, "correlate_1d launch") : ok();
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Multi-response family (fused) and the composite ops.
+
+namespace {
+
+struct FilterKey {
+    double s0, s1;
+    uint32_t o0, o1;
+    bool operator==(const FilterKey &o) const { return s0 == o.s0 && s1 == o.s1 && o0 == o.o0 && o1 == o.o1; }
+};
+
+struct FamilyPlan {
+    std::vector<FilterKey> filters;
+    struct Out { int kind; int fa, fb; float alpha, beta, bias; };
+    std::vector<Out> outs;
+};
+
+int add_filter(FamilyPlan *pl, FilterKey k) {
+    for (size_t i = 0; i < pl->filters.size(); ++i)
+        if (pl->filters[i] == k) return (int)i;
+    pl->filters.push_back(k);
+    return (int)pl->filters.size() - 1;
+}
+
+lucem_status check_sigma(double s, const char *name) {
+    if (!std::isfinite(s) || s < 0.0)
+        return fail(LUCEM_ERR_INVALID_PARAMETER,
+                    "invalid parameter `%s`: sigma must be non-negative and finite, got %g", name, s);
+    return ok();
+}
+
+lucem_status plan_family(const lucem_response *r, int n, FamilyPlan *pl) {
+    lucem_status st;
+    for (int i = 0; i < n; ++i) {
+        const lucem_response &x = r[i];
+        if ((st = check_sigma(x.sigma, "sigma"))) return st;
+        FamilyPlan::Out o{};
+        o.kind = x.kind;
+        o.alpha = 1.0f;
+        o.beta = 0.0f;
+        o.bias = 0.0f;
+        o.fb = -1;
+        switch (x.kind) {
+        case LUCEM_RESP_GAUSSIAN:
+            o.fa = add_filter(pl, {x.sigma, x.sigma, 0, 0});
+            break;
+        case LUCEM_RESP_DOG:
+            if ((st = check_sigma(x.sigma2, "sigma2"))) return st;
+            o.fa = add_filter(pl, {x.sigma, x.sigma, 0, 0});
+            o.fb = add_filter(pl, {x.sigma2, x.sigma2, 0, 0});
+            o.beta = -1.0f;
+            break;
+        case LUCEM_RESP_LAPLACE:
+            o.fa = add_filter(pl, {x.sigma, x.sigma, 2, 0});
+            o.fb = add_filter(pl, {x.sigma, x.sigma, 0, 2});
+            o.beta = 1.0f;
+            break;
+        case LUCEM_RESP_GRAD_MAG:
+            o.fa = add_filter(pl, {x.sigma, x.sigma, 1, 0});
+            o.fb = add_filter(pl, {x.sigma, x.sigma, 0, 1});
+            break;
+        case LUCEM_RESP_UNSHARP:
+            o.fa = -2;
+            o.fb = add_filter(pl, {x.sigma, x.sigma, 0, 0});
+            o.alpha = (float)(1.0 + x.amount);
+            o.beta = (float)(-x.amount);
+            break;
+        default:
+            return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `kind`: %d", x.kind);
+        }
+        pl->outs.push_back(o);
+    }
+    return ok();
+}
+
+bool family_fusable(const FamilyPlan &pl, double truncate) {
+    if ((int)pl.filters.size() > kFamMaxFilters || (int)pl.outs.size() > kFamMaxOutputs) return false;
+    for (auto &f : pl.filters)
+        if (radius_of(truncate, f.s0) > kFamMaxRadius || radius_of(truncate, f.s1) > kFamMaxRadius)
+            return false;
+    return true;
+}
+
+void build_fam(FamParams *fp, const FamilyPlan &pl, double truncate) {
+    fp->n_filters = (int)pl.filters.size();
+    fp->rmax0 = fp->rmax1 = 0;
+    for (int f = 0; f < fp->n_filters; ++f) {
+        const FilterKey &k = pl.filters[f];
+        Pass p0{0, k.s0, k.o0, (int64_t)radius_of(truncate, k.s0)};
+        Pass p1{1, k.s1, k.o1, (int64_t)radius_of(truncate, k.s1)};
+        // sigma == 0 skips the axis (gaussian.rs:217): identity taps.
+        fill_filter_taps(fp, f, k.s0 > 0.0 ? &p0 : nullptr, k.s1 > 0.0 ? &p1 : nullptr);
+        fp->rmax0 = std::max(fp->rmax0, fp->r0[f]);
+        fp->rmax1 = std::max(fp->rmax1, fp->r1[f]);
+    }
+    fp->n_outputs = (int)pl.outs.size();
+    for (int k = 0; k < fp->n_outputs; ++k) {
+        const auto &o = pl.outs[k];
+        FamOutput &fo = fp->outs[k];
+        fo.combine = o.kind == LUCEM_RESP_GRAD_MAG ? (int)Combine::kHypot : (int)Combine::kLinear;
+        fo.fa = o.fa;
+        fo.fb = o.fb;
+        fo.alpha = o.alpha;
+        fo.beta = o.beta;
+        fo.bias = o.bias;
+    }
+}
+
+// Composite responses through per-axis passes (any ndim), mirroring the
+// reference's sequence of gaussian_blur_into + elementwise kernels.
+lucem_status composite_generic(lucem_ctx *ctx, const lucem_tensor *in, const lucem_response &r,
+                               const std::vector<int> &axes, int mode, double cval, double truncate,
+                               double scale, lucem_workspace *ws, void *stream) {
+    const int64_t n = numel(in);
+    float *out = static_cast<float *>(r.out.data);
+    auto blur = [&](double sigma, int order_axis, uint32_t order, float *dst) -> lucem_status {
+        std::vector<Pass> passes;
+        for (int a : axes) {
+            if (!(sigma > 0.0)) continue;
+            uint32_t o = (a == order_axis) ? order : 0;
+            passes.push_back(Pass{a, sigma, o, (int64_t)radius_of(truncate, sigma)});
+        }
+        return run_passes(ctx, in, passes, mode, cval, scale, dst, ws, stream);
+    };
+    auto slot = [&](const char *name, float **p) -> lucem_status {
+        if (!ws) return fail(LUCEM_ERR_INVALID_HANDLE, "a workspace is required");
+        void *v = nullptr;
+        lucem_status st = ws->get(name, (size_t)n * sizeof(float), &v);
+        *p = static_cast<float *>(v);
+        return st;
+    };
+    lucem_status st;
+    int e = 0;
+    switch (r.kind) {
+    case LUCEM_RESP_GAUSSIAN: return blur(r.sigma, -1, 0, out);
+    case LUCEM_RESP_DOG: {  // gaussian.rs:374-390
+        float *lo, *hi;
+        if ((st = slot("dog_low", &lo)) || (st = slot("dog_high", &hi))) return st;
+        if ((st = blur(r.sigma, -1, 0, lo)) || (st = blur(r.sigma2, -1, 0, hi))) return st;
+        e = timed(kPassElementwise, stream, [&] { return launch_linear_comb(lo, hi, out, n, 1.0f, -1.0f, 0.0f, stream); });
+        break;
+    }
+    case LUCEM_RESP_LAPLACE: {  // gaussian.rs:255-288
+        float *term;
+        if ((st = slot("log_term", &term))) return st;
+        for (size_t i = 0; i < axes.size(); ++i) {
+            if (i == 0) {
+                if ((st = blur(r.sigma, axes[i], 2, out))) return st;
+            } else {
+                if ((st = blur(r.sigma, axes[i], 2, term))) return st;
+                if ((e = timed(kPassElementwise, stream, [&] { return launch_linear_comb(out, term, out, n, 1.0f, 1.0f, 0.0f, stream); }))) break;
+            }
+        }
+        break;
+    }
+    case LUCEM_RESP_GRAD_MAG: {  // gaussian.rs:307-356
+        float *acc, *deriv;
+        if ((st = slot("ggm_accum", &acc)) || (st = slot("ggm_deriv", &deriv))) return st;
+        if ((e = timed(kPassElementwise, stream, [&] { return launch_fill(acc, n, 0.0f, stream); }))) break;
+        for (int a : axes) {
+            if ((st = blur(r.sigma, a, 1, deriv))) return st;
+            if ((e = timed(kPassElementwise, stream, [&] { return launch_add_sq(deriv, acc, n, stream); }))) break;
+        }
+        if (!e) e = timed(kPassElementwise, stream, [&] { return launch_sqrt_scale(acc, out, n, 1.0f, stream); });
+        break;
+    }
+    case LUCEM_RESP_UNSHARP: {  // gaussian.rs:407-421
+        float *bl, *x = nullptr;
+        if ((st = slot("unsharp_blur", &bl))) return st;
+        if ((st = blur(r.sigma, -1, 0, bl))) return st;
+        const float *xin = static_cast<const float *>(in->data);
+        if (in->dtype != LUCEM_F32 || scale != 1.0) {
+            if ((st = slot("unsharp_input", &x))) return st;
+            if ((e = timed(kPassElementwise, stream, [&] { return launch_cast(in->data, in->dtype, (float)scale, x, n, stream); }))) break;
+            xin = x;
+        }
+        e = timed(kPassElementwise, stream, [&] { return launch_linear_comb(xin, bl, out, n, (float)(1.0 + r.amount), (float)(-r.amount), 0.0f, stream); });
+        break;
+    }
+    default: return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `kind`: %d", r.kind);
+    }
+    return e ? cuda_fail(e, "elementwise launch") : ok();
+}
+
+lucem_status family_impl(lucem_ctx *ctx, const lucem_tensor *in, const lucem_response *responses,
+                         int32_t n_responses, const std::vector<int> &axes, int32_t mode, double cval,
+                         double truncate, double input_scale, lucem_workspace *ws, void *stream) {
+    lucem_status st;
+    if (!ctx) return fail(LUCEM_ERR_INVALID_HANDLE, "null context");
+    if ((st = check_tensor("input", in))) return st;
+    if ((st = check_mode(mode))) return st;
+    if (n_responses < 0 || (n_responses > 0 && !responses))
+        return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `responses`");
+    for (int i = 0; i < n_responses; ++i) {
+        if ((st = check_tensor("output", &responses[i].out))) return st;
+        if ((st = same_shape("input", in, "output", &responses[i].out))) return st;
+        if ((st = not_aliased(in, &responses[i].out))) return st;
+        if ((st = require_f32_out(&responses[i].out))) return st;
+    }
+    FamilyPlan pl;
+    if ((st = plan_family(responses, n_responses, &pl))) return st;
+    if (numel(in) == 0 || n_responses == 0) return ok();
+    const int nd = in->ndim;
+    bool two_inner = nd >= 2 && axes.size() == 2 && axes[0] == nd - 2 && axes[1] == nd - 1;
+    if (two_inner && family_fusable(pl, truncate)) {
+        FamParams fp;
+        init_fam(&fp, in, mode, cval, input_scale);
+        build_fam(&fp, pl, truncate);
+        for (int k = 0; k < n_responses; ++k) {
+            fp.outs[k].out = static_cast<float *>(responses[k].out.data);
+            fp.outs[k].plane_stride = (int64_t)fp.H * fp.W;
+            fp.outs[k].row_pitch = fp.W;
+        }
+        int e = timed(kPassFamily, stream, [&] { return launch_family_planes(fp, in->dtype, stream); });
+        return e ? cuda_fail(e, "gaussian family launch") : ok();
+    }
+    for (int k = 0; k < n_responses; ++k)
+        if ((st = composite_generic(ctx, in, responses[k], axes, mode, cval, truncate, input_scale, ws,
+                                    stream)))
+            return st;
+    return ok();
+}
+
+std::vector<int> all_axes(int nd) {
+    std::vector<int> a;
+    for (int d = 0; d < nd; ++d) a.push_back(d);
+    return a;
+}
+
+// Isotropic sigma list check: the family path takes one sigma for all axes.
+bool isotropic(const double *s, int n, double *out) {
+    if (n < 1) return false;
+    for (int i = 1; i < n; ++i)
+        if (s[i] != s[0]) return false;
+    *out = s[0];
+    return true;
+}
+
+lucem_status check_sigma_list(const char *name, const double *s, int n, int num_axes) {
+    std::vector<double> v;
+    lucem_status st = broadcast(name, s, n, num_axes, &v);
+    if (st) return st;
+    for (double x : v)
+        if (!std::isfinite(x) || x < 0.0)
+            return fail(LUCEM_ERR_INVALID_PARAMETER,
+                        "invalid parameter `%s`: sigma must be non-negative and finite, got %g", name, x);
+    return ok();
+}
+
+// Per-axis sigmas that differ: compose with generic blurs (run_passes).
+lucem_status composite_axes(lucem_ctx *ctx, const lucem_tensor *in, int kind, const double *s1, int n1,
+                            const double *s2, int n2, double amount, const lucem_gaussian_settings *gs,
+                            lucem_tensor *out, lucem_workspace *ws, void *stream) {
+    const int64_t n = numel(in);
+    float *o = static_cast<float *>(out->data);
+    auto blur = [&](const double *s, int ns, std::vector<uint32_t> orders, float *dst) -> lucem_status {
+        lucem_gaussian_settings x = *gs;
+        x.orders = orders.empty() ? gs->orders : orders.data();
+        x.n_orders = orders.empty() ? gs->n_orders : (int32_t)orders.size();
+        std::vector<Pass> passes;
+        lucem_status st = plan_passes(in->ndim, s, ns, &x, &passes);
+        if (st) return st;
+        return run_passes(ctx, in, passes, gs->mode, gs->cval, gs->input_scale, dst, ws, stream);
+    };
+    auto slot = [&](const char *name, float **p) -> lucem_status {
+        if (!ws) return fail(LUCEM_ERR_INVALID_HANDLE, "a workspace is required");
+        void *v = nullptr;
+        lucem_status st = ws->get(name, (size_t)n * sizeof(float), &v);
+        *p = static_cast<float *>(v);
+        return st;
+    };
+    lucem_status st;
+    int e = 0;
+    const int nd = in->ndim;
+    if (kind == LUCEM_RESP_DOG) {
+        float *lo, *hi;
+        if ((st = slot("dog_low", &lo)) || (st = slot("dog_high", &hi))) return st;
+        if ((st = blur(s1, n1, {}, lo)) || (st = blur(s2, n2, {}, hi))) return st;
+        e = timed(kPassElementwise, stream, [&] { return launch_linear_comb(lo, hi, o, n, 1.0f, -1.0f, 0.0f, stream); });
+    } else if (kind == LUCEM_RESP_UNSHARP) {
+        float *bl, *x = nullptr;
+        if ((st = slot("unsharp_blur", &bl))) return st;
+        if ((st = blur(s1, n1, {}, bl))) return st;
+        const float *xin = static_cast<const float *>(in->data);
+        if (in->dtype != LUCEM_F32 || gs->input_scale != 1.0) {
+            if ((st = slot("unsharp_input", &x))) return st;
+            if ((e = timed(kPassElementwise, stream, [&] { return launch_cast(in->data, in->dtype, (float)gs->input_scale, x, n, stream); })))
+                return cuda_fail(e, "cast");
+            xin = x;
+        }
+        e = timed(kPassElementwise, stream, [&] { return launch_linear_comb(xin, bl, o, n, (float)(1.0 + amount), (float)(-amount), 0.0f, stream); });
+    } else if (kind == LUCEM_RESP_LAPLACE) {
+        float *term;
+        if ((st = slot("log_term", &term))) return st;
+        for (int ax = 0; ax < nd && !e; ++ax) {
+            std::vector<uint32_t> ord(nd, 0);
+            ord[ax] = 2;
+            if (ax == 0) {
+                if ((st = blur(s1, n1, ord, o))) return st;
+            } else {
+                if ((st = blur(s1, n1, ord, term))) return st;
+                e = timed(kPassElementwise, stream, [&] { return launch_linear_comb(o, term, o, n, 1.0f, 1.0f, 0.0f, stream); });
+            }
+        }
+    } else {  // gradient magnitude
+        float *acc, *deriv;
+        if ((st = slot("ggm_accum", &acc)) || (st = slot("ggm_deriv", &deriv))) return st;
+        e = timed(kPassElementwise, stream, [&] { return launch_fill(acc, n, 0.0f, stream); });
+        for (int ax = 0; ax < nd && !e; ++ax) {
+            std::vector<uint32_t> ord(nd, 0);
+            ord[ax] = 1;
+            if ((st = blur(s1, n1, ord, deriv))) return st;
+            e = timed(kPassElementwise, stream, [&] { return launch_add_sq(deriv, acc, n, stream); });
+        }
+        if (!e) e = timed(kPassElementwise, stream, [&] { return launch_sqrt_scale(acc, o, n, 1.0f, stream); });
+    }
+    return e ? cuda_fail(e, "elementwise launch") : ok();
+}
+
+// Shared front end of DoG / LoG / |grad| / unsharp.
+lucem_status composite_entry(lucem_ctx *ctx, const lucem_tensor *in, int kind, const double *s1, int n1,
+                             const double *s2, int n2, double amount,
+                             const lucem_gaussian_settings *gs, lucem_tensor *out, lucem_workspace *ws,
+                             void *stream) {
+    if (!ctx) return fail(LUCEM_ERR_INVALID_HANDLE, "null context");
+    lucem_status st;
+    if ((st = check_in_out(in, out))) return st;
+    if ((st = check_mode(gs->mode))) return st;
+    // Axes the composite filters (LoG / |grad| use all axes).
+    std::vector<int> axes;
+    if (kind == LUCEM_RESP_LAPLACE || kind == LUCEM_RESP_GRAD_MAG) {
+        axes = all_axes(in->ndim);
+    } else {
+        std::vector<Pass> probe;
+        lucem_gaussian_settings x = *gs;
+        x.n_orders = 0;
+        static const double one = 1.0;
+        if ((st = plan_passes(in->ndim, &one, 1, &x, &probe))) return st;
+        for (auto &p : probe) axes.push_back(p.axis);
+    }
+    if ((st = check_sigma_list("sigmas", s1, n1, (int)axes.size()))) return st;
+    if (kind == LUCEM_RESP_DOG && (st = check_sigma_list("high_sigmas", s2, n2, (int)axes.size()))) return st;
+    bool custom_orders = gs->n_orders > 0;
+    for (int i = 0; i < gs->n_orders; ++i) custom_orders = custom_orders && gs->orders[i] != 0;
+    double a = 0, b = 0;
+    bool iso = isotropic(s1, n1, &a) && (kind != LUCEM_RESP_DOG || isotropic(s2, n2, &b)) &&
+               gs->n_radii == 0 && !custom_orders;
+    if (iso) {
+        lucem_response r{};
+        r.kind = kind;
+        r.sigma = a;
+        r.sigma2 = b;
+        r.amount = amount;
+        r.out = *out;
+        return family_impl(ctx, in, &r, 1, axes, gs->mode, gs->cval, gs->truncate, gs->input_scale, ws,
+                           stream);
+    }
+    return composite_axes(ctx, in, kind, s1, n1, s2, n2, amount, gs, out, ws, stream);
+}
+
+}  // namespace
+
+extern "C" {
+
+lucem_status lucem_difference_of_gaussians(lucem_ctx *ctx, const lucem_tensor *in,
+                                           const double *low_sigmas, int32_t n_low,
+                                           const double *high_sigmas, int32_t n_high,
+                                           const lucem_gaussian_settings *settings,
+                                           lucem_tensor *out, lucem_workspace *ws, void *stream) {
+    TimerScope timer_scope(ws);
+    lucem_gaussian_settings def;
+    lucem_gaussian_settings_default(&def);
+    return composite_entry(ctx, in, LUCEM_RESP_DOG, low_sigmas, n_low, high_sigmas, n_high, 0.0,
+                           settings ? settings : &def, out, ws, stream);
+}
+
+lucem_status lucem_gaussian_laplace(lucem_ctx *ctx, const lucem_tensor *in, const double *sigmas,
+                                    int32_t n_sigmas, int32_t mode, double cval, double truncate,
+                                    lucem_tensor *out, lucem_workspace *ws, void *stream) {
+    TimerScope timer_scope(ws);
+    lucem_gaussian_settings s;
+    lucem_gaussian_settings_default(&s);
+    s.mode = mode;
+    s.cval = cval;
+    s.truncate = truncate;
+    return composite_entry(ctx, in, LUCEM_RESP_LAPLACE, sigmas, n_sigmas, nullptr, 0, 0.0, &s, out, ws,
+                           stream);
+}
+
+lucem_status lucem_gaussian_grad_mag(lucem_ctx *ctx, const lucem_tensor *in, const double *sigmas,
+                                     int32_t n_sigmas, int32_t mode, double cval, double truncate,
+                                     lucem_tensor *out, lucem_workspace *ws, void *stream) {
+    TimerScope timer_scope(ws);
+    lucem_gaussian_settings s;
+    lucem_gaussian_settings_default(&s);
+    s.mode = mode;
+    s.cval = cval;
+    s.truncate = truncate;
+    return composite_entry(ctx, in, LUCEM_RESP_GRAD_MAG, sigmas, n_sigmas, nullptr, 0, 0.0, &s, out, ws,
+                           stream);
+}
+
+lucem_status lucem_unsharp_mask(lucem_ctx *ctx, const lucem_tensor *in, const double *sigmas,
+                                int32_t n_sigmas, double amount,
+                                const lucem_gaussian_settings *settings, lucem_tensor *out,
+                                lucem_workspace *ws, void *stream) {
+    TimerScope timer_scope(ws);
+    lucem_gaussian_settings def;
+    lucem_gaussian_settings_default(&def);
+    return composite_entry(ctx, in, LUCEM_RESP_UNSHARP, sigmas, n_sigmas, nullptr, 0, amount,
+                           settings ? settings : &def, out, ws, stream);
+}
+
+lucem_status lucem_gaussian_family(lucem_ctx *ctx, const lucem_tensor *in,
+                                   const lucem_response *responses, int32_t n_responses,
+                                   int32_t mode, double cval, double truncate, double input_scale,
+                                   lucem_workspace *ws, void *stream) {
+    TimerScope timer_scope(ws);
+    lucem_status st;
+    if ((st = check_tensor("input", in))) return st;
+    if (in->ndim < 2)
+        return fail(LUCEM_ERR_INVALID_DIMENSION, "gaussian_family expects >=2-D array, got %d-D shape %s",
+                    in->ndim, dims_str(in).c_str());
+    std::vector<int> axes = {in->ndim - 2, in->ndim - 1};
+    return family_impl(ctx, in, responses, n_responses, axes, mode, cval, truncate, input_scale, ws,
+                       stream);
+}
+
+// crates/lucem-core/src/tiling.rs:54-78.
+lucem_status lucem_schedule(const int64_t dims[3], const int64_t block[3], const int64_t halo[3],
+                            lucem_block *out, int64_t cap, int64_t *n_out) {
+    if (!dims || !block || !halo || !n_out) return fail(LUCEM_ERR_INVALID_PARAMETER, "null argument");
+    for (int a = 0; a < 3; ++a)
+        if (dims[a] < 0 || block[a] < 0 || halo[a] < 0)
+            return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `dims`: negative value");
+    *n_out = 0;
+    if (dims[0] == 0 || dims[1] == 0 || dims[2] == 0) return ok();
+    int64_t step[3];
+    for (int a = 0; a < 3; ++a) step[a] = block[a] == 0 ? dims[a] : std::min(block[a], dims[a]);
+    int64_t count = 0;
+    for (int64_t z = 0; z < dims[0]; z += step[0])
+        for (int64_t y = 0; y < dims[1]; y += step[1])
+            for (int64_t x = 0; x < dims[2]; x += step[2]) {
+                if (out && count < cap) {
+                    lucem_block &b = out[count];
+                    int64_t o[3] = {z, y, x};
+                    b.index = count;
+                    for (int a = 0; a < 3; ++a) {
+                        b.origin[a] = o[a];
+                        b.size[a] = std::min(step[a], dims[a] - o[a]);
+                        int64_t start = o[a] > halo[a] ? o[a] - halo[a] : 0;
+                        int64_t end = std::min(o[a] + b.size[a] + halo[a], dims[a]);
+                        b.read_origin[a] = start;
+                        b.read_size[a] = end - start;
+                    }
+                }
+                ++count;
+            }
+    *n_out = count;
+    return ok();
+}
+
+lucem_status lucem_gaussian_family_tiles(lucem_ctx *ctx, const lucem_tensor *slide,
+                                         const lucem_block *blocks, int64_t n_blocks,
+                                         const lucem_response *responses, int32_t n_responses,
+                                         int32_t mode, double cval, double truncate,
+                                         double input_scale, int32_t persistent,
+                                         lucem_workspace *ws, void *stream) {
+    TimerScope timer_scope(ws);
+    lucem_status st;
+    if (!ctx) return fail(LUCEM_ERR_INVALID_HANDLE, "null context");
+    if (!ws) return fail(LUCEM_ERR_INVALID_HANDLE, "a workspace is required");
+    if ((st = check_tensor("slide", slide))) return st;
+    if (slide->ndim != 2 && slide->ndim != 3)
+        return fail(LUCEM_ERR_INVALID_DIMENSION, "gaussian_family_tiles expects 2-D or 3-D array, got %d-D shape %s",
+                    slide->ndim, dims_str(slide).c_str());
+    if ((st = check_mode(mode))) return st;
+    const int nd = slide->ndim;
+    const int64_t C = nd == 3 ? slide->dims[0] : 1, H = slide->dims[nd - 2], W = slide->dims[nd - 1];
+    if (H >= (1 << 30) || W >= (1 << 30))
+        return fail(LUCEM_ERR_TOO_MANY_ELEMENTS, "slide side exceeds 2^30");
+    for (int i = 0; i < n_responses; ++i) {
+        if ((st = check_tensor("output", &responses[i].out))) return st;
+        if ((st = same_shape("slide", slide, "output", &responses[i].out))) return st;
+        if ((st = not_aliased(slide, &responses[i].out))) return st;
+        if ((st = require_f32_out(&responses[i].out))) return st;
+    }
+    if (n_blocks < 0 || (n_blocks > 0 && !blocks)) return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `blocks`");
+    FamilyPlan pl;
+    if ((st = plan_family(responses, n_responses, &pl))) return st;
+    if (!family_fusable(pl, truncate))
+        return fail(LUCEM_ERR_INVALID_PARAMETER,
+                    "invalid parameter `responses`: at most %d filters / %d outputs of radius <= %d per tiled walk",
+                    kFamMaxFilters, kFamMaxOutputs, kFamMaxRadius);
+    if (numel(slide) == 0 || n_blocks == 0 || n_responses == 0) return ok();
+    int th, tw;
+    family_tile_dims(&th, &tw);
+    // Work list: every channel x every block (tiling.rs Block -> read / owned boxes).
+    std::vector<FamWork> work;
+    work.reserve((size_t)(C * n_blocks));
+    int64_t tiles = 0;
+    for (int64_t c = 0; c < C; ++c)
+        for (int64_t i = 0; i < n_blocks; ++i) {
+            const lucem_block &b = blocks[i];
+            bool valid = b.read_origin[1] >= 0 && b.read_origin[2] >= 0 && b.read_size[1] > 0 &&
+                         b.read_size[2] > 0 && b.read_origin[1] + b.read_size[1] <= H &&
+                         b.read_origin[2] + b.read_size[2] <= W && b.origin[1] >= b.read_origin[1] &&
+                         b.origin[2] >= b.read_origin[2] &&
+                         b.origin[1] + b.size[1] <= b.read_origin[1] + b.read_size[1] &&
+                         b.origin[2] + b.size[2] <= b.read_origin[2] + b.read_size[2] && b.size[1] > 0 &&
+                         b.size[2] > 0;
+            if (!valid)
+                return fail(LUCEM_ERR_INVALID_PARAMETER,
+                            "invalid parameter `blocks`: block %lld is outside the slide or its read box",
+                            (long long)i);
+            FamWork w;
+            w.channel = (int32_t)c;
+            w.read_y = (int32_t)b.read_origin[1];
+            w.read_x = (int32_t)b.read_origin[2];
+            w.read_h = (int32_t)b.read_size[1];
+            w.read_w = (int32_t)b.read_size[2];
+            w.own_y = (int32_t)b.origin[1];
+            w.own_x = (int32_t)b.origin[2];
+            w.own_h = (int32_t)b.size[1];
+            w.own_w = (int32_t)b.size[2];
+            w.tile_begin = (int32_t)tiles;
+            tiles += ((b.size[1] + th - 1) / th) * ((b.size[2] + tw - 1) / tw);
+            work.push_back(w);
+        }
+    if (tiles >= (int64_t)1 << 31) return fail(LUCEM_ERR_TOO_MANY_ELEMENTS, "too many tiles in one walk");
+    // Upload the work list once per distinct list (it is then reused, which
+    // also lets a CUDA graph capture later calls).
+    void *wdev = nullptr;
+    Slot *wslot = nullptr;
+    size_t wbytes = work.size() * sizeof(FamWork);
+    if ((st = ws->get("tile_work", wbytes + sizeof(int32_t) * 4, &wdev, &wslot))) return st;
+    std::string key(reinterpret_cast<const char *>(work.data()), wbytes);
+    if (wslot->key != key) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        cudaStreamIsCapturing(static_cast<cudaStream_t>(stream), &cs);
+        if (cs != cudaStreamCaptureStatusNone)
+            return fail(LUCEM_ERR_INVALID_PARAMETER,
+                        "a new tile list cannot be uploaded during stream capture: call once before capturing");
+        CUDA_TRY(cudaMemcpyAsync(wdev, work.data(), wbytes, cudaMemcpyHostToDevice,
+                                 static_cast<cudaStream_t>(stream)),
+                 "uploading the tile list");
+        CUDA_TRY(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)), "tile list upload");
+        wslot->key = key;
+    }
+    void *cnt = nullptr;
+    if ((st = ws->get("tile_counter", 64, &cnt))) return st;
+
+    FamParams fp;
+    std::memset(&fp, 0, sizeof fp);
+    fp.in = slide->data;
+    fp.H = (int32_t)H;
+    fp.W = (int32_t)W;
+    fp.B = (int32_t)C;
+    fp.in_plane_stride = H * W;
+    fp.in_row_pitch = W;
+    fp.mode = mode;
+    fp.cval = (float)cval;
+    fp.in_scale = (float)input_scale;
+    build_fam(&fp, pl, truncate);
+    for (int k = 0; k < n_responses; ++k) {
+        fp.outs[k].out = static_cast<float *>(responses[k].out.data);
+        fp.outs[k].plane_stride = H * W;
+        fp.outs[k].row_pitch = W;
+    }
+    const FamWork *wd = static_cast<const FamWork *>(wdev);
+    int e = 0;
+    if (persistent) {
+        CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(int32_t), static_cast<cudaStream_t>(stream)), "counter reset");
+        size_t smem = family_smem_bytes(fp.rmax0, fp.rmax1);
+        int per_sm = (int)std::max<size_t>(1, std::min<size_t>(4, (200 * 1024) / (smem + 2048)));
+        e = timed(kPassFamily, stream, [&] { return launch_family_work(fp, slide->dtype, wd, (int32_t)work.size(), (int32_t)tiles, 0,
+                               static_cast<int32_t *>(cnt), ctx->sms * per_sm, stream); });
+    } else {
+        for (size_t i = 0; i < work.size() && !e; ++i) {
+            int32_t t0 = work[i].tile_begin;
+            int32_t t1 = i + 1 < work.size() ? work[i + 1].tile_begin : (int32_t)tiles;
+            // One launch per block and channel: the plain per-tile drop-in.
+            e = timed(kPassFamily, stream, [&] { return launch_family_work(fp, slide->dtype, wd + i, 1, t1 - t0, t0, nullptr, 0, stream); });
+        }
+    }
+    return e ? cuda_fail(e, "tiled family launch") : ok();
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Richardson-Lucy.
+
+namespace {
+
+// Extension halo along one axis: zero padding needs none; the other modes
+// extend by k/2 on each side (the reference's correlation reads at most k/2
+// samples past either border of the image).
+int64_t rl_halo(int64_t k, int mode) { return mode == LUCEM_PAD_CONSTANT ? 0 : k / 2; }
+
+// Smallest grid length that keeps the circular correlation equal to the
+// padded linear one: n + k/2 for zero padding (the correlation reaches
+// k - 1 - k/2 <= k/2 samples past one side), n + 2*(k/2) with an extension.
+int64_t rl_min_length(int64_t n, int64_t k, int mode) {
+    return mode == LUCEM_PAD_CONSTANT ? n + k / 2 : n + 2 * (k / 2);
+}
+
+bool good_factors(int64_t n) {
+    if (n < 1) return false;
+    for (int f : {2, 3, 5, 7})
+        while (n % f == 0) n /= f;
+    return n == 1;
+}
+
+lucem_status rl_grid_impl(const int64_t *dims, const int64_t *kdims, int ndim, int mode,
+                          const int64_t *requested, int64_t *grid) {
+    for (int d = 0; d < ndim; ++d) {
+        bool x_axis = d == ndim - 1;
+        int64_t need = rl_min_length(dims[d], kdims[d], mode);
+        int64_t r = requested ? requested[d] : 0;
+        if (r > 0) {
+            if (r < need)
+                return fail(LUCEM_ERR_INVALID_PARAMETER,
+                            "invalid parameter `grid`: axis %d length %lld is below the %lld the padding needs",
+                            d, (long long)r, (long long)need);
+            if (!good_factors(r) || (x_axis && (r & 1)))
+                return fail(LUCEM_ERR_INVALID_PARAMETER,
+                            "invalid parameter `grid`: axis %d length %lld must factor into 2, 3, 5, 7%s",
+                            d, (long long)r, x_axis ? " and be even" : "");
+            grid[d] = r;
+        } else {
+            grid[d] = fft_good_length(need, x_axis);
+        }
+        if (grid[d] > 16384)
+            return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `grid`: axis %d length %lld exceeds 16384",
+                        d, (long long)grid[d]);
+    }
+    return ok();
+}
+
+// Twiddle tables e^{-2 pi i m / n}, m < n, from double-precision cos/sin;
+// f32 copies are rounded once from the f64 values.
+lucem_status twiddles(lucem_ctx *ctx, int64_t n, const float2_ **f32, const double **f64) {
+    std::vector<double> d((size_t)(2 * n));
+    for (int64_t m = 0; m < n; ++m) {
+        // Reduce the angle to the first octant's accuracy by exact symmetry.
+        double a = 2.0 * M_PI * (double)m / (double)n;
+        d[2 * m] = std::cos(a);
+        d[2 * m + 1] = -std::sin(a);
+    }
+    // Exact values at the quarter points.
+    for (int64_t m = 0; m < n; ++m) {
+        if ((4 * m) % n == 0) {
+            int64_t q = (4 * m) / n;
+            const double re[4] = {1, 0, -1, 0}, im[4] = {0, -1, 0, 1};
+            d[2 * m] = re[q];
+            d[2 * m + 1] = im[q];
+        }
+    }
+    std::vector<float> f((size_t)(2 * n));
+    for (size_t i = 0; i < f.size(); ++i) f[i] = (float)d[i];
+    int err = 0;
+    std::string k = "tw-f32-" + std::to_string(n);
+    void *pf = ctx->get_or_upload(k, f.data(), f.size() * sizeof(float), &err);
+    if (!pf) return cuda_fail(err, "twiddle upload");
+    k = "tw-f64-" + std::to_string(n);
+    void *pd = ctx->get_or_upload(k, d.data(), d.size() * sizeof(double), &err);
+    if (!pd) return cuda_fail(err, "twiddle upload");
+    *f32 = static_cast<const float2_ *>(pf);
+    *f64 = static_cast<const double *>(pd);
+    return ok();
+}
+
+// Device table position -> frequency of the in-place forward transform of
+// length n (the order the transfer function is stored in).
+lucem_status rev_table(lucem_ctx *ctx, int64_t n, const int32_t **out) {
+    FftPlan plan;
+    if (!fft_make_plan(n, &plan))
+        return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `grid`: length %lld has no plan", (long long)n);
+    std::vector<int32_t> t((size_t)n);
+    fft_rev_table(plan, t.data());
+    int err = 0;
+    void *d = ctx->get_or_upload("rev-" + std::to_string(n), t.data(), t.size() * sizeof(int32_t), &err);
+    if (!d) return cuda_fail(err, "permutation upload");
+    *out = static_cast<const int32_t *>(d);
+    return ok();
+}
+
+}  // namespace
+
+extern "C" {
+
+lucem_status lucem_rl_grid(const int64_t *dims, const int64_t *kdims, int32_t ndim, int32_t mode,
+                           const int64_t *requested, int64_t *grid_out) {
+    if (!dims || !kdims || !grid_out) return fail(LUCEM_ERR_INVALID_PARAMETER, "null argument");
+    if (ndim < 1 || ndim > 3) return fail(LUCEM_ERR_INVALID_DIMENSION, "richardson_lucy expects 2-D or 3-D");
+    lucem_status st = check_mode(mode);
+    if (st) return st;
+    return rl_grid_impl(dims, kdims, ndim, mode, requested, grid_out);
+}
+
+int64_t lucem_fft_good_length(int64_t n, int32_t even) { return fft_good_length(n, even != 0); }
+
+lucem_status lucem_richardson_lucy(lucem_ctx *ctx, const lucem_tensor *in, const lucem_tensor *psf,
+                                   const lucem_rl_settings *settings, lucem_tensor *out,
+                                   lucem_workspace *ws, void *stream) {
+    TimerScope timer_scope(ws);
+    if (!ctx) return fail(LUCEM_ERR_INVALID_HANDLE, "null context");
+    if (!ws) return fail(LUCEM_ERR_INVALID_HANDLE, "a workspace is required");
+    lucem_rl_settings def;
+    lucem_rl_settings_default(&def);
+    const lucem_rl_settings *s = settings ? settings : &def;
+    lucem_status st;
+    cudaStream_t cs = static_cast<cudaStream_t>(stream);
+    // crates/lucem-ops/src/restore/deconvolve.rs:53-71 (same order of checks).
+    if ((st = check_tensor("input", in)) || (st = check_tensor("output", out)) ||
+        (st = check_tensor("psf", psf)))
+        return st;
+    if ((st = same_shape("input", in, "output", out))) return st;
+    if ((st = not_aliased(in, out))) return st;
+    if (in->ndim != 2 && in->ndim != 3)
+        return fail(LUCEM_ERR_INVALID_DIMENSION, "richardson_lucy input expects 2 or 3-D array, got %d-D shape %s",
+                    in->ndim, dims_str(in).c_str());
+    if (psf->ndim != in->ndim)
+        return fail(LUCEM_ERR_INVALID_DIMENSION, "richardson_lucy psf expects %d-D array, got %d-D shape %s",
+                    in->ndim, psf->ndim, dims_str(psf).c_str());
+    if (numel(psf) == 0) return fail(LUCEM_ERR_INVALID_WEIGHTS, "psf: PSF cannot be empty");
+    if (s->num_iter < 1)
+        return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `num_iter`: num_iter must be >= 1");
+    if (in->dtype != LUCEM_F32 || psf->dtype != LUCEM_F32 || out->dtype != LUCEM_F32)
+        return fail(LUCEM_ERR_UNSUPPORTED_DTYPE, "richardson_lucy takes f32 input, psf and output");
+    if ((st = check_mode(s->mode))) return st;
+    if (numel(in) == 0) return ok();
+
+    const int nd = in->ndim;
+    int64_t dims[3] = {1, 1, 1}, kd[3] = {1, 1, 1}, grid[3] = {1, 1, 1};
+    for (int d = 0; d < nd; ++d) {
+        dims[3 - nd + d] = in->dims[d];
+        kd[3 - nd + d] = psf->dims[d];
+    }
+    int64_t req[3] = {0, 0, 0};
+    for (int d = 0; d < nd; ++d) req[3 - nd + d] = s->grid[d];
+    if ((st = rl_grid_impl(dims + (3 - nd), kd + (3 - nd), nd, s->mode, req + (3 - nd), grid + (3 - nd))))
+        return st;
+
+    RlGeom g{};
+    g.ndim = nd;
+    g.Z = (int32_t)dims[0]; g.Y = (int32_t)dims[1]; g.X = (int32_t)dims[2];
+    g.Pz = (int32_t)grid[0]; g.Py = (int32_t)grid[1]; g.Px = (int32_t)grid[2];
+    g.hz = nd == 3 ? (int32_t)rl_halo(kd[0], s->mode) : 0;
+    g.hy = (int32_t)rl_halo(kd[1], s->mode);
+    g.hx = (int32_t)rl_halo(kd[2], s->mode);
+    g.Hx = g.Px / 2 + 1;
+    g.Hp = (g.Hx + 15) & ~15;
+    g.mode = s->mode;
+
+    // deconvolve.rs:77-88: the PSF goes to the host, is normalised in f64.
+    const int64_t kn = numel(psf);
+    std::vector<float> hp((size_t)kn);
+    CUDA_TRY(cudaMemcpyAsync(hp.data(), psf->data, (size_t)kn * sizeof(float), cudaMemcpyDeviceToHost, cs),
+             "psf download");
+    CUDA_TRY(cudaStreamSynchronize(cs), "psf download");
+    double sum = 0.0;
+    for (float v : hp) sum += (double)v;
+    const double norm = std::fabs(sum) > 1e-12 ? 1.0 / sum : 1.0;
+    std::vector<double> pn((size_t)kn);
+    for (int64_t i = 0; i < kn; ++i) pn[(size_t)i] = (double)hp[(size_t)i] * norm;
+
+    const float2_ *tw32[3];
+    const double *tw64[3];
+    for (int d = 0; d < 3; ++d)
+        if ((st = twiddles(ctx, grid[d], &tw32[d], &tw64[d]))) return st;
+
+    // Transfer functions: convolution with the PSF centred at k-1-k/2 and
+    // correlation with it centred at k/2 (convolve.rs:144-145 with the flip at
+    // deconvolve.rs:82-88); equal for odd sizes.
+    int32_t kdi[3] = {(int32_t)kd[0], (int32_t)kd[1], (int32_t)kd[2]};
+    int32_t c_conv[3], c_corr[3];
+    bool same_centre = true;
+    for (int d = 0; d < 3; ++d) {
+        c_conv[d] = (int32_t)(kd[d] - 1 - kd[d] / 2);
+        c_corr[d] = (int32_t)(kd[d] / 2);
+        same_centre = same_centre && c_conv[d] == c_corr[d];
+    }
+    const size_t hbytes = (size_t)g.Pz * g.Py * g.Hp * sizeof(float2_);
+    std::string key(reinterpret_cast<const char *>(pn.data()), pn.size() * sizeof(double));
+    key.append(reinterpret_cast<const char *>(kdi), sizeof kdi);
+    key.append(reinterpret_cast<const char *>(grid), sizeof grid);
+    key.append(reinterpret_cast<const char *>(&g.Hp), sizeof g.Hp);
+    void *h_conv = nullptr, *h_corr = nullptr;
+    Slot *sl_conv = nullptr, *sl_corr = nullptr;
+    if ((st = ws->get("rl_otf_conv", hbytes, &h_conv, &sl_conv))) return st;
+    if (!same_centre && (st = ws->get("rl_otf_corr", hbytes, &h_corr, &sl_corr))) return st;
+    if (same_centre) h_corr = h_conv;
+    bool fresh = sl_conv->key != key || (!same_centre && sl_corr->key != key);
+    if (fresh) {
+        const int32_t *rev_y = nullptr, *rev_z = nullptr;
+        if ((st = rev_table(ctx, grid[1], &rev_y)) || (st = rev_table(ctx, grid[0], &rev_z))) return st;
+        void *psf64 = nullptr, *wa = nullptr, *wb = nullptr;
+        if ((st = ws->get("rl_psf64", (size_t)kn * sizeof(double), &psf64))) return st;
+        if ((st = ws->get("rl_otf_a", (size_t)kd[0] * kd[1] * g.Hp * 16, &wa))) return st;
+        if ((st = ws->get("rl_otf_b", (size_t)kd[0] * g.Py * g.Hp * 16, &wb))) return st;
+        CUDA_TRY(cudaMemcpyAsync(psf64, pn.data(), (size_t)kn * sizeof(double), cudaMemcpyHostToDevice, cs),
+                 "psf upload");
+        if (ws->t()) ws->t()->begin(kPassRlOtf, stream);
+        int e = rl_launch_otf(g, static_cast<const double *>(psf64), kdi, c_conv, static_cast<double *>(wa),
+                              static_cast<double *>(wb), h_conv, tw64[2], tw64[1], tw64[0], rev_y, rev_z,
+                              stream);
+        if (ws->t()) ws->t()->end(kPassRlOtf, stream);
+        if (e) return cuda_fail(e, "transfer function launch");
+        if (!same_centre) {
+            e = rl_launch_otf(g, static_cast<const double *>(psf64), kdi, c_corr, static_cast<double *>(wa),
+                              static_cast<double *>(wb), h_corr, tw64[2], tw64[1], tw64[0], rev_y,
+                              rev_z, stream);
+            if (e) return cuda_fail(e, "transfer function launch");
+        }
+        // The host PSF copy must outlive the upload.
+        CUDA_TRY(cudaStreamSynchronize(cs), "transfer function");
+        sl_conv->key = key;
+        if (sl_corr) sl_corr->key = key;
+    }
+
+    void *s1 = nullptr, *s2 = nullptr;
+    if ((st = ws->get("rl_s1", (size_t)g.Z * g.Y * g.Hp * sizeof(float2_), &s1))) return st;
+    if (nd == 3 && (st = ws->get("rl_s2", (size_t)g.Z * g.Py * g.Hp * sizeof(float2_), &s2))) return st;
+    RlBuffers b{};
+    b.s1 = s1;
+    b.s2 = s2;
+    b.h_conv = h_conv;
+    b.h_corr = h_corr;
+    b.tw_x = tw32[2];
+    b.tw_y = tw32[1];
+    b.tw_z = tw32[0];
+    // deconvolve.rs:104.
+    double eps = s->has_filter_epsilon ? s->filter_epsilon : 1e-12;
+    eps = std::max(eps, 1e-15);
+    int e = rl_launch_iterations(g, b, static_cast<const float *>(in->data), static_cast<float *>(out->data),
+                                 s->num_iter, s->clip, (float)eps, stream, ws->t());
+    return e ? cuda_fail(e, "richardson_lucy launch") : ok();
+}
+
+}  // extern "C"

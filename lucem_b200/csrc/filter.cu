@@ -1,0 +1,652 @@
+// filter.cu -- sm_100a kernels for lucem-ops' separable Gaussian family.
+//
+// family_kernel: every Gaussian-family response of one 2-D input in one pass.
+//   Reference path replaced: gaussian_blur_into -> separable::run ->
+//   correlate_1d_kernel, one launch per axis, plus linear_comb_kernel /
+//   add_sq_kernel / sqrt_scale_kernel for DoG, LoG, gradient magnitude and
+//   unsharp (crates/lucem-ops/src/filter/gaussian.rs:176-435,
+//   crates/lucem-ops/src/filter/kernels/convolve.rs:14-59,
+//   crates/lucem-ops/src/filter/kernels/gradient.rs:36-52,
+//   crates/lucem-ops/src/core/kernels/elementwise.rs:136-149).
+//   A 64x64 output tile plus its halo is staged once in shared memory with
+//   the u8/u16 -> f32 cast (and scale) fused into the load.  For each
+//   separable filter the axis-0 pass (rows, first, as the reference orders
+//   its passes) runs over the tile and the columns of the axis-1 halo and is
+//   stored transposed; the axis-1 pass then reads it conflict-free.  Each
+//   thread keeps 8 outputs in registers along the filtered direction and
+//   slides over the taps 8 at a time, so shared-memory loads are 1/8 of the
+//   FMAs.  Responses that combine two filters (DoG, LoG, |grad|, unsharp) are
+//   accumulated in registers across filters and written once.
+//
+// correlate_1d kernels: the reference's 1-D correlation along any axis of an
+//   N-D array ([outer, len, inner] view, crates/lucem-core/src/shape.rs:9-20),
+//   any weights, origin and pad mode, staged through shared memory; same
+//   accumulation order as the reference (f32, taps ascending).
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "internal.h"
+
+namespace lucem {
+
+namespace {
+
+constexpr int kTH = 64;        // output tile rows
+constexpr int kTW = 64;        // output tile columns
+constexpr int kThreads = 256;
+constexpr int kITP = kTH + 1;  // pitch of the transposed intermediate (odd: conflict-free)
+
+// crates/lucem-ops/src/core/kernels/pad.rs:11-34.
+template <int MODE>
+__device__ __forceinline__ int pad_index(int p, int len) {
+    if (p >= 0 && p < len) return p;
+    if (MODE == LUCEM_PAD_CONSTANT) return -1;
+    if (MODE == LUCEM_PAD_NEAREST) return p < 0 ? 0 : len - 1;
+    if (MODE == LUCEM_PAD_WRAP) return ((p % len) + len) % len;
+    if (MODE == LUCEM_PAD_REFLECT) {
+        int period = 2 * len;
+        int r = ((p % period) + period) % period;
+        return r < len ? r : period - 1 - r;
+    }
+    int period = max(2 * len - 2, 1);  // mirror
+    int r = ((p % period) + period) % period;
+    return r < len ? r : period - r;
+}
+
+template <typename T>
+__device__ __forceinline__ float load_as_float(const T *p) { return static_cast<float>(__ldg(p)); }
+
+// Where one CTA tile sits.  Coordinates of the read box are absolute (slide
+// or plane); the pad map applies at the read box's borders.
+struct TileGeom {
+    int plane;
+    int rb_y, rb_x, rb_h, rb_w;   // read box
+    int oy, ox;                   // output tile origin (absolute)
+    int th, tw;                   // valid rows / cols of this tile
+};
+
+template <typename T, int MODE>
+__device__ void family_tile(const FamParams &p, const TileGeom &g, float *A, float *IT) {
+    const int tid = threadIdx.x;
+    const int R0 = p.rmax0, R1 = p.rmax1;
+    const int AW = kTW + 2 * R1;
+    const int AH = kTH + 2 * R0;
+    const T *in = static_cast<const T *>(p.in) + (int64_t)g.plane * p.in_plane_stride;
+
+    // Phase 0: tile + halo -> A (f32), pad map relative to the read box.
+    for (int idx = tid; idx < AH * AW; idx += kThreads) {
+        int r = idx / AW, c = idx - r * AW;
+        int ry = g.oy - g.rb_y - R0 + r;  // row relative to the read box
+        int rx = g.ox - g.rb_x - R1 + c;
+        int py = pad_index<MODE>(ry, g.rb_h);
+        int px = pad_index<MODE>(rx, g.rb_w);
+        float v;
+        if (py < 0 || px < 0) v = p.cval;
+        else v = load_as_float(in + (int64_t)(g.rb_y + py) * p.in_row_pitch + (g.rb_x + px)) * p.in_scale;
+        A[idx] = v;
+    }
+    __syncthreads();
+
+    // Output accumulators: 2 work items x 8 pixels per thread, per output.
+    float acc[kFamMaxOutputs][2][8];
+#pragma unroll
+    for (int k = 0; k < kFamMaxOutputs; ++k)
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int j = 0; j < 8; ++j) acc[k][i][j] = 0.0f;
+
+    // Item -> (y, x-chunk) mapping of the axis-1 pass: a warp covers 8 rows x
+    // 4 chunks of 8 columns (bank = 8*xchunk + t + y: conflict-free).
+    int ys[2], xcs[2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+        int q = i * kThreads + tid;
+        int lane = q & 31, wt = q >> 5;
+        ys[i] = (wt & 7) * 8 + (lane & 7);
+        xcs[i] = (wt >> 3) * 4 + (lane >> 3);
+    }
+
+    // Identity terms (unsharp) read the staged input at the output pixel.
+#pragma unroll
+    for (int k = 0; k < kFamMaxOutputs; ++k) {
+        if (k >= p.n_outputs) break;
+        const FamOutput &o = p.outs[k];
+        if (o.fa == -2 || o.fb == -2) {
+            float coef = o.fa == -2 ? o.alpha : o.beta;
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    float v = A[(ys[i] + R0) * AW + xcs[i] * 8 + j + R1];
+                    acc[k][i][j] = acc[k][i][j] + coef * v;
+                }
+        }
+    }
+
+    for (int f = 0; f < p.n_filters; ++f) {
+        const int r0 = p.r0[f], r1 = p.r1[f];
+        const int n0 = 2 * r0 + 1, n1 = 2 * r1 + 1;
+        const int CW = kTW + 2 * r1;          // intermediate columns for this filter
+        const int aoff_r = R0 - r0, aoff_c = R1 - r1;
+        const float *w0 = p.taps0[f];
+        const float *w1 = p.taps1[f];
+
+        // Phase 1: axis-0 pass.  Item (c, yc): column c of the intermediate,
+        // rows yc*8 .. yc*8+7.  Writes IT[c][y] (transposed).
+        for (int q = tid; q < CW * 8; q += kThreads) {
+            int c = q % CW, yc = q / CW;
+            const float *col = A + (yc * 8 + aoff_r) * AW + c + aoff_c;
+            float o[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) o[j] = 0.0f;
+            float win[16];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) win[j] = col[j * AW];
+            for (int s0 = 0; s0 < n0; s0 += 8) {
+                // Window slots past n0 + 6 only meet zero taps: load 0 there so
+                // no read leaves the staged rows.
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                    win[8 + j] = (s0 + 8 + j <= n0 + 6) ? col[(s0 + 8 + j) * AW] : 0.0f;
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    float w = w0[s0 + u];
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) o[j] = fmaf(w, win[j + u], o[j]);
+                }
+#pragma unroll
+                for (int j = 0; j < 8; ++j) win[j] = win[8 + j];
+            }
+            if (MODE == LUCEM_PAD_CONSTANT) {
+                // A column outside the read box is cval itself in the
+                // reference's intermediate (its axis-1 pass pads the axis-0
+                // result with cval).
+                int rx = g.ox - g.rb_x - r1 + c;
+                if (rx < 0 || rx >= g.rb_w) {
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) o[j] = p.cval;
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < 8; ++j) IT[c * kITP + yc * 8 + j] = o[j];
+        }
+        __syncthreads();
+
+        // Phase 2: axis-1 pass, 8 consecutive columns per item.
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            const float *row = IT + (xcs[i] * 8) * kITP + ys[i];
+            float o[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) o[j] = 0.0f;
+            float win[16];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) win[j] = row[j * kITP];
+            for (int s0 = 0; s0 < n1; s0 += 8) {
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                    win[8 + j] = (s0 + 8 + j <= n1 + 6) ? row[(s0 + 8 + j) * kITP] : 0.0f;
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    float w = w1[s0 + u];
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) o[j] = fmaf(w, win[j + u], o[j]);
+                }
+#pragma unroll
+                for (int j = 0; j < 8; ++j) win[j] = win[8 + j];
+            }
+            // Fold this filter into every response that uses it.
+#pragma unroll
+            for (int k = 0; k < kFamMaxOutputs; ++k) {
+                if (k >= p.n_outputs) break;
+                const FamOutput &oo = p.outs[k];
+                if (oo.combine == (int)Combine::kHypot) {
+                    if (oo.fa == f || oo.fb == f) {
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) acc[k][i][j] = fmaf(o[j], o[j], acc[k][i][j]);
+                    }
+                } else {
+                    // Two terms at most, added to an exact 0: the result does
+                    // not depend on which filter runs first.
+                    if (oo.fa == f) {
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) acc[k][i][j] = acc[k][i][j] + oo.alpha * o[j];
+                    }
+                    if (oo.fb == f) {
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) acc[k][i][j] = acc[k][i][j] + oo.beta * o[j];
+                    }
+                }
+            }
+        }
+        __syncthreads();  // IT is rewritten by the next filter
+    }
+
+    // Epilogue: bias / sqrt, then 32-byte row segments per thread (a warp
+    // writes 8 rows x 128 contiguous bytes).
+#pragma unroll
+    for (int k = 0; k < kFamMaxOutputs; ++k) {
+        if (k >= p.n_outputs) break;
+        const FamOutput &oo = p.outs[k];
+        float *obase = oo.out + (int64_t)g.plane * oo.plane_stride;
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            int y = ys[i], x = xcs[i] * 8;
+            if (y >= g.th) continue;
+            float v[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                float a = acc[k][i][j];
+                if (oo.combine == (int)Combine::kHypot) v[j] = sqrtf(fmaxf(a, 0.0f)) * oo.alpha;
+                else v[j] = a + oo.bias;
+            }
+            float *dst = obase + (int64_t)(g.oy + y) * oo.row_pitch + g.ox + x;
+            bool vec_ok = (x + 8 <= g.tw) && ((reinterpret_cast<uintptr_t>(dst) & 15) == 0);
+            if (vec_ok) {
+                reinterpret_cast<float4 *>(dst)[0] = make_float4(v[0], v[1], v[2], v[3]);
+                reinterpret_cast<float4 *>(dst)[1] = make_float4(v[4], v[5], v[6], v[7]);
+            } else {
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                    if (x + j < g.tw) dst[j] = v[j];
+            }
+        }
+    }
+}
+
+// Planes launch: B planes of [H, W], each its own read and owned box.
+template <typename T, int MODE>
+__global__ void __launch_bounds__(kThreads)
+family_planes_kernel(const __grid_constant__ FamParams p, int tiles_y, int tiles_x) {
+    extern __shared__ float4 smem4[];
+    float *A = reinterpret_cast<float *>(smem4);
+    float *IT = A + (kTH + 2 * p.rmax0) * (kTW + 2 * p.rmax1);
+    const int per_plane = tiles_y * tiles_x;
+    const int total = per_plane * p.B;
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        TileGeom g;
+        g.plane = t / per_plane;
+        int r = t - g.plane * per_plane;
+        int ty = r / tiles_x, tx = r - ty * tiles_x;
+        g.rb_y = 0; g.rb_x = 0; g.rb_h = p.H; g.rb_w = p.W;
+        g.oy = ty * kTH; g.ox = tx * kTW;
+        g.th = min(kTH, p.H - g.oy); g.tw = min(kTW, p.W - g.ox);
+        family_tile<T, MODE>(p, g, A, IT);
+        __syncthreads();
+    }
+}
+
+// Work-list launch: tiles of uneven blocks of a [C, H, W] slide.  With a
+// counter the CTAs are persistent and take tiles from it; without one each
+// CTA walks tiles blockIdx.x, +gridDim.x, ...
+template <typename T, int MODE>
+__global__ void __launch_bounds__(kThreads)
+family_work_kernel(const __grid_constant__ FamParams p, const FamWork *__restrict__ work, int n_work,
+                   int n_tiles, int tile_base, int *counter) {
+    extern __shared__ float4 smem4[];
+    float *A = reinterpret_cast<float *>(smem4);
+    float *IT = A + (kTH + 2 * p.rmax0) * (kTW + 2 * p.rmax1);
+    __shared__ int next_tile;
+    int t = counter ? -1 : (int)blockIdx.x;
+    while (true) {
+        if (counter) {
+            if (threadIdx.x == 0) next_tile = atomicAdd(counter, 1);
+            __syncthreads();
+            t = next_tile;
+            __syncthreads();
+        }
+        if (t >= n_tiles) break;
+        // Binary search for the work item owning tile t (global index tg).
+        const int tg = t + tile_base;
+        int lo = 0, hi = n_work - 1;
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (work[mid].tile_begin <= tg) lo = mid; else hi = mid - 1;
+        }
+        const FamWork w = work[lo];
+        int local = tg - w.tile_begin;
+        int tiles_x = (w.own_w + kTW - 1) / kTW;
+        int ty = local / tiles_x, tx = local - ty * tiles_x;
+        TileGeom g;
+        g.plane = w.channel;
+        g.rb_y = w.read_y; g.rb_x = w.read_x; g.rb_h = w.read_h; g.rb_w = w.read_w;
+        g.oy = w.own_y + ty * kTH; g.ox = w.own_x + tx * kTW;
+        g.th = min(kTH, w.own_y + w.own_h - g.oy); g.tw = min(kTW, w.own_x + w.own_w - g.ox);
+        family_tile<T, MODE>(p, g, A, IT);
+        __syncthreads();
+        if (!counter) t += gridDim.x;
+    }
+}
+
+template <typename T>
+int dispatch_planes(const FamParams &p, size_t smem, int grid, int ty, int tx, cudaStream_t s) {
+    switch (p.mode) {
+#define CASE(M)                                                                                   \
+    case M:                                                                                       \
+        cudaFuncSetAttribute(family_planes_kernel<T, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                             (int)smem);                                                          \
+        family_planes_kernel<T, M><<<grid, kThreads, smem, s>>>(p, ty, tx);                       \
+        break;
+        CASE(0) CASE(1) CASE(2) CASE(3) CASE(4)
+#undef CASE
+    default: return (int)cudaErrorInvalidValue;
+    }
+    return (int)cudaGetLastError();
+}
+
+template <typename T>
+int dispatch_work(const FamParams &p, size_t smem, int grid, const FamWork *work, int n_work,
+                  int n_tiles, int tile_base, int *counter, cudaStream_t s) {
+    switch (p.mode) {
+#define CASE(M)                                                                                  \
+    case M:                                                                                      \
+        cudaFuncSetAttribute(family_work_kernel<T, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                             (int)smem);                                                         \
+        family_work_kernel<T, M><<<grid, kThreads, smem, s>>>(p, work, n_work, n_tiles, tile_base, counter); \
+        break;
+        CASE(0) CASE(1) CASE(2) CASE(3) CASE(4)
+#undef CASE
+    default: return (int)cudaErrorInvalidValue;
+    }
+    return (int)cudaGetLastError();
+}
+
+int sm_count() {
+    static int n = 0;
+    if (n == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 148;
+    }
+    return n;
+}
+
+}  // namespace
+
+int family_tile_dims(int *th, int *tw) {
+    *th = kTH;
+    *tw = kTW;
+    return 0;
+}
+
+size_t family_smem_bytes(int rmax0, int rmax1) {
+    size_t a = (size_t)(kTH + 2 * rmax0) * (kTW + 2 * rmax1);
+    size_t it = (size_t)(kTW + 2 * rmax1) * kITP;
+    return (a + it) * sizeof(float) + 64;
+}
+
+int launch_family_planes(const FamParams &p, int in_dtype, void *stream) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int ty = (p.H + kTH - 1) / kTH, tx = (p.W + kTW - 1) / kTW;
+    int64_t total = (int64_t)ty * tx * p.B;
+    if (total == 0) return 0;
+    size_t smem = family_smem_bytes(p.rmax0, p.rmax1);
+    int grid = (int)(total < (int64_t)sm_count() * 64 ? total : (int64_t)sm_count() * 64);
+    switch (in_dtype) {
+    case LUCEM_U8: return dispatch_planes<uint8_t>(p, smem, grid, ty, tx, s);
+    case LUCEM_U16: return dispatch_planes<uint16_t>(p, smem, grid, ty, tx, s);
+    case LUCEM_F32: return dispatch_planes<float>(p, smem, grid, ty, tx, s);
+    default: return (int)cudaErrorInvalidValue;
+    }
+}
+
+int launch_family_work(const FamParams &p, int in_dtype, const FamWork *work_dev, int32_t n_work,
+                       int32_t n_tiles_total, int32_t tile_base, int32_t *counter_dev,
+                       int32_t persistent_ctas, void *stream) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (n_tiles_total == 0) return 0;
+    size_t smem = family_smem_bytes(p.rmax0, p.rmax1);
+    int grid = counter_dev ? persistent_ctas : n_tiles_total;
+    switch (in_dtype) {
+    case LUCEM_U8: return dispatch_work<uint8_t>(p, smem, grid, work_dev, n_work, n_tiles_total, tile_base, counter_dev, s);
+    case LUCEM_U16: return dispatch_work<uint16_t>(p, smem, grid, work_dev, n_work, n_tiles_total, tile_base, counter_dev, s);
+    case LUCEM_F32: return dispatch_work<float>(p, smem, grid, work_dev, n_work, n_tiles_total, tile_base, counter_dev, s);
+    default: return (int)cudaErrorInvalidValue;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Generic 1-D correlation (crates/lucem-ops/src/filter/kernels/convolve.rs:14-59).
+
+namespace {
+
+constexpr int kRowSeg = 1024;      // outputs per CTA along a contiguous axis
+constexpr int kRowMaxHalo = 15360; // beyond this: direct kernel
+constexpr int kColI = 64, kColK = 32;
+constexpr int kColMaxHalo = 960;
+
+template <typename T, int MODE>
+__global__ void __launch_bounds__(256)
+corr_row_kernel(const T *__restrict__ in, float scale, float *__restrict__ out, int64_t outer,
+                int len, const float *__restrict__ w, int size, int left, float cval) {
+    extern __shared__ float4 smem4[];
+    float *S = reinterpret_cast<float *>(smem4);
+    float *Wsm = S + kRowSeg + size - 1;
+    const int segs = (len + kRowSeg - 1) / kRowSeg;
+    for (int t = threadIdx.x; t < size; t += blockDim.x) Wsm[t] = w[t];
+    for (int64_t b = blockIdx.x; b < outer * segs; b += gridDim.x) {
+        int64_t o = b / segs;
+        int i0 = (int)(b - o * segs) * kRowSeg;
+        const T *row = in + o * len;
+        int n_in = kRowSeg + size - 1;
+        __syncthreads();
+        for (int j = threadIdx.x; j < n_in; j += blockDim.x) {
+            int q = pad_index<MODE>(i0 - left + j, len);
+            S[j] = q < 0 ? cval : static_cast<float>(row[q]) * scale;
+        }
+        __syncthreads();
+        for (int j = threadIdx.x; j < kRowSeg; j += blockDim.x) {
+            if (i0 + j >= len) break;
+            float acc = 0.0f;
+            for (int t = 0; t < size; ++t) acc = fmaf(Wsm[t], S[j + t], acc);
+            out[o * len + i0 + j] = acc;
+        }
+    }
+}
+
+template <typename T, int MODE>
+__global__ void __launch_bounds__(256)
+corr_col_kernel(const T *__restrict__ in, float scale, float *__restrict__ out, int64_t outer,
+                int len, int64_t inner, const float *__restrict__ w, int size, int left, float cval) {
+    extern __shared__ float4 smem4[];
+    float *S = reinterpret_cast<float *>(smem4);  // [kColI + size - 1][kColK]
+    float *Wsm = S + (kColI + size - 1) * kColK;
+    const int64_t ks = (inner + kColK - 1) / kColK;
+    const int is = (len + kColI - 1) / kColI;
+    const int64_t nblk = outer * is * ks;
+    for (int t = threadIdx.x; t < size; t += blockDim.x) Wsm[t] = w[t];
+    const int kk = threadIdx.x & (kColK - 1);
+    const int ig = threadIdx.x / kColK;  // 0..7, 8 outputs each
+    for (int64_t b = blockIdx.x; b < nblk; b += gridDim.x) {
+        int64_t o = b / (is * ks);
+        int64_t r = b - o * is * ks;
+        int i0 = (int)(r / ks) * kColI;
+        int64_t k0 = (r % ks) * kColK;
+        const T *base = in + o * len * inner;
+        int n_in = kColI + size - 1;
+        __syncthreads();
+        for (int j = threadIdx.x; j < n_in * kColK; j += blockDim.x) {
+            int ii = j / kColK, kc = j - ii * kColK;
+            int64_t k = k0 + kc;
+            float v = 0.0f;
+            if (k < inner) {
+                int q = pad_index<MODE>(i0 - left + ii, len);
+                v = q < 0 ? cval : static_cast<float>(base[(int64_t)q * inner + k]) * scale;
+            }
+            S[j] = v;
+        }
+        __syncthreads();
+        int64_t k = k0 + kk;
+        if (k < inner) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                int ii = ig * 8 + j;
+                if (i0 + ii >= len) break;
+                float acc = 0.0f;
+                for (int t = 0; t < size; ++t) acc = fmaf(Wsm[t], S[(ii + t) * kColK + kk], acc);
+                out[(o * len + i0 + ii) * inner + k] = acc;
+            }
+        }
+    }
+}
+
+template <typename T, int MODE>
+__global__ void corr_direct_kernel(const T *__restrict__ in, float scale, float *__restrict__ out,
+                                   int64_t total, int len, int64_t inner,
+                                   const float *__restrict__ w, int size, int left, float cval) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        int64_t i = (e / inner) % len;
+        int64_t base = e - i * inner;
+        int start = (int)i - left;
+        float acc = 0.0f;
+        for (int t = 0; t < size; ++t) {
+            int q = pad_index<MODE>(start + t, len);
+            float v = q < 0 ? cval : static_cast<float>(in[base + (int64_t)q * inner]) * scale;
+            acc = fmaf(w[t], v, acc);
+        }
+        out[e] = acc;
+    }
+}
+
+template <typename T, int MODE>
+int corr_launch(const T *in, float scale, float *out, int64_t outer, int64_t len, int64_t inner,
+                const float *w, int size, int left, float cval, cudaStream_t s) {
+    const int sms = sm_count();
+    if (inner == 1 && size - 1 <= kRowMaxHalo) {
+        size_t smem = (size_t)(kRowSeg + 2 * size) * sizeof(float) + 16;
+        int64_t nb = outer * ((len + kRowSeg - 1) / kRowSeg);
+        int grid = (int)(nb < (int64_t)sms * 16 ? nb : (int64_t)sms * 16);
+        cudaFuncSetAttribute(corr_row_kernel<T, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        corr_row_kernel<T, MODE><<<grid, 256, smem, s>>>(in, scale, out, outer, (int)len, w, size, left, cval);
+    } else if (inner > 1 && size - 1 <= kColMaxHalo) {
+        size_t smem = (size_t)((kColI + size - 1) * kColK + size) * sizeof(float) + 16;
+        int64_t nb = outer * ((len + kColI - 1) / kColI) * ((inner + kColK - 1) / kColK);
+        int grid = (int)(nb < (int64_t)sms * 16 ? nb : (int64_t)sms * 16);
+        cudaFuncSetAttribute(corr_col_kernel<T, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        corr_col_kernel<T, MODE><<<grid, 256, smem, s>>>(in, scale, out, outer, (int)len, inner, w, size, left, cval);
+    } else {
+        int64_t total = outer * len * inner;
+        int64_t nb = (total + 255) / 256;
+        int grid = (int)(nb < (int64_t)sms * 32 ? nb : (int64_t)sms * 32);
+        corr_direct_kernel<T, MODE><<<grid, 256, 0, s>>>(in, scale, out, total, (int)len, inner, w, size, left, cval);
+    }
+    return (int)cudaGetLastError();
+}
+
+template <typename T>
+int corr_mode(const T *in, float scale, float *out, int64_t outer, int64_t len, int64_t inner,
+              const float *w, int size, int left, int mode, float cval, cudaStream_t s) {
+    switch (mode) {
+    case 0: return corr_launch<T, 0>(in, scale, out, outer, len, inner, w, size, left, cval, s);
+    case 1: return corr_launch<T, 1>(in, scale, out, outer, len, inner, w, size, left, cval, s);
+    case 2: return corr_launch<T, 2>(in, scale, out, outer, len, inner, w, size, left, cval, s);
+    case 3: return corr_launch<T, 3>(in, scale, out, outer, len, inner, w, size, left, cval, s);
+    case 4: return corr_launch<T, 4>(in, scale, out, outer, len, inner, w, size, left, cval, s);
+    default: return (int)cudaErrorInvalidValue;
+    }
+}
+
+// ---- elementwise -----------------------------------------------------------
+
+__global__ void linear_comb_kernel(const float *__restrict__ a, const float *__restrict__ b,
+                                   float *__restrict__ out, int64_t n, float alpha, float beta,
+                                   float bias) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        float v = alpha * a[i];
+        if (b) v = v + beta * b[i];
+        out[i] = v + bias;
+    }
+}
+
+__global__ void add_sq_kernel(const float *__restrict__ d, float *__restrict__ acc, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        float g = d[i];
+        acc[i] = fmaf(g, g, acc[i]);
+    }
+}
+
+__global__ void sqrt_scale_kernel(const float *__restrict__ acc, float *__restrict__ out, int64_t n,
+                                  float scale) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = sqrtf(fmaxf(acc[i], 0.0f)) * scale;
+}
+
+template <typename T>
+__global__ void cast_kernel(const T *__restrict__ in, float scale, float *__restrict__ out, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = static_cast<float>(in[i]) * scale;
+}
+
+__global__ void fill_kernel(float *__restrict__ out, int64_t n, float v) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = v;
+}
+
+int ew_grid(int64_t n) {
+    int64_t nb = (n + 255) / 256;
+    int64_t cap = (int64_t)sm_count() * 16;
+    return (int)(nb < cap ? (nb > 0 ? nb : 1) : cap);
+}
+
+}  // namespace
+
+int launch_correlate_1d(const void *in, int in_dtype, float in_scale, float *out, int64_t outer,
+                        int64_t len, int64_t inner, const float *w_dev, int32_t size, int32_t left,
+                        int32_t mode, float cval, void *stream) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    switch (in_dtype) {
+    case LUCEM_U8: return corr_mode(static_cast<const uint8_t *>(in), in_scale, out, outer, len, inner, w_dev, size, left, mode, cval, s);
+    case LUCEM_U16: return corr_mode(static_cast<const uint16_t *>(in), in_scale, out, outer, len, inner, w_dev, size, left, mode, cval, s);
+    case LUCEM_F32: return corr_mode(static_cast<const float *>(in), in_scale, out, outer, len, inner, w_dev, size, left, mode, cval, s);
+    default: return (int)cudaErrorInvalidValue;
+    }
+}
+
+int launch_linear_comb(const float *a, const float *b, float *out, int64_t n, float alpha,
+                       float beta, float bias, void *stream) {
+    if (n == 0) return 0;
+    linear_comb_kernel<<<ew_grid(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(a, b, out, n, alpha, beta, bias);
+    return (int)cudaGetLastError();
+}
+
+int launch_add_sq(const float *d, float *acc, int64_t n, void *stream) {
+    if (n == 0) return 0;
+    add_sq_kernel<<<ew_grid(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(d, acc, n);
+    return (int)cudaGetLastError();
+}
+
+int launch_sqrt_scale(const float *acc, float *out, int64_t n, float scale, void *stream) {
+    if (n == 0) return 0;
+    sqrt_scale_kernel<<<ew_grid(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(acc, out, n, scale);
+    return (int)cudaGetLastError();
+}
+
+int launch_cast(const void *in, int in_dtype, float scale, float *out, int64_t n, void *stream) {
+    if (n == 0) return 0;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    switch (in_dtype) {
+    case LUCEM_U8: cast_kernel<<<ew_grid(n), 256, 0, s>>>(static_cast<const uint8_t *>(in), scale, out, n); break;
+    case LUCEM_U16: cast_kernel<<<ew_grid(n), 256, 0, s>>>(static_cast<const uint16_t *>(in), scale, out, n); break;
+    case LUCEM_F32: cast_kernel<<<ew_grid(n), 256, 0, s>>>(static_cast<const float *>(in), scale, out, n); break;
+    default: return (int)cudaErrorInvalidValue;
+    }
+    return (int)cudaGetLastError();
+}
+
+int launch_fill(float *out, int64_t n, float v, void *stream) {
+    if (n == 0) return 0;
+    fill_kernel<<<ew_grid(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(out, n, v);
+    return (int)cudaGetLastError();
+}
+
+}  // namespace lucem

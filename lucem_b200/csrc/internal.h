@@ -1,0 +1,163 @@
+// internal.h -- shared declarations of the lucem_b200 implementation (host
+// C++ and CUDA).  Not part of the C ABI.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+
+#include "lucem_b200.h"
+
+namespace lucem {
+
+// Kernels index with 32-bit integers: crates/lucem-core/src/compute/limits.rs:12.
+constexpr int64_t kMaxDeviceElements = 0xFFFFFFFFll;
+
+// ---- separable filters -------------------------------------------------
+
+// Largest radius the fused 2-D family kernel takes per axis (65 taps); wider
+// filters run as per-axis passes.
+constexpr int kFamMaxRadius = 32;
+constexpr int kFamMaxTaps = 2 * kFamMaxRadius + 1;
+constexpr int kFamMaxFilters = 8;
+constexpr int kFamMaxOutputs = 4;
+constexpr int kFamTapStride = 72;  // taps per filter axis, zero padded (multiple of 8)
+
+enum class Combine : int32_t { kLinear = 0, kHypot = 1 };
+
+struct FamOutput {
+    float *out;        // f32 [B, H, W] (plane/row strides below)
+    int64_t plane_stride;
+    int64_t row_pitch;
+    int32_t combine;   // Combine
+    int32_t fa, fb;    // filter indices (fb < 0: single term)
+    float alpha, beta, bias;
+    // fa or fb == -2 names the input sample itself (unsharp).
+};
+
+// One launch of the fused 2-D family kernel over B planes of [H, W] (or over
+// work items of a slide, see FamWork).
+struct FamParams {
+    const void *in;
+    int64_t in_plane_stride;
+    int64_t in_row_pitch;
+    int32_t B, H, W;
+    int32_t mode;
+    float cval;
+    float in_scale;
+    int32_t n_filters;
+    int32_t n_outputs;
+    int32_t rmax0, rmax1;          // largest radius per axis over the filters
+    int32_t r0[kFamMaxFilters];    // radius, axis 0 (rows)
+    int32_t r1[kFamMaxFilters];    // radius, axis 1 (columns)
+    FamOutput outs[kFamMaxOutputs];
+    float taps0[kFamMaxFilters][kFamTapStride];
+    float taps1[kFamMaxFilters][kFamTapStride];
+};
+
+// One tile of a batched walk: the read box of one channel and the owned box
+// inside it (absolute slide coordinates).
+struct FamWork {
+    int32_t channel;
+    int32_t read_y, read_x, read_h, read_w;
+    int32_t own_y, own_x, own_h, own_w;
+    int32_t tile_begin;   // first CTA tile index of this item in the flattened list
+};
+
+// Launchers (filter.cu).  All return cudaGetLastError() as int.
+int launch_family_planes(const FamParams &p, int in_dtype, void *stream);
+// Tiles [tile_base, tile_base + n_tiles) of the work list (global tile
+// indices); with counter_dev the launch is persistent (persistent_ctas CTAs).
+int launch_family_work(const FamParams &p, int in_dtype, const FamWork *work_dev, int32_t n_work,
+                       int32_t n_tiles, int32_t tile_base, int32_t *counter_dev,
+                       int32_t persistent_ctas, void *stream);
+int family_tile_dims(int *th, int *tw);
+size_t family_smem_bytes(int rmax0, int rmax1);
+
+// Generic 1-D correlation along one axis of an [outer, len, inner] view.
+int launch_correlate_1d(const void *in, int in_dtype, float in_scale, float *out, int64_t outer,
+                        int64_t len, int64_t inner, const float *w_dev, int32_t size, int32_t left,
+                        int32_t mode, float cval, void *stream);
+// out = alpha*a + beta*b + bias (b may be null: beta ignored).
+int launch_linear_comb(const float *a, const float *b, float *out, int64_t n, float alpha,
+                       float beta, float bias, void *stream);
+// acc += d*d
+int launch_add_sq(const float *d, float *acc, int64_t n, void *stream);
+// out = sqrt(max(acc,0)) * scale
+int launch_sqrt_scale(const float *acc, float *out, int64_t n, float scale, void *stream);
+// out = (float)in * scale (u8/u16/f32 -> f32)
+int launch_cast(const void *in, int in_dtype, float scale, float *out, int64_t n, void *stream);
+int launch_fill(float *out, int64_t n, float v, void *stream);
+
+// ---- per-kernel timing ---------------------------------------------------
+
+enum PassKind : int {
+    kPassRlRow = 0,      // row pass: C2R, RL epilogue, R2C
+    kPassRlColFwd,       // column pass, forward transform
+    kPassRlColFull,      // column pass, forward * H * inverse
+    kPassRlColInv,       // column pass, inverse transform
+    kPassRlOtf,          // transfer-function build
+    kPassFamily,         // fused 2-D Gaussian family
+    kPassCorrelate,      // per-axis correlation
+    kPassElementwise,    // combine / cast / fill
+    kPassCount
+};
+const char *pass_name(int kind);
+
+// Brackets launches with events when a workspace has timing enabled.
+struct PassTimer {
+    virtual ~PassTimer() = default;
+    virtual void begin(int kind, void *stream) = 0;
+    virtual void end(int kind, void *stream) = 0;
+};
+
+// ---- FFT / Richardson-Lucy ---------------------------------------------
+
+constexpr int kFftMaxStages = 16;
+
+struct FftPlan {
+    int32_t n;
+    int32_t nstages;
+    int32_t radix[kFftMaxStages];
+};
+
+bool fft_make_plan(int64_t n, FftPlan *plan);
+// out[p] = frequency held at position p after the in-place forward transform.
+void fft_rev_table(const FftPlan &plan, int32_t *out);
+int64_t fft_good_length(int64_t n, bool even);
+
+struct float2_ { float x, y; };
+
+// Geometry of one RL problem on its FFT grid.  Axes are (z, y, x); 2-D inputs
+// have Z = Pz = 1.
+struct RlGeom {
+    int32_t ndim;
+    int32_t Z, Y, X;         // image
+    int32_t Pz, Py, Px;      // grid
+    int32_t hz, hy, hx;      // extension halo per axis (0 for zero padding)
+    int32_t Hx;              // Px/2 + 1
+    int32_t Hp;              // spectrum row pitch (complex elements)
+    int32_t mode;
+};
+
+struct RlBuffers {
+    void *s1;      // complex [Z][Y][Hp]
+    void *s2;      // complex [Z][Py][Hp] (3-D only)
+    const void *h_conv;  // complex [Pz][Py][Hp]
+    const void *h_corr;  // complex [Pz][Py][Hp] (may equal h_conv)
+    const float2_ *tw_x, *tw_y, *tw_z;  // twiddle tables e^{-2 pi i k / n}, n = Px, Py, Pz
+};
+
+int rl_launch_iterations(const RlGeom &g, const RlBuffers &b, const float *obs, float *est_out,
+                         int32_t num_iter, int32_t clip, float eps, void *stream, PassTimer *timer);
+// OTF of the normalised PSF `psf_dev` (f64 [kz][ky][kx]) centred at `centre`,
+// scaled by 1/(Pz*Py*Px), into complex [Pz][Py][Hp] (f32).  Work buffers are
+// f64 complex of size kz*ky*Hp and kz*Py*Hp.
+// Rows of H are stored at the digit-reversed positions of the y and z plans
+// (rev_y / rev_z from fft_rev_table; rev_z unused for 2-D).
+int rl_launch_otf(const RlGeom &g, const double *psf_dev, const int32_t kdims[3],
+                  const int32_t centre[3], double *work_a, double *work_b, void *h_out,
+                  const double *twd_x, const double *twd_y, const double *twd_z,
+                  const int32_t *rev_y, const int32_t *rev_z, void *stream);
+
+}  // namespace lucem

@@ -1,0 +1,587 @@
+// rl.cu -- Richardson-Lucy deconvolution on FFT convolution, sm_100a.
+//
+// Reference: richardson_lucy_into (crates/lucem-ops/src/restore/deconvolve.rs
+// :45-149) runs per iteration
+//   est_conv = correlate_2d(est, flipped psf)        (a convolution)
+//   rel_blur = obs / (|est_conv| < eps ? eps : est_conv)   (rl_div_clamp_kernel,
+//              restore/kernels/deconvolve.rs:8-22)
+//   err_est  = correlate_2d(rel_blur, psf)           (the adjoint)
+//   est      = est * err_est  (+ clip on the last iteration, rl_mul_clamp_kernel
+//              restore/kernels/deconvolve.rs:27-43)
+// with direct spatial correlations.  Here both correlations are products with
+// the PSF's transfer function on an FFT grid (Pz, Py, Px).  The pad mode is
+// honoured by extending each array by h = k/2 samples per axis with the
+// reference's pad map (zero padding == PadMode::Constant needs no extension),
+// which makes the linear correlation on the extended array equal to the
+// reference's padded correlation on the image.
+//
+// Data flow per iteration (3-D; 2-D drops the z pass and fuses the
+// transfer-function product into its y pass):
+//   row pass   : C2R(x) -> ratio epilogue -> x extension -> R2C(x)    [s1]
+//   y forward  : rows pad(j - hy) of s1 -> FFT(y) -> s2
+//   z pass     : planes pad(j - hz) of s2 -> FFT(z) -> * H -> IFFT(z) -> s2
+//   y inverse  : s2 -> IFFT(y) -> rows [hy, hy+Y) -> s1
+//   row pass   : C2R(x) -> update epilogue (est *= corr) -> R2C(x)     [s1]
+//   ... same three column passes with conj(H) ...
+// The real-to-complex transforms pack the real row into Px/2 complex samples
+// (x[2m] + i x[2m+1]) and split / merge the half spectrum around that
+// transform.  The transfer functions carry the 1/(Pz*Py*Px) normalisation.
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "fft.cuh"
+#include "internal.h"
+
+namespace lucem {
+
+namespace {
+
+using fft::cadd;
+using fft::cmul;
+using fft::csub;
+
+template <int MODE>
+__device__ __forceinline__ int pad_index(int p, int len) {
+    if (p >= 0 && p < len) return p;
+    if (MODE == LUCEM_PAD_CONSTANT) return -1;
+    if (MODE == LUCEM_PAD_NEAREST) return p < 0 ? 0 : len - 1;
+    if (MODE == LUCEM_PAD_WRAP) return ((p % len) + len) % len;
+    if (MODE == LUCEM_PAD_REFLECT) {
+        int period = 2 * len;
+        int r = ((p % period) + period) % period;
+        return r < len ? r : period - 1 - r;
+    }
+    int period = max(2 * len - 2, 1);
+    int r = ((p % period) + period) % period;
+    return r < len ? r : period - r;
+}
+
+__device__ __forceinline__ int pad_index_rt(int p, int len, int mode) {
+    switch (mode) {
+    case LUCEM_PAD_CONSTANT: return pad_index<LUCEM_PAD_CONSTANT>(p, len);
+    case LUCEM_PAD_NEAREST: return pad_index<LUCEM_PAD_NEAREST>(p, len);
+    case LUCEM_PAD_WRAP: return pad_index<LUCEM_PAD_WRAP>(p, len);
+    case LUCEM_PAD_MIRROR: return pad_index<LUCEM_PAD_MIRROR>(p, len);
+    default: return pad_index<LUCEM_PAD_REFLECT>(p, len);
+    }
+}
+
+enum ColMode : int { kColFwd = 0, kColInv = 1, kColFull = 2 };
+
+// One transform along a strided axis over many columns.  Column c maps to
+// (outer = c / Hx, kx = c % Hx); element (row, c) sits at
+// outer*outer_stride + row*row_stride + kx.  Forward output rows are in the
+// plan's digit-reversed order and inverse input rows are expected in it.
+struct ColPass {
+    int32_t ncols, Hx;
+    const float2 *src;
+    int64_t src_outer, src_row;
+    int32_t n_img, halo;          // forward load: row j <- src row pad(j - halo, n_img)
+    float2 *dst;
+    int64_t dst_outer, dst_row;
+    int32_t store_begin, store_count;
+    int32_t mode;                 // ColMode
+    int32_t pad_mode;
+    const float2 *H;              // transfer function (kColFull)
+    int64_t h_outer, h_row;
+    int32_t conj_h;
+    FftPlan plan;
+    const float2 *tw;             // e^{-2 pi i m / n}, m < n
+    int32_t C, CP;
+};
+
+__global__ void __launch_bounds__(512, 1) col_pass_kernel(const __grid_constant__ ColPass p) {
+    extern __shared__ float4 smem4[];
+    const int n = p.plan.n;
+    float2 *tws = reinterpret_cast<float2 *>(smem4);
+    float2 *buf = tws + n;
+    const int C = p.C, CP = p.CP, T = blockDim.x, tid = threadIdx.x;
+    for (int i = tid; i < n; i += T) tws[i] = p.tw[i];
+    const fft::Tw tw{tws, 1};
+    const int ntiles = (p.ncols + C - 1) / C;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int c0 = tile * C;
+        // Load (lanes along columns: coalesced in kx).
+        for (int it = tid; it < n * C; it += T) {
+            int row = it / C, c = it - row * C;
+            int col = c0 + c;
+            float2 v = make_float2(0.f, 0.f);
+            if (col < p.ncols) {
+                int outer = col / p.Hx, kx = col - outer * p.Hx;
+                int srow;
+                if (p.mode == kColInv) srow = row;
+                else srow = row < p.n_img + 2 * p.halo ? pad_index_rt(row - p.halo, p.n_img, p.pad_mode) : -1;
+                if (srow >= 0) v = p.src[outer * p.src_outer + srow * p.src_row + kx];
+            }
+            buf[row * CP + c] = v;
+        }
+        __syncthreads();
+        if (p.mode == kColInv) fft::inverse(buf, n, C, CP, p.plan.radix, p.plan.nstages, tw);
+        else fft::forward(buf, n, C, CP, p.plan.radix, p.plan.nstages, tw);
+        if (p.mode == kColFull) {
+            // Row `row` holds the frequency rev(row); H is stored in the same order.
+            for (int it = tid; it < n * C; it += T) {
+                int row = it / C, c = it - row * C;
+                int col = c0 + c;
+                if (col < p.ncols) {
+                    int outer = col / p.Hx, kx = col - outer * p.Hx;
+                    float2 h = p.H[outer * p.h_outer + row * p.h_row + kx];
+                    if (p.conj_h) h.y = -h.y;
+                    buf[row * CP + c] = cmul(buf[row * CP + c], h);
+                }
+            }
+            __syncthreads();
+            fft::inverse(buf, n, C, CP, p.plan.radix, p.plan.nstages, tw);
+        }
+        // Store.
+        const int rows = p.mode == kColFwd ? n : p.store_count;
+        const int r0 = p.mode == kColFwd ? 0 : p.store_begin;
+        for (int it = tid; it < rows * C; it += T) {
+            int row = it / C, c = it - row * C;
+            int col = c0 + c;
+            if (col < p.ncols) {
+                int outer = col / p.Hx, kx = col - outer * p.Hx;
+                p.dst[outer * p.dst_outer + row * p.dst_row + kx] = buf[(r0 + row) * CP + c];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+enum RowKind : int { kRowInit = 0, kRowRatio = 1, kRowUpdate = 2 };
+
+// The x axis: C2R, the Richardson-Lucy epilogue on the image columns, the x
+// extension and R2C, for C rows per tile.
+struct RowPass {
+    int32_t nrows, X, Px, M, Hx, Hp, hx;
+    int32_t pad_mode;
+    int32_t kind;                 // RowKind
+    const float *obs;             // [nrows][X]        (ratio)
+    float *est;                   // [nrows][X]        (update)
+    int32_t est_first, last, clip;
+    float eps;
+    float2 *s1;                   // [nrows][Hp]
+    FftPlan plan;                 // M-point
+    const float2 *tw;             // table of length Px
+    int32_t C, CP;
+};
+
+__global__ void __launch_bounds__(512, 1) row_pass_kernel(const __grid_constant__ RowPass p) {
+    extern __shared__ float4 smem4[];
+    const int Px = p.Px, M = p.M;
+    const int C = p.C, CP = p.CP, T = blockDim.x, tid = threadIdx.x;
+    float2 *tws = reinterpret_cast<float2 *>(smem4);
+    float2 *bufA = tws + Px;
+    float2 *bufB = bufA + (M + 1) * CP;
+    for (int i = tid; i < Px; i += T) tws[i] = p.tw[i];
+    const fft::Tw twM{tws, 2};   // W_M^m = W_Px^{2m}
+    const int ntiles = (p.nrows + C - 1) / C;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int row0 = tile * C;
+        float2 *buf = bufA;  // holds the natural-order real row after C2R
+        __syncthreads();
+        if (p.kind != kRowInit) {
+            // Half spectrum X[0..M] of each row (lanes along k: coalesced).
+            for (int it = tid; it < (M + 1) * C; it += T) {
+                int c = it / (M + 1), k = it - c * (M + 1);
+                int row = row0 + c;
+                float2 v = make_float2(0.f, 0.f);
+                if (row < p.nrows) v = p.s1[(int64_t)row * p.Hp + k];
+                bufA[k * CP + c] = v;
+            }
+            __syncthreads();
+            // Merge the half spectrum into the packed M-point spectrum:
+            // Z[k] = (X[k] + X*[M-k]) + i (X[k] - X*[M-k]) W_Px^{-k}.
+            for (int it = tid; it < (M / 2 + 1) * C; it += T) {
+                int k = it / C, c = it - k * C;
+                float2 xk = bufA[k * CP + c], xm = bufA[(M - k) * CP + c];
+                float2 xmc = make_float2(xm.x, -xm.y), xkc = make_float2(xk.x, -xk.y);
+                float2 wk = tws[k];
+                wk.y = -wk.y;  // W^{-k}
+                float2 e = cadd(xk, xmc), d = cmul(csub(xk, xmc), wk);
+                float2 zk = make_float2(e.x - d.y, e.y + d.x);
+                if (k != 0 && 2 * k != M) {
+                    float2 wm = tws[M - k];
+                    wm.y = -wm.y;
+                    float2 e2 = cadd(xm, xkc), d2 = cmul(csub(xm, xkc), wm);
+                    bufA[(M - k) * CP + c] = make_float2(e2.x - d2.y, e2.y + d2.x);
+                }
+                bufA[k * CP + c] = zk;
+            }
+            __syncthreads();
+            buf = fft::stockham(bufA, bufB, M, C, CP, p.plan.radix, p.plan.nstages, twM, true);
+        }
+        float *bufr = reinterpret_cast<float *>(buf);
+        // Epilogue on the image columns; the real sample at position i of the
+        // row is component (i & 1) of packed element i >> 1.
+        const bool emit = !(p.kind == kRowUpdate && p.last);
+        for (int it = tid; it < p.X * C; it += T) {
+            int c = it / p.X, xi = it - c * p.X;
+            int row = row0 + c;
+            if (row >= p.nrows) continue;
+            int i = xi + p.hx;
+            float *slot = bufr + ((i >> 1) * CP + c) * 2 + (i & 1);
+            int64_t g = (int64_t)row * p.X + xi;
+            float v;
+            if (p.kind == kRowInit) {
+                v = 0.5f;
+            } else if (p.kind == kRowRatio) {
+                float conv = *slot;
+                float d = fabsf(conv) < p.eps ? p.eps : conv;
+                v = p.obs[g] / d;
+            } else {
+                float corr = *slot;
+                float old = p.est_first ? 0.5f : p.est[g];
+                v = old * corr;
+                if (p.last && p.clip) v = fminf(fmaxf(v, -1.0f), 1.0f);
+                p.est[g] = v;
+            }
+            if (emit) *slot = v;
+        }
+        if (!emit) continue;
+        __syncthreads();
+        // Extension along x: positions [0, hx) and [hx+X, hx+X+hx) take the
+        // pad-mapped image samples, everything past X + 2*hx is zero.
+        for (int it = tid; it < Px * C; it += T) {
+            int c = it / Px, j = it - c * Px;
+            if (j >= p.hx && j < p.hx + p.X) continue;
+            float v = 0.0f;
+            if (j < p.X + 2 * p.hx) {
+                int q = pad_index_rt(j - p.hx, p.X, p.pad_mode);
+                if (q >= 0) {
+                    int s = q + p.hx;
+                    v = bufr[((s >> 1) * CP + c) * 2 + (s & 1)];
+                }
+            }
+            bufr[((j >> 1) * CP + c) * 2 + (j & 1)] = v;
+        }
+        __syncthreads();
+        float2 *other = buf == bufA ? bufB : bufA;
+        float2 *z = fft::stockham(buf, other, M, C, CP, p.plan.radix, p.plan.nstages, twM, false);
+        // Split the packed spectrum into the half spectrum:
+        // X[k] = 1/2 (Z[k] + Z*[M-k]) - i/2 W_Px^k (Z[k] - Z*[M-k]).
+        for (int it = tid; it < (M / 2 + 1) * C; it += T) {
+            int k = it / C, c = it - k * C;
+            float2 zk = z[k * CP + c];
+            float2 zm = z[((M - k) % M) * CP + c];
+            float2 zmc = make_float2(zm.x, -zm.y), zkc = make_float2(zk.x, -zk.y);
+            float2 e = cadd(zk, zmc), d = cmul(csub(zk, zmc), tws[k]);
+            float2 xk = make_float2(0.5f * (e.x + d.y), 0.5f * (e.y - d.x));
+            float2 e2 = cadd(zm, zkc), d2 = cmul(csub(zm, zkc), tws[M - k]);
+            float2 xm = make_float2(0.5f * (e2.x + d2.y), 0.5f * (e2.y - d2.x));
+            z[k * CP + c] = xk;
+            if (2 * k != M) z[(M - k) * CP + c] = xm;
+        }
+        __syncthreads();
+        for (int it = tid; it < (M + 1) * C; it += T) {
+            int c = it / (M + 1), k = it - c * (M + 1);
+            int row = row0 + c;
+            if (row < p.nrows) p.s1[(int64_t)row * p.Hp + k] = z[k * CP + c];
+        }
+    }
+}
+
+// ---- transfer function (FP64, direct small-support DFT per axis) ----------
+
+// A[z][y][kx] = sum_x psf[z][y][x] e^{-2 pi i kx (x - cx) / Px}
+__global__ void otf_x_kernel(const double *__restrict__ psf, int kz, int ky, int kx, int cx, int Px,
+                             int Hx, int Hp, const double2 *__restrict__ twd, double2 *__restrict__ A) {
+    int64_t total = (int64_t)kz * ky * Hx;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        int f = (int)(e % Hx);
+        int64_t zy = e / Hx;
+        const double *row = psf + zy * kx;
+        double re = 0.0, im = 0.0;
+        for (int x = 0; x < kx; ++x) {
+            int m = (int)(((int64_t)f * (x - cx)) % Px);
+            if (m < 0) m += Px;
+            double2 w = twd[m];
+            double v = row[x];
+            re = fma(v, w.x, re);
+            im = fma(v, w.y, im);
+        }
+        A[zy * Hp + f] = make_double2(re, im);
+    }
+}
+
+// B[z][py][kx] = sum_y A[z][y][kx] e^{-2 pi i ky (y - cy) / Py}, ky = rev_y(py)
+__global__ void otf_y_kernel(const double2 *__restrict__ A, int kz, int ky, int cy, int Py, int Hx,
+                             int Hp, const double2 *__restrict__ twd, const int *__restrict__ rev_y,
+                             double2 *__restrict__ B) {
+    int64_t total = (int64_t)kz * Py * Hx;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        int f = (int)(e % Hx);
+        int64_t r = e / Hx;
+        int py = (int)(r % Py);
+        int fy = rev_y[py];
+        int z = (int)(r / Py);
+        double re = 0.0, im = 0.0;
+        for (int y = 0; y < ky; ++y) {
+            int m = (int)(((int64_t)fy * (y - cy)) % Py);
+            if (m < 0) m += Py;
+            double2 w = twd[m];
+            double2 a = A[((int64_t)z * ky + y) * Hp + f];
+            re += a.x * w.x - a.y * w.y;
+            im += a.x * w.y + a.y * w.x;
+        }
+        B[((int64_t)z * Py + py) * Hp + f] = make_double2(re, im);
+    }
+}
+
+// H[pz][py][kx] = scale * sum_z B[z][py][kx] e^{-2 pi i kz (z - cz) / Pz}, kz = rev_z(pz),
+// rounded to f32
+__global__ void otf_z_kernel(const double2 *__restrict__ B, int kz, int cz, int Pz, int Py, int Hx,
+                             int Hp, const double2 *__restrict__ twd, const int *__restrict__ rev_z,
+                             double scale, float2 *__restrict__ H) {
+    int64_t total = (int64_t)Pz * Py * Hx;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        int f = (int)(e % Hx);
+        int64_t r = e / Hx;
+        int py = (int)(r % Py);
+        int pz = (int)(r / Py);
+        int fz = rev_z[pz];
+        double re = 0.0, im = 0.0;
+        for (int z = 0; z < kz; ++z) {
+            int m = (int)(((int64_t)fz * (z - cz)) % Pz);
+            if (m < 0) m += Pz;
+            double2 w = twd[m];
+            double2 b = B[((int64_t)z * Py + py) * Hp + f];
+            re += b.x * w.x - b.y * w.y;
+            im += b.x * w.y + b.y * w.x;
+        }
+        H[((int64_t)pz * Py + py) * Hp + f] = make_float2((float)(re * scale), (float)(im * scale));
+    }
+}
+
+int sms() {
+    int dev = 0, n = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n > 0 ? n : 148;
+}
+
+// Columns per CTA and threads for a length-n column transform.
+void col_shape(int n, int *C, int *T) {
+    int c = 64;
+    while (c > 4 && (int64_t)n * c > 16384) c >>= 1;
+    // About 8 butterflies' worth of values per thread and stage.
+    int t = (int)(((int64_t)n * c / 16 + 31) / 32) * 32;
+    if (t < 128) t = 128;
+    if (t > 512) t = 512;
+    *C = c;
+    *T = t;
+}
+
+int launch_col(ColPass p, cudaStream_t s) {
+    int C, T;
+    col_shape(p.plan.n, &C, &T);
+    p.C = C;
+    p.CP = C + 1;
+    size_t smem = ((size_t)p.plan.n + (size_t)p.plan.n * p.CP) * sizeof(float2);
+    int ntiles = (p.ncols + C - 1) / C;
+    int per_sm = (int)((227 * 1024) / (smem + 1024));
+    if (per_sm < 1) per_sm = 1;
+    int grid = ntiles < sms() * per_sm ? ntiles : sms() * per_sm;
+    cudaFuncSetAttribute(col_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    col_pass_kernel<<<grid, T, smem, s>>>(p);
+    return (int)cudaGetLastError();
+}
+
+int launch_row(RowPass p, cudaStream_t s) {
+    const int M = p.M;
+    // Two (M+1) x (C+1) buffers plus the twiddles, about 100 KB at most.
+    int C = 16;
+    while (C > 2 && ((size_t)p.Px + 2 * (size_t)(M + 1) * (C + 1)) * sizeof(float2) > 110 * 1024) C >>= 1;
+    int T = (int)(((int64_t)M * C / 8 + 31) / 32) * 32;
+    if (T < 128) T = 128;
+    if (T > 512) T = 512;
+    p.C = C;
+    p.CP = C + 1;
+    size_t smem = ((size_t)p.Px + 2 * (size_t)(M + 1) * p.CP) * sizeof(float2);
+    int ntiles = (p.nrows + C - 1) / C;
+    int per_sm = (int)((227 * 1024) / (smem + 1024));
+    if (per_sm < 1) per_sm = 1;
+    int grid = ntiles < sms() * per_sm ? ntiles : sms() * per_sm;
+    cudaFuncSetAttribute(row_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    row_pass_kernel<<<grid, T, smem, s>>>(p);
+    return (int)cudaGetLastError();
+}
+
+}  // namespace
+
+// Radix plan: 8s first, then 4, 2, 3, 5, 7.
+bool fft_make_plan(int64_t n, FftPlan *plan) {
+    plan->n = (int32_t)n;
+    plan->nstages = 0;
+    int64_t m = n;
+    const int order[] = {8, 4, 2, 3, 5, 7};
+    for (int r : order) {
+        while (m % r == 0 && plan->nstages < kFftMaxStages) {
+            plan->radix[plan->nstages++] = r;
+            m /= r;
+        }
+    }
+    return m == 1 && n >= 1;
+}
+
+// Position -> frequency of the in-place forward transform (see fft.cuh).
+void fft_rev_table(const FftPlan &plan, int32_t *out) {
+    const int n = plan.n;
+    for (int p = 0; p < n; ++p) {
+        int digits[kFftMaxStages];
+        int w = n, q = p;
+        for (int i = 0; i < plan.nstages; ++i) {
+            w /= plan.radix[i];
+            digits[i] = q / w;
+            q %= w;
+        }
+        int f = 0;
+        for (int i = plan.nstages - 1; i >= 0; --i) f = f * plan.radix[i] + digits[i];
+        out[p] = f;
+    }
+}
+
+int64_t fft_good_length(int64_t n, bool even) {
+    if (n < 1) n = 1;
+    for (int64_t m = n;; ++m) {
+        if (even && (m & 1)) continue;
+        int64_t r = m;
+        for (int f : {2, 3, 5, 7})
+            while (r % f == 0) r /= f;
+        if (r == 1) return m;
+    }
+}
+
+int rl_launch_iterations(const RlGeom &g, const RlBuffers &b, const float *obs, float *est_out,
+                         int32_t num_iter, int32_t clip, float eps, void *stream, PassTimer *timer) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    auto timed_col = [&](const ColPass &c) -> int {
+        int kind = c.mode == kColFwd ? kPassRlColFwd : (c.mode == kColFull ? kPassRlColFull : kPassRlColInv);
+        if (timer) timer->begin(kind, stream);
+        int e = launch_col(c, s);
+        if (timer) timer->end(kind, stream);
+        return e;
+    };
+    auto timed_row = [&](const RowPass &r) -> int {
+        if (timer) timer->begin(kPassRlRow, stream);
+        int e = launch_row(r, s);
+        if (timer) timer->end(kPassRlRow, stream);
+        return e;
+    };
+    const int nrows = g.Z * g.Y;
+    RowPass rp{};
+    rp.nrows = nrows;
+    rp.X = g.X;
+    rp.Px = g.Px;
+    rp.M = g.Px / 2;
+    rp.Hx = g.Hx;
+    rp.Hp = g.Hp;
+    rp.hx = g.hx;
+    rp.pad_mode = g.mode;
+    rp.obs = obs;
+    rp.est = est_out;
+    rp.clip = clip;
+    rp.eps = eps;
+    rp.s1 = static_cast<float2 *>(b.s1);
+    rp.tw = reinterpret_cast<const float2 *>(b.tw_x);
+    if (!fft_make_plan(rp.M, &rp.plan)) return (int)cudaErrorInvalidValue;
+
+    FftPlan py_plan, pz_plan;
+    if (!fft_make_plan(g.Py, &py_plan)) return (int)cudaErrorInvalidValue;
+    if (g.ndim == 3 && !fft_make_plan(g.Pz, &pz_plan)) return (int)cudaErrorInvalidValue;
+    float2 *s1 = static_cast<float2 *>(b.s1);
+    float2 *s2 = static_cast<float2 *>(b.s2);
+
+    auto conv_pair = [&](const void *H, int conj) -> int {
+        int e;
+        if (g.ndim == 2) {
+            ColPass c{};
+            c.ncols = g.Hx; c.Hx = g.Hx;
+            c.src = s1; c.src_outer = 0; c.src_row = g.Hp;
+            c.n_img = g.Y; c.halo = g.hy;
+            c.dst = s1; c.dst_outer = 0; c.dst_row = g.Hp;
+            c.store_begin = g.hy; c.store_count = g.Y;
+            c.mode = kColFull; c.pad_mode = g.mode;
+            c.H = static_cast<const float2 *>(H); c.h_outer = 0; c.h_row = g.Hp; c.conj_h = conj;
+            c.plan = py_plan; c.tw = reinterpret_cast<const float2 *>(b.tw_y);
+            return timed_col(c);
+        }
+        ColPass yf{};
+        yf.ncols = g.Z * g.Hx; yf.Hx = g.Hx;
+        yf.src = s1; yf.src_outer = (int64_t)g.Y * g.Hp; yf.src_row = g.Hp;
+        yf.n_img = g.Y; yf.halo = g.hy;
+        yf.dst = s2; yf.dst_outer = (int64_t)g.Py * g.Hp; yf.dst_row = g.Hp;
+        yf.mode = kColFwd; yf.pad_mode = g.mode;
+        yf.plan = py_plan; yf.tw = reinterpret_cast<const float2 *>(b.tw_y);
+        if ((e = timed_col(yf))) return e;
+        ColPass zp{};
+        zp.ncols = g.Py * g.Hx; zp.Hx = g.Hx;
+        zp.src = s2; zp.src_outer = g.Hp; zp.src_row = (int64_t)g.Py * g.Hp;
+        zp.n_img = g.Z; zp.halo = g.hz;
+        zp.dst = s2; zp.dst_outer = g.Hp; zp.dst_row = (int64_t)g.Py * g.Hp;
+        zp.store_begin = g.hz; zp.store_count = g.Z;
+        zp.mode = kColFull; zp.pad_mode = g.mode;
+        zp.H = static_cast<const float2 *>(H); zp.h_outer = g.Hp; zp.h_row = (int64_t)g.Py * g.Hp;
+        zp.conj_h = conj;
+        zp.plan = pz_plan; zp.tw = reinterpret_cast<const float2 *>(b.tw_z);
+        if ((e = timed_col(zp))) return e;
+        ColPass yi{};
+        yi.ncols = g.Z * g.Hx; yi.Hx = g.Hx;
+        yi.src = s2; yi.src_outer = (int64_t)g.Py * g.Hp; yi.src_row = g.Hp;
+        yi.n_img = g.Py; yi.halo = 0;
+        yi.dst = s1; yi.dst_outer = (int64_t)g.Y * g.Hp; yi.dst_row = g.Hp;
+        yi.store_begin = g.hy; yi.store_count = g.Y;
+        yi.mode = kColInv; yi.pad_mode = g.mode;
+        yi.plan = py_plan; yi.tw = reinterpret_cast<const float2 *>(b.tw_y);
+        return timed_col(yi);
+    };
+
+    int e;
+    rp.kind = kRowInit;
+    if ((e = timed_row(rp))) return e;
+    for (int it = 0; it < num_iter; ++it) {
+        if ((e = conv_pair(b.h_conv, 0))) return e;
+        rp.kind = kRowRatio;
+        if ((e = timed_row(rp))) return e;
+        if ((e = conv_pair(b.h_corr, 1))) return e;
+        rp.kind = kRowUpdate;
+        rp.est_first = it == 0;
+        rp.last = it + 1 == num_iter;
+        if ((e = timed_row(rp))) return e;
+    }
+    return 0;
+}
+
+int rl_launch_otf(const RlGeom &g, const double *psf_dev, const int32_t kdims[3],
+                  const int32_t centre[3], double *work_a, double *work_b, void *h_out,
+                  const double *twd_x, const double *twd_y, const double *twd_z,
+                  const int32_t *rev_y, const int32_t *rev_z, void *stream) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int kz = kdims[0], ky = kdims[1], kx = kdims[2];
+    double2 *A = reinterpret_cast<double2 *>(work_a);
+    double2 *B = reinterpret_cast<double2 *>(work_b);
+    const double scale = 1.0 / ((double)g.Pz * (double)g.Py * (double)g.Px);
+    auto grid_for = [](int64_t total) {
+        int64_t nb = (total + 255) / 256;
+        int64_t cap = (int64_t)sms() * 32;
+        return (int)(nb < cap ? (nb > 0 ? nb : 1) : cap);
+    };
+    int64_t ta = (int64_t)kz * ky * g.Hx;
+    otf_x_kernel<<<grid_for(ta), 256, 0, s>>>(psf_dev, kz, ky, kx, centre[2], g.Px, g.Hx, g.Hp,
+                                               reinterpret_cast<const double2 *>(twd_x), A);
+    int64_t tb = (int64_t)kz * g.Py * g.Hx;
+    otf_y_kernel<<<grid_for(tb), 256, 0, s>>>(A, kz, ky, centre[1], g.Py, g.Hx, g.Hp,
+                                               reinterpret_cast<const double2 *>(twd_y), rev_y, B);
+    int64_t tz = (int64_t)g.Pz * g.Py * g.Hx;
+    otf_z_kernel<<<grid_for(tz), 256, 0, s>>>(B, kz, centre[0], g.Pz, g.Py, g.Hx, g.Hp,
+                                               reinterpret_cast<const double2 *>(twd_z), rev_z, scale,
+                                               static_cast<float2 *>(h_out));
+    return (int)cudaGetLastError();
+}
+
+}  // namespace lucem

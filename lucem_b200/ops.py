@@ -1,0 +1,525 @@
+"""lucem-ops' Gaussian family and Richardson-Lucy on torch CUDA tensors.
+
+Each function mirrors the reference function of the same name
+(crates/lucem-ops/src/filter/gaussian.rs, filter/convolve.rs,
+restore/deconvolve.rs): same parameters, defaults, argument checks and error
+kinds (raised as LucemError, a ValueError carrying the lucem_status).  Arrays
+are zero-copy device tensors; work is queued on the current torch stream.
+
+Inputs may be float32, uint8 or uint16 (the cast to f32 is fused into the
+kernels' load); outputs are float32.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import threading
+from dataclasses import dataclass
+from typing import Optional, Sequence
+
+import numpy as np
+import torch
+
+from . import _native as N
+from ._native import LucemError
+
+__all__ = [
+    "LucemError", "PadMode", "Block", "context", "Workspace", "gaussian_kernel_1d", "gaussian_radius",
+    "pad_index", "gaussian_blur", "gaussian_1d", "correlate_1d", "convolve_1d",
+    "difference_of_gaussians", "gaussian_laplace", "gaussian_grad_mag", "unsharp_mask",
+    "gaussian_family", "schedule", "gaussian_family_tiles", "richardson_lucy", "rl_grid",
+    "gaussian_halo", "op_halo",
+]
+
+
+class PadMode:
+    """crates/lucem-ops/src/core/pad.rs:15-68."""
+
+    REFLECT, CONSTANT, NEAREST, MIRROR, WRAP = 0, 1, 2, 3, 4
+
+    @staticmethod
+    def parse(mode) -> int:
+        if isinstance(mode, (int, np.integer)):
+            return int(mode)
+        out = C.c_int32()
+        N.check(N.lib().lucem_pad_mode_parse(str(mode).encode(), C.byref(out)))
+        return out.value
+
+
+_DTYPES = {torch.float32: N.F32, torch.uint8: N.U8, torch.uint16: N.U16}
+
+# ---------------------------------------------------------------------------
+# Context / workspace
+
+
+class _Ctx:
+    def __init__(self, device: int):
+        self.device = device
+        h = C.c_void_p()
+        N.check(N.lib().lucem_ctx_create(device, C.byref(h)))
+        self.handle = h
+
+
+_ctx_lock = threading.Lock()
+_ctxs: dict = {}
+
+
+def context(device: Optional[int] = None) -> _Ctx:
+    """The library context of a CUDA device (created once per process)."""
+    if device is None:
+        device = torch.cuda.current_device()
+    with _ctx_lock:
+        if device not in _ctxs:
+            with torch.cuda.device(device):
+                _ctxs[device] = _Ctx(device)
+        return _ctxs[device]
+
+
+class Workspace:
+    """Grow-only device scratch (crates/lucem-core/src/memory/workspace.rs).
+    One workspace serves one thread of work at a time."""
+
+    def __init__(self, device: Optional[int] = None):
+        self.ctx = context(device)
+        h = C.c_void_p()
+        N.check(N.lib().lucem_workspace_create(self.ctx.handle, C.byref(h)))
+        self.handle = h
+
+    @property
+    def capacity_bytes(self) -> int:
+        return int(N.lib().lucem_workspace_capacity_bytes(self.handle))
+
+    def set_timing(self, enable: bool = True):
+        """Bracket every kernel this workspace's calls launch with CUDA events
+        (restarts the totals)."""
+        N.check(N.lib().lucem_workspace_set_timing(self.handle, int(bool(enable))))
+
+    def timings(self) -> dict:
+        """{kernel kind: (launches, total device ms)} since timing was enabled;
+        synchronises on the recorded events."""
+        cap = 16
+        names = C.create_string_buffer(32 * cap)
+        ms = (C.c_double * cap)()
+        cnt = (C.c_int64 * cap)()
+        n = C.c_int32()
+        N.check(N.lib().lucem_workspace_timings(self.handle, names, ms, cnt, cap, C.byref(n)))
+        out = {}
+        for i in range(min(n.value, cap)):
+            name = names.raw[32 * i:32 * i + 32].split(b"\0", 1)[0].decode()
+            out[name] = (int(cnt[i]), float(ms[i]))
+        return out
+
+    def close(self):
+        if self.handle:
+            N.lib().lucem_workspace_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_tls = threading.local()
+
+
+def _default_ws(device: int) -> Workspace:
+    d = getattr(_tls, "ws", None)
+    if d is None:
+        d = _tls.ws = {}
+    if device not in d:
+        d[device] = Workspace(device)
+    return d[device]
+
+
+# ---------------------------------------------------------------------------
+# helpers
+
+
+def _tensor(t: torch.Tensor, name: str) -> N.Tensor:
+    if not isinstance(t, torch.Tensor):
+        raise TypeError(f"{name} must be a torch.Tensor")
+    if not t.is_cuda:
+        raise LucemError(7, f"invalid parameter `{name}`: must be a CUDA tensor")
+    if t.dtype not in _DTYPES:
+        raise LucemError(13, f"{name}: unsupported element type {t.dtype}")
+    if not t.is_contiguous():
+        raise LucemError(7, f"invalid parameter `{name}`: must be C-contiguous")
+    if t.dim() > N.MAX_DIMS:
+        raise LucemError(3, f"{name} expects at most {N.MAX_DIMS}-D array, got {t.dim()}-D")
+    d = N.Tensor()
+    d.data = t.data_ptr() if t.numel() > 0 else None
+    d.dtype = _DTYPES[t.dtype]
+    d.ndim = t.dim()
+    for i, s in enumerate(t.shape):
+        d.dims[i] = int(s)
+    return d
+
+
+def _stream(t: torch.Tensor) -> C.c_void_p:
+    return C.c_void_p(torch.cuda.current_stream(t.device).cuda_stream)
+
+
+def _out_like(x: torch.Tensor, out: Optional[torch.Tensor]) -> torch.Tensor:
+    if out is None:
+        return torch.empty(x.shape, dtype=torch.float32, device=x.device)
+    return out
+
+
+def _doubles(v) -> tuple:
+    if np.isscalar(v):
+        v = [v]
+    v = [float(a) for a in v]
+    return (C.c_double * max(1, len(v)))(*v), len(v)
+
+
+def _ctx_ws(x: torch.Tensor, workspace: Optional[Workspace]):
+    dev = x.device.index if x.device.index is not None else torch.cuda.current_device()
+    ctx = context(dev)
+    ws = workspace if workspace is not None else _default_ws(dev)
+    return ctx, ws
+
+
+def _gaussian_settings(orders, mode, cval, truncate, radii, axes, channel_axis, input_scale, keep):
+    s = N.GaussianSettings()
+    N.lib().lucem_gaussian_settings_default(C.byref(s))
+    if orders is not None:
+        if np.isscalar(orders):
+            orders = [orders]
+        arr = (C.c_uint32 * len(orders))(*[int(o) for o in orders])
+        keep.append(arr)
+        s.orders = arr
+        s.n_orders = len(orders)
+    s.mode = PadMode.parse(mode)
+    s.cval = float(cval)
+    s.truncate = float(truncate)
+    if radii is not None:
+        if np.isscalar(radii):
+            radii = [radii]
+        arr = (C.c_int64 * len(radii))(*[int(r) for r in radii])
+        keep.append(arr)
+        s.radii = arr
+        s.n_radii = len(radii)
+    if axes is not None:
+        arr = (C.c_int64 * max(1, len(axes)))(*[int(a) for a in axes])
+        keep.append(arr)
+        s.axes = arr
+        s.n_axes = len(axes)
+    if channel_axis is not None:
+        s.has_channel_axis = 1
+        s.channel_axis = int(channel_axis)
+    s.input_scale = float(input_scale)
+    return s
+
+
+# ---------------------------------------------------------------------------
+# host helpers
+
+
+def gaussian_kernel_1d(sigma: float, order: int, radius: int) -> np.ndarray:
+    """crates/lucem-ops/src/filter/gaussian.rs:22-63 (f64 taps)."""
+    out = np.empty(2 * int(radius) + 1, np.float64)
+    N.check(N.lib().lucem_gaussian_kernel_1d(float(sigma), int(order), int(radius),
+                                             out.ctypes.data_as(C.POINTER(C.c_double))))
+    return out
+
+
+def gaussian_radius(sigma: float, truncate: float = 4.0) -> int:
+    """crates/lucem-ops/src/filter/gaussian.rs:83-85."""
+    return int(N.lib().lucem_gaussian_radius(float(truncate), float(sigma)))
+
+
+def pad_index(p: int, n: int, mode="reflect") -> int:
+    """crates/lucem-ops/src/core/kernels/pad.rs:11-34 (-1: constant fill)."""
+    return int(N.lib().lucem_pad_index(int(p), int(n), PadMode.parse(mode)))
+
+
+def gaussian_halo(ndim: int, sigmas, truncate: float = 4.0):
+    """GaussianBlur::halo (crates/lucem-ops/src/filter/gaussian.rs:160-172)."""
+    if np.isscalar(sigmas):
+        sigmas = [sigmas]
+    out = []
+    for d in range(ndim):
+        s = sigmas[d] if d < len(sigmas) else (sigmas[0] if sigmas else 0.0)
+        r = gaussian_radius(s, truncate) if s > 0 else 0
+        out.append((r, r))
+    return out
+
+
+def op_halo(op: str, sigma: float = 0.0, low_sigma: float = 0.0, high_sigma: float = 0.0) -> int:
+    """Op::halo for the Gaussian ops (engine/lucem-pipeline/src/ops.rs:434-438):
+    ceil(4 sigma)."""
+    s = lambda v: int(np.ceil(4.0 * max(v, 0.0)))  # noqa: E731
+    if op in ("gaussian_blur", "unsharp_mask"):
+        return s(sigma)
+    if op == "difference_of_gaussians":
+        return s(max(low_sigma, high_sigma))
+    raise ValueError(f"no halo rule for {op}")
+
+
+# ---------------------------------------------------------------------------
+# filters
+
+
+def gaussian_blur(x: torch.Tensor, sigmas, *, orders=None, mode="reflect", cval=0.0, truncate=4.0, radii=None,
+                  axes=None, channel_axis=None, input_scale=1.0, out: Optional[torch.Tensor] = None,
+                  workspace: Optional[Workspace] = None) -> torch.Tensor:
+    """gaussian_blur / gaussian_blur_into (crates/lucem-ops/src/filter/gaussian.rs:176-250)."""
+    ctx, ws = _ctx_ws(x, workspace)
+    out = _out_like(x, out)
+    keep = []
+    s = _gaussian_settings(orders, mode, cval, truncate, radii, axes, channel_axis, input_scale, keep)
+    sig, ns = _doubles(sigmas)
+    ti, to = _tensor(x, "input"), _tensor(out, "output")
+    N.check(N.lib().lucem_gaussian_blur(ctx.handle, C.byref(ti), sig, ns, C.byref(s), C.byref(to), ws.handle,
+                                        _stream(x)))
+    return out
+
+
+def gaussian_1d(x: torch.Tensor, sigma: float, *, axis=-1, order=0, mode="reflect", cval=0.0, truncate=4.0,
+                radius=None, out: Optional[torch.Tensor] = None) -> torch.Tensor:
+    """gaussian_1d / gaussian_1d_into (crates/lucem-ops/src/filter/gaussian.rs:66-130)."""
+    ctx, _ = _ctx_ws(x, None)
+    out = _out_like(x, out)
+    s = N.Gaussian1dSettings()
+    N.lib().lucem_gaussian_1d_settings_default(C.byref(s))
+    s.axis, s.order, s.mode = int(axis), int(order), PadMode.parse(mode)
+    s.cval, s.truncate = float(cval), float(truncate)
+    s.radius = -1 if radius is None else int(radius)
+    ti, to = _tensor(x, "input"), _tensor(out, "output")
+    N.check(N.lib().lucem_gaussian_1d(ctx.handle, C.byref(ti), float(sigma), C.byref(s), C.byref(to), _stream(x)))
+    return out
+
+
+def correlate_1d(x: torch.Tensor, weights, *, axis=-1, mode="reflect", cval=0.0, origin=0,
+                 out: Optional[torch.Tensor] = None) -> torch.Tensor:
+    """correlate_1d (crates/lucem-ops/src/filter/convolve.rs:40-92)."""
+    ctx, _ = _ctx_ws(x, None)
+    out = _out_like(x, out)
+    w = np.ascontiguousarray(np.asarray(weights, dtype=np.float64).reshape(-1))
+    s = N.Correlate1dSettings(int(axis), PadMode.parse(mode), float(cval), int(origin))
+    ti, to = _tensor(x, "input"), _tensor(out, "output")
+    wp = w.ctypes.data_as(C.POINTER(C.c_double)) if w.size else None
+    N.check(N.lib().lucem_correlate_1d(ctx.handle, C.byref(ti), wp, int(w.size), C.byref(s), C.byref(to),
+                                       _stream(x)))
+    return out
+
+
+def convolve_1d(x: torch.Tensor, weights, *, axis=-1, mode="reflect", cval=0.0, origin=0,
+                out: Optional[torch.Tensor] = None) -> torch.Tensor:
+    """convolve_1d (crates/lucem-ops/src/filter/convolve.rs:95-109): correlation
+    with reversed weights and the mirrored origin."""
+    w = np.asarray(weights, dtype=np.float64).reshape(-1)
+    size = w.size
+    if size == 0:
+        raise LucemError(6, "weights: filter weights cannot be empty")
+    lo, hi = -(size // 2), (size - 1) // 2
+    if not lo <= origin <= hi:
+        raise LucemError(5, f"origin {origin} is out of bounds for window of size {size} (must be in {lo}..={hi})")
+    mirrored = -int(origin) - (1 if size % 2 == 0 else 0)
+    return correlate_1d(x, w[::-1].copy(), axis=axis, mode=mode, cval=cval, origin=mirrored, out=out)
+
+
+def difference_of_gaussians(x: torch.Tensor, low_sigmas, high_sigmas, *, mode="reflect", cval=0.0, truncate=4.0,
+                            axes=None, channel_axis=None, input_scale=1.0, out: Optional[torch.Tensor] = None,
+                            workspace: Optional[Workspace] = None) -> torch.Tensor:
+    """difference_of_gaussians (crates/lucem-ops/src/filter/gaussian.rs:374-404)."""
+    ctx, ws = _ctx_ws(x, workspace)
+    out = _out_like(x, out)
+    keep = []
+    s = _gaussian_settings(None, mode, cval, truncate, None, axes, channel_axis, input_scale, keep)
+    lo, nlo = _doubles(low_sigmas)
+    hi, nhi = _doubles(high_sigmas)
+    ti, to = _tensor(x, "input"), _tensor(out, "output")
+    N.check(N.lib().lucem_difference_of_gaussians(ctx.handle, C.byref(ti), lo, nlo, hi, nhi, C.byref(s),
+                                                  C.byref(to), ws.handle, _stream(x)))
+    return out
+
+
+def gaussian_laplace(x: torch.Tensor, sigmas, *, mode="reflect", cval=0.0, truncate=4.0,
+                     out: Optional[torch.Tensor] = None, workspace: Optional[Workspace] = None) -> torch.Tensor:
+    """gaussian_laplace (crates/lucem-ops/src/filter/gaussian.rs:255-303)."""
+    ctx, ws = _ctx_ws(x, workspace)
+    out = _out_like(x, out)
+    sig, ns = _doubles(sigmas)
+    ti, to = _tensor(x, "input"), _tensor(out, "output")
+    N.check(N.lib().lucem_gaussian_laplace(ctx.handle, C.byref(ti), sig, ns, PadMode.parse(mode), float(cval),
+                                           float(truncate), C.byref(to), ws.handle, _stream(x)))
+    return out
+
+
+def gaussian_grad_mag(x: torch.Tensor, sigmas, *, mode="reflect", cval=0.0, truncate=4.0,
+                      out: Optional[torch.Tensor] = None, workspace: Optional[Workspace] = None) -> torch.Tensor:
+    """gaussian_grad_mag (crates/lucem-ops/src/filter/gaussian.rs:307-371)."""
+    ctx, ws = _ctx_ws(x, workspace)
+    out = _out_like(x, out)
+    sig, ns = _doubles(sigmas)
+    ti, to = _tensor(x, "input"), _tensor(out, "output")
+    N.check(N.lib().lucem_gaussian_grad_mag(ctx.handle, C.byref(ti), sig, ns, PadMode.parse(mode), float(cval),
+                                            float(truncate), C.byref(to), ws.handle, _stream(x)))
+    return out
+
+
+def unsharp_mask(x: torch.Tensor, sigmas, amount: float, *, mode="reflect", cval=0.0, truncate=4.0, axes=None,
+                 channel_axis=None, input_scale=1.0, out: Optional[torch.Tensor] = None,
+                 workspace: Optional[Workspace] = None) -> torch.Tensor:
+    """unsharp_mask (crates/lucem-ops/src/filter/gaussian.rs:407-435)."""
+    ctx, ws = _ctx_ws(x, workspace)
+    out = _out_like(x, out)
+    keep = []
+    s = _gaussian_settings(None, mode, cval, truncate, None, axes, channel_axis, input_scale, keep)
+    sig, ns = _doubles(sigmas)
+    ti, to = _tensor(x, "input"), _tensor(out, "output")
+    N.check(N.lib().lucem_unsharp_mask(ctx.handle, C.byref(ti), sig, ns, float(amount), C.byref(s), C.byref(to),
+                                       ws.handle, _stream(x)))
+    return out
+
+
+_KINDS = {"gaussian": N.RESP_GAUSSIAN, "dog": N.RESP_DOG, "laplace": N.RESP_LAPLACE,
+          "grad_mag": N.RESP_GRAD_MAG, "unsharp": N.RESP_UNSHARP}
+
+
+def _responses(specs, outs):
+    arr = (N.Response * max(1, len(specs)))()
+    for i, (spec, o) in enumerate(zip(specs, outs)):
+        kind = spec[0]
+        r = arr[i]
+        r.kind = _KINDS[kind]
+        r.sigma = float(spec[1])
+        if kind == "dog":
+            r.sigma2 = float(spec[2])
+        if kind == "unsharp":
+            r.amount = float(spec[2])
+        r.out = _tensor(o, "output")
+    return arr
+
+
+def gaussian_family(x: torch.Tensor, responses: Sequence[tuple], *, mode="reflect", cval=0.0, truncate=4.0,
+                    input_scale=1.0, outs: Optional[Sequence[torch.Tensor]] = None,
+                    workspace: Optional[Workspace] = None):
+    """Several Gaussian-family responses of one input over its last two axes in
+    one fused pass.  `responses`: ("gaussian", s), ("dog", s_low, s_high),
+    ("laplace", s), ("grad_mag", s), ("unsharp", s, amount).  Each equals the
+    reference function of that name on `x`."""
+    ctx, ws = _ctx_ws(x, workspace)
+    if outs is None:
+        outs = [torch.empty(x.shape, dtype=torch.float32, device=x.device) for _ in responses]
+    arr = _responses(responses, outs)
+    ti = _tensor(x, "input")
+    N.check(N.lib().lucem_gaussian_family(ctx.handle, C.byref(ti), arr, len(responses), PadMode.parse(mode),
+                                          float(cval), float(truncate), float(input_scale), ws.handle, _stream(x)))
+    return list(outs)
+
+
+# ---------------------------------------------------------------------------
+# tiling / batched tiles
+
+
+@dataclass(frozen=True)
+class Block:
+    """crates/lucem-core/src/tiling.rs:13-49 ([z, y, x])."""
+
+    index: int
+    origin: tuple
+    size: tuple
+    read_origin: tuple
+    read_size: tuple
+
+    def inner_offset(self):
+        return tuple(self.origin[a] - self.read_origin[a] for a in range(3))
+
+    def read_dims(self):
+        return [self.read_size[1], self.read_size[2]] if self.read_size[0] == 1 else list(self.read_size)
+
+
+def _blocks_c(blocks):
+    arr = (N.Block * max(1, len(blocks)))()
+    for i, b in enumerate(blocks):
+        arr[i].index = b.index
+        for a in range(3):
+            arr[i].origin[a] = b.origin[a]
+            arr[i].size[a] = b.size[a]
+            arr[i].read_origin[a] = b.read_origin[a]
+            arr[i].read_size[a] = b.read_size[a]
+    return arr
+
+
+def schedule(dims, block, halo):
+    """crates/lucem-core/src/tiling.rs:54-78."""
+    d = (C.c_int64 * 3)(*dims)
+    b = (C.c_int64 * 3)(*block)
+    h = (C.c_int64 * 3)(*halo)
+    n = C.c_int64()
+    N.check(N.lib().lucem_schedule(d, b, h, None, 0, C.byref(n)))
+    arr = (N.Block * max(1, n.value))()
+    N.check(N.lib().lucem_schedule(d, b, h, arr, n.value, C.byref(n)))
+    return [Block(int(a.index), tuple(a.origin), tuple(a.size), tuple(a.read_origin), tuple(a.read_size))
+            for a in arr[: n.value]]
+
+
+class TileWalk:
+    """A prepared batched walk: the block list marshalled once, so repeated calls
+    (and CUDA-graph capture of them) do no host work beyond the launch."""
+
+    def __init__(self, blocks):
+        self.blocks = list(blocks)
+        self._arr = _blocks_c(self.blocks)
+
+
+def gaussian_family_tiles(slide: torch.Tensor, blocks, responses: Sequence[tuple], *, mode="reflect", cval=0.0,
+                          truncate=4.0, input_scale=1.0, persistent=True,
+                          outs: Optional[Sequence[torch.Tensor]] = None, workspace: Optional[Workspace] = None):
+    """The tile walk of engine/lucem-pipeline/src/custom.rs:199-251 with a
+    Gaussian-family function per block, over every channel of a [C, H, W] (or
+    [H, W]) slide.  persistent=True: one persistent launch over the whole work
+    list; False: one launch per block and channel (the plain drop-in)."""
+    ctx, ws = _ctx_ws(slide, workspace)
+    if outs is None:
+        outs = [torch.empty(slide.shape, dtype=torch.float32, device=slide.device) for _ in responses]
+    walk = blocks if isinstance(blocks, TileWalk) else TileWalk(blocks)
+    arr = _responses(responses, outs)
+    ts = _tensor(slide, "slide")
+    N.check(N.lib().lucem_gaussian_family_tiles(ctx.handle, C.byref(ts), walk._arr, len(walk.blocks), arr,
+                                                len(responses), PadMode.parse(mode), float(cval), float(truncate),
+                                                float(input_scale), int(bool(persistent)), ws.handle,
+                                                _stream(slide)))
+    return list(outs)
+
+
+# ---------------------------------------------------------------------------
+# Richardson-Lucy
+
+
+def rl_grid(dims, kdims, mode="reflect", grid=None):
+    """The FFT grid richardson_lucy uses for these sizes."""
+    nd = len(dims)
+    d = (C.c_int64 * 3)(*dims)
+    k = (C.c_int64 * 3)(*kdims)
+    g = (C.c_int64 * 3)()
+    req = (C.c_int64 * 3)(*(list(grid) if grid is not None else [0] * nd))
+    N.check(N.lib().lucem_rl_grid(d, k, nd, PadMode.parse(mode), req, g))
+    return tuple(int(v) for v in g[:nd])
+
+
+def richardson_lucy(x: torch.Tensor, psf: torch.Tensor, *, num_iter: int = 30, clip: bool = True,
+                    filter_epsilon: Optional[float] = None, mode="reflect", grid=None,
+                    out: Optional[torch.Tensor] = None, workspace: Optional[Workspace] = None) -> torch.Tensor:
+    """richardson_lucy (crates/lucem-ops/src/restore/deconvolve.rs:45-162) for
+    2-D and 3-D inputs, on FFT convolution.  `grid` overrides the FFT lengths."""
+    ctx, ws = _ctx_ws(x, workspace)
+    out = _out_like(x, out)
+    s = N.RlSettings()
+    N.lib().lucem_rl_settings_default(C.byref(s))
+    s.num_iter = int(num_iter)
+    s.clip = int(bool(clip))
+    if filter_epsilon is not None:
+        s.has_filter_epsilon = 1
+        s.filter_epsilon = float(filter_epsilon)
+    s.mode = PadMode.parse(mode)
+    if grid is not None:
+        for i, g in enumerate(grid):
+            s.grid[i] = int(g)
+    ti, tp, to = _tensor(x, "input"), _tensor(psf, "psf"), _tensor(out, "output")
+    N.check(N.lib().lucem_richardson_lucy(ctx.handle, C.byref(ti), C.byref(tp), C.byref(s), C.byref(to),
+                                          ws.handle, _stream(x)))
+    return out

@@ -1,0 +1,333 @@
+"""Python face of the oracle: ctypes over oracle/_build/liblucem_oracle.so plus
+an FP64 FFT Richardson-Lucy in numpy.
+
+TEST INFRASTRUCTURE ONLY.  The parity tests, the smoke check and the
+benchmark's CPU-baseline leg use it as the checker; the product never imports
+it.  Parity status: pinned to the reference's own known-answer tests and to
+scipy.ndimage fixtures, not to bit-level CubeCL output (the reference cannot be
+built here); see lucem_oracle.h.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import sys
+
+import numpy as np
+import scipy.fft as sfft
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+if _HERE not in sys.path:
+    sys.path.insert(0, _HERE)
+import build as _build  # noqa: E402
+
+_lib = None
+
+PAD_MODES = {"reflect": 0, "constant": 1, "nearest": 2, "mirror": 3, "wrap": 4}
+
+
+def parse_mode(mode) -> int:
+    """crates/lucem-ops/src/core/pad.rs:47-56 (aliases included)."""
+    if isinstance(mode, int):
+        return mode
+    m = mode.strip().lower()
+    aliases = {"symmetric": "reflect", "grid-mirror": "reflect", "grid-constant": "constant",
+               "zeros": "constant", "edge": "nearest", "replicate": "nearest",
+               "grid-wrap": "wrap", "periodic": "wrap"}
+    m = aliases.get(m, m)
+    if m not in PAD_MODES:
+        raise ValueError(f"boundary pad mode '{mode}' is not supported")
+    return PAD_MODES[m]
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = _build.build()
+        L = C.CDLL(path)
+        P = C.c_void_p
+        i64p = C.POINTER(C.c_int64)
+        L.orc_gaussian_kernel_1d.argtypes = [C.c_double, C.c_uint32, C.c_int64, P]
+        L.orc_resolved_radius.argtypes = [C.c_double, C.c_double]
+        L.orc_resolved_radius.restype = C.c_int64
+        L.orc_pad_index.argtypes = [C.c_int64, C.c_int64, C.c_int]
+        L.orc_pad_index.restype = C.c_int64
+        for s, real in (("f32", C.c_float), ("f64", C.c_double)):
+            getattr(L, f"orc_correlate_1d_{s}").argtypes = [P, P, i64p, C.c_int, C.c_int, P, C.c_int64,
+                                                             C.c_int32, C.c_int, real]
+            getattr(L, f"orc_gaussian_blur_{s}").argtypes = [P, P, i64p, C.c_int, P, C.c_int, P, P, P,
+                                                              C.c_int, C.c_double, C.c_double]
+            getattr(L, f"orc_correlate_nd_{s}").argtypes = [P, P, i64p, C.c_int, P, i64p, C.c_int, real]
+            getattr(L, f"orc_richardson_lucy_{s}").argtypes = [P, P, P, i64p, i64p, C.c_int, C.c_int,
+                                                                C.c_int, C.c_double, C.c_int]
+        L.orc_linear_comb_f32.argtypes = [P, P, P, C.c_int64, C.c_float, C.c_float, C.c_float]
+        L.orc_gaussian_laplace_f32.argtypes = [P, P, i64p, C.c_int, P, C.c_int, C.c_double, C.c_double]
+        L.orc_gaussian_grad_mag_f32.argtypes = [P, P, i64p, C.c_int, P, C.c_int, C.c_double, C.c_double]
+        L.orc_difference_of_gaussians_f32.argtypes = [P, P, i64p, C.c_int, P, P, C.c_int, C.c_double,
+                                                      C.c_double]
+        L.orc_unsharp_mask_f32.argtypes = [P, P, i64p, C.c_int, P, C.c_double, C.c_int, C.c_double,
+                                           C.c_double]
+        L.orc_set_threads.argtypes = [C.c_int]
+        L.orc_get_threads.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _dims(shape):
+    return (C.c_int64 * max(1, len(shape)))(*shape)
+
+
+def _sfx(dtype):
+    if dtype == np.float32:
+        return "f32"
+    if dtype == np.float64:
+        return "f64"
+    raise TypeError(f"oracle supports float32/float64, got {dtype}")
+
+
+def set_threads(n: int):
+    lib().orc_set_threads(int(n))
+
+
+def get_threads() -> int:
+    return lib().orc_get_threads()
+
+
+def gaussian_kernel_1d(sigma: float, order: int, radius: int) -> np.ndarray:
+    out = np.empty(2 * radius + 1, np.float64)
+    lib().orc_gaussian_kernel_1d(float(sigma), int(order), int(radius), _ptr(out))
+    return out
+
+
+def resolved_radius(truncate: float, sigma: float) -> int:
+    return int(lib().orc_resolved_radius(float(truncate), float(sigma)))
+
+
+def pad_index(p: int, n: int, mode) -> int:
+    return int(lib().orc_pad_index(int(p), int(n), parse_mode(mode)))
+
+
+def _norm_axis(axis: int, ndim: int) -> int:
+    a = axis + ndim if axis < 0 else axis
+    if not 0 <= a < ndim:
+        raise ValueError(f"axis {axis} is out of bounds for array of dimension {ndim}")
+    return a
+
+
+def correlate_1d(x: np.ndarray, w, axis=-1, mode="reflect", cval=0.0, origin=0) -> np.ndarray:
+    """crates/lucem-ops/src/filter/convolve.rs:40-92 (weights cast to x's type)."""
+    x = np.ascontiguousarray(x)
+    s = _sfx(x.dtype)
+    w = np.ascontiguousarray(np.asarray(w, dtype=np.float64).astype(x.dtype))
+    out = np.empty_like(x)
+    if x.size == 0:
+        return out
+    ax = _norm_axis(axis, x.ndim)
+    getattr(lib(), f"orc_correlate_1d_{s}")(_ptr(x), _ptr(out), _dims(x.shape), x.ndim, ax, _ptr(w),
+                                             len(w), int(origin), parse_mode(mode), float(cval))
+    return out
+
+
+def broadcast_per_axis(name, values, n):
+    """crates/lucem-ops/src/core/check.rs:95-109."""
+    values = list(values)
+    if n == 0:
+        return []
+    if len(values) == 1:
+        return values * n
+    if len(values) == n:
+        return values
+    raise ValueError(f"invalid parameter `{name}`: expected 1 or {n} values, got {len(values)}")
+
+
+def blur_axes(ndim, axes=None, channel_axis=None):
+    """crates/lucem-ops/src/filter/gaussian.rs:184-188 (numpy axis rules)."""
+    if axes is None:
+        out = list(range(ndim))
+    else:
+        out = []
+        for a in axes:
+            n = _norm_axis(a, ndim)
+            if n in out:
+                raise ValueError(f"repeated axis {a}")
+            out.append(n)
+    if channel_axis is not None:
+        ch = _norm_axis(channel_axis, ndim)
+        out = [a for a in out if a != ch]
+    return out
+
+
+def gaussian_blur(x, sigmas, orders=(0,), mode="reflect", cval=0.0, truncate=4.0, radii=None,
+                  axes=None, channel_axis=None) -> np.ndarray:
+    """crates/lucem-ops/src/filter/gaussian.rs:176-250."""
+    x = np.ascontiguousarray(x)
+    s = _sfx(x.dtype)
+    if np.isscalar(sigmas):
+        sigmas = [sigmas]
+    ax = blur_axes(x.ndim, axes, channel_axis)
+    sig = broadcast_per_axis("sigmas", sigmas, len(ax))
+    for v in sig:
+        if not np.isfinite(v) or v < 0:
+            raise ValueError(f"sigma must be non-negative and finite, got {v}")
+    ords = broadcast_per_axis("orders", orders, len(ax))
+    rad = broadcast_per_axis("radii", radii, len(ax)) if radii is not None else [-1] * len(ax)
+    out = np.empty_like(x)
+    if x.size == 0:
+        return out
+    n = max(1, len(ax))
+    axes_c = (C.c_int * n)(*ax)
+    sig_c = (C.c_double * n)(*sig)
+    ord_c = (C.c_uint32 * n)(*ords)
+    rad_c = (C.c_int64 * n)(*rad)
+    getattr(lib(), f"orc_gaussian_blur_{s}")(_ptr(x), _ptr(out), _dims(x.shape), x.ndim, axes_c, len(ax),
+                                              sig_c, ord_c, rad_c, parse_mode(mode), float(cval),
+                                              float(truncate))
+    return out
+
+
+def _sig_all(sigmas, ndim):
+    if np.isscalar(sigmas):
+        sigmas = [sigmas]
+    return (C.c_double * max(1, ndim))(*broadcast_per_axis("sigmas", sigmas, ndim))
+
+
+def gaussian_laplace(x, sigmas, mode="reflect", cval=0.0, truncate=4.0):
+    x = np.ascontiguousarray(x, np.float32)
+    out = np.empty_like(x)
+    lib().orc_gaussian_laplace_f32(_ptr(x), _ptr(out), _dims(x.shape), x.ndim, _sig_all(sigmas, x.ndim),
+                                   parse_mode(mode), float(cval), float(truncate))
+    return out
+
+
+def gaussian_grad_mag(x, sigmas, mode="reflect", cval=0.0, truncate=4.0):
+    x = np.ascontiguousarray(x, np.float32)
+    out = np.empty_like(x)
+    lib().orc_gaussian_grad_mag_f32(_ptr(x), _ptr(out), _dims(x.shape), x.ndim, _sig_all(sigmas, x.ndim),
+                                    parse_mode(mode), float(cval), float(truncate))
+    return out
+
+
+def difference_of_gaussians(x, low, high, mode="reflect", cval=0.0, truncate=4.0):
+    x = np.ascontiguousarray(x, np.float32)
+    out = np.empty_like(x)
+    lib().orc_difference_of_gaussians_f32(_ptr(x), _ptr(out), _dims(x.shape), x.ndim,
+                                          _sig_all(low, x.ndim), _sig_all(high, x.ndim),
+                                          parse_mode(mode), float(cval), float(truncate))
+    return out
+
+
+def unsharp_mask(x, sigmas, amount, mode="reflect", cval=0.0, truncate=4.0):
+    x = np.ascontiguousarray(x, np.float32)
+    out = np.empty_like(x)
+    lib().orc_unsharp_mask_f32(_ptr(x), _ptr(out), _dims(x.shape), x.ndim, _sig_all(sigmas, x.ndim),
+                               float(amount), parse_mode(mode), float(cval), float(truncate))
+    return out
+
+
+def correlate_nd(x, w, mode="reflect", cval=0.0):
+    x = np.ascontiguousarray(x)
+    s = _sfx(x.dtype)
+    w = np.ascontiguousarray(np.asarray(w).astype(x.dtype))
+    assert w.ndim == x.ndim and 1 <= x.ndim <= 3
+    out = np.empty_like(x)
+    getattr(lib(), f"orc_correlate_nd_{s}")(_ptr(x), _ptr(out), _dims(x.shape), x.ndim, _ptr(w),
+                                             _dims(w.shape), parse_mode(mode), float(cval))
+    return out
+
+
+def rl_epsilon(filter_epsilon=None) -> float:
+    """crates/lucem-ops/src/restore/deconvolve.rs:104."""
+    return max(1e-12 if filter_epsilon is None else float(filter_epsilon), 1e-15)
+
+
+def richardson_lucy(obs, psf, num_iter=30, clip=True, filter_epsilon=None, mode="reflect"):
+    """crates/lucem-ops/src/restore/deconvolve.rs:45-162 in the obs dtype, any
+    ndim 1..3 (direct spatial correlation, as the reference computes it)."""
+    obs = np.ascontiguousarray(obs)
+    s = _sfx(obs.dtype)
+    psf = np.ascontiguousarray(np.asarray(psf).astype(obs.dtype))
+    assert psf.ndim == obs.ndim
+    if psf.size == 0:
+        raise ValueError("psf: PSF cannot be empty")
+    if num_iter < 1:
+        raise ValueError("invalid parameter `num_iter`: num_iter must be >= 1")
+    out = np.empty_like(obs)
+    if obs.size == 0:
+        return out
+    rc = getattr(lib(), f"orc_richardson_lucy_{s}")(_ptr(obs), _ptr(psf), _ptr(out), _dims(obs.shape),
+                                                     _dims(psf.shape), obs.ndim, int(num_iter), int(bool(clip)),
+                                                     rl_epsilon(filter_epsilon), parse_mode(mode))
+    assert rc == 0
+    return out
+
+
+def centred_otf(psf_norm: np.ndarray, grid, centre) -> np.ndarray:
+    """Zero-padded PSF with tap `centre` wrapped to the origin (the convention of
+    crates/lucem-ops/src/restore/kernels/deconvolve.rs:79-99), real FFT over `grid`."""
+    buf = np.zeros(grid, np.float64)
+    idx = np.indices(psf_norm.shape).reshape(psf_norm.ndim, -1)
+    dst = tuple((idx[d] - centre[d]) % grid[d] for d in range(psf_norm.ndim))
+    np.add.at(buf, dst, psf_norm.reshape(-1).astype(np.float64))
+    return sfft.rfftn(buf, axes=tuple(range(psf_norm.ndim)), workers=-1)
+
+
+def richardson_lucy_fft64(obs, psf, num_iter=30, clip=False, filter_epsilon=None, grid=None):
+    """FP64 Richardson-Lucy with zero padding (PadMode::Constant, cval 0) computed
+    through FFTs on `grid` (>= dims + k - 1 per axis).  Mathematically equal to
+    the reference's direct Constant-mode iteration (deconvolve.rs:109-147)."""
+    obs = np.asarray(obs, np.float64)
+    psf = np.asarray(psf, np.float64)
+    nd = obs.ndim
+    if grid is None:
+        grid = tuple(obs.shape[d] + psf.shape[d] - 1 for d in range(nd))
+    ssum = psf.sum()
+    norm = 1.0 / ssum if abs(ssum) > 1e-12 else 1.0
+    p = psf * norm
+    k = psf.shape
+    # correlate(src, flipped psf) == convolution with p centred at k-1-k//2;
+    # correlate(src, p) == correlation with p centred at k//2 (convolve.rs:144-145).
+    h_conv = centred_otf(p, grid, [k[d] - 1 - k[d] // 2 for d in range(nd)])
+    h_corr = np.conj(centred_otf(p, grid, [k[d] // 2 for d in range(nd)]))
+    eps = rl_epsilon(filter_epsilon)
+    sl = tuple(slice(0, n) for n in obs.shape)
+    est = np.full(obs.shape, 0.5)
+    for it in range(num_iter):
+        ax = tuple(range(nd))
+        conv = sfft.irfftn(sfft.rfftn(est, grid, axes=ax, workers=-1) * h_conv, grid, axes=ax, workers=-1)[sl]
+        safe = np.where(np.abs(conv) < eps, eps, conv)
+        ratio = obs / safe
+        corr = sfft.irfftn(sfft.rfftn(ratio, grid, axes=ax, workers=-1) * h_corr, grid, axes=ax,
+                           workers=-1)[sl]
+        est = est * corr
+        if clip and it + 1 == num_iter:
+            est = np.clip(est, -1.0, 1.0)
+    return est
+
+
+def assert_close(got, want, rtol, context=""):
+    """crates/lucem-core/src/test_support.rs:42-50: |g - w| <= rtol*|w| + rtol*max|w|."""
+    got = np.asarray(got, np.float64).reshape(-1)
+    want = np.asarray(want, np.float64).reshape(-1)
+    assert got.shape == want.shape, f"{context}: {got.size} values, expected {want.size}"
+    scale = np.max(np.abs(want)) if want.size else 0.0
+    bad = np.abs(got - want) > rtol * np.abs(want) + rtol * scale
+    if bad.any():
+        i = int(np.argmax(bad))
+        raise AssertionError(f"{context}: index {i}: got {got[i]}, expected {want[i]} (rtol {rtol}); "
+                             f"{int(bad.sum())} of {bad.size} outside")
+
+
+def max_rel_err(got, want) -> float:
+    """The smallest rtol for which assert_close passes."""
+    got = np.asarray(got, np.float64).reshape(-1)
+    want = np.asarray(want, np.float64).reshape(-1)
+    if want.size == 0:
+        return 0.0
+    scale = np.max(np.abs(want))
+    den = np.abs(want) + scale
+    den = np.where(den == 0, 1.0, den)
+    return float(np.max(np.abs(got - want) / den))

@@ -1,0 +1,177 @@
+"""The oracle (oracle/, a CPU restatement of the reference path) pinned against
+the reference's own known-answer tests and against scipy fixtures.  CPU only."""
+import os
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def sample_f64(n):
+    """crates/lucem-ops/src/test_support.rs:10-12."""
+    i = np.arange(n, dtype=np.int64)
+    return ((i * 7919 + 104729) % 1013).astype(np.float64) * 0.1 - 50.0
+
+
+def host_pad_index(p, n, mode):
+    """crates/lucem-ops/src/test_support.rs:21-46 (the reference's own f64 model)."""
+    if 0 <= p < n:
+        return p
+    if mode == "constant":
+        return None
+    if mode == "nearest":
+        return min(max(p, 0), n - 1)
+    if mode == "wrap":
+        return p % n
+    if mode == "reflect":
+        period = 2 * n
+        r = p % period
+        return r if r < n else period - 1 - r
+    if n <= 1:
+        return 0
+    period = 2 * n - 2
+    r = p % period
+    return r if r < n else period - r
+
+
+def host_correlate_1d(x, dims, w, axis, mode, cval, origin):
+    """crates/lucem-ops/src/filter/convolve.rs:185-209."""
+    outer = int(np.prod(dims[:axis], dtype=np.int64))
+    length = dims[axis]
+    inner = int(np.prod(dims[axis + 1:], dtype=np.int64))
+    left = len(w) // 2 + origin
+    out = np.zeros(len(x))
+    for idx in range(len(x)):
+        i = (idx // inner) % length
+        base = idx - i * inner
+        start = i - left
+        s = 0.0
+        for t, wt in enumerate(w):
+            q = host_pad_index(start + t, length, mode)
+            s += wt * (cval if q is None else x[base + q * inner])
+        out[idx] = s
+    return out
+
+
+MODES = ["reflect", "constant", "nearest", "mirror", "wrap"]
+
+
+def test_gaussian_kernel_sums(oracle):
+    """crates/lucem-ops/src/filter/gaussian.rs:442-446."""
+    k0 = oracle.gaussian_kernel_1d(2.0, 0, 8)
+    assert abs(k0.sum() - 1.0) < 1e-12
+    k1 = oracle.gaussian_kernel_1d(2.0, 1, 8)
+    assert abs(k1.sum()) < 1e-12
+    assert oracle.resolved_radius(4.0, 2.0) == 8
+    assert len(oracle.gaussian_kernel_1d(2.0, 0, 8)) == 17
+
+
+def test_constant_image_stays_constant(oracle):
+    """crates/lucem-ops/src/filter/gaussian.rs:448-457."""
+    x = sample_f64(17 * 21).reshape(17, 21).astype(np.float32)
+    assert oracle.gaussian_blur(x, [1.5]).shape == (17, 21)
+    ones = np.full((17, 21), 7.25, np.float32)
+    oracle.assert_close(oracle.gaussian_blur(ones, [2.0]), np.full(ones.shape, 7.25), 1e-5, "constant")
+
+
+@pytest.mark.parametrize("dims", [[1], [7], [32, 33], [5, 1, 9]])
+def test_correlate_1d_matches_reference_host_model(oracle, dims):
+    """crates/lucem-ops/src/filter/convolve.rs:211-228 restated."""
+    x = sample_f64(int(np.prod(dims)))
+    xf = x.astype(np.float32).reshape(dims)
+    for axis in range(len(dims)):
+        for w, origin in (([1.0, -2.0, 3.0], 0), ([0.5] * 4, -1)):
+            for mode in MODES:
+                got = oracle.correlate_1d(xf, w, axis=axis, mode=mode, cval=1.5, origin=origin)
+                want = host_correlate_1d(x, dims, w, axis, mode, 1.5, origin)
+                oracle.assert_close(got, want, 1e-5, f"{dims} axis {axis} {mode}")
+
+
+def test_pad_index_matches_reference_model(oracle):
+    for n in (1, 2, 5, 8):
+        for p in range(-23, 30):
+            for m in MODES:
+                q = host_pad_index(p, n, m)
+                assert oracle.pad_index(p, n, m) == (-1 if q is None else q), (p, n, m)
+
+
+def test_scipy_fixtures_pin_the_restatement(oracle):
+    g = np.load(os.path.join(HERE, "golden", "scipy_filters.npz"))
+    x2, x3 = g["x2"], g["x3"]
+    for key in g["cases"]:
+        key = str(key)
+        if key.startswith("g2_"):
+            _, mode, sigma, order = key.split("_")
+            got = oracle.gaussian_blur(x2, [float(sigma)], orders=[int(order[0]), int(order[1])], mode=mode, cval=1.5)
+        else:
+            got = oracle.gaussian_blur(x3, [1.0, 2.0, 1.5], mode=key.split("_")[1], cval=1.5)
+        assert np.abs(got - g[key]).max() <= 1e-10 * max(1.0, np.abs(g[key]).max()), key
+    # The f32 restatement stays within the reference's 1e-5 of FP64.
+    got32 = oracle.gaussian_blur(x2.astype(np.float32), [2.0], orders=[0, 2], mode="reflect", cval=1.5)
+    oracle.assert_close(got32, g["g2_reflect_2.0_02"], 1e-5, "f32")
+
+
+def test_composites_against_scipy(oracle):
+    g = np.load(os.path.join(HERE, "golden", "scipy_filters.npz"))
+    x2 = g["x2"].astype(np.float32)
+    oracle.assert_close(oracle.gaussian_laplace(x2, [2.0]), g["laplace_reflect_2.0"], 1e-5, "LoG")
+    oracle.assert_close(oracle.gaussian_grad_mag(x2, [1.5]), g["gradmag_reflect_1.5"], 1e-5, "|grad|")
+    dog = oracle.difference_of_gaussians(x2, [1.0], [3.0])
+    want = oracle.gaussian_blur(g["x2"], [1.0]) - oracle.gaussian_blur(g["x2"], [3.0])
+    oracle.assert_close(dog, want, 1e-5, "DoG")
+    um = oracle.unsharp_mask(x2, [2.0], 0.7)
+    oracle.assert_close(um, 1.7 * g["x2"] - 0.7 * oracle.gaussian_blur(g["x2"], [2.0]), 1e-5, "unsharp")
+
+
+def test_rl_delta_psf_recovers_image(oracle):
+    """crates/lucem-ops/src/restore/deconvolve.rs:517-539."""
+    img = (np.arange(64, dtype=np.float32) / 64.0 * 0.8 + 0.1).reshape(8, 8)
+    psf = np.zeros((3, 3), np.float32)
+    psf[1, 1] = 1.0
+    out = oracle.richardson_lucy(img, psf, num_iter=15, clip=False)
+    oracle.assert_close(out, img.astype(np.float64), 1e-4, "delta psf")
+
+
+def test_rl_box_psf_sharpens(oracle):
+    """crates/lucem-ops/src/restore/deconvolve.rs:551-566."""
+    spot = np.full((8, 8), 0.1, np.float32)
+    spot[4, 4] = 0.9
+    box = np.full((3, 3), 1.0 / 9.0, np.float32)
+    blurred = oracle.correlate_nd(spot, box, mode="reflect")
+    restored = oracle.richardson_lucy(blurred, box, num_iter=25, clip=True)
+    assert restored[4, 4] > blurred[4, 4] + 0.15
+
+
+def test_rl_direct_equals_fft_formulation(oracle):
+    """Zero-padded RL computed directly (as the reference) equals the FFT form,
+    odd and even PSF sizes, 2-D and 3-D (FP64)."""
+    rng = np.random.default_rng(5)
+    for shape, kshape in (((21, 17), (5, 4)), ((20, 19), (7, 7)), ((6, 9, 11), (3, 4, 5))):
+        obs = rng.uniform(0.1, 1.0, shape)
+        psf = rng.uniform(0.0, 1.0, kshape)
+        a = oracle.richardson_lucy(obs, psf, num_iter=6, clip=False, filter_epsilon=1e-6, mode="constant")
+        b = oracle.richardson_lucy_fft64(obs, psf, num_iter=6, filter_epsilon=1e-6)
+        assert np.abs(a - b).max() < 1e-12 * np.abs(a).max(), shape
+
+
+def test_tiled_equals_whole(oracle):
+    """engine/lucem-pipeline/src/custom.rs:478-495: blocks of 128 with a halo of
+    16, each blurred on its read part and cropped, equal the whole image."""
+    x = sample_f64(300 * 310).reshape(300, 310).astype(np.float32)
+    whole = oracle.gaussian_blur(x, [2.0, 2.0])
+    got = np.zeros_like(whole)
+    for y in range(0, 300, 128):
+        for xx in range(0, 310, 128):
+            sy, sx = min(128, 300 - y), min(128, 310 - xx)
+            ry0, rx0 = max(0, y - 16), max(0, xx - 16)
+            ry1, rx1 = min(300, y + sy + 16), min(310, xx + sx + 16)
+            part = oracle.gaussian_blur(np.ascontiguousarray(x[ry0:ry1, rx0:rx1]), [2.0, 2.0])
+            got[y:y + sy, xx:xx + sx] = part[y - ry0:y - ry0 + sy, xx - rx0:xx - rx0 + sx]
+    assert np.abs(got - whole).max() < 1e-3
+
+
+def test_halo_of_sigma_two_is_eight(oracle):
+    """bindings/python/tests/test_runtime_io.py:28."""
+    assert oracle.resolved_radius(4.0, 2.0) == 8
+    assert int(np.ceil(4 * 2.0)) == 8
