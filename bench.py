@@ -322,7 +322,10 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--iters", type=int, default=ITERS, help="Richardson-Lucy iterations per step (metric: 50)")
     args = ap.parse_args()
+    global ITERS
+    ITERS = args.iters
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

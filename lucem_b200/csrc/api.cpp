@@ -1503,21 +1503,6 @@ lucem_status twiddles(lucem_ctx *ctx, int64_t n, const float2_ **f32, const doub
     return ok();
 }
 
-// Device table position -> frequency of the in-place forward transform of
-// length n (the order the transfer function is stored in).
-lucem_status rev_table(lucem_ctx *ctx, int64_t n, const int32_t **out) {
-    FftPlan plan;
-    if (!fft_make_plan(n, &plan))
-        return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `grid`: length %lld has no plan", (long long)n);
-    std::vector<int32_t> t((size_t)n);
-    fft_rev_table(plan, t.data());
-    int err = 0;
-    void *d = ctx->get_or_upload("rev-" + std::to_string(n), t.data(), t.size() * sizeof(int32_t), &err);
-    if (!d) return cuda_fail(err, "permutation upload");
-    *out = static_cast<const int32_t *>(d);
-    return ok();
-}
-
 }  // namespace
 
 extern "C" {
@@ -1626,8 +1611,6 @@ lucem_status lucem_richardson_lucy(lucem_ctx *ctx, const lucem_tensor *in, const
     if (same_centre) h_corr = h_conv;
     bool fresh = sl_conv->key != key || (!same_centre && sl_corr->key != key);
     if (fresh) {
-        const int32_t *rev_y = nullptr, *rev_z = nullptr;
-        if ((st = rev_table(ctx, grid[1], &rev_y)) || (st = rev_table(ctx, grid[0], &rev_z))) return st;
         void *psf64 = nullptr, *wa = nullptr, *wb = nullptr;
         if ((st = ws->get("rl_psf64", (size_t)kn * sizeof(double), &psf64))) return st;
         if ((st = ws->get("rl_otf_a", (size_t)kd[0] * kd[1] * g.Hp * 16, &wa))) return st;
@@ -1636,14 +1619,12 @@ lucem_status lucem_richardson_lucy(lucem_ctx *ctx, const lucem_tensor *in, const
                  "psf upload");
         if (ws->t()) ws->t()->begin(kPassRlOtf, stream);
         int e = rl_launch_otf(g, static_cast<const double *>(psf64), kdi, c_conv, static_cast<double *>(wa),
-                              static_cast<double *>(wb), h_conv, tw64[2], tw64[1], tw64[0], rev_y, rev_z,
-                              stream);
+                              static_cast<double *>(wb), h_conv, tw64[2], tw64[1], tw64[0], stream);
         if (ws->t()) ws->t()->end(kPassRlOtf, stream);
         if (e) return cuda_fail(e, "transfer function launch");
         if (!same_centre) {
             e = rl_launch_otf(g, static_cast<const double *>(psf64), kdi, c_corr, static_cast<double *>(wa),
-                              static_cast<double *>(wb), h_corr, tw64[2], tw64[1], tw64[0], rev_y,
-                              rev_z, stream);
+                              static_cast<double *>(wb), h_corr, tw64[2], tw64[1], tw64[0], stream);
             if (e) return cuda_fail(e, "transfer function launch");
         }
         // The host PSF copy must outlive the upload.

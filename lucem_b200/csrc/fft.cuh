@@ -1,30 +1,15 @@
-// fft.cuh -- in-place shared-memory FFT used by the Richardson-Lucy passes.
+// fft.cuh -- shared-memory self-sorting (Stockham) FFT for any length whose
+// factors are 2, 3, 5 and 7: the generic path of the Richardson-Lucy passes
+// (power-of-two lengths take the register-resident transform in
+// fft_fast.cuh).
 //
 // A CTA transforms C independent sequences ("columns") of length n that sit
 // in shared memory as buf[row * CP + c] (CP = C + 1: both the column-major
 // butterfly accesses and the row-major transposing loads are free of bank
-// conflicts).  Lanes run along c, so a warp touches consecutive words.
-//
-// Column transforms (forward / inverse along y and z) are in place:
-// decimation in frequency (Gentleman-Sande) forward leaves the spectrum in
-// mixed-radix digit-reversed order, decimation in time inverse takes that
-// order back to natural order.  Nothing is ever permuted: the pointwise
-// product between the two (the transfer function) is stored in the same
-// digit-reversed order.  Row transforms (x, whose half spectrum is loaded and
-// stored along k) use the two-buffer self-sorting (Stockham) form at the end
-// of this file, natural order in and out.  Each thread holds one radix-R
-// butterfly at a time, so register use stays at a few dozen values per thread
-// whatever the length.
-//
-// Forward stage (block length L, radix R, stride s = L / R), butterfly
-// (block b, offset j < s):
-//   y = DFT_R(x[bL + j + r s]);  x[bL + j + k s] = y[k] * W_L^{j k}
-// Inverse stage (s = product of the later radices, L = s R):
-//   x'[r] = x[bL + j + r s] * W_L^{-j r};  x[bL + j + k s] = IDFT_R(x')[k]
-// Position p of the forward output holds frequency rev(p): with stage radices
-// R1..Rs, p = sum_i d_i n/(R1..Ri) and rev(p) = d_1 + R1 (d_2 + R2 (d_3 ...)).
-// Twiddles W_n^m = e^{-2 pi i m / n} come from a table computed in double
-// precision on the host and rounded once to float (no device sin/cos).
+// conflicts).  Lanes run along c.  Each stage reads one buffer and writes the
+// other; each thread holds one radix-R butterfly at a time.  Twiddles
+// W_n^m = e^{-2 pi i m / n} come from a table computed in double precision on
+// the host and rounded once to float (no device sin/cos).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -163,91 +148,6 @@ struct DftOdd {
 template <> struct Dft<3> : DftOdd<3> {};
 template <> struct Dft<5> : DftOdd<5> {};
 template <> struct Dft<7> : DftOdd<7> {};
-
-// Forward (DIF) stage with block length L.
-template <int R>
-__device__ __forceinline__ void dif_stage(float2 *buf, int n, int C, int CP, int L, const Tw &tw) {
-    const int s = L / R;
-    const int nb = (n / R) * C;
-    const int tws = n / L;
-    for (int item = threadIdx.x; item < nb; item += blockDim.x) {
-        const int c = item % C, q = item / C;
-        const int b = q / s, j = q - b * s;
-        float2 *p = buf + (b * L + j) * CP + c;
-        float2 v[R];
-#pragma unroll
-        for (int r = 0; r < R; ++r) v[r] = p[r * s * CP];
-        Dft<R>::run(v, false);
-        p[0] = v[0];
-#pragma unroll
-        for (int k = 1; k < R; ++k) p[k * s * CP] = j ? cmul(v[k], tw.get(j * k * tws, false)) : v[k];
-    }
-    __syncthreads();
-}
-
-// Inverse (DIT) stage with sub-block length s (block length s * R).
-template <int R>
-__device__ __forceinline__ void dit_stage(float2 *buf, int n, int C, int CP, int s, const Tw &tw) {
-    const int L = s * R;
-    const int nb = (n / R) * C;
-    const int tws = n / L;
-    for (int item = threadIdx.x; item < nb; item += blockDim.x) {
-        const int c = item % C, q = item / C;
-        const int b = q / s, j = q - b * s;
-        float2 *p = buf + (b * L + j) * CP + c;
-        float2 v[R];
-        v[0] = p[0];
-#pragma unroll
-        for (int r = 1; r < R; ++r) {
-            float2 x = p[r * s * CP];
-            v[r] = j ? cmul(x, tw.get(j * r * tws, true)) : x;
-        }
-        Dft<R>::run(v, true);
-#pragma unroll
-        for (int k = 0; k < R; ++k) p[k * s * CP] = v[k];
-    }
-    __syncthreads();
-}
-
-// Forward transform: natural order in, digit-reversed out.  The caller
-// synchronises after filling buf.
-__device__ __forceinline__ void forward(float2 *buf, int n, int C, int CP, const int *radix, int nstages,
-                                        const Tw &tw) {
-    int L = n;
-    for (int i = 0; i < nstages; ++i) {
-        const int R = radix[i];
-        switch (R) {
-        case 8: dif_stage<8>(buf, n, C, CP, L, tw); break;
-        case 4: dif_stage<4>(buf, n, C, CP, L, tw); break;
-        case 2: dif_stage<2>(buf, n, C, CP, L, tw); break;
-        case 3: dif_stage<3>(buf, n, C, CP, L, tw); break;
-        case 5: dif_stage<5>(buf, n, C, CP, L, tw); break;
-        case 7: dif_stage<7>(buf, n, C, CP, L, tw); break;
-        default: break;
-        }
-        L /= R;
-    }
-}
-
-// Inverse transform (unnormalised): digit-reversed in, natural order out.
-__device__ __forceinline__ void inverse(float2 *buf, int n, int C, int CP, const int *radix, int nstages,
-                                        const Tw &tw) {
-    int s = 1;
-    for (int i = nstages - 1; i >= 0; --i) {
-        const int R = radix[i];
-        switch (R) {
-        case 8: dit_stage<8>(buf, n, C, CP, s, tw); break;
-        case 4: dit_stage<4>(buf, n, C, CP, s, tw); break;
-        case 2: dit_stage<2>(buf, n, C, CP, s, tw); break;
-        case 3: dit_stage<3>(buf, n, C, CP, s, tw); break;
-        case 5: dit_stage<5>(buf, n, C, CP, s, tw); break;
-        case 7: dit_stage<7>(buf, n, C, CP, s, tw); break;
-        default: break;
-        }
-        s *= R;
-    }
-}
-
 
 // ---- self-sorting (Stockham) transform, two buffers ----------------------
 // Natural order in and out.  Stage with radix R after Ns = product of the

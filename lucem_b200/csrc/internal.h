@@ -122,8 +122,6 @@ struct FftPlan {
 };
 
 bool fft_make_plan(int64_t n, FftPlan *plan);
-// out[p] = frequency held at position p after the in-place forward transform.
-void fft_rev_table(const FftPlan &plan, int32_t *out);
 int64_t fft_good_length(int64_t n, bool even);
 
 struct float2_ { float x, y; };
@@ -153,11 +151,8 @@ int rl_launch_iterations(const RlGeom &g, const RlBuffers &b, const float *obs, 
 // OTF of the normalised PSF `psf_dev` (f64 [kz][ky][kx]) centred at `centre`,
 // scaled by 1/(Pz*Py*Px), into complex [Pz][Py][Hp] (f32).  Work buffers are
 // f64 complex of size kz*ky*Hp and kz*Py*Hp.
-// Rows of H are stored at the digit-reversed positions of the y and z plans
-// (rev_y / rev_z from fft_rev_table; rev_z unused for 2-D).
 int rl_launch_otf(const RlGeom &g, const double *psf_dev, const int32_t kdims[3],
                   const int32_t centre[3], double *work_a, double *work_b, void *h_out,
-                  const double *twd_x, const double *twd_y, const double *twd_z,
-                  const int32_t *rev_y, const int32_t *rev_z, void *stream);
+                  const double *twd_x, const double *twd_y, const double *twd_z, void *stream);
 
 }  // namespace lucem

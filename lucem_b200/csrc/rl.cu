@@ -32,6 +32,7 @@
 #include <cstdint>
 
 #include "fft.cuh"
+#include "fft_fast.cuh"
 #include "internal.h"
 
 namespace lucem {
@@ -92,18 +93,20 @@ struct ColPass {
     int32_t C, CP;
 };
 
+// Generic column pass (any 2/3/5/7-smooth length): self-sorting transform in
+// shared memory, two buffers, natural order in and out.
 __global__ void __launch_bounds__(512, 1) col_pass_kernel(const __grid_constant__ ColPass p) {
     extern __shared__ float4 smem4[];
     const int n = p.plan.n;
     float2 *tws = reinterpret_cast<float2 *>(smem4);
-    float2 *buf = tws + n;
+    float2 *bufA = tws + n;
+    float2 *bufB = bufA + n * p.CP;
     const int C = p.C, CP = p.CP, T = blockDim.x, tid = threadIdx.x;
     for (int i = tid; i < n; i += T) tws[i] = p.tw[i];
     const fft::Tw tw{tws, 1};
     const int ntiles = (p.ncols + C - 1) / C;
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const int c0 = tile * C;
-        // Load (lanes along columns: coalesced in kx).
         for (int it = tid; it < n * C; it += T) {
             int row = it / C, c = it - row * C;
             int col = c0 + c;
@@ -115,13 +118,11 @@ __global__ void __launch_bounds__(512, 1) col_pass_kernel(const __grid_constant_
                 else srow = row < p.n_img + 2 * p.halo ? pad_index_rt(row - p.halo, p.n_img, p.pad_mode) : -1;
                 if (srow >= 0) v = p.src[outer * p.src_outer + srow * p.src_row + kx];
             }
-            buf[row * CP + c] = v;
+            bufA[row * CP + c] = v;
         }
         __syncthreads();
-        if (p.mode == kColInv) fft::inverse(buf, n, C, CP, p.plan.radix, p.plan.nstages, tw);
-        else fft::forward(buf, n, C, CP, p.plan.radix, p.plan.nstages, tw);
+        float2 *buf = fft::stockham(bufA, bufB, n, C, CP, p.plan.radix, p.plan.nstages, tw, p.mode == kColInv);
         if (p.mode == kColFull) {
-            // Row `row` holds the frequency rev(row); H is stored in the same order.
             for (int it = tid; it < n * C; it += T) {
                 int row = it / C, c = it - row * C;
                 int col = c0 + c;
@@ -133,9 +134,8 @@ __global__ void __launch_bounds__(512, 1) col_pass_kernel(const __grid_constant_
                 }
             }
             __syncthreads();
-            fft::inverse(buf, n, C, CP, p.plan.radix, p.plan.nstages, tw);
+            buf = fft::stockham(buf, buf == bufA ? bufB : bufA, n, C, CP, p.plan.radix, p.plan.nstages, tw, true);
         }
-        // Store.
         const int rows = p.mode == kColFwd ? n : p.store_count;
         const int r0 = p.mode == kColFwd ? 0 : p.store_begin;
         for (int it = tid; it < rows * C; it += T) {
@@ -147,6 +147,85 @@ __global__ void __launch_bounds__(512, 1) col_pass_kernel(const __grid_constant_
             }
         }
         __syncthreads();
+    }
+}
+
+// Fast column pass for power-of-two lengths N = N1 * N2 (fft_fast.cuh):
+// each thread loads its N2 values straight from global memory (lanes along
+// columns: coalesced), transforms in registers with one shared-memory
+// exchange per direction, multiplies by H in registers and stores back.
+template <int N1, int N2, int C>
+__global__ void __launch_bounds__(N1 * C, 65536 / (N1 * C * 128)) col_fast_kernel(const __grid_constant__ ColPass p) {
+    using L = fftc::ColLayout<N1, N2, C>;
+    using F = fftc::TwoStep<N1, N2, L>;
+    constexpr int N = N1 * N2;
+    extern __shared__ float4 smem4[];
+    float2 *tws = reinterpret_cast<float2 *>(smem4);
+    float2 *xb = tws + N;
+    const int tid = threadIdx.x, c = tid % C, t = tid / C;
+    for (int i = tid; i < N; i += N1 * C) tws[i] = p.tw[i];
+    __syncthreads();
+    const int ntiles = (p.ncols + C - 1) / C;
+    const int n_ext = p.n_img + 2 * p.halo;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int col = tile * C + c;
+        const bool ok = col < p.ncols;
+        int outer = 0, kx = 0;
+        if (ok) {
+            outer = col / p.Hx;
+            kx = col - outer * p.Hx;
+        }
+        float2 v[N2];
+        if (p.mode == kColInv) {
+            const float2 *src = p.src + outer * p.src_outer + kx;
+#pragma unroll
+            for (int j = 0; j < N2; ++j) v[j] = ok ? src[(int64_t)F::freq(t, j) * p.src_row] : make_float2(0.f, 0.f);
+            F::inverse(v, t, c, xb, tws, 1);
+        } else {
+            const float2 *src = p.src + outer * p.src_outer + kx;
+            const float2 *h = p.H + outer * p.h_outer + kx;
+            // Short transforms prefetch the transfer function with the data
+            // (one memory round trip per tile instead of two).
+            constexpr bool kPrefetchH = N2 <= 16;
+            float2 hv[kPrefetchH ? N2 : 1];
+            if (kPrefetchH && p.mode == kColFull) {
+#pragma unroll
+                for (int j = 0; j < (kPrefetchH ? N2 : 1); ++j)
+                    hv[j] = ok ? h[(int64_t)F::freq(t, j) * p.h_row] : make_float2(0.f, 0.f);
+            }
+#pragma unroll
+            for (int i = 0; i < N2; ++i) {
+                const int row = t + N1 * i;
+                int srow = row < n_ext ? pad_index_rt(row - p.halo, p.n_img, p.pad_mode) : -1;
+                v[i] = (ok && srow >= 0) ? src[(int64_t)srow * p.src_row] : make_float2(0.f, 0.f);
+            }
+            F::forward(v, t, c, xb, tws, 1);
+            if (p.mode == kColFwd) {
+                float2 *dst = p.dst + outer * p.dst_outer + kx;
+                if (ok) {
+#pragma unroll
+                    for (int j = 0; j < N2; ++j) dst[(int64_t)F::freq(t, j) * p.dst_row] = v[j];
+                }
+                continue;
+            }
+#pragma unroll
+            for (int j = 0; j < N2; ++j) {
+                float2 hj;
+                if constexpr (kPrefetchH) hj = hv[j];
+                else hj = ok ? h[(int64_t)F::freq(t, j) * p.h_row] : make_float2(0.f, 0.f);
+                if (p.conj_h) hj.y = -hj.y;
+                v[j] = fftc::mul(v[j], hj);
+            }
+            F::inverse(v, t, c, xb, tws, 1);
+        }
+        float2 *dst = p.dst + outer * p.dst_outer + kx;
+        if (ok) {
+#pragma unroll
+            for (int i = 0; i < N2; ++i) {
+                const int row = t + N1 * i - p.store_begin;
+                if (row >= 0 && row < p.store_count) dst[(int64_t)row * p.dst_row] = v[i];
+            }
+        }
     }
 }
 
@@ -283,6 +362,152 @@ __global__ void __launch_bounds__(512, 1) row_pass_kernel(const __grid_constant_
     }
 }
 
+// Fast row pass for packed lengths M = N1 * N2 (powers of two): R rows per
+// CTA, lanes along the row (coalesced), the M-point transforms in registers.
+template <int N1, int N2, int R>
+__global__ void __launch_bounds__(N1 * R, 65536 / (N1 * R * 128)) row_fast_kernel(const __grid_constant__ RowPass p) {
+    using L = fftc::RowLayout<N1, N2, R>;
+    using F = fftc::TwoStep<N1, N2, L>;
+    constexpr int M = N1 * N2, Px = 2 * M;
+    constexpr int SP = M + 1;  // spectrum row pitch (complex)
+    constexpr int U = (L::kBuf > R * SP ? L::kBuf : R * SP);
+    extern __shared__ float4 smem4[];
+    float2 *tws = reinterpret_cast<float2 *>(smem4);  // W_Px^m, m < Px
+    float2 *xb = tws + Px;                             // exchange / spectrum / real rows
+    const int tid = threadIdx.x, t = tid % N1, r = tid / N1;
+    for (int i = tid; i < Px; i += N1 * R) tws[i] = p.tw[i];
+    __syncthreads();
+    const int ntiles = (p.nrows + R - 1) / R;
+    const bool emit_last = !(p.kind == kRowUpdate && p.last);
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int row = tile * R + r;
+        const bool ok = row < p.nrows;
+        float2 *spec = xb + r * SP;
+        float2 v[N2];
+        if (p.kind != kRowInit) {
+            const float2 *s1 = p.s1 + (int64_t)(ok ? row : 0) * p.Hp;
+            for (int k = t; k <= M; k += N1) spec[k] = ok ? s1[k] : make_float2(0.f, 0.f);
+            __syncthreads();
+            // Z[k] = (X[k] + X*[M-k]) + i (X[k] - X*[M-k]) W_Px^{-k}
+            for (int k = t; 2 * k <= M; k += N1) {
+                float2 xk = spec[k], xm = spec[M - k];
+                float2 xmc = fftc::conjf2(xm), xkc = fftc::conjf2(xk);
+                float2 e = fftc::add(xk, xmc), d = fftc::mul(fftc::sub(xk, xmc), fftc::conjf2(tws[k]));
+                float2 zk = make_float2(e.x - d.y, e.y + d.x);
+                if (k != 0 && 2 * k != M) {
+                    float2 e2 = fftc::add(xm, xkc), d2 = fftc::mul(fftc::sub(xm, xkc), fftc::conjf2(tws[M - k]));
+                    spec[M - k] = make_float2(e2.x - d2.y, e2.y + d2.x);
+                }
+                spec[k] = zk;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int j = 0; j < N2; ++j) v[j] = spec[F::freq(t, j)];
+            __syncthreads();
+            F::inverse(v, t, r, xb, tws, 2);
+        }
+        // v[i] = (x[2m], x[2m+1]), m = t + N1 i.  Epilogue on the image
+        // columns, 8 values of m at a time: all loads of a chunk are issued
+        // before its stores (the image pointers do not alias).
+        {
+            const int64_t gbase = (int64_t)(ok ? row : 0) * p.X;
+            const float *__restrict__ obs = p.obs;
+            float *__restrict__ est = p.est;
+            constexpr int CH = N2 < 8 ? N2 : 8;
+#pragma unroll
+            for (int i0 = 0; i0 < N2; i0 += CH) {
+                float in[2 * CH];
+#pragma unroll
+                for (int q = 0; q < 2 * CH; ++q) {
+                    const int xi = 2 * (t + N1 * (i0 + q / 2)) + (q & 1) - p.hx;
+                    const bool inside = ok && xi >= 0 && xi < p.X;
+                    in[q] = 0.0f;
+                    if (p.kind == kRowRatio && inside) in[q] = obs[gbase + xi];
+                    if (p.kind == kRowUpdate && !p.est_first && inside) in[q] = est[gbase + xi];
+                }
+#pragma unroll
+                for (int q = 0; q < 2 * CH; ++q) {
+                    const int i = i0 + q / 2;
+                    const int xi = 2 * (t + N1 * i) + (q & 1) - p.hx;
+                    const bool inside = xi >= 0 && xi < p.X;
+                    const float val = (q & 1) ? v[i].y : v[i].x;
+                    float nv = 0.0f;
+                    if (inside) {
+                        if (p.kind == kRowInit) {
+                            nv = 0.5f;
+                        } else if (p.kind == kRowRatio) {
+                            const float d = fabsf(val) < p.eps ? p.eps : val;
+                            nv = in[q] / d;
+                        } else {
+                            const float old = p.est_first ? 0.5f : in[q];
+                            nv = old * val;
+                            if (p.last && p.clip) nv = fminf(fmaxf(nv, -1.0f), 1.0f);
+                        }
+                    }
+                    if (q & 1) v[i].y = nv; else v[i].x = nv;
+                }
+                if (p.kind == kRowUpdate && ok) {
+#pragma unroll
+                    for (int q = 0; q < 2 * CH; ++q) {
+                        const int i = i0 + q / 2;
+                        const int xi = 2 * (t + N1 * i) + (q & 1) - p.hx;
+                        if (xi >= 0 && xi < p.X) est[gbase + xi] = (q & 1) ? v[i].y : v[i].x;
+                    }
+                }
+            }
+        }
+        if (!emit_last) continue;
+        if (p.hx > 0) {
+            // Extension along x by the pad map: positions outside
+            // [hx, hx + X) take image samples, past X + 2 hx zero.
+            float *real = reinterpret_cast<float *>(spec);
+#pragma unroll
+            for (int i = 0; i < N2; ++i) {
+                const int m = t + N1 * i;
+                real[2 * m] = v[i].x;
+                real[2 * m + 1] = v[i].y;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int i = 0; i < N2; ++i) {
+                const int m = t + N1 * i;
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const int pos = 2 * m + e;
+                    if (pos >= p.hx && pos < p.hx + p.X) continue;
+                    float nv = 0.0f;
+                    if (pos < p.X + 2 * p.hx) {
+                        int q = pad_index_rt(pos - p.hx, p.X, p.pad_mode);
+                        if (q >= 0) nv = real[q + p.hx];
+                    }
+                    if (e) v[i].y = nv; else v[i].x = nv;
+                }
+            }
+            __syncthreads();
+        }
+        F::forward(v, t, r, xb, tws, 2);
+#pragma unroll
+        for (int j = 0; j < N2; ++j) spec[F::freq(t, j)] = v[j];
+        __syncthreads();
+        // X[k] = 1/2 (Z[k] + Z*[M-k]) - i/2 W_Px^k (Z[k] - Z*[M-k]);  Z[M] = Z[0].
+        for (int k = t; 2 * k <= M; k += N1) {
+            float2 zk = spec[k], zm = spec[k == 0 ? 0 : M - k];
+            float2 zmc = fftc::conjf2(zm), zkc = fftc::conjf2(zk);
+            float2 e = fftc::add(zk, zmc), d = fftc::mul(fftc::sub(zk, zmc), tws[k]);
+            float2 e2 = fftc::add(zm, zkc), d2 = fftc::mul(fftc::sub(zm, zkc), tws[M - k]);
+            spec[k] = make_float2(0.5f * (e.x + d.y), 0.5f * (e.y - d.x));
+            if (2 * k != M) spec[M - k] = make_float2(0.5f * (e2.x + d2.y), 0.5f * (e2.y - d2.x));
+        }
+        __syncthreads();
+        if (ok) {
+            float2 *s1 = p.s1 + (int64_t)row * p.Hp;
+            for (int k = t; k <= M; k += N1) s1[k] = spec[k];
+        }
+        __syncthreads();
+    }
+    (void)U;
+}
+
 // ---- transfer function (FP64, direct small-support DFT per axis) ----------
 
 // A[z][y][kx] = sum_x psf[z][y][x] e^{-2 pi i kx (x - cx) / Px}
@@ -307,17 +532,16 @@ __global__ void otf_x_kernel(const double *__restrict__ psf, int kz, int ky, int
     }
 }
 
-// B[z][py][kx] = sum_y A[z][y][kx] e^{-2 pi i ky (y - cy) / Py}, ky = rev_y(py)
+// B[z][ky][kx] = sum_y A[z][y][kx] e^{-2 pi i ky (y - cy) / Py}
 __global__ void otf_y_kernel(const double2 *__restrict__ A, int kz, int ky, int cy, int Py, int Hx,
-                             int Hp, const double2 *__restrict__ twd, const int *__restrict__ rev_y,
+                             int Hp, const double2 *__restrict__ twd,
                              double2 *__restrict__ B) {
     int64_t total = (int64_t)kz * Py * Hx;
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
          e += (int64_t)gridDim.x * blockDim.x) {
         int f = (int)(e % Hx);
         int64_t r = e / Hx;
-        int py = (int)(r % Py);
-        int fy = rev_y[py];
+        int fy = (int)(r % Py);
         int z = (int)(r / Py);
         double re = 0.0, im = 0.0;
         for (int y = 0; y < ky; ++y) {
@@ -328,33 +552,31 @@ __global__ void otf_y_kernel(const double2 *__restrict__ A, int kz, int ky, int 
             re += a.x * w.x - a.y * w.y;
             im += a.x * w.y + a.y * w.x;
         }
-        B[((int64_t)z * Py + py) * Hp + f] = make_double2(re, im);
+        B[((int64_t)z * Py + fy) * Hp + f] = make_double2(re, im);
     }
 }
 
-// H[pz][py][kx] = scale * sum_z B[z][py][kx] e^{-2 pi i kz (z - cz) / Pz}, kz = rev_z(pz),
-// rounded to f32
+// H[kz][ky][kx] = scale * sum_z B[z][ky][kx] e^{-2 pi i kz (z - cz) / Pz}, rounded to f32
 __global__ void otf_z_kernel(const double2 *__restrict__ B, int kz, int cz, int Pz, int Py, int Hx,
-                             int Hp, const double2 *__restrict__ twd, const int *__restrict__ rev_z,
+                             int Hp, const double2 *__restrict__ twd,
                              double scale, float2 *__restrict__ H) {
     int64_t total = (int64_t)Pz * Py * Hx;
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
          e += (int64_t)gridDim.x * blockDim.x) {
         int f = (int)(e % Hx);
         int64_t r = e / Hx;
-        int py = (int)(r % Py);
-        int pz = (int)(r / Py);
-        int fz = rev_z[pz];
+        int fy = (int)(r % Py);
+        int fz = (int)(r / Py);
         double re = 0.0, im = 0.0;
         for (int z = 0; z < kz; ++z) {
             int m = (int)(((int64_t)fz * (z - cz)) % Pz);
             if (m < 0) m += Pz;
             double2 w = twd[m];
-            double2 b = B[((int64_t)z * Py + py) * Hp + f];
+            double2 b = B[((int64_t)z * Py + fy) * Hp + f];
             re += b.x * w.x - b.y * w.y;
             im += b.x * w.y + b.y * w.x;
         }
-        H[((int64_t)pz * Py + py) * Hp + f] = make_float2((float)(re * scale), (float)(im * scale));
+        H[((int64_t)fz * Py + fy) * Hp + f] = make_float2((float)(re * scale), (float)(im * scale));
     }
 }
 
@@ -365,24 +587,52 @@ int sms() {
     return n > 0 ? n : 148;
 }
 
-// Columns per CTA and threads for a length-n column transform.
-void col_shape(int n, int *C, int *T) {
-    int c = 64;
-    while (c > 4 && (int64_t)n * c > 16384) c >>= 1;
-    // About 8 butterflies' worth of values per thread and stage.
-    int t = (int)(((int64_t)n * c / 16 + 31) / 32) * 32;
-    if (t < 128) t = 128;
-    if (t > 512) t = 512;
-    *C = c;
-    *T = t;
+template <int N1, int N2, int C>
+int launch_col_fast(const ColPass &p, cudaStream_t s) {
+    using L = fftc::ColLayout<N1, N2, C>;
+    constexpr int N = N1 * N2;
+    size_t smem = ((size_t)N + (size_t)L::kBuf) * sizeof(float2);
+    int ntiles = (p.ncols + C - 1) / C;
+    int per_sm = (int)((200 * 1024) / (smem + 1024));
+    per_sm = per_sm < 1 ? 1 : (per_sm > 8 ? 8 : per_sm);
+    int grid = ntiles < sms() * per_sm ? ntiles : sms() * per_sm;
+    cudaFuncSetAttribute(col_fast_kernel<N1, N2, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    col_fast_kernel<N1, N2, C><<<grid, N1 * C, smem, s>>>(p);
+    return (int)cudaGetLastError();
+}
+
+template <int N1, int N2, int R>
+int launch_row_fast(const RowPass &p, cudaStream_t s) {
+    using L = fftc::RowLayout<N1, N2, R>;
+    constexpr int M = N1 * N2;
+    constexpr int U = L::kBuf > R * (M + 1) ? L::kBuf : R * (M + 1);
+    size_t smem = ((size_t)2 * M + (size_t)U) * sizeof(float2);
+    int ntiles = (p.nrows + R - 1) / R;
+    int per_sm = (int)((200 * 1024) / (smem + 1024));
+    per_sm = per_sm < 1 ? 1 : (per_sm > 8 ? 8 : per_sm);
+    int grid = ntiles < sms() * per_sm ? ntiles : sms() * per_sm;
+    cudaFuncSetAttribute(row_fast_kernel<N1, N2, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    row_fast_kernel<N1, N2, R><<<grid, N1 * R, smem, s>>>(p);
+    return (int)cudaGetLastError();
 }
 
 int launch_col(ColPass p, cudaStream_t s) {
-    int C, T;
-    col_shape(p.plan.n, &C, &T);
+    switch (p.plan.n) {
+    case 64: return launch_col_fast<8, 8, 16>(p, s);
+    case 128: return launch_col_fast<8, 16, 16>(p, s);
+    case 256: return launch_col_fast<16, 16, 16>(p, s);
+    case 512: return launch_col_fast<16, 32, 16>(p, s);
+    case 1024: return launch_col_fast<32, 32, 8>(p, s);
+    default: break;
+    }
+    // Generic: two (n x (C+1)) buffers plus twiddles within ~200 KB.
+    int C = 64;
+    while (C > 2 && ((size_t)p.plan.n * (1 + 2 * (size_t)(C + 1))) * sizeof(float2) > 200 * 1024) C >>= 1;
+    int T = (int)(((int64_t)p.plan.n * C / 8 + 31) / 32) * 32;
+    T = T < 128 ? 128 : (T > 512 ? 512 : T);
     p.C = C;
     p.CP = C + 1;
-    size_t smem = ((size_t)p.plan.n + (size_t)p.plan.n * p.CP) * sizeof(float2);
+    size_t smem = ((size_t)p.plan.n + 2 * (size_t)p.plan.n * p.CP) * sizeof(float2);
     int ntiles = (p.ncols + C - 1) / C;
     int per_sm = (int)((227 * 1024) / (smem + 1024));
     if (per_sm < 1) per_sm = 1;
@@ -393,6 +643,14 @@ int launch_col(ColPass p, cudaStream_t s) {
 }
 
 int launch_row(RowPass p, cudaStream_t s) {
+    switch (p.M) {
+    case 64: return launch_row_fast<8, 8, 32>(p, s);
+    case 128: return launch_row_fast<8, 16, 32>(p, s);
+    case 256: return launch_row_fast<16, 16, 16>(p, s);
+    case 512: return launch_row_fast<16, 32, 16>(p, s);
+    case 1024: return launch_row_fast<32, 32, 8>(p, s);
+    default: break;
+    }
     const int M = p.M;
     // Two (M+1) x (C+1) buffers plus the twiddles, about 100 KB at most.
     int C = 16;
@@ -427,23 +685,6 @@ bool fft_make_plan(int64_t n, FftPlan *plan) {
         }
     }
     return m == 1 && n >= 1;
-}
-
-// Position -> frequency of the in-place forward transform (see fft.cuh).
-void fft_rev_table(const FftPlan &plan, int32_t *out) {
-    const int n = plan.n;
-    for (int p = 0; p < n; ++p) {
-        int digits[kFftMaxStages];
-        int w = n, q = p;
-        for (int i = 0; i < plan.nstages; ++i) {
-            w /= plan.radix[i];
-            digits[i] = q / w;
-            q %= w;
-        }
-        int f = 0;
-        for (int i = plan.nstages - 1; i >= 0; --i) f = f * plan.radix[i] + digits[i];
-        out[p] = f;
-    }
 }
 
 int64_t fft_good_length(int64_t n, bool even) {
@@ -559,8 +800,7 @@ int rl_launch_iterations(const RlGeom &g, const RlBuffers &b, const float *obs, 
 
 int rl_launch_otf(const RlGeom &g, const double *psf_dev, const int32_t kdims[3],
                   const int32_t centre[3], double *work_a, double *work_b, void *h_out,
-                  const double *twd_x, const double *twd_y, const double *twd_z,
-                  const int32_t *rev_y, const int32_t *rev_z, void *stream) {
+                  const double *twd_x, const double *twd_y, const double *twd_z, void *stream) {
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const int kz = kdims[0], ky = kdims[1], kx = kdims[2];
     double2 *A = reinterpret_cast<double2 *>(work_a);
@@ -576,10 +816,10 @@ int rl_launch_otf(const RlGeom &g, const double *psf_dev, const int32_t kdims[3]
                                                reinterpret_cast<const double2 *>(twd_x), A);
     int64_t tb = (int64_t)kz * g.Py * g.Hx;
     otf_y_kernel<<<grid_for(tb), 256, 0, s>>>(A, kz, ky, centre[1], g.Py, g.Hx, g.Hp,
-                                               reinterpret_cast<const double2 *>(twd_y), rev_y, B);
+                                               reinterpret_cast<const double2 *>(twd_y), B);
     int64_t tz = (int64_t)g.Pz * g.Py * g.Hx;
     otf_z_kernel<<<grid_for(tz), 256, 0, s>>>(B, kz, centre[0], g.Pz, g.Py, g.Hx, g.Hp,
-                                               reinterpret_cast<const double2 *>(twd_z), rev_z, scale,
+                                               reinterpret_cast<const double2 *>(twd_z), scale,
                                                static_cast<float2 *>(h_out));
     return (int)cudaGetLastError();
 }

@@ -63,10 +63,17 @@ _ctx_lock = threading.Lock()
 _ctxs: dict = {}
 
 
-def context(device: Optional[int] = None) -> _Ctx:
-    """The library context of a CUDA device (created once per process)."""
+def _device_index(device) -> int:
     if device is None:
-        device = torch.cuda.current_device()
+        return torch.cuda.current_device()
+    if isinstance(device, torch.device):
+        return device.index if device.index is not None else torch.cuda.current_device()
+    return int(device)
+
+
+def context(device=None) -> _Ctx:
+    """The library context of a CUDA device (created once per process)."""
+    device = _device_index(device)
     with _ctx_lock:
         if device not in _ctxs:
             with torch.cuda.device(device):
@@ -78,8 +85,8 @@ class Workspace:
     """Grow-only device scratch (crates/lucem-core/src/memory/workspace.rs).
     One workspace serves one thread of work at a time."""
 
-    def __init__(self, device: Optional[int] = None):
-        self.ctx = context(device)
+    def __init__(self, device=None):
+        self.ctx = context(_device_index(device))
         h = C.c_void_p()
         N.check(N.lib().lucem_workspace_create(self.ctx.handle, C.byref(h)))
         self.handle = h

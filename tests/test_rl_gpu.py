@@ -143,3 +143,32 @@ def test_errors_mirror_the_reference():
         lb.richardson_lucy(x, torch.ones((3, 3), device="cuda"), mode="constant", grid=(8, 10))
     assert e.value.name == "INVALID_PARAMETER"
     assert lb.richardson_lucy(torch.ones((0, 5), device="cuda"), torch.ones((3, 3), device="cuda")).shape == (0, 5)
+
+
+@pytest.mark.parametrize("py,px", [(64, 128), (128, 256), (256, 512), (512, 1024), (1024, 2048), (128, 2048),
+                                   (1024, 128)])
+@pytest.mark.parametrize("mode", ["constant", "reflect"])
+def test_2d_register_fft_lengths(oracle, py, px, mode):
+    """Every power-of-two length of the register-resident transforms (rows:
+    packed lengths 64..1024, columns 64..1024) against the reference's direct
+    iteration."""
+    h, w = py // 2 - 3, px // 2 - 5
+    rng = np.random.default_rng(py * 7 + px)
+    obs = rng.uniform(0.5, 2.0, (h, w)).astype(np.float32)
+    psf = rng.uniform(0.0, 1.0, (5, 7)).astype(np.float32)
+    got = host(lb.richardson_lucy(dev(obs), dev(psf), num_iter=3, clip=False, filter_epsilon=1e-6, mode=mode,
+                                  grid=(py, px)))
+    want = oracle.richardson_lucy(obs, psf, num_iter=3, clip=False, filter_epsilon=1e-6, mode=mode)
+    oracle.assert_close(got, want.astype(np.float64), RTOL, f"{py}x{px} {mode}")
+
+
+@pytest.mark.parametrize("grid", [(64, 64, 128), (128, 256, 64), (256, 128, 256), (64, 512, 128), (64, 1024, 256)])
+def test_3d_register_fft_lengths(oracle, grid):
+    rng = np.random.default_rng(sum(grid))
+    shape = (min(20, grid[0] // 2), min(40, grid[1] // 2 - 2), min(50, grid[2] // 2 - 3))
+    obs = rng.uniform(0.5, 2.0, shape).astype(np.float32)
+    psf = rng.uniform(0.0, 1.0, (3, 5, 3)).astype(np.float32)
+    got = host(lb.richardson_lucy(dev(obs), dev(psf), num_iter=3, clip=False, filter_epsilon=1e-6, mode="reflect",
+                                  grid=grid))
+    want = oracle.richardson_lucy(obs, psf, num_iter=3, clip=False, filter_epsilon=1e-6, mode="reflect")
+    oracle.assert_close(got, want.astype(np.float64), RTOL, str(grid))
