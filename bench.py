@@ -317,6 +317,7 @@ def run_ours(args, rank, world, local_rank):
 
 
 def main():
+    global ITERS
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
@@ -324,7 +325,6 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--iters", type=int, default=ITERS, help="Richardson-Lucy iterations per step (metric: 50)")
     args = ap.parse_args()
-    global ITERS
     ITERS = args.iters
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -524,12 +524,7 @@ void lucem_rl_settings_default(lucem_rl_settings *s) {
 
 namespace {
 
-struct Pass {
-    int axis;
-    double sigma;
-    uint32_t order;
-    int64_t radius;
-};
+using Pass = lucem::GaussPass;
 
 // crates/lucem-ops/src/filter/gaussian.rs:184-219.
 lucem_status plan_passes(int ndim, const double *sigmas, int n_sigmas, const lucem_gaussian_settings *s,
@@ -1653,3 +1648,54 @@ lucem_status lucem_richardson_lucy(lucem_ctx *ctx, const lucem_tensor *in, const
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Helpers shared with other translation units (internal.h).
+
+namespace lucem {
+
+lucem_status gaussian_blur_plan(const lucem_tensor *in, const double *sigmas, int32_t n_sigmas,
+                                const lucem_gaussian_settings *settings, const lucem_tensor *out,
+                                std::vector<GaussPass> *passes) {
+    lucem_gaussian_settings def;
+    lucem_gaussian_settings_default(&def);
+    const lucem_gaussian_settings *s = settings ? settings : &def;
+    lucem_status st;
+    if ((st = check_in_out(in, out))) return st;
+    if ((st = check_mode(s->mode))) return st;
+    return plan_passes(in->ndim, sigmas, n_sigmas, s, passes);
+}
+
+bool gaussian_fuse_last_two(const lucem_tensor *in, const std::vector<GaussPass> &passes) {
+    const int nd = in->ndim;
+    const size_t np = passes.size();
+    return np >= 2 && passes[np - 2].axis == nd - 2 && passes[np - 1].axis == nd - 1 &&
+           passes[np - 2].radius <= kFamMaxRadius && passes[np - 1].radius <= kFamMaxRadius &&
+           in->dims[nd - 2] < (1 << 30) && in->dims[nd - 1] < (1 << 30);
+}
+
+std::vector<float> gaussian_pass_taps(const GaussPass &p) { return taps_f32(p.sigma, p.order, p.radius); }
+
+void gaussian_fused_params(FamParams *fp, const lucem_tensor *view, int mode, double cval, float scale,
+                           const GaussPass &rows, const GaussPass &cols, float *out) {
+    init_fam(fp, view, mode, cval, scale);
+    fp->n_filters = 1;
+    fill_filter_taps(fp, 0, &rows, &cols);
+    fp->rmax0 = fp->r0[0];
+    fp->rmax1 = fp->r1[0];
+    fp->n_outputs = 1;
+    FamOutput &o = fp->outs[0];
+    o.out = out;
+    o.plane_stride = (int64_t)fp->H * fp->W;
+    o.row_pitch = fp->W;
+    o.combine = (int)Combine::kLinear;
+    o.fa = 0;
+    o.fb = -1;
+    o.alpha = 1.0f;
+    o.beta = 0.0f;
+    o.bias = 0.0f;
+}
+
+lucem_status set_error(lucem_status st, const char *msg) { return fail(st, "%s", msg); }
+
+}  // namespace lucem

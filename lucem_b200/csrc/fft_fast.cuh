@@ -18,7 +18,7 @@
 // 2 pi m / L by exact octant reduction on the integer m and a Taylor
 // polynomial on [0, pi/4] (double precision, rounded once to float).  The
 // run-time twiddles W_N^{t k2} come from a table the host computes in double
-// precision.
+// precision, rearranged per CTA into conflict-free shared tables.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -174,20 +174,35 @@ struct RowLayout {
 };
 
 // Two-step transform; thread (c, t), t < N1, c = the sequence in the CTA.
+// Run-time twiddles come from two shared tables built once per CTA (see
+// build_tables), laid out so that lanes read consecutive entries whichever
+// of t or c varies across the warp:
+//   tf[k2 * N1 + t]  = W_N^{t k2}   (forward, step 1)
+//   ti[n1 * N2 + k2] = W_N^{-n1 k2} (inverse, before the exchange)
 template <int N1_, int N2_, class Layout>
 struct TwoStep {
     static constexpr int N1 = N1_, N2 = N2_, N = N1 * N2, S = N2 / N1;
+    static constexpr int kTables = 2 * N;  // complex entries of tf + ti
     static_assert(N2 % N1 == 0, "N2 must be a multiple of N1");
 
+    // `w` holds W_N^m at w[m * ws], m < N.  Caller synchronises afterwards.
+    __device__ __forceinline__ static void build_tables(float2 *tf, float2 *ti, const float2 *w, int ws) {
+        for (int i = threadIdx.x; i < N; i += blockDim.x) {
+            const int k2 = i / N1, t = i % N1;
+            tf[i] = w[t * k2 * ws];
+            const int n1 = i / N2, kk = i % N2;
+            ti[i] = conjf2(w[n1 * kk * ws]);
+        }
+    }
+
     // v[i] = x[t + N1 i]  ->  v[s N1 + p] = X[(t + N1 s) + N2 bitrev_N1(p)]
-    // (see freq).  `tw` holds W_N^m at tw[m * tws].  Ends synchronised.
-    __device__ __forceinline__ static void forward(float2 *v, int t, int c, float2 *xb, const float2 *tw,
-                                                   int tws) {
+    // (see freq).  Ends synchronised.
+    __device__ __forceinline__ static void forward(float2 *v, int t, int c, float2 *xb, const float2 *tf) {
         rdft<N2, false>(v);  // v[p] = Y[bitrev(p)]
 #pragma unroll
         for (int p = 0; p < N2; ++p) {
             const int k2 = bitrev(p, N2);
-            float2 y = k2 ? mul(v[p], tw[t * k2 * tws]) : v[p];
+            float2 y = k2 ? mul(v[p], tf[k2 * N1 + t]) : v[p];
             xb[Layout::idx(k2, t, c)] = y;
         }
         __syncthreads();
@@ -202,8 +217,7 @@ struct TwoStep {
     }
 
     // Inverse (unnormalised) of the forward layout: v[i] = N x[t + N1 i] on return.
-    __device__ __forceinline__ static void inverse(float2 *v, int t, int c, float2 *xb, const float2 *tw,
-                                                   int tws) {
+    __device__ __forceinline__ static void inverse(float2 *v, int t, int c, float2 *xb, const float2 *ti) {
 #pragma unroll
         for (int s = 0; s < S; ++s) {
             const int k2 = t + N1 * s;
@@ -211,7 +225,7 @@ struct TwoStep {
 #pragma unroll
             for (int n1 = 0; n1 < N1; ++n1) {
                 float2 z = v[s * N1 + n1];
-                if (n1) z = mul(z, conjf2(tw[n1 * k2 * tws]));
+                if (n1) z = mul(z, ti[n1 * N2 + k2]);
                 xb[Layout::idx(k2, n1, c)] = z;
             }
         }

@@ -5,6 +5,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <string>
+#include <vector>
 
 #include "lucem_b200.h"
 
@@ -88,6 +89,32 @@ int launch_sqrt_scale(const float *acc, float *out, int64_t n, float scale, void
 // out = (float)in * scale (u8/u16/f32 -> f32)
 int launch_cast(const void *in, int in_dtype, float scale, float *out, int64_t n, void *stream);
 int launch_fill(float *out, int64_t n, float v, void *stream);
+
+// ---- Gaussian planning shared by the entry points (api.cpp) ---------------
+
+// One 1-D pass of a separable Gaussian (crates/lucem-ops/src/filter/gaussian.rs:204-219).
+struct GaussPass {
+    int axis;
+    double sigma;
+    uint32_t order;
+    int64_t radius;
+};
+
+// Every check lucem_gaussian_blur makes, then its pass list.
+lucem_status gaussian_blur_plan(const lucem_tensor *in, const double *sigmas, int32_t n_sigmas,
+                                const lucem_gaussian_settings *settings, const lucem_tensor *out,
+                                std::vector<GaussPass> *passes);
+// True when the last two passes are the two innermost axes (ascending) and
+// both fit the fused 2-D kernel.
+bool gaussian_fuse_last_two(const lucem_tensor *in, const std::vector<GaussPass> &passes);
+// f32 taps of one pass.
+std::vector<float> gaussian_pass_taps(const GaussPass &p);
+// Fused 2-D launch parameters for one separable filter over the last two
+// axes of `view` into `out`.
+void gaussian_fused_params(FamParams *fp, const lucem_tensor *view, int mode, double cval, float scale,
+                           const GaussPass &rows, const GaussPass &cols, float *out);
+// Records `msg` as the calling thread's last error and returns `st`.
+lucem_status set_error(lucem_status st, const char *msg);
 
 // ---- per-kernel timing ---------------------------------------------------
 

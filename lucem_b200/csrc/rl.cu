@@ -160,13 +160,16 @@ __global__ void __launch_bounds__(N1 * C, 65536 / (N1 * C * 128)) col_fast_kerne
     using F = fftc::TwoStep<N1, N2, L>;
     constexpr int N = N1 * N2;
     extern __shared__ float4 smem4[];
-    float2 *tws = reinterpret_cast<float2 *>(smem4);
-    float2 *xb = tws + N;
+    float2 *tf = reinterpret_cast<float2 *>(smem4);
+    float2 *ti = tf + N;
+    float2 *xb = ti + N;
     const int tid = threadIdx.x, c = tid % C, t = tid / C;
-    for (int i = tid; i < N; i += N1 * C) tws[i] = p.tw[i];
+    F::build_tables(tf, ti, p.tw, 1);
     __syncthreads();
     const int ntiles = (p.ncols + C - 1) / C;
     const int n_ext = p.n_img + 2 * p.halo;
+    // Element offsets within one column fit 32 bits (checked by the host).
+    const int src_row = (int)p.src_row, dst_row = (int)p.dst_row, h_row = (int)p.h_row;
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const int col = tile * C + c;
         const bool ok = col < p.ncols;
@@ -175,15 +178,14 @@ __global__ void __launch_bounds__(N1 * C, 65536 / (N1 * C * 128)) col_fast_kerne
             outer = col / p.Hx;
             kx = col - outer * p.Hx;
         }
+        const float2 *src = p.src + (outer * p.src_outer + kx);
         float2 v[N2];
         if (p.mode == kColInv) {
-            const float2 *src = p.src + outer * p.src_outer + kx;
 #pragma unroll
-            for (int j = 0; j < N2; ++j) v[j] = ok ? src[(int64_t)F::freq(t, j) * p.src_row] : make_float2(0.f, 0.f);
-            F::inverse(v, t, c, xb, tws, 1);
+            for (int j = 0; j < N2; ++j) v[j] = ok ? src[F::freq(t, j) * src_row] : make_float2(0.f, 0.f);
+            F::inverse(v, t, c, xb, ti);
         } else {
-            const float2 *src = p.src + outer * p.src_outer + kx;
-            const float2 *h = p.H + outer * p.h_outer + kx;
+            const float2 *h = p.H + (outer * p.h_outer + kx);
             // Short transforms prefetch the transfer function with the data
             // (one memory round trip per tile instead of two).
             constexpr bool kPrefetchH = N2 <= 16;
@@ -191,20 +193,20 @@ __global__ void __launch_bounds__(N1 * C, 65536 / (N1 * C * 128)) col_fast_kerne
             if (kPrefetchH && p.mode == kColFull) {
 #pragma unroll
                 for (int j = 0; j < (kPrefetchH ? N2 : 1); ++j)
-                    hv[j] = ok ? h[(int64_t)F::freq(t, j) * p.h_row] : make_float2(0.f, 0.f);
+                    hv[j] = ok ? h[F::freq(t, j) * h_row] : make_float2(0.f, 0.f);
             }
 #pragma unroll
             for (int i = 0; i < N2; ++i) {
                 const int row = t + N1 * i;
                 int srow = row < n_ext ? pad_index_rt(row - p.halo, p.n_img, p.pad_mode) : -1;
-                v[i] = (ok && srow >= 0) ? src[(int64_t)srow * p.src_row] : make_float2(0.f, 0.f);
+                v[i] = (ok && srow >= 0) ? src[srow * src_row] : make_float2(0.f, 0.f);
             }
-            F::forward(v, t, c, xb, tws, 1);
+            F::forward(v, t, c, xb, tf);
             if (p.mode == kColFwd) {
-                float2 *dst = p.dst + outer * p.dst_outer + kx;
+                float2 *dst = p.dst + (outer * p.dst_outer + kx);
                 if (ok) {
 #pragma unroll
-                    for (int j = 0; j < N2; ++j) dst[(int64_t)F::freq(t, j) * p.dst_row] = v[j];
+                    for (int j = 0; j < N2; ++j) dst[F::freq(t, j) * dst_row] = v[j];
                 }
                 continue;
             }
@@ -212,18 +214,18 @@ __global__ void __launch_bounds__(N1 * C, 65536 / (N1 * C * 128)) col_fast_kerne
             for (int j = 0; j < N2; ++j) {
                 float2 hj;
                 if constexpr (kPrefetchH) hj = hv[j];
-                else hj = ok ? h[(int64_t)F::freq(t, j) * p.h_row] : make_float2(0.f, 0.f);
+                else hj = ok ? h[F::freq(t, j) * h_row] : make_float2(0.f, 0.f);
                 if (p.conj_h) hj.y = -hj.y;
                 v[j] = fftc::mul(v[j], hj);
             }
-            F::inverse(v, t, c, xb, tws, 1);
+            F::inverse(v, t, c, xb, ti);
         }
-        float2 *dst = p.dst + outer * p.dst_outer + kx;
+        float2 *dst = p.dst + (outer * p.dst_outer + kx);
         if (ok) {
 #pragma unroll
             for (int i = 0; i < N2; ++i) {
                 const int row = t + N1 * i - p.store_begin;
-                if (row >= 0 && row < p.store_count) dst[(int64_t)row * p.dst_row] = v[i];
+                if (row >= 0 && row < p.store_count) dst[row * dst_row] = v[i];
             }
         }
     }
@@ -373,9 +375,12 @@ __global__ void __launch_bounds__(N1 * R, 65536 / (N1 * R * 128)) row_fast_kerne
     constexpr int U = (L::kBuf > R * SP ? L::kBuf : R * SP);
     extern __shared__ float4 smem4[];
     float2 *tws = reinterpret_cast<float2 *>(smem4);  // W_Px^m, m < Px
-    float2 *xb = tws + Px;                             // exchange / spectrum / real rows
+    float2 *tf = tws + Px;                              // W_M tables (fft_fast.cuh)
+    float2 *ti = tf + M;
+    float2 *xb = ti + M;                                // exchange / spectrum / real rows
     const int tid = threadIdx.x, t = tid % N1, r = tid / N1;
     for (int i = tid; i < Px; i += N1 * R) tws[i] = p.tw[i];
+    F::build_tables(tf, ti, p.tw, 2);  // W_M^m = W_Px^{2m}
     __syncthreads();
     const int ntiles = (p.nrows + R - 1) / R;
     const bool emit_last = !(p.kind == kRowUpdate && p.last);
@@ -404,7 +409,7 @@ __global__ void __launch_bounds__(N1 * R, 65536 / (N1 * R * 128)) row_fast_kerne
 #pragma unroll
             for (int j = 0; j < N2; ++j) v[j] = spec[F::freq(t, j)];
             __syncthreads();
-            F::inverse(v, t, r, xb, tws, 2);
+            F::inverse(v, t, r, xb, ti);
         }
         // v[i] = (x[2m], x[2m+1]), m = t + N1 i.  Epilogue on the image
         // columns, 8 values of m at a time: all loads of a chunk are issued
@@ -485,7 +490,7 @@ __global__ void __launch_bounds__(N1 * R, 65536 / (N1 * R * 128)) row_fast_kerne
             }
             __syncthreads();
         }
-        F::forward(v, t, r, xb, tws, 2);
+        F::forward(v, t, r, xb, tf);
 #pragma unroll
         for (int j = 0; j < N2; ++j) spec[F::freq(t, j)] = v[j];
         __syncthreads();
@@ -591,7 +596,7 @@ template <int N1, int N2, int C>
 int launch_col_fast(const ColPass &p, cudaStream_t s) {
     using L = fftc::ColLayout<N1, N2, C>;
     constexpr int N = N1 * N2;
-    size_t smem = ((size_t)N + (size_t)L::kBuf) * sizeof(float2);
+    size_t smem = ((size_t)2 * N + (size_t)L::kBuf) * sizeof(float2);
     int ntiles = (p.ncols + C - 1) / C;
     int per_sm = (int)((200 * 1024) / (smem + 1024));
     per_sm = per_sm < 1 ? 1 : (per_sm > 8 ? 8 : per_sm);
@@ -606,7 +611,7 @@ int launch_row_fast(const RowPass &p, cudaStream_t s) {
     using L = fftc::RowLayout<N1, N2, R>;
     constexpr int M = N1 * N2;
     constexpr int U = L::kBuf > R * (M + 1) ? L::kBuf : R * (M + 1);
-    size_t smem = ((size_t)2 * M + (size_t)U) * sizeof(float2);
+    size_t smem = ((size_t)2 * M + 2 * (size_t)M + (size_t)U) * sizeof(float2);
     int ntiles = (p.nrows + R - 1) / R;
     int per_sm = (int)((200 * 1024) / (smem + 1024));
     per_sm = per_sm < 1 ? 1 : (per_sm > 8 ? 8 : per_sm);
