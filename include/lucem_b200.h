@@ -201,6 +201,25 @@ lucem_status lucem_gaussian_family(lucem_ctx *ctx, const lucem_tensor *in,
                                    int32_t mode, double cval, double truncate, double input_scale,
                                    lucem_workspace *ws, void *stream);
 
+/* Allocation-free lucem_gaussian_blur.  No counterpart in the reference.
+ * For callers that cannot allocate device memory: a host runtime whose device
+ * memory all comes from its own pool under a fixed budget (a cudaMalloc behind
+ * its back would escape that accounting or fail because the pool already holds
+ * the memory), or a service that must not grow its footprint or synchronise
+ * the device with cudaMalloc/cudaFree while it works.  Same arguments, checks
+ * and results as lucem_gaussian_blur, minus the context and workspace: the
+ * intermediate buffers and taps live in one static device array of the library
+ * (2 x 4,194,304 floats + 16,384 taps, about 32 MiB, held by every GPU that
+ * loads the library until exit).  Inputs of more than 4,194,304 elements are
+ * refused with LUCEM_ERR_TOO_MANY_ELEMENTS.  The first call on a device looks
+ * up the array's device address (once per device, on the current device);
+ * make that first call before any stream capture.  Every call shares the
+ * array: calls that overlap on the GPU race, so serialise them.  No
+ * cudaMalloc, cudaFree or allocating library routine is called. */
+lucem_status lucem_gaussian_blur_noalloc(const lucem_tensor *in, const double *sigmas, int32_t n_sigmas,
+                                         const lucem_gaussian_settings *settings, lucem_tensor *out,
+                                         void *stream);
+
 /* ---- tiling and batched tiles ---------------------------------------- */
 
 /* crates/lucem-core/src/tiling.rs:13-49 Block ([z, y, x]). */

@@ -87,6 +87,7 @@ SIGNATURES = {
     "lucem_pad_index": (I64, [I64, I64, I32]),
     "lucem_gaussian_settings_default": (None, [C.POINTER(GaussianSettings)]),
     "lucem_gaussian_blur": (I32, [P, TP, DP, I32, C.POINTER(GaussianSettings), TP, P, P]),
+    "lucem_gaussian_blur_noalloc": (I32, [TP, DP, I32, C.POINTER(GaussianSettings), TP, P]),
     "lucem_gaussian_1d_settings_default": (None, [C.POINTER(Gaussian1dSettings)]),
     "lucem_gaussian_1d": (I32, [P, TP, D, C.POINTER(Gaussian1dSettings), TP, P]),
     "lucem_correlate_1d": (I32, [P, TP, DP, I64, C.POINTER(Correlate1dSettings), TP, P]),
