@@ -186,27 +186,105 @@ def gaussian_secondary(dev, peak):
     x = torch.from_numpy(lb.synth.blob_image()).to(dev)
     out = torch.empty(x.shape, dtype=torch.float32, device=dev)
     ws = lb.Workspace(dev)
+    # L2 flush between calls: write a buffer larger than L2, then read another one
+    # so the write-back of the dirty lines is not charged to the timed call.
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    flush_read = torch.ones(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    sink = torch.empty((), dtype=torch.float32, device=dev)
     s = torch.cuda.current_stream(dev)
     for _ in range(5):
         lb.gaussian_blur(x, 2.0, out=out, workspace=ws)
+    # Device time of each launch from the library's own events (recorded in
+    # C++ right around the launch, so host-side call overhead is excluded),
+    # L2 flushed before every call.
     n = 50
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
     torch.cuda.synchronize(dev)
-    for a, b in evs:
+    ws.set_timing(True)
+    for _ in range(n):
         flush.fill_(1.0)
-        a.record(s)
+        torch.sum(flush_read, dim=0, out=sink)
         lb.gaussian_blur(x, 2.0, out=out, workspace=ws)
-        b.record(s)
-    torch.cuda.synchronize(dev)
-    ms = float(np.mean([a.elapsed_time(b) for a, b in evs]))
+    kinds = ws.timings()
+    ws.set_timing(False)
+    launches, total_ms = kinds["gaussian_family"]
+    ms = total_ms / n
     px = x.numel()
     bytes_ = px * (2 + 4)
     achieved = bytes_ / (ms * 1e-3) / 1e9
     return {"metric": "Gaussian GPix/s (2048x2048 u16 blob image, sigma 2, 17 taps, reflect, f32 out)",
-            "value": px / (ms * 1e-3) / 1e9, "unit": "GPix/s", "ms_per_call": ms, "l2": "flushed between calls",
+            "value": px / (ms * 1e-3) / 1e9, "unit": "GPix/s", "ms_per_call": ms, "l2": "flushed between calls (256 MB write, then 256 MB read)",
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": profile_traffic("gaussian_family_2048")}}
+
+
+def tiles_secondary(dev, peak, steps=3):
+    """The tiled slide: 5 x 34560 x 24960 u16, 1024^2 blocks with a 32 px halo
+    (uneven edge blocks), G(1), G(2), G(4), DoG(1, 3) per block and channel,
+    Reflect at the read part's borders.  Persistent walk (one launch, captured
+    in a CUDA graph) against one launch per block and channel."""
+    import torch
+
+    import lucem_b200 as lb
+
+    C, H, W = 5, 34560, 24960
+    slide = lb.synth.blob_slide(C, H, W, device=dev)
+    blocks = lb.schedule((1, H, W), (1, 1024, 1024), (0, 32, 32))
+    walk = lb.ops.TileWalk(blocks)
+    resp = [("gaussian", 1.0), ("gaussian", 2.0), ("gaussian", 4.0), ("dog", 1.0, 3.0)]
+    outs = [torch.empty((C, H, W), dtype=torch.float32, device=dev) for _ in resp]
+    ws = lb.Workspace(dev)
+    s = torch.cuda.current_stream(dev)
+
+    def call(persistent):
+        lb.gaussian_family_tiles(slide, walk, resp, persistent=persistent, outs=outs, workspace=ws)
+
+    call(True)
+    call(False)
+    torch.cuda.synchronize(dev)
+    ws.set_timing(True)
+    call(True)
+    kinds = ws.timings()
+    ws.set_timing(False)
+
+    def timed(fn, n):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        a.record(s)
+        for _ in range(n):
+            fn()
+        b.record(s)
+        torch.cuda.synchronize(dev)
+        return a.elapsed_time(b) / n
+
+    ms_persistent = timed(lambda: call(True), steps)
+    ms_per_tile = timed(lambda: call(False), 1)
+    # The persistent walk replayed from a CUDA graph.
+    g = torch.cuda.CUDAGraph()
+    side = torch.cuda.Stream(dev)
+    side.wait_stream(s)
+    with torch.cuda.stream(side):
+        call(True)
+        torch.cuda.synchronize(dev)
+        with torch.cuda.graph(g, stream=side):
+            call(True)
+    torch.cuda.synchronize(dev)
+    ms_graph = timed(g.replay, steps)
+    px = C * H * W
+    bytes_ = px * (2 + 4 * len(resp))
+    best = min(ms_persistent, ms_graph)
+    achieved = bytes_ / (best * 1e-3) / 1e9
+    launches = sum(c for c, _ in kinds.values())
+    del outs, slide
+    torch.cuda.empty_cache()
+    return {"metric": "Gaussian-family GPix/s (5x34560x24960 u16 slide, 1024^2 blocks + 32 px halo, "
+                      "G1 G2 G4 DoG(1,3), channel-pixels)",
+            "value": px / (best * 1e-3) / 1e9, "unit": "GPix/s", "ms_per_walk": best,
+            "ms_persistent": ms_persistent, "ms_graph_replay": ms_graph, "ms_per_tile_launches": ms_per_tile,
+            "batched_vs_per_tile": ms_per_tile / best, "launches_persistent": launches,
+            "launches_per_tile": len(blocks) * C,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": profile_traffic("gaussian_family_tiles"),
+                         "algorithmic_bytes": bytes_}}
 
 
 def run_ours(args, rank, world, local_rank):
@@ -313,6 +391,8 @@ def run_ours(args, rank, world, local_rank):
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches_per_step * args.steps, "clocks": clocks, "step_kernels": step_kernels,
             "secondary": {"gaussian_2048": gaussian_secondary(dev, peak)}}
+    if args.tiles:
+        line["secondary"]["gaussian_tiles"] = tiles_secondary(dev, peak)
     print(json.dumps(line), flush=True)
 
 
@@ -324,6 +404,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--iters", type=int, default=ITERS, help="Richardson-Lucy iterations per step (metric: 50)")
+    ap.add_argument("--tiles", type=int, default=1, help="also measure the tiled-slide Gaussian family walk")
     args = ap.parse_args()
     ITERS = args.iters
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -74,7 +74,14 @@ size_t dtype_size(int dt) {
     }
 }
 
-lucem_status check_tensor(const char *name, const lucem_tensor *t) {
+lucem_status check_tensor_cap(const char *name, const lucem_tensor *t, int skip_leading);
+
+lucem_status check_tensor(const char *name, const lucem_tensor *t) { return check_tensor_cap(name, t, 0); }
+
+// As check_tensor, with the element cap applied to the trailing dims after
+// `skip_leading` dims (a stack of planes whose kernels index each plane with
+// 64-bit plane offsets).
+lucem_status check_tensor_cap(const char *name, const lucem_tensor *t, int skip_leading) {
     if (!t) return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `%s`: null tensor", name);
     if (t->ndim < 0 || t->ndim > LUCEM_MAX_DIMS)
         return fail(LUCEM_ERR_INVALID_DIMENSION, "%s expects 0..%d-D array, got %d-D", name,
@@ -86,6 +93,7 @@ lucem_status check_tensor(const char *name, const lucem_tensor *t) {
     for (int i = 0; i < t->ndim; ++i) {
         if (t->dims[i] < 0)
             return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `%s`: negative dimension", name);
+        if (i < skip_leading) continue;
         if (t->dims[i] != 0 && n > kMaxDeviceElements / t->dims[i])
             return fail(LUCEM_ERR_TOO_MANY_ELEMENTS,
                         "%s %s needs more than %lld elements in one device buffer (kernels use "
@@ -625,17 +633,19 @@ lucem_status generic_pass(lucem_ctx *ctx, const lucem_tensor *shape, const void 
 }
 
 void fill_filter_taps(FamParams *fp, int f, const Pass *p0, const Pass *p1) {
-    // p0: axis 0 (rows) pass or null (identity), p1: axis 1 (columns).
+    // p0: axis 0 (rows) pass or null (identity), p1: axis 1 (columns).  Taps
+    // are stored as (w, w) pairs at the kernel radius, centred.
     std::memset(fp->taps0[f], 0, sizeof fp->taps0[f]);
     std::memset(fp->taps1[f], 0, sizeof fp->taps1[f]);
-    auto put = [](float *dst, const Pass *p) -> int {
+    auto put = [](float2_ *dst, const Pass *p) -> int {
         if (!p) {
-            dst[0] = 1.0f;
+            dst[0] = float2_{1.0f, 1.0f};
             return 0;
         }
         std::vector<float> t = taps_f32(p->sigma, p->order, p->radius);
-        for (size_t i = 0; i < t.size(); ++i) dst[i] = t[i];
-        return (int)p->radius;
+        const int r = (int)p->radius, rk = fam_kernel_radius(r);
+        for (size_t i = 0; i < t.size(); ++i) dst[i + (rk - r)] = float2_{t[i], t[i]};
+        return rk;
     };
     fp->r0[f] = put(fp->taps0[f], p0);
     fp->r1[f] = put(fp->taps1[f], p1);
@@ -1297,7 +1307,9 @@ lucem_status lucem_gaussian_family_tiles(lucem_ctx *ctx, const lucem_tensor *sli
     lucem_status st;
     if (!ctx) return fail(LUCEM_ERR_INVALID_HANDLE, "null context");
     if (!ws) return fail(LUCEM_ERR_INVALID_HANDLE, "a workspace is required");
-    if ((st = check_tensor("slide", slide))) return st;
+    // The element cap applies per channel plane (crates/lucem-core/src/compute/limits.rs:12
+    // bounds one buffer; the walk reads one block of one channel at a time).
+    if ((st = check_tensor_cap("slide", slide, slide && slide->ndim == 3 ? 1 : 0))) return st;
     if (slide->ndim != 2 && slide->ndim != 3)
         return fail(LUCEM_ERR_INVALID_DIMENSION, "gaussian_family_tiles expects 2-D or 3-D array, got %d-D shape %s",
                     slide->ndim, dims_str(slide).c_str());
@@ -1307,7 +1319,7 @@ lucem_status lucem_gaussian_family_tiles(lucem_ctx *ctx, const lucem_tensor *sli
     if (H >= (1 << 30) || W >= (1 << 30))
         return fail(LUCEM_ERR_TOO_MANY_ELEMENTS, "slide side exceeds 2^30");
     for (int i = 0; i < n_responses; ++i) {
-        if ((st = check_tensor("output", &responses[i].out))) return st;
+        if ((st = check_tensor_cap("output", &responses[i].out, responses[i].out.ndim == 3 ? 1 : 0))) return st;
         if ((st = same_shape("slide", slide, "output", &responses[i].out))) return st;
         if ((st = not_aliased(slide, &responses[i].out))) return st;
         if ((st = require_f32_out(&responses[i].out))) return st;

@@ -36,7 +36,7 @@ namespace {
 constexpr int kTH = 64;        // output tile rows
 constexpr int kTW = 64;        // output tile columns
 constexpr int kThreads = 256;
-constexpr int kITP = kTH + 1;  // pitch of the transposed intermediate (odd: conflict-free)
+constexpr int kITP = 66;       // pitch of the transposed intermediate (even: 8-byte pairs)
 
 // crates/lucem-ops/src/core/kernels/pad.rs:11-34.
 template <int MODE>
@@ -55,6 +55,17 @@ __device__ __forceinline__ int pad_index(int p, int len) {
     return r < len ? r : period - r;
 }
 
+__device__ __forceinline__ int pad_index_rt(int p, int len, int mode) {
+    if (p >= 0 && p < len) return p;
+    switch (mode) {
+    case LUCEM_PAD_CONSTANT: return -1;
+    case LUCEM_PAD_NEAREST: return pad_index<LUCEM_PAD_NEAREST>(p, len);
+    case LUCEM_PAD_WRAP: return pad_index<LUCEM_PAD_WRAP>(p, len);
+    case LUCEM_PAD_MIRROR: return pad_index<LUCEM_PAD_MIRROR>(p, len);
+    default: return pad_index<LUCEM_PAD_REFLECT>(p, len);
+    }
+}
+
 template <typename T>
 __device__ __forceinline__ float load_as_float(const T *p) { return static_cast<float>(__ldg(p)); }
 
@@ -67,184 +78,225 @@ struct TileGeom {
     int th, tw;                   // valid rows / cols of this tile
 };
 
-template <typename T, int MODE>
+// Axis-0 pass of one filter with kernel radius R over the staged tile A
+// (pitch AWP): item = (column pair, 8 rows).  Every output is accumulated in
+// tap order with packed f32x2 FMAs (two columns per instruction), taps
+// (w, w) in registers 16 at a time.  Writes IT[c][y] (c from cstart).
+template <int R>
+__device__ __forceinline__ void vpass(const float *__restrict__ A, int AWP, int row0, int cstart, int ncols,
+                                   const float2 *__restrict__ w, float *__restrict__ IT) {
+    constexpr int NT = 2 * R + 1;
+    const int npairs = ncols / 2;
+    for (int q = threadIdx.x; q < npairs * 8; q += kThreads) {
+        const int cp = q % npairs, yc = q / npairs;
+        const float *col = A + (yc * 8 + row0) * AWP + cstart + 2 * cp;
+        float2 acc[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[j] = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int s0 = 0; s0 < NT; s0 += 8) {
+            constexpr int kBlk = 8;
+            float2 wv[kBlk];
+#pragma unroll
+            for (int u = 0; u < kBlk; ++u)
+                if (s0 + u < NT) wv[u] = w[s0 + u];
+#pragma unroll
+            for (int m = 0; m < kBlk + 7; ++m) {
+                if (s0 + m >= NT + 7) break;
+                const float2 x = *reinterpret_cast<const float2 *>(col + (s0 + m) * AWP);
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const int u = m - j;
+                    if (u >= 0 && u < kBlk && s0 + u < NT) acc[j] = __ffma2_rn(wv[u], x, acc[j]);
+                }
+            }
+        }
+        float *o0 = IT + (2 * cp) * kITP + yc * 8;
+        float *o1 = o0 + kITP;
+#pragma unroll
+        for (int j = 0; j < 8; j += 2) {
+            *reinterpret_cast<float2 *>(o0 + j) = make_float2(acc[j].x, acc[j + 1].x);
+            *reinterpret_cast<float2 *>(o1 + j) = make_float2(acc[j].y, acc[j + 1].y);
+        }
+    }
+}
+
+// Axis-1 pass with kernel radius R: thread = (row pair yp, 8 columns from
+// x0); reads IT[x0 + m][2 yp .. 2 yp + 1] as one 8-byte word per tap row.
+template <int R>
+__device__ __forceinline__ void hpass(const float *__restrict__ IT, int x0, int yp, const float2 *__restrict__ w,
+                                   float2 *__restrict__ out) {
+    constexpr int NT = 2 * R + 1;
+    const float *row = IT + x0 * kITP + 2 * yp;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) out[j] = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int s0 = 0; s0 < NT; s0 += 8) {
+        constexpr int kBlk = 8;
+        float2 wv[kBlk];
+#pragma unroll
+        for (int u = 0; u < kBlk; ++u)
+            if (s0 + u < NT) wv[u] = w[s0 + u];
+#pragma unroll
+        for (int m = 0; m < kBlk + 7; ++m) {
+            if (s0 + m >= NT + 7) break;
+            const float2 x = *reinterpret_cast<const float2 *>(row + (s0 + m) * kITP);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int u = m - j;
+                if (u >= 0 && u < kBlk && s0 + u < NT) out[j] = __ffma2_rn(wv[u], x, out[j]);
+            }
+        }
+    }
+}
+
+#define LUCEM_RADII(X) X(0) X(2) X(4) X(6) X(8) X(10) X(12) X(14) X(16) X(20) X(24) X(28) X(32)
+
+__device__ __forceinline__ void vpass_r(int R, const float *A, int AWP, int row0, int cstart, int ncols,
+                                        const float2 *w, float *IT) {
+    switch (R) {
+#define V(r) \
+    case r: vpass<r>(A, AWP, row0, cstart, ncols, w, IT); break;
+        LUCEM_RADII(V)
+#undef V
+    default: break;
+    }
+}
+
+__device__ __forceinline__ void hpass_r(int R, const float *IT, int x0, int yp, const float2 *w, float2 *out) {
+    switch (R) {
+#define H(r) \
+    case r: hpass<r>(IT, x0, yp, w, out); break;
+        LUCEM_RADII(H)
+#undef H
+    default: break;
+    }
+}
+
+// One 64 x 64 output tile: stage tile + halo (cast fused), then per filter
+// the axis-0 pass into IT and the axis-1 pass into registers, folded into
+// every response that uses the filter; responses written once at the end.
+template <typename T, int NOUT>
 __device__ void family_tile(const FamParams &p, const TileGeom &g, float *A, float *IT) {
     const int tid = threadIdx.x;
     const int R0 = p.rmax0, R1 = p.rmax1;
-    const int AW = kTW + 2 * R1;
+    const int AWP = kTW + 2 * R1;   // even (R1 even)
     const int AH = kTH + 2 * R0;
     const T *in = static_cast<const T *>(p.in) + (int64_t)g.plane * p.in_plane_stride;
 
-    // Phase 0: tile + halo -> A (f32), pad map relative to the read box.
-    for (int idx = tid; idx < AH * AW; idx += kThreads) {
-        int r = idx / AW, c = idx - r * AW;
-        int ry = g.oy - g.rb_y - R0 + r;  // row relative to the read box
-        int rx = g.ox - g.rb_x - R1 + c;
-        int py = pad_index<MODE>(ry, g.rb_h);
-        int px = pad_index<MODE>(rx, g.rb_w);
-        float v;
-        if (py < 0 || px < 0) v = p.cval;
-        else v = load_as_float(in + (int64_t)(g.rb_y + py) * p.in_row_pitch + (g.rb_x + px)) * p.in_scale;
-        A[idx] = v;
+    // Phase 0: tile + halo -> A (f32), pad map relative to the read box.  A
+    // warp stages one row at a time (row map once per row, lanes along x).
+    {
+        const int lane = tid & 31, warp = tid >> 5;
+        const int rx0 = g.ox - g.rb_x - R1;
+        for (int r = warp; r < AH; r += kThreads / 32) {
+            const int py = pad_index_rt(g.oy - g.rb_y - R0 + r, g.rb_h, p.mode);
+            float *arow = A + r * AWP;
+            if (py < 0) {
+                for (int c = lane; c < AWP; c += 32) arow[c] = p.cval;
+                continue;
+            }
+            const T *src = in + (int64_t)(g.rb_y + py) * p.in_row_pitch + g.rb_x;
+            for (int c = lane; c < AWP; c += 32) {
+                const int px = pad_index_rt(rx0 + c, g.rb_w, p.mode);
+                arow[c] = px < 0 ? p.cval : load_as_float(src + px) * p.in_scale;
+            }
+        }
     }
     __syncthreads();
 
-    // Output accumulators: 2 work items x 8 pixels per thread, per output.
-    float acc[kFamMaxOutputs][2][8];
+    // Axis-1 item of this thread: a warp covers 8 row pairs x 4 chunks of 8
+    // columns (8-byte bank = 8 * chunk + pair: conflict-free).
+    const int lane = tid & 31, wt = tid >> 5;
+    const int yp = (wt & 3) * 8 + (lane & 7);    // row pair: rows 2 yp, 2 yp + 1
+    const int xc = (wt >> 2) * 4 + (lane >> 3);  // columns xc * 8 .. + 7
+    float2 acc[NOUT][8];
 #pragma unroll
-    for (int k = 0; k < kFamMaxOutputs; ++k)
+    for (int k = 0; k < NOUT; ++k)
 #pragma unroll
-        for (int i = 0; i < 2; ++i)
-#pragma unroll
-            for (int j = 0; j < 8; ++j) acc[k][i][j] = 0.0f;
-
-    // Item -> (y, x-chunk) mapping of the axis-1 pass: a warp covers 8 rows x
-    // 4 chunks of 8 columns (bank = 8*xchunk + t + y: conflict-free).
-    int ys[2], xcs[2];
-#pragma unroll
-    for (int i = 0; i < 2; ++i) {
-        int q = i * kThreads + tid;
-        int lane = q & 31, wt = q >> 5;
-        ys[i] = (wt & 7) * 8 + (lane & 7);
-        xcs[i] = (wt >> 3) * 4 + (lane >> 3);
-    }
+        for (int j = 0; j < 8; ++j) acc[k][j] = make_float2(0.f, 0.f);
 
     // Identity terms (unsharp) read the staged input at the output pixel.
 #pragma unroll
-    for (int k = 0; k < kFamMaxOutputs; ++k) {
+    for (int k = 0; k < NOUT; ++k) {
         if (k >= p.n_outputs) break;
         const FamOutput &o = p.outs[k];
         if (o.fa == -2 || o.fb == -2) {
-            float coef = o.fa == -2 ? o.alpha : o.beta;
+            const float coef = o.fa == -2 ? o.alpha : o.beta;
 #pragma unroll
-            for (int i = 0; i < 2; ++i)
-#pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    float v = A[(ys[i] + R0) * AW + xcs[i] * 8 + j + R1];
-                    acc[k][i][j] = acc[k][i][j] + coef * v;
-                }
+            for (int j = 0; j < 8; ++j) {
+                const float a0 = A[(2 * yp + R0) * AWP + xc * 8 + j + R1];
+                const float a1 = A[(2 * yp + 1 + R0) * AWP + xc * 8 + j + R1];
+                acc[k][j] = make_float2(acc[k][j].x + coef * a0, acc[k][j].y + coef * a1);
+            }
         }
     }
 
     for (int f = 0; f < p.n_filters; ++f) {
         const int r0 = p.r0[f], r1 = p.r1[f];
-        const int n0 = 2 * r0 + 1, n1 = 2 * r1 + 1;
-        const int CW = kTW + 2 * r1;          // intermediate columns for this filter
-        const int aoff_r = R0 - r0, aoff_c = R1 - r1;
-        const float *w0 = p.taps0[f];
-        const float *w1 = p.taps1[f];
-
-        // Phase 1: axis-0 pass.  Item (c, yc): column c of the intermediate,
-        // rows yc*8 .. yc*8+7.  Writes IT[c][y] (transposed).
-        for (int q = tid; q < CW * 8; q += kThreads) {
-            int c = q % CW, yc = q / CW;
-            const float *col = A + (yc * 8 + aoff_r) * AW + c + aoff_c;
-            float o[8];
-#pragma unroll
-            for (int j = 0; j < 8; ++j) o[j] = 0.0f;
-            float win[16];
-#pragma unroll
-            for (int j = 0; j < 8; ++j) win[j] = col[j * AW];
-            for (int s0 = 0; s0 < n0; s0 += 8) {
-                // Window slots past n0 + 6 only meet zero taps: load 0 there so
-                // no read leaves the staged rows.
-#pragma unroll
-                for (int j = 0; j < 8; ++j)
-                    win[8 + j] = (s0 + 8 + j <= n0 + 6) ? col[(s0 + 8 + j) * AW] : 0.0f;
-#pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    float w = w0[s0 + u];
-#pragma unroll
-                    for (int j = 0; j < 8; ++j) o[j] = fmaf(w, win[j + u], o[j]);
-                }
-#pragma unroll
-                for (int j = 0; j < 8; ++j) win[j] = win[8 + j];
-            }
-            if (MODE == LUCEM_PAD_CONSTANT) {
-                // A column outside the read box is cval itself in the
-                // reference's intermediate (its axis-1 pass pads the axis-0
-                // result with cval).
-                int rx = g.ox - g.rb_x - r1 + c;
-                if (rx < 0 || rx >= g.rb_w) {
-#pragma unroll
-                    for (int j = 0; j < 8; ++j) o[j] = p.cval;
-                }
-            }
-#pragma unroll
-            for (int j = 0; j < 8; ++j) IT[c * kITP + yc * 8 + j] = o[j];
-        }
+        const int ncols = kTW + 2 * r1;           // even
+        const int cstart = R1 - r1;               // even
+        vpass_r(r0, A, AWP, R0 - r0, cstart, ncols, reinterpret_cast<const float2 *>(p.taps0[f]), IT);
         __syncthreads();
-
-        // Phase 2: axis-1 pass, 8 consecutive columns per item.
-#pragma unroll
-        for (int i = 0; i < 2; ++i) {
-            const float *row = IT + (xcs[i] * 8) * kITP + ys[i];
-            float o[8];
-#pragma unroll
-            for (int j = 0; j < 8; ++j) o[j] = 0.0f;
-            float win[16];
-#pragma unroll
-            for (int j = 0; j < 8; ++j) win[j] = row[j * kITP];
-            for (int s0 = 0; s0 < n1; s0 += 8) {
-#pragma unroll
-                for (int j = 0; j < 8; ++j)
-                    win[8 + j] = (s0 + 8 + j <= n1 + 6) ? row[(s0 + 8 + j) * kITP] : 0.0f;
-#pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    float w = w1[s0 + u];
-#pragma unroll
-                    for (int j = 0; j < 8; ++j) o[j] = fmaf(w, win[j + u], o[j]);
-                }
-#pragma unroll
-                for (int j = 0; j < 8; ++j) win[j] = win[8 + j];
+        if (p.mode == LUCEM_PAD_CONSTANT) {
+            // A column outside the read box is cval itself in the reference's
+            // intermediate (its axis-1 pass pads the axis-0 result with cval).
+            for (int q = tid; q < ncols; q += kThreads) {
+                const int rx = g.ox - g.rb_x - r1 + q;
+                if (rx < 0 || rx >= g.rb_w)
+                    for (int y = 0; y < kTH; ++y) IT[q * kITP + y] = p.cval;
             }
-            // Fold this filter into every response that uses it.
+            __syncthreads();
+        }
+        float2 o[8];
+        hpass_r(r1, IT, xc * 8, yp, reinterpret_cast<const float2 *>(p.taps1[f]), o);
+        // Fold this filter into every response that uses it.
 #pragma unroll
-            for (int k = 0; k < kFamMaxOutputs; ++k) {
-                if (k >= p.n_outputs) break;
-                const FamOutput &oo = p.outs[k];
-                if (oo.combine == (int)Combine::kHypot) {
-                    if (oo.fa == f || oo.fb == f) {
+        for (int k = 0; k < NOUT; ++k) {
+            if (k >= p.n_outputs) break;
+            const FamOutput &oo = p.outs[k];
+            if (oo.combine == (int)Combine::kHypot) {
+                if (oo.fa == f || oo.fb == f) {
 #pragma unroll
-                        for (int j = 0; j < 8; ++j) acc[k][i][j] = fmaf(o[j], o[j], acc[k][i][j]);
-                    }
-                } else {
-                    // Two terms at most, added to an exact 0: the result does
-                    // not depend on which filter runs first.
-                    if (oo.fa == f) {
+                    for (int j = 0; j < 8; ++j) acc[k][j] = __ffma2_rn(o[j], o[j], acc[k][j]);
+                }
+            } else {
+                // Two terms at most, added to an exact 0: the result does not
+                // depend on which filter runs first.
+                if (oo.fa == f) {
+                    const float2 al = make_float2(oo.alpha, oo.alpha);
 #pragma unroll
-                        for (int j = 0; j < 8; ++j) acc[k][i][j] = acc[k][i][j] + oo.alpha * o[j];
-                    }
-                    if (oo.fb == f) {
+                    for (int j = 0; j < 8; ++j) acc[k][j] = __ffma2_rn(al, o[j], acc[k][j]);
+                }
+                if (oo.fb == f) {
+                    const float2 be = make_float2(oo.beta, oo.beta);
 #pragma unroll
-                        for (int j = 0; j < 8; ++j) acc[k][i][j] = acc[k][i][j] + oo.beta * o[j];
-                    }
+                    for (int j = 0; j < 8; ++j) acc[k][j] = __ffma2_rn(be, o[j], acc[k][j]);
                 }
             }
         }
         __syncthreads();  // IT is rewritten by the next filter
     }
 
-    // Epilogue: bias / sqrt, then 32-byte row segments per thread (a warp
-    // writes 8 rows x 128 contiguous bytes).
+    // Epilogue: bias / sqrt, then two 32-byte row segments per thread.
 #pragma unroll
-    for (int k = 0; k < kFamMaxOutputs; ++k) {
+    for (int k = 0; k < NOUT; ++k) {
         if (k >= p.n_outputs) break;
         const FamOutput &oo = p.outs[k];
         float *obase = oo.out + (int64_t)g.plane * oo.plane_stride;
 #pragma unroll
-        for (int i = 0; i < 2; ++i) {
-            int y = ys[i], x = xcs[i] * 8;
+        for (int h = 0; h < 2; ++h) {
+            const int y = 2 * yp + h, x = xc * 8;
             if (y >= g.th) continue;
             float v[8];
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
-                float a = acc[k][i][j];
+                const float a = h ? acc[k][j].y : acc[k][j].x;
                 if (oo.combine == (int)Combine::kHypot) v[j] = sqrtf(fmaxf(a, 0.0f)) * oo.alpha;
                 else v[j] = a + oo.bias;
             }
             float *dst = obase + (int64_t)(g.oy + y) * oo.row_pitch + g.ox + x;
-            bool vec_ok = (x + 8 <= g.tw) && ((reinterpret_cast<uintptr_t>(dst) & 15) == 0);
+            const bool vec_ok = (x + 8 <= g.tw) && ((reinterpret_cast<uintptr_t>(dst) & 15) == 0);
             if (vec_ok) {
                 reinterpret_cast<float4 *>(dst)[0] = make_float4(v[0], v[1], v[2], v[3]);
                 reinterpret_cast<float4 *>(dst)[1] = make_float4(v[4], v[5], v[6], v[7]);
@@ -258,8 +310,8 @@ __device__ void family_tile(const FamParams &p, const TileGeom &g, float *A, flo
 }
 
 // Planes launch: B planes of [H, W], each its own read and owned box.
-template <typename T, int MODE>
-__global__ void __launch_bounds__(kThreads)
+template <typename T, int NOUT>
+__global__ void __launch_bounds__(kThreads, 2)
 family_planes_kernel(const __grid_constant__ FamParams p, int tiles_y, int tiles_x) {
     extern __shared__ float4 smem4[];
     float *A = reinterpret_cast<float *>(smem4);
@@ -274,7 +326,7 @@ family_planes_kernel(const __grid_constant__ FamParams p, int tiles_y, int tiles
         g.rb_y = 0; g.rb_x = 0; g.rb_h = p.H; g.rb_w = p.W;
         g.oy = ty * kTH; g.ox = tx * kTW;
         g.th = min(kTH, p.H - g.oy); g.tw = min(kTW, p.W - g.ox);
-        family_tile<T, MODE>(p, g, A, IT);
+        family_tile<T, NOUT>(p, g, A, IT);
         __syncthreads();
     }
 }
@@ -282,8 +334,8 @@ family_planes_kernel(const __grid_constant__ FamParams p, int tiles_y, int tiles
 // Work-list launch: tiles of uneven blocks of a [C, H, W] slide.  With a
 // counter the CTAs are persistent and take tiles from it; without one each
 // CTA walks tiles blockIdx.x, +gridDim.x, ...
-template <typename T, int MODE>
-__global__ void __launch_bounds__(kThreads)
+template <typename T, int NOUT>
+__global__ void __launch_bounds__(kThreads, 2)
 family_work_kernel(const __grid_constant__ FamParams p, const FamWork *__restrict__ work, int n_work,
                    int n_tiles, int tile_base, int *counter) {
     extern __shared__ float4 smem4[];
@@ -315,43 +367,39 @@ family_work_kernel(const __grid_constant__ FamParams p, const FamWork *__restric
         g.rb_y = w.read_y; g.rb_x = w.read_x; g.rb_h = w.read_h; g.rb_w = w.read_w;
         g.oy = w.own_y + ty * kTH; g.ox = w.own_x + tx * kTW;
         g.th = min(kTH, w.own_y + w.own_h - g.oy); g.tw = min(kTW, w.own_x + w.own_w - g.ox);
-        family_tile<T, MODE>(p, g, A, IT);
+        family_tile<T, NOUT>(p, g, A, IT);
         __syncthreads();
         if (!counter) t += gridDim.x;
     }
 }
 
-template <typename T>
+template <typename T, int NOUT>
 int dispatch_planes(const FamParams &p, size_t smem, int grid, int ty, int tx, cudaStream_t s) {
-    switch (p.mode) {
-#define CASE(M)                                                                                   \
-    case M:                                                                                       \
-        cudaFuncSetAttribute(family_planes_kernel<T, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                             (int)smem);                                                          \
-        family_planes_kernel<T, M><<<grid, kThreads, smem, s>>>(p, ty, tx);                       \
-        break;
-        CASE(0) CASE(1) CASE(2) CASE(3) CASE(4)
-#undef CASE
-    default: return (int)cudaErrorInvalidValue;
-    }
+    cudaFuncSetAttribute(family_planes_kernel<T, NOUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    family_planes_kernel<T, NOUT><<<grid, kThreads, smem, s>>>(p, ty, tx);
+    return (int)cudaGetLastError();
+}
+
+template <typename T, int NOUT>
+int dispatch_work(const FamParams &p, size_t smem, int grid, const FamWork *work, int n_work,
+                  int n_tiles, int tile_base, int *counter, cudaStream_t s) {
+    cudaFuncSetAttribute(family_work_kernel<T, NOUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    family_work_kernel<T, NOUT><<<grid, kThreads, smem, s>>>(p, work, n_work, n_tiles, tile_base, counter);
     return (int)cudaGetLastError();
 }
 
 template <typename T>
-int dispatch_work(const FamParams &p, size_t smem, int grid, const FamWork *work, int n_work,
-                  int n_tiles, int tile_base, int *counter, cudaStream_t s) {
-    switch (p.mode) {
-#define CASE(M)                                                                                  \
-    case M:                                                                                      \
-        cudaFuncSetAttribute(family_work_kernel<T, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                             (int)smem);                                                         \
-        family_work_kernel<T, M><<<grid, kThreads, smem, s>>>(p, work, n_work, n_tiles, tile_base, counter); \
-        break;
-        CASE(0) CASE(1) CASE(2) CASE(3) CASE(4)
-#undef CASE
-    default: return (int)cudaErrorInvalidValue;
-    }
-    return (int)cudaGetLastError();
+int dispatch_planes_n(const FamParams &p, size_t smem, int grid, int ty, int tx, cudaStream_t s) {
+    return p.n_outputs == 1 ? dispatch_planes<T, 1>(p, smem, grid, ty, tx, s)
+                            : dispatch_planes<T, kFamMaxOutputs>(p, smem, grid, ty, tx, s);
+}
+
+template <typename T>
+int dispatch_work_n(const FamParams &p, size_t smem, int grid, const FamWork *work, int n_work, int n_tiles,
+                    int tile_base, int *counter, cudaStream_t s) {
+    return p.n_outputs == 1 ? dispatch_work<T, 1>(p, smem, grid, work, n_work, n_tiles, tile_base, counter, s)
+                            : dispatch_work<T, kFamMaxOutputs>(p, smem, grid, work, n_work, n_tiles, tile_base,
+                                                               counter, s);
 }
 
 int sm_count() {
@@ -387,9 +435,9 @@ int launch_family_planes(const FamParams &p, int in_dtype, void *stream) {
     size_t smem = family_smem_bytes(p.rmax0, p.rmax1);
     int grid = (int)(total < (int64_t)sm_count() * 64 ? total : (int64_t)sm_count() * 64);
     switch (in_dtype) {
-    case LUCEM_U8: return dispatch_planes<uint8_t>(p, smem, grid, ty, tx, s);
-    case LUCEM_U16: return dispatch_planes<uint16_t>(p, smem, grid, ty, tx, s);
-    case LUCEM_F32: return dispatch_planes<float>(p, smem, grid, ty, tx, s);
+    case LUCEM_U8: return dispatch_planes_n<uint8_t>(p, smem, grid, ty, tx, s);
+    case LUCEM_U16: return dispatch_planes_n<uint16_t>(p, smem, grid, ty, tx, s);
+    case LUCEM_F32: return dispatch_planes_n<float>(p, smem, grid, ty, tx, s);
     default: return (int)cudaErrorInvalidValue;
     }
 }
@@ -402,9 +450,9 @@ int launch_family_work(const FamParams &p, int in_dtype, const FamWork *work_dev
     size_t smem = family_smem_bytes(p.rmax0, p.rmax1);
     int grid = counter_dev ? persistent_ctas : n_tiles_total;
     switch (in_dtype) {
-    case LUCEM_U8: return dispatch_work<uint8_t>(p, smem, grid, work_dev, n_work, n_tiles_total, tile_base, counter_dev, s);
-    case LUCEM_U16: return dispatch_work<uint16_t>(p, smem, grid, work_dev, n_work, n_tiles_total, tile_base, counter_dev, s);
-    case LUCEM_F32: return dispatch_work<float>(p, smem, grid, work_dev, n_work, n_tiles_total, tile_base, counter_dev, s);
+    case LUCEM_U8: return dispatch_work_n<uint8_t>(p, smem, grid, work_dev, n_work, n_tiles_total, tile_base, counter_dev, s);
+    case LUCEM_U16: return dispatch_work_n<uint16_t>(p, smem, grid, work_dev, n_work, n_tiles_total, tile_base, counter_dev, s);
+    case LUCEM_F32: return dispatch_work_n<float>(p, smem, grid, work_dev, n_work, n_tiles_total, tile_base, counter_dev, s);
     default: return (int)cudaErrorInvalidValue;
     }
 }

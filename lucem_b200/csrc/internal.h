@@ -17,12 +17,22 @@ constexpr int64_t kMaxDeviceElements = 0xFFFFFFFFll;
 // ---- separable filters -------------------------------------------------
 
 // Largest radius the fused 2-D family kernel takes per axis (65 taps); wider
-// filters run as per-axis passes.
+// filters run as per-axis passes.  The kernel is compiled for the even radii
+// 0, 2, ..., 16, 20, 24, 28, 32; a filter of another radius runs at the next
+// one up with zero taps at both ends (fam_kernel_radius).
 constexpr int kFamMaxRadius = 32;
 constexpr int kFamMaxTaps = 2 * kFamMaxRadius + 1;
 constexpr int kFamMaxFilters = 8;
 constexpr int kFamMaxOutputs = 4;
-constexpr int kFamTapStride = 72;  // taps per filter axis, zero padded (multiple of 8)
+constexpr int kFamTapStride = 66;  // tap pairs per filter axis (>= 2 * kFamMaxRadius + 1)
+
+inline int fam_kernel_radius(int r) {
+    if (r <= 0) return 0;
+    if (r <= 16) return (r + 1) & ~1;
+    return (r + 3) & ~3;
+}
+
+struct float2_ { float x, y; };
 
 enum class Combine : int32_t { kLinear = 0, kHypot = 1 };
 
@@ -48,12 +58,14 @@ struct FamParams {
     float in_scale;
     int32_t n_filters;
     int32_t n_outputs;
-    int32_t rmax0, rmax1;          // largest radius per axis over the filters
-    int32_t r0[kFamMaxFilters];    // radius, axis 0 (rows)
-    int32_t r1[kFamMaxFilters];    // radius, axis 1 (columns)
+    int32_t rmax0, rmax1;          // largest kernel radius per axis over the filters
+    int32_t r0[kFamMaxFilters];    // kernel radius (fam_kernel_radius), axis 0 (rows)
+    int32_t r1[kFamMaxFilters];    // kernel radius, axis 1 (columns)
     FamOutput outs[kFamMaxOutputs];
-    float taps0[kFamMaxFilters][kFamTapStride];
-    float taps1[kFamMaxFilters][kFamTapStride];
+    // Taps as (w, w) pairs for the packed f32x2 FMA, 2 r + 1 per filter axis,
+    // zero padded from the filter's own radius to its kernel radius.
+    float2_ taps0[kFamMaxFilters][kFamTapStride];
+    float2_ taps1[kFamMaxFilters][kFamTapStride];
 };
 
 // One tile of a batched walk: the read box of one channel and the owned box
@@ -151,7 +163,6 @@ struct FftPlan {
 bool fft_make_plan(int64_t n, FftPlan *plan);
 int64_t fft_good_length(int64_t n, bool even);
 
-struct float2_ { float x, y; };
 
 // Geometry of one RL problem on its FFT grid.  Axes are (z, y, x); 2-D inputs
 // have Z = Pz = 1.
