@@ -138,6 +138,15 @@ lucem_status lucem_gaussian_blur(lucem_ctx *ctx, const lucem_tensor *in, const d
                                  int32_t n_sigmas, const lucem_gaussian_settings *settings,
                                  lucem_tensor *out, lucem_workspace *ws, void *stream);
 
+/* The adjoint (transpose) of lucem_gaussian_blur's linear map in -> out with
+ * the same sigmas and settings: grad_in = A^T grad_out, where out = A in + b
+ * (b: the cval term of the constant mode).  It is the backward pass of
+ * gaussian_blur for reverse-mode differentiation; the reference has no
+ * counterpart (its filters are not differentiable).  f32 gradient in and
+ * out; every pad mode (halo reads fold back onto the samples they came from). */
+lucem_status lucem_gaussian_blur_adjoint(lucem_ctx *ctx, const lucem_tensor *grad_out, const double *sigmas,
+                                         int32_t n_sigmas, const lucem_gaussian_settings *settings,
+                                         lucem_tensor *grad_in, lucem_workspace *ws, void *stream);
 /* crates/lucem-ops/src/filter/gaussian.rs:66-118 (Gaussian1d, gaussian_1d_into).
  * radius < 0 means None. */
 typedef struct lucem_gaussian_1d_settings {
@@ -273,6 +282,31 @@ void lucem_rl_settings_default(lucem_rl_settings *s);
 lucem_status lucem_richardson_lucy(lucem_ctx *ctx, const lucem_tensor *in, const lucem_tensor *psf,
                                    const lucem_rl_settings *settings, lucem_tensor *out,
                                    lucem_workspace *ws, void *stream);
+/* Reverse mode through lucem_richardson_lucy (the reference's
+ * richardson_lucy is not differentiable; no counterpart there): given
+ * d loss / d out, writes d loss / d psf (through the PSF normalisation;
+ * optional, NULL to skip) and d loss / d in (optional).  The iterations are
+ * recomputed from checkpoints kept every `checkpoint_every` iterations
+ * (device memory: ceil(T/k) + k + 8 volumes and 5 spectra).  Zero padding
+ * (LUCEM_PAD_CONSTANT) and clip off only.  Synchronises the stream (PSF in,
+ * PSF gradient out). */
+lucem_status lucem_richardson_lucy_backward(lucem_ctx *ctx, const lucem_tensor *in, const lucem_tensor *psf,
+                                            const lucem_rl_settings *settings, const lucem_tensor *grad_out,
+                                            int32_t checkpoint_every, lucem_tensor *grad_psf,
+                                            lucem_tensor *grad_in, lucem_workspace *ws, void *stream);
+/* The forward model of richardson_lucy as an operator: out = psf (*) x, the
+ * convolution centred at k-1-k/2 per axis, zero padding, the PSF as given
+ * (not normalised), 2-D or 3-D f32 on the FFT grid (grid NULL or 0 =
+ * automatic).  The reference computes it inside richardson_lucy as
+ * correlate with the flipped PSF (crates/lucem-ops/src/restore/deconvolve.rs:120). */
+lucem_status lucem_fft_convolve(lucem_ctx *ctx, const lucem_tensor *x, const lucem_tensor *psf, int32_t mode,
+                                const int64_t *grid, lucem_tensor *out, lucem_workspace *ws, void *stream);
+/* Its reverse mode (no counterpart in the reference): grad_x = A^T grad_out
+ * and grad_psf, each optional (NULL to skip). */
+lucem_status lucem_fft_convolve_backward(lucem_ctx *ctx, const lucem_tensor *x, const lucem_tensor *psf,
+                                         int32_t mode, const int64_t *grid, const lucem_tensor *grad_out,
+                                         lucem_tensor *grad_x, lucem_tensor *grad_psf, lucem_workspace *ws,
+                                         void *stream);
 /* The grid lucem_richardson_lucy would use (host only). */
 lucem_status lucem_rl_grid(const int64_t *dims, const int64_t *kdims, int32_t ndim, int32_t mode,
                            const int64_t *requested, int64_t *grid_out);

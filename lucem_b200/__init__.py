@@ -13,5 +13,6 @@ package is its host-side mirror of the reference's Python/Rust operator API.
 from .ops import *  # noqa: F401,F403
 from .ops import __all__ as _ops_all
 from . import synth  # noqa: F401
+from . import autograd  # noqa: F401
 
-__all__ = list(_ops_all) + ["synth"]
+__all__ = list(_ops_all) + ["synth", "autograd"]

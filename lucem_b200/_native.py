@@ -87,6 +87,7 @@ SIGNATURES = {
     "lucem_pad_index": (I64, [I64, I64, I32]),
     "lucem_gaussian_settings_default": (None, [C.POINTER(GaussianSettings)]),
     "lucem_gaussian_blur": (I32, [P, TP, DP, I32, C.POINTER(GaussianSettings), TP, P, P]),
+    "lucem_gaussian_blur_adjoint": (I32, [P, TP, DP, I32, C.POINTER(GaussianSettings), TP, P, P]),
     "lucem_gaussian_blur_noalloc": (I32, [TP, DP, I32, C.POINTER(GaussianSettings), TP, P]),
     "lucem_gaussian_1d_settings_default": (None, [C.POINTER(Gaussian1dSettings)]),
     "lucem_gaussian_1d": (I32, [P, TP, D, C.POINTER(Gaussian1dSettings), TP, P]),
@@ -102,6 +103,9 @@ SIGNATURES = {
     "lucem_rl_settings_default": (None, [C.POINTER(RlSettings)]),
     "lucem_richardson_lucy": (I32, [P, TP, TP, C.POINTER(RlSettings), TP, P, P]),
     "lucem_rl_grid": (I32, [I64P, I64P, I32, I32, I64P, I64P]),
+    "lucem_richardson_lucy_backward": (I32, [P, TP, TP, C.POINTER(RlSettings), TP, I32, TP, TP, P, P]),
+    "lucem_fft_convolve": (I32, [P, TP, TP, I32, I64P, TP, P, P]),
+    "lucem_fft_convolve_backward": (I32, [P, TP, TP, I32, I64P, TP, TP, TP, P, P]),
     "lucem_fft_good_length": (I64, [I64, I32]),
 }
 

@@ -738,6 +738,63 @@ lucem_status run_passes(lucem_ctx *ctx, const lucem_tensor *in, const std::vecto
     return ok();
 }
 
+// The adjoint of run_passes' linear map x -> out (f32 in and out): the
+// adjoint of each pass in reverse order.  One pass's adjoint is the
+// zero-padded correlation with the reversed taps plus the fold of the halo
+// reads back onto the positions the pad mode mapped them to
+// (launch_adjoint_fold).  `scale` is the forward's input_scale; cval does not
+// enter (it belongs to the map's constant term).
+lucem_status adjoint_passes(lucem_ctx *ctx, const lucem_tensor *shape, const float *g,
+                            const std::vector<Pass> &passes, int mode, double scale, float *out,
+                            lucem_workspace *ws, void *stream) {
+    const int64_t n = numel(shape);
+    if (n == 0) return ok();
+    const size_t np = passes.size();
+    if (np == 0) {
+        int e = timed(kPassElementwise, stream, [&] { return launch_cast(g, LUCEM_F32, (float)scale, out, n, stream); });
+        return e ? cuda_fail(e, "copy launch") : ok();
+    }
+    float *bufs[2] = {nullptr, nullptr};
+    const size_t needed = np >= 3 ? 2 : np - 1;
+    for (size_t i = 0; i < needed; ++i) {
+        if (!ws) return fail(LUCEM_ERR_INVALID_HANDLE, "a workspace is required for multi-pass filters");
+        void *p = nullptr;
+        lucem_status st = ws->get(i == 0 ? "sep_ping" : "sep_pong", (size_t)n * sizeof(float), &p);
+        if (st) return st;
+        bufs[i] = static_cast<float *>(p);
+    }
+    const float *src = g;
+    float src_scale = (float)scale;
+    int ping = 0;
+    for (size_t k = 0; k < np; ++k) {
+        const Pass &p = passes[np - 1 - k];
+        float *dst = k + 1 == np ? out : bufs[ping];
+        const std::vector<float> w = taps_f32(p.sigma, p.order, p.radius);
+        const std::vector<float> wr(w.rbegin(), w.rend());
+        const float *w_dev = nullptr, *wr_dev = nullptr;
+        lucem_status st;
+        const std::string key = tap_key(p.sigma, p.order, p.radius);
+        if ((st = cached_weights(ctx, key, w, &w_dev)) || (st = cached_weights(ctx, "rev-" + key, wr, &wr_dev)))
+            return st;
+        int64_t outer, len, inner;
+        split_axis(shape, p.axis, &outer, &len, &inner);
+        const int size = (int)(2 * p.radius + 1), left = size / 2;
+        int e = timed(kPassCorrelate, stream, [&] {
+            return launch_correlate_1d(src, LUCEM_F32, src_scale, dst, outer, len, inner, wr_dev, size,
+                                       size - 1 - left, LUCEM_PAD_CONSTANT, 0.0f, stream);
+        });
+        if (!e)
+            e = timed(kPassCorrelate, stream, [&] {
+                return launch_adjoint_fold(src, src_scale, dst, outer, len, inner, w_dev, size, left, mode, stream);
+            });
+        if (e) return cuda_fail(e, "adjoint pass launch");
+        src = dst;
+        src_scale = 1.0f;
+        ping ^= 1;
+    }
+    return ok();
+}
+
 lucem_status check_in_out(const lucem_tensor *in, const lucem_tensor *out) {
     lucem_status st;
     if ((st = check_tensor("input", in))) return st;
@@ -769,6 +826,25 @@ lucem_status lucem_gaussian_blur(lucem_ctx *ctx, const lucem_tensor *in, const d
     if ((st = plan_passes(in->ndim, sigmas, n_sigmas, s, &passes))) return st;
     return run_passes(ctx, in, passes, s->mode, s->cval, s->input_scale, static_cast<float *>(out->data),
                       ws, stream);
+}
+
+lucem_status lucem_gaussian_blur_adjoint(lucem_ctx *ctx, const lucem_tensor *grad_out, const double *sigmas,
+                                         int32_t n_sigmas, const lucem_gaussian_settings *settings,
+                                         lucem_tensor *grad_in, lucem_workspace *ws, void *stream) {
+    TimerScope timer_scope(ws);
+    if (!ctx) return fail(LUCEM_ERR_INVALID_HANDLE, "null context");
+    lucem_gaussian_settings def;
+    lucem_gaussian_settings_default(&def);
+    const lucem_gaussian_settings *s = settings ? settings : &def;
+    lucem_status st;
+    if ((st = check_in_out(grad_out, grad_in))) return st;
+    if (grad_out->dtype != LUCEM_F32)
+        return fail(LUCEM_ERR_UNSUPPORTED_DTYPE, "gaussian_blur_adjoint takes an f32 gradient");
+    if ((st = check_mode(s->mode))) return st;
+    std::vector<Pass> passes;
+    if ((st = plan_passes(grad_out->ndim, sigmas, n_sigmas, s, &passes))) return st;
+    return adjoint_passes(ctx, grad_out, static_cast<const float *>(grad_out->data), passes, s->mode,
+                          s->input_scale, static_cast<float *>(grad_in->data), ws, stream);
 }
 
 lucem_status lucem_gaussian_1d(lucem_ctx *ctx, const lucem_tensor *in, double sigma,
@@ -1510,6 +1586,231 @@ lucem_status twiddles(lucem_ctx *ctx, int64_t n, const float2_ **f32, const doub
     return ok();
 }
 
+// Argument checks of the RL-family entry points
+// (crates/lucem-ops/src/restore/deconvolve.rs:53-71, same order).
+lucem_status rl_check(const lucem_tensor *in, const lucem_tensor *psf, const lucem_tensor *out, int32_t num_iter,
+                      int32_t mode, const char *what) {
+    lucem_status st;
+    if ((st = check_tensor("input", in)) || (st = check_tensor("output", out)) || (st = check_tensor("psf", psf)))
+        return st;
+    if ((st = same_shape("input", in, "output", out))) return st;
+    if ((st = not_aliased(in, out))) return st;
+    if (in->ndim != 2 && in->ndim != 3)
+        return fail(LUCEM_ERR_INVALID_DIMENSION, "%s input expects 2 or 3-D array, got %d-D shape %s", what,
+                    in->ndim, dims_str(in).c_str());
+    if (psf->ndim != in->ndim)
+        return fail(LUCEM_ERR_INVALID_DIMENSION, "%s psf expects %d-D array, got %d-D shape %s", what, in->ndim,
+                    psf->ndim, dims_str(psf).c_str());
+    if (numel(psf) == 0) return fail(LUCEM_ERR_INVALID_WEIGHTS, "psf: PSF cannot be empty");
+    if (num_iter < 1) return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `num_iter`: num_iter must be >= 1");
+    if (in->dtype != LUCEM_F32 || psf->dtype != LUCEM_F32 || out->dtype != LUCEM_F32)
+        return fail(LUCEM_ERR_UNSUPPORTED_DTYPE, "%s takes f32 input, psf and output", what);
+    return check_mode(mode);
+}
+
+// deconvolve.rs:104.
+float rl_eps(const lucem_rl_settings *s) {
+    const double eps = s->has_filter_epsilon ? s->filter_epsilon : 1e-12;
+    return (float)std::max(eps, 1e-15);
+}
+
+// One problem's geometry, transfer functions and spectrum buffers.
+struct RlSetup {
+    RlGeom g{};
+    RlBuffers b{};
+    int64_t kd[3] = {1, 1, 1}, grid[3] = {1, 1, 1};
+    int64_t kn = 0;
+    int32_t c_conv[3] = {0, 0, 0}, c_corr[3] = {0, 0, 0};
+    bool same_centre = true;
+    bool norm_active = false;  // the PSF was scaled by norm = 1 / sum(psf)
+    double norm = 1.0;
+    std::vector<double> pn;    // the PSF the transfer functions were built from (f64)
+};
+
+// Geometry, PSF (normalised on the host in f64 when `normalise`, as
+// deconvolve.rs:77-88 does), transfer functions (cached per workspace by
+// content) and the two spectrum buffers.  Synchronises the stream once (the
+// PSF download) and once more when the transfer functions are rebuilt.
+lucem_status rl_prepare(lucem_ctx *ctx, const lucem_tensor *in, const lucem_tensor *psf, int32_t mode,
+                        const int64_t *grid_req, bool normalise, lucem_workspace *ws, void *stream, RlSetup *su) {
+    lucem_status st;
+    cudaStream_t cs = static_cast<cudaStream_t>(stream);
+    const int nd = in->ndim;
+    int64_t dims[3] = {1, 1, 1};
+    for (int d = 0; d < nd; ++d) {
+        dims[3 - nd + d] = in->dims[d];
+        su->kd[3 - nd + d] = psf->dims[d];
+    }
+    int64_t req[3] = {0, 0, 0};
+    for (int d = 0; d < nd; ++d) req[3 - nd + d] = grid_req ? grid_req[d] : 0;
+    if ((st = rl_grid_impl(dims + (3 - nd), su->kd + (3 - nd), nd, mode, req + (3 - nd), su->grid + (3 - nd))))
+        return st;
+    const int64_t *kd = su->kd, *grid = su->grid;
+    RlGeom &g = su->g;
+    g.ndim = nd;
+    g.Z = (int32_t)dims[0]; g.Y = (int32_t)dims[1]; g.X = (int32_t)dims[2];
+    g.Pz = (int32_t)grid[0]; g.Py = (int32_t)grid[1]; g.Px = (int32_t)grid[2];
+    g.hz = nd == 3 ? (int32_t)rl_halo(kd[0], mode) : 0;
+    g.hy = (int32_t)rl_halo(kd[1], mode);
+    g.hx = (int32_t)rl_halo(kd[2], mode);
+    g.Hx = g.Px / 2 + 1;
+    g.Hp = (g.Hx + 15) & ~15;
+    g.mode = mode;
+
+    const int64_t kn = numel(psf);
+    su->kn = kn;
+    std::vector<float> hp((size_t)kn);
+    CUDA_TRY(cudaMemcpyAsync(hp.data(), psf->data, (size_t)kn * sizeof(float), cudaMemcpyDeviceToHost, cs),
+             "psf download");
+    CUDA_TRY(cudaStreamSynchronize(cs), "psf download");
+    double sum = 0.0;
+    for (float v : hp) sum += (double)v;
+    su->norm_active = normalise && std::fabs(sum) > 1e-12;
+    su->norm = su->norm_active ? 1.0 / sum : 1.0;
+    su->pn.resize((size_t)kn);
+    for (int64_t i = 0; i < kn; ++i) su->pn[(size_t)i] = (double)hp[(size_t)i] * su->norm;
+    const std::vector<double> &pn = su->pn;
+
+    const float2_ *tw32[3];
+    const double *tw64[3];
+    for (int d = 0; d < 3; ++d)
+        if ((st = twiddles(ctx, grid[d], &tw32[d], &tw64[d]))) return st;
+
+    // Transfer functions: convolution with the PSF centred at k-1-k/2 and
+    // correlation with it centred at k/2 (convolve.rs:144-145 with the flip at
+    // deconvolve.rs:82-88); equal for odd sizes.
+    int32_t kdi[3] = {(int32_t)kd[0], (int32_t)kd[1], (int32_t)kd[2]};
+    su->same_centre = true;
+    for (int d = 0; d < 3; ++d) {
+        su->c_conv[d] = (int32_t)(kd[d] - 1 - kd[d] / 2);
+        su->c_corr[d] = (int32_t)(kd[d] / 2);
+        su->same_centre = su->same_centre && su->c_conv[d] == su->c_corr[d];
+    }
+    const bool same_centre = su->same_centre;
+    const size_t hbytes = (size_t)g.Pz * g.Py * g.Hp * sizeof(float2_);
+    std::string key(reinterpret_cast<const char *>(pn.data()), pn.size() * sizeof(double));
+    key.append(reinterpret_cast<const char *>(kdi), sizeof kdi);
+    key.append(reinterpret_cast<const char *>(grid), 3 * sizeof(int64_t));
+    key.append(reinterpret_cast<const char *>(&g.Hp), sizeof g.Hp);
+    void *h_conv = nullptr, *h_corr = nullptr;
+    Slot *sl_conv = nullptr, *sl_corr = nullptr;
+    if ((st = ws->get("rl_otf_conv", hbytes, &h_conv, &sl_conv))) return st;
+    if (!same_centre && (st = ws->get("rl_otf_corr", hbytes, &h_corr, &sl_corr))) return st;
+    if (same_centre) h_corr = h_conv;
+    const bool fresh = sl_conv->key != key || (!same_centre && sl_corr->key != key);
+    if (fresh) {
+        void *psf64 = nullptr, *wa = nullptr, *wb = nullptr;
+        if ((st = ws->get("rl_psf64", (size_t)kn * sizeof(double), &psf64))) return st;
+        if ((st = ws->get("rl_otf_a", (size_t)kd[0] * kd[1] * g.Hp * 16, &wa))) return st;
+        if ((st = ws->get("rl_otf_b", (size_t)kd[0] * g.Py * g.Hp * 16, &wb))) return st;
+        CUDA_TRY(cudaMemcpyAsync(psf64, pn.data(), (size_t)kn * sizeof(double), cudaMemcpyHostToDevice, cs),
+                 "psf upload");
+        if (ws->t()) ws->t()->begin(kPassRlOtf, stream);
+        int e = rl_launch_otf(g, static_cast<const double *>(psf64), kdi, su->c_conv, static_cast<double *>(wa),
+                              static_cast<double *>(wb), h_conv, tw64[2], tw64[1], tw64[0], stream);
+        if (ws->t()) ws->t()->end(kPassRlOtf, stream);
+        if (e) return cuda_fail(e, "transfer function launch");
+        if (!same_centre) {
+            e = rl_launch_otf(g, static_cast<const double *>(psf64), kdi, su->c_corr, static_cast<double *>(wa),
+                              static_cast<double *>(wb), h_corr, tw64[2], tw64[1], tw64[0], stream);
+            if (e) return cuda_fail(e, "transfer function launch");
+        }
+        // The host PSF copy must outlive the upload.
+        CUDA_TRY(cudaStreamSynchronize(cs), "transfer function");
+        sl_conv->key = key;
+        if (sl_corr) sl_corr->key = key;
+    }
+
+    void *s1 = nullptr, *s2 = nullptr;
+    if ((st = ws->get("rl_s1", (size_t)g.Z * g.Y * g.Hp * sizeof(float2_), &s1))) return st;
+    if (nd == 3 && (st = ws->get("rl_s2", (size_t)g.Z * g.Py * g.Hp * sizeof(float2_), &s2))) return st;
+    RlBuffers &b = su->b;
+    b.s1 = s1;
+    b.s2 = s2;
+    b.h_conv = h_conv;
+    b.h_corr = h_corr;
+    b.tw_x = tw32[2];
+    b.tw_y = tw32[1];
+    b.tw_z = tw32[0];
+    return ok();
+}
+
+// Workspace buffers of the reverse passes: the full set for the unrolled
+// iterations (full_rl), or the few the convolution's gradient needs.
+lucem_status rl_bwd_buffers(const RlSetup &su, int T, int K, bool full_rl, lucem_workspace *ws, RlBwdBuffers *w) {
+    lucem_status st;
+    const RlGeom &g = su.g;
+    const size_t vb = (size_t)g.Z * g.Y * g.X * sizeof(float);
+    const size_t sb = (size_t)g.Pz * g.Py * g.Hp * sizeof(float2_);
+    std::memset(w, 0, sizeof *w);
+    void *p = nullptr;
+    auto vol = [&](const char *name, size_t count, float **dst) -> lucem_status {
+        lucem_status s2 = ws->get(name, vb * count, &p);
+        if (!s2) *dst = static_cast<float *>(p);
+        return s2;
+    };
+    auto spec = [&](const char *name, float2_ **dst) -> lucem_status {
+        lucem_status s2 = ws->get(name, sb, &p);
+        if (!s2) *dst = static_cast<float2_ *>(p);
+        return s2;
+    };
+    if (full_rl) {
+        const int nseg = (T + K - 1) / K;
+        if ((st = vol("rlb_ckpt", (size_t)nseg, &w->ckpt)) || (st = vol("rlb_seg", (size_t)K, &w->seg))) return st;
+        const char *names[8] = {"rlb_c", "rlb_r", "rlb_a", "rlb_abar", "rlb_rbar", "rlb_cbar", "rlb_t", "rlb_ebar"};
+        float **dst[8] = {&w->c, &w->r, &w->a, &w->abar, &w->rbar, &w->cbar, &w->t, &w->ebar};
+        for (int i = 0; i < 8; ++i)
+            if ((st = vol(names[i], 1, dst[i]))) return st;
+        if ((st = spec("rlb_spec_r", &w->spec_r)) || (st = spec("rlb_spec_abar", &w->spec_abar))) return st;
+        if (!su.same_centre && (st = spec("rlb_pbar2", &w->pbar2))) return st;
+    } else {
+        if ((st = vol("rlb_c", 1, &w->c)) || (st = vol("rlb_t", 1, &w->t))) return st;
+    }
+    if ((st = spec("rlb_spec_e", &w->spec_e)) || (st = spec("rlb_spec_cbar", &w->spec_cbar)) ||
+        (st = spec("rlb_pbar1", &w->pbar1)))
+        return st;
+    const size_t fz = g.ndim == 3 ? (size_t)g.Pz : 1;
+    if ((st = ws->get("rlb_full_s1", fz * g.Py * g.Hp * sizeof(float2_), &w->full_s1))) return st;
+    if (g.ndim == 3 && (st = ws->get("rlb_full_s2", fz * g.Py * g.Hp * sizeof(float2_), &w->full_s2))) return st;
+    if ((st = ws->get("rlb_full_real", fz * g.Py * g.Px * sizeof(float), &p))) return st;
+    w->full_real = static_cast<float *>(p);
+    for (int d = 0; d < 3; ++d) {
+        w->kdims[d] = (int32_t)su.kd[d];
+        w->c_conv[d] = su.c_conv[d];
+        w->c_corr[d] = su.c_corr[d];
+    }
+    return ok();
+}
+
+// d loss / d psf from d loss / d (the PSF the transfer functions were built
+// from).  Through the host normalisation p_n = p * norm, norm = 1 / sum(p):
+// g_p = norm * (g_n - sum(g_n * p_n)).  gcorr (even sides) adds the
+// correlation's lags.  Synchronises the stream.
+lucem_status psf_grad_finish(const RlSetup &su, const float *gconv, const float *gcorr, bool normalised,
+                             lucem_tensor *grad_psf, void *stream) {
+    cudaStream_t cs = static_cast<cudaStream_t>(stream);
+    const int64_t kn = su.kn;
+    std::vector<float> a((size_t)kn), b(gcorr ? (size_t)kn : 0);
+    CUDA_TRY(cudaMemcpyAsync(a.data(), gconv, (size_t)kn * sizeof(float), cudaMemcpyDeviceToHost, cs), "psf grad");
+    if (gcorr)
+        CUDA_TRY(cudaMemcpyAsync(b.data(), gcorr, (size_t)kn * sizeof(float), cudaMemcpyDeviceToHost, cs), "psf grad");
+    CUDA_TRY(cudaStreamSynchronize(cs), "psf grad");
+    std::vector<double> gn((size_t)kn);
+    for (int64_t i = 0; i < kn; ++i) gn[(size_t)i] = (double)a[(size_t)i] + (gcorr ? (double)b[(size_t)i] : 0.0);
+    std::vector<float> out((size_t)kn);
+    if (normalised && su.norm_active) {
+        double dot = 0.0;
+        for (int64_t i = 0; i < kn; ++i) dot += gn[(size_t)i] * su.pn[(size_t)i];
+        for (int64_t i = 0; i < kn; ++i) out[(size_t)i] = (float)(su.norm * (gn[(size_t)i] - dot));
+    } else {
+        for (int64_t i = 0; i < kn; ++i) out[(size_t)i] = (float)gn[(size_t)i];
+    }
+    CUDA_TRY(cudaMemcpyAsync(grad_psf->data, out.data(), (size_t)kn * sizeof(float), cudaMemcpyHostToDevice, cs),
+             "psf grad upload");
+    CUDA_TRY(cudaStreamSynchronize(cs), "psf grad upload");
+    return ok();
+}
+
 }  // namespace
 
 extern "C" {
@@ -1535,128 +1836,117 @@ lucem_status lucem_richardson_lucy(lucem_ctx *ctx, const lucem_tensor *in, const
     lucem_rl_settings_default(&def);
     const lucem_rl_settings *s = settings ? settings : &def;
     lucem_status st;
-    cudaStream_t cs = static_cast<cudaStream_t>(stream);
-    // crates/lucem-ops/src/restore/deconvolve.rs:53-71 (same order of checks).
-    if ((st = check_tensor("input", in)) || (st = check_tensor("output", out)) ||
-        (st = check_tensor("psf", psf)))
-        return st;
-    if ((st = same_shape("input", in, "output", out))) return st;
-    if ((st = not_aliased(in, out))) return st;
-    if (in->ndim != 2 && in->ndim != 3)
-        return fail(LUCEM_ERR_INVALID_DIMENSION, "richardson_lucy input expects 2 or 3-D array, got %d-D shape %s",
-                    in->ndim, dims_str(in).c_str());
-    if (psf->ndim != in->ndim)
-        return fail(LUCEM_ERR_INVALID_DIMENSION, "richardson_lucy psf expects %d-D array, got %d-D shape %s",
-                    in->ndim, psf->ndim, dims_str(psf).c_str());
-    if (numel(psf) == 0) return fail(LUCEM_ERR_INVALID_WEIGHTS, "psf: PSF cannot be empty");
-    if (s->num_iter < 1)
-        return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `num_iter`: num_iter must be >= 1");
-    if (in->dtype != LUCEM_F32 || psf->dtype != LUCEM_F32 || out->dtype != LUCEM_F32)
-        return fail(LUCEM_ERR_UNSUPPORTED_DTYPE, "richardson_lucy takes f32 input, psf and output");
-    if ((st = check_mode(s->mode))) return st;
+    if ((st = rl_check(in, psf, out, s->num_iter, s->mode, "richardson_lucy"))) return st;
     if (numel(in) == 0) return ok();
-
-    const int nd = in->ndim;
-    int64_t dims[3] = {1, 1, 1}, kd[3] = {1, 1, 1}, grid[3] = {1, 1, 1};
-    for (int d = 0; d < nd; ++d) {
-        dims[3 - nd + d] = in->dims[d];
-        kd[3 - nd + d] = psf->dims[d];
-    }
-    int64_t req[3] = {0, 0, 0};
-    for (int d = 0; d < nd; ++d) req[3 - nd + d] = s->grid[d];
-    if ((st = rl_grid_impl(dims + (3 - nd), kd + (3 - nd), nd, s->mode, req + (3 - nd), grid + (3 - nd))))
-        return st;
-
-    RlGeom g{};
-    g.ndim = nd;
-    g.Z = (int32_t)dims[0]; g.Y = (int32_t)dims[1]; g.X = (int32_t)dims[2];
-    g.Pz = (int32_t)grid[0]; g.Py = (int32_t)grid[1]; g.Px = (int32_t)grid[2];
-    g.hz = nd == 3 ? (int32_t)rl_halo(kd[0], s->mode) : 0;
-    g.hy = (int32_t)rl_halo(kd[1], s->mode);
-    g.hx = (int32_t)rl_halo(kd[2], s->mode);
-    g.Hx = g.Px / 2 + 1;
-    g.Hp = (g.Hx + 15) & ~15;
-    g.mode = s->mode;
-
-    // deconvolve.rs:77-88: the PSF goes to the host, is normalised in f64.
-    const int64_t kn = numel(psf);
-    std::vector<float> hp((size_t)kn);
-    CUDA_TRY(cudaMemcpyAsync(hp.data(), psf->data, (size_t)kn * sizeof(float), cudaMemcpyDeviceToHost, cs),
-             "psf download");
-    CUDA_TRY(cudaStreamSynchronize(cs), "psf download");
-    double sum = 0.0;
-    for (float v : hp) sum += (double)v;
-    const double norm = std::fabs(sum) > 1e-12 ? 1.0 / sum : 1.0;
-    std::vector<double> pn((size_t)kn);
-    for (int64_t i = 0; i < kn; ++i) pn[(size_t)i] = (double)hp[(size_t)i] * norm;
-
-    const float2_ *tw32[3];
-    const double *tw64[3];
-    for (int d = 0; d < 3; ++d)
-        if ((st = twiddles(ctx, grid[d], &tw32[d], &tw64[d]))) return st;
-
-    // Transfer functions: convolution with the PSF centred at k-1-k/2 and
-    // correlation with it centred at k/2 (convolve.rs:144-145 with the flip at
-    // deconvolve.rs:82-88); equal for odd sizes.
-    int32_t kdi[3] = {(int32_t)kd[0], (int32_t)kd[1], (int32_t)kd[2]};
-    int32_t c_conv[3], c_corr[3];
-    bool same_centre = true;
-    for (int d = 0; d < 3; ++d) {
-        c_conv[d] = (int32_t)(kd[d] - 1 - kd[d] / 2);
-        c_corr[d] = (int32_t)(kd[d] / 2);
-        same_centre = same_centre && c_conv[d] == c_corr[d];
-    }
-    const size_t hbytes = (size_t)g.Pz * g.Py * g.Hp * sizeof(float2_);
-    std::string key(reinterpret_cast<const char *>(pn.data()), pn.size() * sizeof(double));
-    key.append(reinterpret_cast<const char *>(kdi), sizeof kdi);
-    key.append(reinterpret_cast<const char *>(grid), sizeof grid);
-    key.append(reinterpret_cast<const char *>(&g.Hp), sizeof g.Hp);
-    void *h_conv = nullptr, *h_corr = nullptr;
-    Slot *sl_conv = nullptr, *sl_corr = nullptr;
-    if ((st = ws->get("rl_otf_conv", hbytes, &h_conv, &sl_conv))) return st;
-    if (!same_centre && (st = ws->get("rl_otf_corr", hbytes, &h_corr, &sl_corr))) return st;
-    if (same_centre) h_corr = h_conv;
-    bool fresh = sl_conv->key != key || (!same_centre && sl_corr->key != key);
-    if (fresh) {
-        void *psf64 = nullptr, *wa = nullptr, *wb = nullptr;
-        if ((st = ws->get("rl_psf64", (size_t)kn * sizeof(double), &psf64))) return st;
-        if ((st = ws->get("rl_otf_a", (size_t)kd[0] * kd[1] * g.Hp * 16, &wa))) return st;
-        if ((st = ws->get("rl_otf_b", (size_t)kd[0] * g.Py * g.Hp * 16, &wb))) return st;
-        CUDA_TRY(cudaMemcpyAsync(psf64, pn.data(), (size_t)kn * sizeof(double), cudaMemcpyHostToDevice, cs),
-                 "psf upload");
-        if (ws->t()) ws->t()->begin(kPassRlOtf, stream);
-        int e = rl_launch_otf(g, static_cast<const double *>(psf64), kdi, c_conv, static_cast<double *>(wa),
-                              static_cast<double *>(wb), h_conv, tw64[2], tw64[1], tw64[0], stream);
-        if (ws->t()) ws->t()->end(kPassRlOtf, stream);
-        if (e) return cuda_fail(e, "transfer function launch");
-        if (!same_centre) {
-            e = rl_launch_otf(g, static_cast<const double *>(psf64), kdi, c_corr, static_cast<double *>(wa),
-                              static_cast<double *>(wb), h_corr, tw64[2], tw64[1], tw64[0], stream);
-            if (e) return cuda_fail(e, "transfer function launch");
-        }
-        // The host PSF copy must outlive the upload.
-        CUDA_TRY(cudaStreamSynchronize(cs), "transfer function");
-        sl_conv->key = key;
-        if (sl_corr) sl_corr->key = key;
-    }
-
-    void *s1 = nullptr, *s2 = nullptr;
-    if ((st = ws->get("rl_s1", (size_t)g.Z * g.Y * g.Hp * sizeof(float2_), &s1))) return st;
-    if (nd == 3 && (st = ws->get("rl_s2", (size_t)g.Z * g.Py * g.Hp * sizeof(float2_), &s2))) return st;
-    RlBuffers b{};
-    b.s1 = s1;
-    b.s2 = s2;
-    b.h_conv = h_conv;
-    b.h_corr = h_corr;
-    b.tw_x = tw32[2];
-    b.tw_y = tw32[1];
-    b.tw_z = tw32[0];
-    // deconvolve.rs:104.
-    double eps = s->has_filter_epsilon ? s->filter_epsilon : 1e-12;
-    eps = std::max(eps, 1e-15);
-    int e = rl_launch_iterations(g, b, static_cast<const float *>(in->data), static_cast<float *>(out->data),
-                                 s->num_iter, s->clip, (float)eps, stream, ws->t());
+    RlSetup su;
+    if ((st = rl_prepare(ctx, in, psf, s->mode, s->grid, true, ws, stream, &su))) return st;
+    int e = rl_launch_iterations(su.g, su.b, static_cast<const float *>(in->data), static_cast<float *>(out->data),
+                                 s->num_iter, s->clip, rl_eps(s), stream, ws->t());
     return e ? cuda_fail(e, "richardson_lucy launch") : ok();
+}
+
+lucem_status lucem_richardson_lucy_backward(lucem_ctx *ctx, const lucem_tensor *in, const lucem_tensor *psf,
+                                            const lucem_rl_settings *settings, const lucem_tensor *grad_out,
+                                            int32_t checkpoint_every, lucem_tensor *grad_psf,
+                                            lucem_tensor *grad_in, lucem_workspace *ws, void *stream) {
+    TimerScope timer_scope(ws);
+    if (!ctx) return fail(LUCEM_ERR_INVALID_HANDLE, "null context");
+    if (!ws) return fail(LUCEM_ERR_INVALID_HANDLE, "a workspace is required");
+    lucem_rl_settings def;
+    lucem_rl_settings_default(&def);
+    const lucem_rl_settings *s = settings ? settings : &def;
+    lucem_status st;
+    if ((st = rl_check(in, psf, grad_out, s->num_iter, s->mode, "richardson_lucy_backward"))) return st;
+    if (s->mode != LUCEM_PAD_CONSTANT || s->clip)
+        return fail(LUCEM_ERR_INVALID_PARAMETER,
+                    "invalid parameter `settings`: the backward pass takes zero padding (mode constant) and clip off");
+    if (checkpoint_every < 1)
+        return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `checkpoint_every`: must be >= 1");
+    if (grad_psf) {
+        if ((st = check_tensor("grad_psf", grad_psf)) || (st = same_shape("psf", psf, "grad_psf", grad_psf)) ||
+            (st = require_f32_out(grad_psf)))
+            return st;
+    }
+    if (grad_in) {
+        if ((st = check_tensor("grad_in", grad_in)) || (st = same_shape("input", in, "grad_in", grad_in)) ||
+            (st = require_f32_out(grad_in)) || (st = not_aliased(grad_out, grad_in)))
+            return st;
+    }
+    if (numel(in) == 0) return ok();
+    RlSetup su;
+    if ((st = rl_prepare(ctx, in, psf, s->mode, s->grid, true, ws, stream, &su))) return st;
+    RlBwdBuffers w;
+    const int T = s->num_iter, K = checkpoint_every < T ? checkpoint_every : T;
+    if ((st = rl_bwd_buffers(su, T, K, true, ws, &w))) return st;
+    void *gp = nullptr;
+    if ((st = ws->get("rlb_gpsf", (size_t)su.kn * 2 * sizeof(float), &gp))) return st;
+    float *gconv = static_cast<float *>(gp), *gcorr = gconv + su.kn;
+    int e = rl_backward(su.g, su.b, w, static_cast<const float *>(in->data), T, K, rl_eps(s),
+                        static_cast<const float *>(grad_out->data), gconv, w.pbar2 ? gcorr : nullptr,
+                        grad_in ? static_cast<float *>(grad_in->data) : nullptr, stream, ws->t());
+    if (e) return cuda_fail(e, "richardson_lucy_backward launch");
+    if (grad_psf) return psf_grad_finish(su, gconv, w.pbar2 ? gcorr : nullptr, true, grad_psf, stream);
+    return ok();
+}
+
+lucem_status lucem_fft_convolve(lucem_ctx *ctx, const lucem_tensor *x, const lucem_tensor *psf, int32_t mode,
+                                const int64_t *grid, lucem_tensor *out, lucem_workspace *ws, void *stream) {
+    TimerScope timer_scope(ws);
+    if (!ctx) return fail(LUCEM_ERR_INVALID_HANDLE, "null context");
+    if (!ws) return fail(LUCEM_ERR_INVALID_HANDLE, "a workspace is required");
+    lucem_status st;
+    if ((st = rl_check(x, psf, out, 1, mode, "fft_convolve"))) return st;
+    if (mode != LUCEM_PAD_CONSTANT)
+        return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `mode`: fft_convolve takes zero padding");
+    if (numel(x) == 0) return ok();
+    int64_t req[3] = {0, 0, 0};
+    if (grid)
+        for (int d = 0; d < x->ndim; ++d) req[d] = grid[d];
+    RlSetup su;
+    if ((st = rl_prepare(ctx, x, psf, mode, req, false, ws, stream, &su))) return st;
+    int e = rl_apply(su.g, su.b, su.b.h_conv, 0, static_cast<const float *>(x->data), static_cast<float *>(out->data),
+                     stream, ws->t());
+    return e ? cuda_fail(e, "fft_convolve launch") : ok();
+}
+
+lucem_status lucem_fft_convolve_backward(lucem_ctx *ctx, const lucem_tensor *x, const lucem_tensor *psf,
+                                         int32_t mode, const int64_t *grid, const lucem_tensor *grad_out,
+                                         lucem_tensor *grad_x, lucem_tensor *grad_psf, lucem_workspace *ws,
+                                         void *stream) {
+    TimerScope timer_scope(ws);
+    if (!ctx) return fail(LUCEM_ERR_INVALID_HANDLE, "null context");
+    if (!ws) return fail(LUCEM_ERR_INVALID_HANDLE, "a workspace is required");
+    lucem_status st;
+    if ((st = rl_check(x, psf, grad_out, 1, mode, "fft_convolve_backward"))) return st;
+    if (mode != LUCEM_PAD_CONSTANT)
+        return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `mode`: fft_convolve takes zero padding");
+    if (grad_x) {
+        if ((st = check_tensor("grad_x", grad_x)) || (st = same_shape("input", x, "grad_x", grad_x)) ||
+            (st = require_f32_out(grad_x)) || (st = not_aliased(grad_out, grad_x)))
+            return st;
+    }
+    if (grad_psf) {
+        if ((st = check_tensor("grad_psf", grad_psf)) || (st = same_shape("psf", psf, "grad_psf", grad_psf)) ||
+            (st = require_f32_out(grad_psf)))
+            return st;
+    }
+    if (numel(x) == 0) return ok();
+    int64_t req[3] = {0, 0, 0};
+    if (grid)
+        for (int d = 0; d < x->ndim; ++d) req[d] = grid[d];
+    RlSetup su;
+    if ((st = rl_prepare(ctx, x, psf, mode, req, false, ws, stream, &su))) return st;
+    RlBwdBuffers w;
+    if ((st = rl_bwd_buffers(su, 1, 1, false, ws, &w))) return st;
+    void *gp = nullptr;
+    if (grad_psf && (st = ws->get("rlb_gpsf", (size_t)su.kn * 2 * sizeof(float), &gp))) return st;
+    int e = rl_convolve_backward(su.g, su.b, w, static_cast<const float *>(x->data),
+                                 static_cast<const float *>(grad_out->data),
+                                 grad_x ? static_cast<float *>(grad_x->data) : nullptr,
+                                 grad_psf ? static_cast<float *>(gp) : nullptr, stream, ws->t());
+    if (e) return cuda_fail(e, "fft_convolve_backward launch");
+    if (grad_psf) return psf_grad_finish(su, static_cast<float *>(gp), nullptr, false, grad_psf, stream);
+    return ok();
 }
 
 }  // extern "C"

@@ -660,6 +660,48 @@ int launch_correlate_1d(const void *in, int in_dtype, float in_scale, float *out
     }
 }
 
+// Halo part of the adjoint of one correlate_1d pass.  The forward pass reads
+// in[pad(i + t - left)] for output i and tap t; its adjoint scatters
+// w[t] * g[i] back to pad(i + t - left).  The interior part (positions that
+// are already inside the line) is a zero-padded correlation with the reversed
+// taps (launch_correlate_1d); this kernel adds, per line, what the forward
+// read from the extended positions p < 0 and p >= len, at pad(p) (nothing for
+// the constant mode).  One thread owns one line, so the sums into a line are
+// race-free and in a fixed order.
+__global__ void adjoint_fold_kernel(const float *__restrict__ g, float scale, float *__restrict__ out,
+                                    int64_t outer, int64_t len, int64_t inner, const float *__restrict__ w,
+                                    int size, int left, int mode) {
+    const int64_t lines = outer * inner;
+    const int n = (int)len;
+    for (int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; l < lines;
+         l += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t o = l / inner, c = l - o * inner;
+        const float *gl = g + o * len * inner + c;
+        float *ol = out + o * len * inner + c;
+        // Extended positions: [-left, 0) then [n, n + size - 1 - left).
+        const int n_lo = left, n_hi = size - 1 - left;
+        for (int k = 0; k < n_lo + n_hi; ++k) {
+            const int p = k < n_lo ? k - left : n + (k - n_lo);
+            const int q = pad_index_rt(p, n, mode);
+            if (q < 0) continue;
+            // taps t with i = p + left - t inside [0, n)
+            const int t0 = max(0, p + left - n + 1), t1 = min(size - 1, p + left);
+            float acc = 0.0f;
+            for (int t = t0; t <= t1; ++t) acc = fmaf(w[t], gl[(int64_t)(p + left - t) * inner], acc);
+            ol[(int64_t)q * inner] += scale * acc;
+        }
+    }
+}
+
+int launch_adjoint_fold(const float *g, float scale, float *out, int64_t outer, int64_t len, int64_t inner,
+                        const float *w_dev, int32_t size, int32_t left, int32_t mode, void *stream) {
+    const int64_t lines = outer * inner;
+    if (lines == 0 || mode == LUCEM_PAD_CONSTANT) return 0;
+    adjoint_fold_kernel<<<ew_grid(lines), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        g, scale, out, outer, len, inner, w_dev, size, left, mode);
+    return (int)cudaGetLastError();
+}
+
 int launch_linear_comb(const float *a, const float *b, float *out, int64_t n, float alpha,
                        float beta, float bias, void *stream) {
     if (n == 0) return 0;

@@ -91,6 +91,11 @@ size_t family_smem_bytes(int rmax0, int rmax1);
 int launch_correlate_1d(const void *in, int in_dtype, float in_scale, float *out, int64_t outer,
                         int64_t len, int64_t inner, const float *w_dev, int32_t size, int32_t left,
                         int32_t mode, float cval, void *stream);
+// Halo part of the adjoint of launch_correlate_1d (f32 in): out[pad(p)] +=
+// scale * sum_t w[t] g[p + left - t] over the extended positions p outside
+// [0, len).  No-op for the constant mode.
+int launch_adjoint_fold(const float *g, float scale, float *out, int64_t outer, int64_t len, int64_t inner,
+                        const float *w_dev, int32_t size, int32_t left, int32_t mode, void *stream);
 // out = alpha*a + beta*b + bias (b may be null: beta ignored).
 int launch_linear_comb(const float *a, const float *b, float *out, int64_t n, float alpha,
                        float beta, float bias, void *stream);
@@ -186,6 +191,36 @@ struct RlBuffers {
 
 int rl_launch_iterations(const RlGeom &g, const RlBuffers &b, const float *obs, float *est_out,
                          int32_t num_iter, int32_t clip, float eps, void *stream, PassTimer *timer);
+// out = H x (conj 0) or conj(H) x (conj 1) over the image region, zero
+// padding (the geometry's mode must be constant).  Uses b.s1 / b.s2.
+int rl_apply(const RlGeom &g, const RlBuffers &b, const void *H, int conj, const float *x, float *out,
+             void *stream, PassTimer *timer);
+
+// Scratch of the reverse passes (device pointers; V = Z*Y*X floats per
+// volume, S = Pz*Py*Hp complex per spectrum).
+struct RlBwdBuffers {
+    float *ckpt;                  // ceil(T/K) volumes
+    float *seg;                   // K volumes
+    float *c, *r, *a, *abar, *rbar, *cbar, *t, *ebar;  // one volume each
+    float2_ *spec_e, *spec_r, *spec_abar, *spec_cbar;  // one spectrum each
+    float2_ *pbar1, *pbar2;       // PSF cross-spectrum accumulators (pbar2: even sides only)
+    void *full_s1, *full_s2;      // complex [Pz][Py][Hp] (full-grid inverse)
+    float *full_real;             // [Pz][Py][Px]
+    int32_t kdims[3], c_conv[3], c_corr[3];
+};
+
+// Reverse mode of rl_launch_iterations (clip off, zero padding): from
+// d loss / d (estimate after T iterations) `ebar_T`, writes the PSF gradient
+// at the convolution centre (gpsf_conv) and, when the two centres differ,
+// the correlation's share at its centre (gpsf_corr; null otherwise), and
+// d loss / d obs into ybar (optional).  Checkpoints every K iterations.
+int rl_backward(const RlGeom &g, const RlBuffers &b, const RlBwdBuffers &w, const float *y, int T, int K,
+                float eps, const float *ebar_T, float *gpsf_conv, float *gpsf_corr, float *ybar, void *stream,
+                PassTimer *timer);
+// Gradients of out = conv(psf, x): gx (optional) and gpsf (optional, at the
+// convolution centre).  Uses w.c, w.t, w.spec_e, w.spec_cbar, w.pbar1, full_*.
+int rl_convolve_backward(const RlGeom &g, const RlBuffers &b, const RlBwdBuffers &w, const float *x,
+                         const float *gout, float *gx, float *gpsf, void *stream, PassTimer *timer);
 // OTF of the normalised PSF `psf_dev` (f64 [kz][ky][kx]) centred at `centre`,
 // scaled by 1/(Pz*Py*Px), into complex [Pz][Py][Hp] (f32).  Work buffers are
 // f64 complex of size kz*ky*Hp and kz*Py*Hp.

@@ -88,6 +88,7 @@ struct ColPass {
     const float2 *H;              // transfer function (kColFull)
     int64_t h_outer, h_row;
     int32_t conj_h;
+    float2 *spec_out;             // kColFull: also store the forward spectrum here (H's layout), or null
     FftPlan plan;
     const float2 *tw;             // e^{-2 pi i m / n}, m < n
     int32_t C, CP;
@@ -128,6 +129,7 @@ __global__ void __launch_bounds__(512, 1) col_pass_kernel(const __grid_constant_
                 int col = c0 + c;
                 if (col < p.ncols) {
                     int outer = col / p.Hx, kx = col - outer * p.Hx;
+                    if (p.spec_out) p.spec_out[outer * p.h_outer + row * p.h_row + kx] = buf[row * CP + c];
                     float2 h = p.H[outer * p.h_outer + row * p.h_row + kx];
                     if (p.conj_h) h.y = -h.y;
                     buf[row * CP + c] = cmul(buf[row * CP + c], h);
@@ -202,6 +204,11 @@ __global__ void __launch_bounds__(N1 * C, 65536 / (N1 * C * 128)) col_fast_kerne
                 v[i] = (ok && srow >= 0) ? src[srow * src_row] : make_float2(0.f, 0.f);
             }
             F::forward(v, t, c, xb, tf);
+            if (p.mode == kColFull && p.spec_out != nullptr && ok) {
+                float2 *so = p.spec_out + (outer * p.h_outer + kx);
+#pragma unroll
+                for (int j = 0; j < N2; ++j) so[F::freq(t, j) * h_row] = v[j];
+            }
             if (p.mode == kColFwd) {
                 float2 *dst = p.dst + (outer * p.dst_outer + kx);
                 if (ok) {
@@ -231,7 +238,9 @@ __global__ void __launch_bounds__(N1 * C, 65536 / (N1 * C * 128)) col_fast_kerne
     }
 }
 
-enum RowKind : int { kRowInit = 0, kRowRatio = 1, kRowUpdate = 2 };
+// Row pass kinds: the RL iteration's three (start from the constant 0.5,
+// ratio, update) and the plain transforms (a real array in, or out).
+enum RowKind : int { kRowInit = 0, kRowRatio = 1, kRowUpdate = 2, kRowRealIn = 3, kRowRealOut = 4 };
 
 // The x axis: C2R, the Richardson-Lucy epilogue on the image columns, the x
 // extension and R2C, for C rows per tile.
@@ -239,8 +248,8 @@ struct RowPass {
     int32_t nrows, X, Px, M, Hx, Hp, hx;
     int32_t pad_mode;
     int32_t kind;                 // RowKind
-    const float *obs;             // [nrows][X]        (ratio)
-    float *est;                   // [nrows][X]        (update)
+    const float *obs;             // [nrows][X]        (ratio; real input of RealIn)
+    float *est;                   // [nrows][X]        (update; real output of RealOut)
     int32_t est_first, last, clip;
     float eps;
     float2 *s1;                   // [nrows][Hp]
@@ -263,7 +272,7 @@ __global__ void __launch_bounds__(512, 1) row_pass_kernel(const __grid_constant_
         const int row0 = tile * C;
         float2 *buf = bufA;  // holds the natural-order real row after C2R
         __syncthreads();
-        if (p.kind != kRowInit) {
+        if (p.kind != kRowInit && p.kind != kRowRealIn) {
             // Half spectrum X[0..M] of each row (lanes along k: coalesced).
             for (int it = tid; it < (M + 1) * C; it += T) {
                 int c = it / (M + 1), k = it - c * (M + 1);
@@ -297,7 +306,7 @@ __global__ void __launch_bounds__(512, 1) row_pass_kernel(const __grid_constant_
         float *bufr = reinterpret_cast<float *>(buf);
         // Epilogue on the image columns; the real sample at position i of the
         // row is component (i & 1) of packed element i >> 1.
-        const bool emit = !(p.kind == kRowUpdate && p.last);
+        const bool emit = !(p.kind == kRowUpdate && p.last) && p.kind != kRowRealOut;
         for (int it = tid; it < p.X * C; it += T) {
             int c = it / p.X, xi = it - c * p.X;
             int row = row0 + c;
@@ -308,6 +317,11 @@ __global__ void __launch_bounds__(512, 1) row_pass_kernel(const __grid_constant_
             float v;
             if (p.kind == kRowInit) {
                 v = 0.5f;
+            } else if (p.kind == kRowRealIn) {
+                v = p.obs[g];
+            } else if (p.kind == kRowRealOut) {
+                v = *slot;
+                p.est[g] = v;
             } else if (p.kind == kRowRatio) {
                 float conv = *slot;
                 float d = fabsf(conv) < p.eps ? p.eps : conv;
@@ -383,13 +397,13 @@ __global__ void __launch_bounds__(N1 * R, 65536 / (N1 * R * 128)) row_fast_kerne
     F::build_tables(tf, ti, p.tw, 2);  // W_M^m = W_Px^{2m}
     __syncthreads();
     const int ntiles = (p.nrows + R - 1) / R;
-    const bool emit_last = !(p.kind == kRowUpdate && p.last);
+    const bool emit_last = !(p.kind == kRowUpdate && p.last) && p.kind != kRowRealOut;
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const int row = tile * R + r;
         const bool ok = row < p.nrows;
         float2 *spec = xb + r * SP;
         float2 v[N2];
-        if (p.kind != kRowInit) {
+        if (p.kind != kRowInit && p.kind != kRowRealIn) {
             const float2 *s1 = p.s1 + (int64_t)(ok ? row : 0) * p.Hp;
             for (int k = t; k <= M; k += N1) spec[k] = ok ? s1[k] : make_float2(0.f, 0.f);
             __syncthreads();
@@ -427,7 +441,7 @@ __global__ void __launch_bounds__(N1 * R, 65536 / (N1 * R * 128)) row_fast_kerne
                     const int xi = 2 * (t + N1 * (i0 + q / 2)) + (q & 1) - p.hx;
                     const bool inside = ok && xi >= 0 && xi < p.X;
                     in[q] = 0.0f;
-                    if (p.kind == kRowRatio && inside) in[q] = obs[gbase + xi];
+                    if ((p.kind == kRowRatio || p.kind == kRowRealIn) && inside) in[q] = obs[gbase + xi];
                     if (p.kind == kRowUpdate && !p.est_first && inside) in[q] = est[gbase + xi];
                 }
 #pragma unroll
@@ -440,6 +454,10 @@ __global__ void __launch_bounds__(N1 * R, 65536 / (N1 * R * 128)) row_fast_kerne
                     if (inside) {
                         if (p.kind == kRowInit) {
                             nv = 0.5f;
+                        } else if (p.kind == kRowRealIn) {
+                            nv = in[q];
+                        } else if (p.kind == kRowRealOut) {
+                            nv = val;
                         } else if (p.kind == kRowRatio) {
                             const float d = fabsf(val) < p.eps ? p.eps : val;
                             nv = in[q] / d;
@@ -451,7 +469,7 @@ __global__ void __launch_bounds__(N1 * R, 65536 / (N1 * R * 128)) row_fast_kerne
                     }
                     if (q & 1) v[i].y = nv; else v[i].x = nv;
                 }
-                if (p.kind == kRowUpdate && ok) {
+                if ((p.kind == kRowUpdate || p.kind == kRowRealOut) && ok) {
 #pragma unroll
                     for (int q = 0; q < 2 * CH; ++q) {
                         const int i = i0 + q / 2;
@@ -703,48 +721,88 @@ int64_t fft_good_length(int64_t n, bool even) {
     }
 }
 
-int rl_launch_iterations(const RlGeom &g, const RlBuffers &b, const float *obs, float *est_out,
-                         int32_t num_iter, int32_t clip, float eps, void *stream, PassTimer *timer) {
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
-    auto timed_col = [&](const ColPass &c) -> int {
+namespace {
+
+// Builds and launches the passes of one problem geometry.
+struct RlRunner {
+    const RlGeom &g;
+    const RlBuffers &b;
+    cudaStream_t s;
+    void *stream;
+    PassTimer *timer;
+    RowPass rp{};
+    FftPlan py_plan{}, pz_plan{};
+    bool ok = true;
+
+    RlRunner(const RlGeom &g_, const RlBuffers &b_, void *stream_, PassTimer *timer_)
+        : g(g_), b(b_), s(static_cast<cudaStream_t>(stream_)), stream(stream_), timer(timer_) {
+        rp.nrows = g.Z * g.Y;
+        rp.X = g.X;
+        rp.Px = g.Px;
+        rp.M = g.Px / 2;
+        rp.Hx = g.Hx;
+        rp.Hp = g.Hp;
+        rp.hx = g.hx;
+        rp.pad_mode = g.mode;
+        rp.s1 = static_cast<float2 *>(b.s1);
+        rp.tw = reinterpret_cast<const float2 *>(b.tw_x);
+        ok = fft_make_plan(rp.M, &rp.plan) && fft_make_plan(g.Py, &py_plan) &&
+             (g.ndim != 3 || fft_make_plan(g.Pz, &pz_plan));
+    }
+
+    int col(const ColPass &c) {
         int kind = c.mode == kColFwd ? kPassRlColFwd : (c.mode == kColFull ? kPassRlColFull : kPassRlColInv);
         if (timer) timer->begin(kind, stream);
         int e = launch_col(c, s);
         if (timer) timer->end(kind, stream);
         return e;
-    };
-    auto timed_row = [&](const RowPass &r) -> int {
+    }
+
+    int row(int kind, const float *in_real, float *out_real, int est_first, int last, int clip, float eps) {
+        RowPass r = rp;
+        r.kind = kind;
+        r.obs = in_real;
+        r.est = out_real;
+        r.est_first = est_first;
+        r.last = last;
+        r.clip = clip;
+        r.eps = eps;
         if (timer) timer->begin(kPassRlRow, stream);
         int e = launch_row(r, s);
         if (timer) timer->end(kPassRlRow, stream);
         return e;
-    };
-    const int nrows = g.Z * g.Y;
-    RowPass rp{};
-    rp.nrows = nrows;
-    rp.X = g.X;
-    rp.Px = g.Px;
-    rp.M = g.Px / 2;
-    rp.Hx = g.Hx;
-    rp.Hp = g.Hp;
-    rp.hx = g.hx;
-    rp.pad_mode = g.mode;
-    rp.obs = obs;
-    rp.est = est_out;
-    rp.clip = clip;
-    rp.eps = eps;
-    rp.s1 = static_cast<float2 *>(b.s1);
-    rp.tw = reinterpret_cast<const float2 *>(b.tw_x);
-    if (!fft_make_plan(rp.M, &rp.plan)) return (int)cudaErrorInvalidValue;
+    }
 
-    FftPlan py_plan, pz_plan;
-    if (!fft_make_plan(g.Py, &py_plan)) return (int)cudaErrorInvalidValue;
-    if (g.ndim == 3 && !fft_make_plan(g.Pz, &pz_plan)) return (int)cudaErrorInvalidValue;
-    float2 *s1 = static_cast<float2 *>(b.s1);
-    float2 *s2 = static_cast<float2 *>(b.s2);
+    ColPass y_forward(float2 *dst, int64_t dst_outer) const {
+        ColPass c{};
+        c.ncols = g.Z * g.Hx; c.Hx = g.Hx;
+        c.src = static_cast<const float2 *>(b.s1); c.src_outer = (int64_t)g.Y * g.Hp; c.src_row = g.Hp;
+        c.n_img = g.Y; c.halo = g.hy;
+        c.dst = dst; c.dst_outer = dst_outer; c.dst_row = g.Hp;
+        c.mode = kColFwd; c.pad_mode = g.mode;
+        c.plan = py_plan; c.tw = reinterpret_cast<const float2 *>(b.tw_y);
+        return c;
+    }
 
-    auto conv_pair = [&](const void *H, int conj) -> int {
-        int e;
+    ColPass y_inverse(const float2 *src, int64_t src_outer) const {
+        ColPass c{};
+        c.ncols = g.Z * g.Hx; c.Hx = g.Hx;
+        c.src = src; c.src_outer = src_outer; c.src_row = g.Hp;
+        c.n_img = g.Py; c.halo = 0;
+        c.dst = static_cast<float2 *>(b.s1); c.dst_outer = (int64_t)g.Y * g.Hp; c.dst_row = g.Hp;
+        c.store_begin = g.hy; c.store_count = g.Y;
+        c.mode = kColInv; c.pad_mode = g.mode;
+        c.plan = py_plan; c.tw = reinterpret_cast<const float2 *>(b.tw_y);
+        return c;
+    }
+
+    // The column passes between the two row passes of one convolution with H
+    // (or correlation with conj(H)): s1 in, s1 out.  spec_out (optional)
+    // receives the full forward spectrum [Pz][Py][Hp] of the row-transformed
+    // input.
+    int pair(const void *H, int conj, float2 *spec_out) {
+        float2 *s1 = static_cast<float2 *>(b.s1);
+        float2 *s2 = static_cast<float2 *>(b.s2);
         if (g.ndim == 2) {
             ColPass c{};
             c.ncols = g.Hx; c.Hx = g.Hx;
@@ -754,17 +812,12 @@ int rl_launch_iterations(const RlGeom &g, const RlBuffers &b, const float *obs, 
             c.store_begin = g.hy; c.store_count = g.Y;
             c.mode = kColFull; c.pad_mode = g.mode;
             c.H = static_cast<const float2 *>(H); c.h_outer = 0; c.h_row = g.Hp; c.conj_h = conj;
+            c.spec_out = spec_out;
             c.plan = py_plan; c.tw = reinterpret_cast<const float2 *>(b.tw_y);
-            return timed_col(c);
+            return col(c);
         }
-        ColPass yf{};
-        yf.ncols = g.Z * g.Hx; yf.Hx = g.Hx;
-        yf.src = s1; yf.src_outer = (int64_t)g.Y * g.Hp; yf.src_row = g.Hp;
-        yf.n_img = g.Y; yf.halo = g.hy;
-        yf.dst = s2; yf.dst_outer = (int64_t)g.Py * g.Hp; yf.dst_row = g.Hp;
-        yf.mode = kColFwd; yf.pad_mode = g.mode;
-        yf.plan = py_plan; yf.tw = reinterpret_cast<const float2 *>(b.tw_y);
-        if ((e = timed_col(yf))) return e;
+        int e;
+        if ((e = col(y_forward(s2, (int64_t)g.Py * g.Hp)))) return e;
         ColPass zp{};
         zp.ncols = g.Py * g.Hx; zp.Hx = g.Hx;
         zp.src = s2; zp.src_outer = g.Hp; zp.src_row = (int64_t)g.Py * g.Hp;
@@ -774,33 +827,272 @@ int rl_launch_iterations(const RlGeom &g, const RlBuffers &b, const float *obs, 
         zp.mode = kColFull; zp.pad_mode = g.mode;
         zp.H = static_cast<const float2 *>(H); zp.h_outer = g.Hp; zp.h_row = (int64_t)g.Py * g.Hp;
         zp.conj_h = conj;
+        zp.spec_out = spec_out;
         zp.plan = pz_plan; zp.tw = reinterpret_cast<const float2 *>(b.tw_z);
-        if ((e = timed_col(zp))) return e;
-        ColPass yi{};
-        yi.ncols = g.Z * g.Hx; yi.Hx = g.Hx;
-        yi.src = s2; yi.src_outer = (int64_t)g.Py * g.Hp; yi.src_row = g.Hp;
-        yi.n_img = g.Py; yi.halo = 0;
-        yi.dst = s1; yi.dst_outer = (int64_t)g.Y * g.Hp; yi.dst_row = g.Hp;
-        yi.store_begin = g.hy; yi.store_count = g.Y;
-        yi.mode = kColInv; yi.pad_mode = g.mode;
-        yi.plan = py_plan; yi.tw = reinterpret_cast<const float2 *>(b.tw_y);
-        return timed_col(yi);
-    };
-
-    int e;
-    rp.kind = kRowInit;
-    if ((e = timed_row(rp))) return e;
-    for (int it = 0; it < num_iter; ++it) {
-        if ((e = conv_pair(b.h_conv, 0))) return e;
-        rp.kind = kRowRatio;
-        if ((e = timed_row(rp))) return e;
-        if ((e = conv_pair(b.h_corr, 1))) return e;
-        rp.kind = kRowUpdate;
-        rp.est_first = it == 0;
-        rp.last = it + 1 == num_iter;
-        if ((e = timed_row(rp))) return e;
+        if ((e = col(zp))) return e;
+        return col(y_inverse(s2, (int64_t)g.Py * g.Hp));
     }
-    return 0;
+
+    // out = H x (conj = 0) or conj(H) x (conj = 1) on the image region.
+    int apply(const void *H, int conj, const float *x, float *out, float2 *spec_out) {
+        int e;
+        if ((e = row(kRowRealIn, x, nullptr, 0, 0, 0, 0.f))) return e;
+        if ((e = pair(H, conj, spec_out))) return e;
+        return row(kRowRealOut, nullptr, out, 0, 0, 0, 0.f);
+    }
+
+    // Unnormalised inverse of a full spectrum [Pz][Py][Hp] onto the image
+    // region (the geometry's Z, Y, X at offsets hz, hy, hx).
+    int spectrum_to_real(const float2 *spec, float *out) {
+        int e;
+        if (g.ndim == 2) {
+            if ((e = col(y_inverse(spec, 0)))) return e;
+        } else {
+            float2 *s2 = static_cast<float2 *>(b.s2);
+            ColPass zi{};
+            zi.ncols = g.Py * g.Hx; zi.Hx = g.Hx;
+            zi.src = spec; zi.src_outer = g.Hp; zi.src_row = (int64_t)g.Py * g.Hp;
+            zi.n_img = g.Pz;
+            zi.dst = s2; zi.dst_outer = g.Hp; zi.dst_row = (int64_t)g.Py * g.Hp;
+            zi.store_begin = g.hz; zi.store_count = g.Z;
+            zi.mode = kColInv; zi.pad_mode = g.mode;
+            zi.plan = pz_plan; zi.tw = reinterpret_cast<const float2 *>(b.tw_z);
+            if ((e = col(zi))) return e;
+            if ((e = col(y_inverse(s2, (int64_t)g.Py * g.Hp)))) return e;
+        }
+        return row(kRowRealOut, nullptr, out, 0, 0, 0, 0.f);
+    }
+
+    // The fused Richardson-Lucy iterations; start from `est_out`'s contents
+    // when from_est, else from the constant 0.5.
+    int iterations(const float *obs, float *est_out, int num_iter, int clip, float eps, bool from_est) {
+        int e;
+        if (from_est) e = row(kRowRealIn, est_out, nullptr, 0, 0, 0, eps);
+        else e = row(kRowInit, nullptr, nullptr, 0, 0, 0, eps);
+        if (e) return e;
+        for (int it = 0; it < num_iter; ++it) {
+            if ((e = pair(b.h_conv, 0, nullptr))) return e;
+            if ((e = row(kRowRatio, obs, nullptr, 0, 0, 0, eps))) return e;
+            if ((e = pair(b.h_corr, 1, nullptr))) return e;
+            if ((e = row(kRowUpdate, nullptr, est_out, it == 0 && !from_est, it + 1 == num_iter, clip, eps))) return e;
+        }
+        return 0;
+    }
+};
+
+// ---- elementwise kernels of the backward pass --------------------------
+
+// r = y / guard(c), guard(c) = eps where |c| < eps (deconvolve.rs:127-131).
+__global__ void rl_ratio_kernel(const float *__restrict__ c, const float *__restrict__ y, float *__restrict__ r,
+                                int64_t n, float eps) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float d = fabsf(c[i]) < eps ? eps : c[i];
+        r[i] = y[i] / d;
+    }
+}
+
+__global__ void rl_mul_kernel(const float *__restrict__ a, const float *__restrict__ b, float *__restrict__ out,
+                              int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = a[i] * b[i];
+}
+
+// cbar = d(loss)/d(c) through r = y / guard(c): zero where the guard holds;
+// ybar += rbar / guard(c) when ybar is given.
+__global__ void rl_cbar_kernel(const float *__restrict__ rbar, const float *__restrict__ y,
+                               const float *__restrict__ c, float *__restrict__ cbar, float *__restrict__ ybar,
+                               int64_t n, float eps) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float ci = c[i];
+        const bool guarded = fabsf(ci) < eps;
+        const float d = guarded ? eps : ci;
+        const float rb = rbar[i];
+        cbar[i] = guarded ? 0.0f : -rb * y[i] / (d * d);
+        if (ybar) ybar[i] += rb / d;
+    }
+}
+
+// ebar = ebar * a + t
+__global__ void rl_ebar_kernel(float *__restrict__ ebar, const float *__restrict__ a, const float *__restrict__ t,
+                               int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        ebar[i] = fmaf(ebar[i], a[i], t[i]);
+}
+
+// acc += x * conj(y) (+ u * conj(v) when u is given), over n complex values.
+__global__ void spec_mac_kernel(float2 *__restrict__ acc, const float2 *__restrict__ x, const float2 *__restrict__ y,
+                                const float2 *__restrict__ u, const float2 *__restrict__ v, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        float2 a = acc[i];
+        const float2 p = x[i], q = y[i];
+        a.x += p.x * q.x + p.y * q.y;
+        a.y += p.y * q.x - p.x * q.y;
+        if (u) {
+            const float2 s = u[i], t = v[i];
+            a.x += s.x * t.x + s.y * t.y;
+            a.y += s.y * t.x - s.x * t.y;
+        }
+        acc[i] = a;
+    }
+}
+
+// out[s] = scale * full[lag(s) mod P], lag = s - centre per axis.
+__global__ void gather_lags_kernel(const float *__restrict__ full, int Pz, int Py, int Px, int kz, int ky, int kx,
+                                   int cz, int cy, int cx, float scale, float *__restrict__ out) {
+    const int n = kz * ky * kx;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int sx = i % kx, sy = (i / kx) % ky, sz = i / (kx * ky);
+        const int z = ((sz - cz) % Pz + Pz) % Pz, y = ((sy - cy) % Py + Py) % Py, x = ((sx - cx) % Px + Px) % Px;
+        out[i] = scale * full[((int64_t)z * Py + y) * Px + x];
+    }
+}
+
+int ew_grid_rl(int64_t n) {
+    const int64_t nb = (n + 255) / 256, cap = (int64_t)sms() * 16;
+    return (int)(nb < cap ? (nb > 0 ? nb : 1) : cap);
+}
+
+// The full-grid geometry (no image region, no halo) used to bring an
+// accumulated cross-spectrum back to lags.
+RlGeom full_geom(const RlGeom &g) {
+    RlGeom gf = g;
+    gf.Z = g.ndim == 3 ? g.Pz : 1;
+    gf.Y = g.Py;
+    gf.X = g.Px;
+    gf.hz = gf.hy = gf.hx = 0;
+    return gf;
+}
+
+}  // namespace
+
+int rl_launch_iterations(const RlGeom &g, const RlBuffers &b, const float *obs, float *est_out,
+                         int32_t num_iter, int32_t clip, float eps, void *stream, PassTimer *timer) {
+    RlRunner run(g, b, stream, timer);
+    if (!run.ok) return (int)cudaErrorInvalidValue;
+    return run.iterations(obs, est_out, num_iter, clip, eps, false);
+}
+
+int rl_apply(const RlGeom &g, const RlBuffers &b, const void *H, int conj, const float *x, float *out,
+             void *stream, PassTimer *timer) {
+    RlRunner run(g, b, stream, timer);
+    if (!run.ok) return (int)cudaErrorInvalidValue;
+    return run.apply(H, conj, x, out, nullptr);
+}
+
+// Reverse mode through the unrolled iterations (clip off), checkpoints every K.
+//   forward:  c = A e;  r = y / guard(c);  a = B r;  e' = e * a
+//     (A: convolution with the PSF centred at k-1-k/2, transfer function
+//      h_conv; B: correlation centred at k/2, conj(h_corr))
+//   backward: abar = ebar * e;  rbar = B^T abar (h_corr);
+//             cbar = -rbar y / d^2 where |c| >= eps, else 0;  ybar += rbar / d;
+//             ebar = ebar * a + A^T cbar (conj(h_conv)).
+//   PSF: dA/dp gives F(cbar) conj(F(e)), dB/dp gives F(r) conj(F(abar)); the
+//   sums over iterations are brought back to lags s - centre by one inverse
+//   transform on the full grid, scaled by 1 / (Pz Py Px).
+int rl_backward(const RlGeom &g, const RlBuffers &b, const RlBwdBuffers &w, const float *y, int T, int K,
+                float eps, const float *ebar_T, float *gpsf_conv, float *gpsf_corr, float *ybar, void *stream,
+                PassTimer *timer) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    RlRunner run(g, b, stream, timer);
+    if (!run.ok) return (int)cudaErrorInvalidValue;
+    const int64_t V = (int64_t)g.Z * g.Y * g.X;
+    const size_t vb = (size_t)V * sizeof(float);
+    const int64_t nspec = (int64_t)g.Pz * g.Py * g.Hp;
+    const int grid = ew_grid_rl(V), sg = ew_grid_rl(nspec);
+    int e;
+    if (K < 1) K = 1;
+    const int nseg = (T + K - 1) / K;
+    float2 *spec_e = reinterpret_cast<float2 *>(w.spec_e), *spec_r = reinterpret_cast<float2 *>(w.spec_r);
+    float2 *spec_abar = reinterpret_cast<float2 *>(w.spec_abar), *spec_cbar = reinterpret_cast<float2 *>(w.spec_cbar);
+    float2 *pbar1 = reinterpret_cast<float2 *>(w.pbar1), *pbar2 = reinterpret_cast<float2 *>(w.pbar2);
+    // Forward, keeping the estimate at the start of every segment.
+    if ((e = launch_fill(w.ckpt, V, 0.5f, stream))) return e;
+    for (int j = 0; j + 1 < nseg; ++j) {
+        float *dst = w.ckpt + (int64_t)(j + 1) * V;
+        if ((e = (int)cudaMemcpyAsync(dst, w.ckpt + (int64_t)j * V, vb, cudaMemcpyDeviceToDevice, s))) return e;
+        if ((e = run.iterations(y, dst, K, 0, eps, true))) return e;
+    }
+    if ((e = (int)cudaMemcpyAsync(w.ebar, ebar_T, vb, cudaMemcpyDeviceToDevice, s))) return e;
+    if ((e = (int)cudaMemsetAsync(pbar1, 0, nspec * sizeof(float2), s))) return e;
+    if (pbar2 && (e = (int)cudaMemsetAsync(pbar2, 0, nspec * sizeof(float2), s))) return e;
+    if (ybar && (e = (int)cudaMemsetAsync(ybar, 0, vb, s))) return e;
+    for (int j = nseg - 1; j >= 0; --j) {
+        const int k0 = j * K, k1 = T < k0 + K ? T : k0 + K;
+        // Recompute the segment's estimates.
+        if ((e = (int)cudaMemcpyAsync(w.seg, w.ckpt + (int64_t)j * V, vb, cudaMemcpyDeviceToDevice, s))) return e;
+        for (int k = k0; k + 1 < k1; ++k) {
+            float *next = w.seg + (int64_t)(k - k0 + 1) * V;
+            if ((e = (int)cudaMemcpyAsync(next, next - V, vb, cudaMemcpyDeviceToDevice, s))) return e;
+            if ((e = run.iterations(y, next, 1, 0, eps, true))) return e;
+        }
+        for (int k = k1 - 1; k >= k0; --k) {
+            const float *ek = w.seg + (int64_t)(k - k0) * V;
+            if ((e = run.apply(b.h_conv, 0, ek, w.c, spec_e))) return e;
+            rl_ratio_kernel<<<grid, 256, 0, s>>>(w.c, y, w.r, V, eps);
+            if ((e = run.apply(b.h_corr, 1, w.r, w.a, spec_r))) return e;
+            rl_mul_kernel<<<grid, 256, 0, s>>>(w.ebar, ek, w.abar, V);
+            if ((e = run.apply(b.h_corr, 0, w.abar, w.rbar, spec_abar))) return e;
+            rl_cbar_kernel<<<grid, 256, 0, s>>>(w.rbar, y, w.c, w.cbar, ybar, V, eps);
+            if ((e = run.apply(b.h_conv, 1, w.cbar, w.t, spec_cbar))) return e;
+            rl_ebar_kernel<<<grid, 256, 0, s>>>(w.ebar, w.a, w.t, V);
+            if (pbar2) {
+                spec_mac_kernel<<<sg, 256, 0, s>>>(pbar1, spec_cbar, spec_e, nullptr, nullptr, nspec);
+                spec_mac_kernel<<<sg, 256, 0, s>>>(pbar2, spec_r, spec_abar, nullptr, nullptr, nspec);
+            } else {
+                spec_mac_kernel<<<sg, 256, 0, s>>>(pbar1, spec_cbar, spec_e, spec_r, spec_abar, nspec);
+            }
+            if ((e = (int)cudaGetLastError())) return e;
+        }
+    }
+    const RlGeom gf = full_geom(g);
+    RlBuffers bf = b;
+    bf.s1 = w.full_s1;
+    bf.s2 = w.full_s2;
+    RlRunner full(gf, bf, stream, timer);
+    if (!full.ok) return (int)cudaErrorInvalidValue;
+    const float scale = 1.0f / ((float)g.Pz * (float)g.Py * (float)g.Px);
+    const int kz = w.kdims[0], ky = w.kdims[1], kx = w.kdims[2];
+    if ((e = full.spectrum_to_real(pbar1, w.full_real))) return e;
+    gather_lags_kernel<<<ew_grid_rl(kz * ky * kx), 256, 0, s>>>(w.full_real, gf.Z, g.Py, g.Px, kz, ky, kx,
+                                                               w.c_conv[0], w.c_conv[1], w.c_conv[2], scale,
+                                                               gpsf_conv);
+    if (pbar2) {
+        if ((e = full.spectrum_to_real(pbar2, w.full_real))) return e;
+        gather_lags_kernel<<<ew_grid_rl(kz * ky * kx), 256, 0, s>>>(w.full_real, gf.Z, g.Py, g.Px, kz, ky, kx,
+                                                                   w.c_corr[0], w.c_corr[1], w.c_corr[2], scale,
+                                                                   gpsf_corr);
+    }
+    return (int)cudaGetLastError();
+}
+
+// Gradients of out = A x (zero padding): gx = A^T gout (conj(h_conv)), and
+// gpsf[s] = sum_y gout[y] x[y - (s - centre)], from F(gout) conj(F(x)).
+int rl_convolve_backward(const RlGeom &g, const RlBuffers &b, const RlBwdBuffers &w, const float *x,
+                         const float *gout, float *gx, float *gpsf, void *stream, PassTimer *timer) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    RlRunner run(g, b, stream, timer);
+    if (!run.ok) return (int)cudaErrorInvalidValue;
+    float2 *spec_x = reinterpret_cast<float2 *>(w.spec_e), *spec_g = reinterpret_cast<float2 *>(w.spec_cbar);
+    float2 *pbar = reinterpret_cast<float2 *>(w.pbar1);
+    int e;
+    if ((e = run.apply(b.h_conv, 1, gout, gx ? gx : w.t, gpsf ? spec_g : nullptr))) return e;
+    if (!gpsf) return 0;
+    if ((e = run.apply(b.h_conv, 0, x, w.c, spec_x))) return e;
+    const int64_t nspec = (int64_t)g.Pz * g.Py * g.Hp;
+    if ((e = (int)cudaMemsetAsync(pbar, 0, nspec * sizeof(float2), s))) return e;
+    spec_mac_kernel<<<ew_grid_rl(nspec), 256, 0, s>>>(pbar, spec_g, spec_x, nullptr, nullptr, nspec);
+    const RlGeom gf = full_geom(g);
+    RlBuffers bf = b;
+    bf.s1 = w.full_s1;
+    bf.s2 = w.full_s2;
+    RlRunner full(gf, bf, stream, timer);
+    if (!full.ok) return (int)cudaErrorInvalidValue;
+    if ((e = full.spectrum_to_real(pbar, w.full_real))) return e;
+    const int kz = w.kdims[0], ky = w.kdims[1], kx = w.kdims[2];
+    gather_lags_kernel<<<ew_grid_rl(kz * ky * kx), 256, 0, s>>>(
+        w.full_real, gf.Z, g.Py, g.Px, kz, ky, kx, w.c_conv[0], w.c_conv[1], w.c_conv[2],
+        1.0f / ((float)g.Pz * (float)g.Py * (float)g.Px), gpsf);
+    return (int)cudaGetLastError();
 }
 
 int rl_launch_otf(const RlGeom &g, const double *psf_dev, const int32_t kdims[3],

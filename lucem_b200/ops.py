@@ -27,7 +27,8 @@ __all__ = [
     "pad_index", "gaussian_blur", "gaussian_1d", "correlate_1d", "convolve_1d",
     "difference_of_gaussians", "gaussian_laplace", "gaussian_grad_mag", "unsharp_mask",
     "gaussian_family", "schedule", "gaussian_family_tiles", "richardson_lucy", "rl_grid",
-    "gaussian_halo", "op_halo",
+    "gaussian_halo", "op_halo", "gaussian_blur_adjoint", "richardson_lucy_backward", "fft_convolve",
+    "fft_convolve_backward",
 ]
 
 
@@ -283,6 +284,23 @@ def gaussian_blur(x: torch.Tensor, sigmas, *, orders=None, mode="reflect", cval=
     return out
 
 
+def gaussian_blur_adjoint(g: torch.Tensor, sigmas, *, orders=None, mode="reflect", truncate=4.0, radii=None,
+                          axes=None, channel_axis=None, input_scale=1.0, out: Optional[torch.Tensor] = None,
+                          workspace: Optional[Workspace] = None) -> torch.Tensor:
+    """The transpose of gaussian_blur's linear map with the same arguments,
+    applied to `g` (f32): the input gradient of gaussian_blur given the output
+    gradient.  No counterpart in the reference."""
+    ctx, ws = _ctx_ws(g, workspace)
+    out = _out_like(g, out)
+    keep = []
+    s = _gaussian_settings(orders, mode, 0.0, truncate, radii, axes, channel_axis, input_scale, keep)
+    sig, ns = _doubles(sigmas)
+    ti, to = _tensor(g, "grad_out"), _tensor(out, "grad_in")
+    N.check(N.lib().lucem_gaussian_blur_adjoint(ctx.handle, C.byref(ti), sig, ns, C.byref(s), C.byref(to),
+                                                ws.handle, _stream(g)))
+    return out
+
+
 def gaussian_1d(x: torch.Tensor, sigma: float, *, axis=-1, order=0, mode="reflect", cval=0.0, truncate=4.0,
                 radius=None, out: Optional[torch.Tensor] = None) -> torch.Tensor:
     """gaussian_1d / gaussian_1d_into (crates/lucem-ops/src/filter/gaussian.rs:66-130)."""
@@ -508,13 +526,7 @@ def rl_grid(dims, kdims, mode="reflect", grid=None):
     return tuple(int(v) for v in g[:nd])
 
 
-def richardson_lucy(x: torch.Tensor, psf: torch.Tensor, *, num_iter: int = 30, clip: bool = True,
-                    filter_epsilon: Optional[float] = None, mode="reflect", grid=None,
-                    out: Optional[torch.Tensor] = None, workspace: Optional[Workspace] = None) -> torch.Tensor:
-    """richardson_lucy (crates/lucem-ops/src/restore/deconvolve.rs:45-162) for
-    2-D and 3-D inputs, on FFT convolution.  `grid` overrides the FFT lengths."""
-    ctx, ws = _ctx_ws(x, workspace)
-    out = _out_like(x, out)
+def _rl_settings(num_iter, clip, filter_epsilon, mode, grid):
     s = N.RlSettings()
     N.lib().lucem_rl_settings_default(C.byref(s))
     s.num_iter = int(num_iter)
@@ -526,7 +538,73 @@ def richardson_lucy(x: torch.Tensor, psf: torch.Tensor, *, num_iter: int = 30, c
     if grid is not None:
         for i, g in enumerate(grid):
             s.grid[i] = int(g)
+    return s
+
+
+def _grid_arg(grid):
+    if grid is None:
+        return None
+    g = list(grid)
+    return (C.c_int64 * 3)(*(g + [0] * (3 - len(g))))
+
+
+def richardson_lucy(x: torch.Tensor, psf: torch.Tensor, *, num_iter: int = 30, clip: bool = True,
+                    filter_epsilon: Optional[float] = None, mode="reflect", grid=None,
+                    out: Optional[torch.Tensor] = None, workspace: Optional[Workspace] = None) -> torch.Tensor:
+    """richardson_lucy (crates/lucem-ops/src/restore/deconvolve.rs:45-162) for
+    2-D and 3-D inputs, on FFT convolution.  `grid` overrides the FFT lengths."""
+    ctx, ws = _ctx_ws(x, workspace)
+    out = _out_like(x, out)
+    s = _rl_settings(num_iter, clip, filter_epsilon, mode, grid)
     ti, tp, to = _tensor(x, "input"), _tensor(psf, "psf"), _tensor(out, "output")
     N.check(N.lib().lucem_richardson_lucy(ctx.handle, C.byref(ti), C.byref(tp), C.byref(s), C.byref(to),
                                           ws.handle, _stream(x)))
     return out
+
+
+def richardson_lucy_backward(x: torch.Tensor, psf: torch.Tensor, grad_out: torch.Tensor, *, num_iter: int = 30,
+                             filter_epsilon: Optional[float] = None, grid=None, checkpoint_every: int = 5,
+                             need_psf: bool = True, need_input: bool = True,
+                             workspace: Optional[Workspace] = None):
+    """(d loss / d psf, d loss / d x) of richardson_lucy(x, psf, clip=False,
+    mode="constant", ...) given d loss / d (its output); either is None when
+    not asked for.  The iterations are recomputed from checkpoints kept every
+    `checkpoint_every` iterations.  No counterpart in the reference."""
+    ctx, ws = _ctx_ws(x, workspace)
+    s = _rl_settings(num_iter, False, filter_epsilon, "constant", grid)
+    gp = torch.empty(psf.shape, dtype=torch.float32, device=x.device) if need_psf else None
+    gx = torch.empty(x.shape, dtype=torch.float32, device=x.device) if need_input else None
+    ti, tp, tg = _tensor(x, "input"), _tensor(psf, "psf"), _tensor(grad_out, "grad_out")
+    tgp = C.byref(_tensor(gp, "grad_psf")) if gp is not None else None
+    tgx = C.byref(_tensor(gx, "grad_in")) if gx is not None else None
+    N.check(N.lib().lucem_richardson_lucy_backward(ctx.handle, C.byref(ti), C.byref(tp), C.byref(s), C.byref(tg),
+                                                   int(checkpoint_every), tgp, tgx, ws.handle, _stream(x)))
+    return gp, gx
+
+
+def fft_convolve(x: torch.Tensor, psf: torch.Tensor, *, grid=None, out: Optional[torch.Tensor] = None,
+                 workspace: Optional[Workspace] = None) -> torch.Tensor:
+    """The forward model of richardson_lucy (deconvolve.rs:120, correlation
+    with the flipped PSF): convolution centred at k-1-k//2 per axis, zero
+    padding, the PSF as given, on the FFT grid."""
+    ctx, ws = _ctx_ws(x, workspace)
+    out = _out_like(x, out)
+    ti, tp, to = _tensor(x, "x"), _tensor(psf, "psf"), _tensor(out, "output")
+    N.check(N.lib().lucem_fft_convolve(ctx.handle, C.byref(ti), C.byref(tp), PadMode.CONSTANT, _grid_arg(grid),
+                                       C.byref(to), ws.handle, _stream(x)))
+    return out
+
+
+def fft_convolve_backward(x: torch.Tensor, psf: torch.Tensor, grad_out: torch.Tensor, *, grid=None,
+                          need_psf: bool = True, need_input: bool = True,
+                          workspace: Optional[Workspace] = None):
+    """(grad_psf, grad_x) of fft_convolve."""
+    ctx, ws = _ctx_ws(x, workspace)
+    gp = torch.empty(psf.shape, dtype=torch.float32, device=x.device) if need_psf else None
+    gx = torch.empty(x.shape, dtype=torch.float32, device=x.device) if need_input else None
+    ti, tp, tg = _tensor(x, "x"), _tensor(psf, "psf"), _tensor(grad_out, "grad_out")
+    tgp = C.byref(_tensor(gp, "grad_psf")) if gp is not None else None
+    tgx = C.byref(_tensor(gx, "grad_x")) if gx is not None else None
+    N.check(N.lib().lucem_fft_convolve_backward(ctx.handle, C.byref(ti), C.byref(tp), PadMode.CONSTANT,
+                                                _grid_arg(grid), C.byref(tg), tgx, tgp, ws.handle, _stream(x)))
+    return gp, gx
