@@ -307,6 +307,53 @@ lucem_status lucem_fft_convolve_backward(lucem_ctx *ctx, const lucem_tensor *x, 
                                          int32_t mode, const int64_t *grid, const lucem_tensor *grad_out,
                                          lucem_tensor *grad_x, lucem_tensor *grad_psf, lucem_workspace *ws,
                                          void *stream);
+/* ---- Batched 2-D Richardson-Lucy --------------------------------------
+ * Many 2-D problems of different sizes and PSFs (the reference runs
+ * richardson_lucy once per image, crates/lucem-ops/src/restore/
+ * deconvolve.rs:45-149).  A plan is built once: each problem gets an FFT
+ * grid from a short list of lengths (m * 2^k, m in {1,3,5,7,9,15,21,25,27},
+ * the cheapest by the autotuned or default pass costs), its transfer
+ * functions and spectrum, and the problems are grouped by length.  A run then
+ * issues, per pass of every iteration, one launch per length group (each
+ * launch walks the work list of all its problems), and nothing else: no
+ * allocation, synchronisation or host copy, so a run can be captured in a
+ * CUDA graph.  per_problem = 1 runs the same kernels one problem at a time
+ * (the per-image baseline).  Arrays obs, psfs and outs hold n tensors each;
+ * the plan keeps their device pointers (they must stay valid).  create
+ * synchronises `stream` and allocates the plan's device memory. */
+typedef struct lucem_rl_batch lucem_rl_batch;
+lucem_status lucem_rl_batch_create(lucem_ctx *ctx, int32_t n, const lucem_tensor *obs, const lucem_tensor *psfs,
+                                   const lucem_rl_settings *settings, lucem_tensor *outs, lucem_workspace *ws,
+                                   void *stream, lucem_rl_batch **out);
+lucem_status lucem_rl_batch_run(lucem_rl_batch *batch, int32_t per_problem, lucem_workspace *timing_ws,
+                                void *stream);
+/* grids: 2 per problem (Py, Px); launches per row / column pass. */
+lucem_status lucem_rl_batch_info(const lucem_rl_batch *batch, int64_t *grids, int32_t *n_row_launches,
+                                 int32_t *n_col_launches);
+void lucem_rl_batch_destroy(lucem_rl_batch *batch);
+
+/* ---- Autotuning of FFT lengths (no counterpart in the reference) -------
+ * Measures the column pass (kind 0) and row pass (kind 1) at each length
+ * (2/3/5/7-smooth) on scratch data and records ns per transformed element in
+ * the context; batched plans then choose grid lengths by these costs.  The
+ * table can be saved to and loaded from a text file. */
+lucem_status lucem_autotune_fft(lucem_ctx *ctx, const int64_t *lengths, int32_t n, lucem_workspace *ws,
+                                void *stream);
+lucem_status lucem_autotune_query(lucem_ctx *ctx, int32_t kind, int64_t length, double *ns_per_element);
+lucem_status lucem_autotune_save(lucem_ctx *ctx, const char *path);
+lucem_status lucem_autotune_load(lucem_ctx *ctx, const char *path);
+
+/* ---- CUDA graphs of launch-only calls ------------------------------------
+ * begin/end bracket a capture of `stream` (not the legacy default stream);
+ * only calls that launch without synchronising or allocating may run inside:
+ * lucem_rl_batch_run, and the filter entry points once a first call with the
+ * same arguments has cached their taps and work lists. */
+typedef struct lucem_graph lucem_graph;
+lucem_status lucem_graph_begin(void *stream);
+lucem_status lucem_graph_end(void *stream, lucem_graph **out);
+lucem_status lucem_graph_launch(lucem_graph *graph, void *stream);
+void lucem_graph_destroy(lucem_graph *graph);
+
 /* The grid lucem_richardson_lucy would use (host only). */
 lucem_status lucem_rl_grid(const int64_t *dims, const int64_t *kdims, int32_t ndim, int32_t mode,
                            const int64_t *requested, int64_t *grid_out);

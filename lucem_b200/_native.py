@@ -106,6 +106,18 @@ SIGNATURES = {
     "lucem_richardson_lucy_backward": (I32, [P, TP, TP, C.POINTER(RlSettings), TP, I32, TP, TP, P, P]),
     "lucem_fft_convolve": (I32, [P, TP, TP, I32, I64P, TP, P, P]),
     "lucem_fft_convolve_backward": (I32, [P, TP, TP, I32, I64P, TP, TP, TP, P, P]),
+    "lucem_rl_batch_create": (I32, [P, I32, TP, TP, C.POINTER(RlSettings), TP, P, P, C.POINTER(P)]),
+    "lucem_rl_batch_run": (I32, [P, I32, P, P]),
+    "lucem_rl_batch_info": (I32, [P, I64P, C.POINTER(I32), C.POINTER(I32)]),
+    "lucem_rl_batch_destroy": (None, [P]),
+    "lucem_autotune_fft": (I32, [P, I64P, I32, P, P]),
+    "lucem_autotune_query": (I32, [P, I32, I64, C.POINTER(C.c_double)]),
+    "lucem_autotune_save": (I32, [P, C.c_char_p]),
+    "lucem_autotune_load": (I32, [P, C.c_char_p]),
+    "lucem_graph_begin": (I32, [P]),
+    "lucem_graph_end": (I32, [P, C.POINTER(P)]),
+    "lucem_graph_launch": (I32, [P, P]),
+    "lucem_graph_destroy": (None, [P]),
     "lucem_fft_good_length": (I64, [I64, I32]),
 }
 

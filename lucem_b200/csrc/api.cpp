@@ -12,6 +12,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "internal.h"
@@ -224,6 +225,8 @@ struct lucem_ctx {
     std::mutex mu;
     // Constant cache: key -> device buffer (crates/lucem-core/src/memory/cache.rs:19-44).
     std::map<std::string, void *> cache;
+    // Autotuned FFT pass costs: (kind 0 column / 1 row, length) -> ns per element.
+    std::map<std::pair<int, int64_t>, double> tune;
     void *get_or_upload(const std::string &key, const void *host, size_t bytes, int *err) {
         std::lock_guard<std::mutex> lk(mu);
         auto it = cache.find(key);
@@ -1527,8 +1530,59 @@ bool good_factors(int64_t n) {
     return n == 1;
 }
 
+// ---- batched 2-D Richardson-Lucy, FFT-length autotuning -------------------
+
+// Relative cost per transformed element of one pass at length n (kind 0:
+// column pass, 1: row pass): the autotuned figure when one was measured for
+// this context (ctx may be null), else 1 for the register-resident
+// power-of-two kernels and, for the shared-memory Stockham kernels (other
+// 2/3/5/7-smooth lengths), the ratio measured on B200: 5 (columns), 2.7 (rows).
+double length_cost(lucem_ctx *ctx, int kind, int64_t n) {
+    auto fast = [kind](int64_t m) {
+        const bool pow2 = (m & (m - 1)) == 0;
+        return kind == 0 ? (pow2 && m >= 64 && m <= 2048) : (pow2 && m >= 128 && m <= 2048);
+    };
+    const double slow = kind == 0 ? 5.0 : 2.7;
+    if (!ctx) return fast(n) ? 1.0 : slow;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    auto it = ctx->tune.find({kind, n});
+    if (it != ctx->tune.end()) return it->second;
+    // Untuned length: the default ratio, in the units of the tuned entries of
+    // this kind when there are any (their mean over the fast lengths).
+    double base = 0.0;
+    int cnt = 0;
+    for (auto &kv : ctx->tune)
+        if (kv.first.first == kind && fast(kv.first.second)) {
+            base += kv.second;
+            ++cnt;
+        }
+    base = cnt ? base / cnt : 1.0;
+    return base * (fast(n) ? 1.0 : slow);
+}
+
+// The grid length chosen for a need: the cheapest of m * 2^k >= need (m in a
+// short list, so that uneven problems of a batch fall into few length groups,
+// one launch each) by length * cost.
+int64_t batch_length(lucem_ctx *ctx, int kind, int64_t need) {
+    static const int ms[] = {1, 3, 5, 7, 9, 15, 21, 25, 27};
+    int64_t best = 0;
+    double best_cost = 0.0;
+    for (int m : ms) {
+        int64_t n = m;
+        while (n < need || (kind == 1 && (n & 1))) n *= 2;
+        if (n > 2 * need + 64) continue;
+        if (kind == 1 && (n / 2) < 2) continue;
+        const double c = (double)n * length_cost(ctx, kind, n);
+        if (best == 0 || c < best_cost || (c == best_cost && n < best)) {
+            best = n;
+            best_cost = c;
+        }
+    }
+    return best > 0 ? best : fft_good_length(need, kind == 1);
+}
+
 lucem_status rl_grid_impl(const int64_t *dims, const int64_t *kdims, int ndim, int mode,
-                          const int64_t *requested, int64_t *grid) {
+                          const int64_t *requested, int64_t *grid, lucem_ctx *ctx = nullptr) {
     for (int d = 0; d < ndim; ++d) {
         bool x_axis = d == ndim - 1;
         int64_t need = rl_min_length(dims[d], kdims[d], mode);
@@ -1544,7 +1598,7 @@ lucem_status rl_grid_impl(const int64_t *dims, const int64_t *kdims, int ndim, i
                             d, (long long)r, x_axis ? " and be even" : "");
             grid[d] = r;
         } else {
-            grid[d] = fft_good_length(need, x_axis);
+            grid[d] = batch_length(ctx, x_axis ? 1 : 0, need);
         }
         if (grid[d] > 16384)
             return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `grid`: axis %d length %lld exceeds 16384",
@@ -1643,7 +1697,8 @@ lucem_status rl_prepare(lucem_ctx *ctx, const lucem_tensor *in, const lucem_tens
     }
     int64_t req[3] = {0, 0, 0};
     for (int d = 0; d < nd; ++d) req[3 - nd + d] = grid_req ? grid_req[d] : 0;
-    if ((st = rl_grid_impl(dims + (3 - nd), su->kd + (3 - nd), nd, mode, req + (3 - nd), su->grid + (3 - nd))))
+    if ((st = rl_grid_impl(dims + (3 - nd), su->kd + (3 - nd), nd, mode, req + (3 - nd), su->grid + (3 - nd),
+                           ctx)))
         return st;
     const int64_t *kd = su->kd, *grid = su->grid;
     RlGeom &g = su->g;
@@ -1813,6 +1868,58 @@ lucem_status psf_grad_finish(const RlSetup &su, const float *gconv, const float 
 
 }  // namespace
 
+// An instantiated capture.
+struct lucem_graph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+// A planned batch: geometry, transfer functions, spectra and the launch
+// groups, all owned by the plan (allocated once at creation).
+struct lucem_rl_batch {
+    int device = 0;
+    std::vector<void *> mem;
+    std::vector<RlBatchGroup> rows, cols;      // problems grouped by length
+    std::vector<RlBatchGroup> rows1, cols1;    // one group per problem
+    std::vector<int64_t> grids;                // (Py, Px) per problem
+    int32_t num_iter = 0, clip = 0, mode = 0;
+    float eps = 0.f;
+    ~lucem_rl_batch() {
+        for (void *p : mem) cudaFree(p);
+    }
+    void *alloc(size_t bytes, int *err) {
+        void *p = nullptr;
+        *err = (int)cudaMalloc(&p, bytes > 0 ? bytes : 16);
+        if (*err) return nullptr;
+        mem.push_back(p);
+        return p;
+    }
+};
+
+namespace {
+
+// Uploads one group's items and records the group.
+template <class Item>
+lucem_status upload_group(lucem_rl_batch *b, int32_t n, std::vector<Item> &items, int tile_unit,
+                          const float2_ *tw, std::vector<RlBatchGroup> *out) {
+    int32_t t = 0;
+    for (auto &it : items) {
+        it.tile_begin = t;
+        int32_t units = 0;
+        if constexpr (std::is_same<Item, RlColItem>::value) units = it.ncols;
+        else units = it.nrows;
+        t += (units + tile_unit - 1) / tile_unit;
+    }
+    int err = 0;
+    void *d = b->alloc(items.size() * sizeof(Item), &err);
+    if (!d) return cuda_fail(err, "batch plan allocation");
+    CUDA_TRY(cudaMemcpy(d, items.data(), items.size() * sizeof(Item), cudaMemcpyHostToDevice), "batch plan upload");
+    out->push_back(RlBatchGroup{n, d, (int32_t)items.size(), t, tw});
+    return ok();
+}
+
+}  // namespace
+
 extern "C" {
 
 lucem_status lucem_rl_grid(const int64_t *dims, const int64_t *kdims, int32_t ndim, int32_t mode,
@@ -1947,6 +2054,307 @@ lucem_status lucem_fft_convolve_backward(lucem_ctx *ctx, const lucem_tensor *x, 
     if (e) return cuda_fail(e, "fft_convolve_backward launch");
     if (grad_psf) return psf_grad_finish(su, static_cast<float *>(gp), nullptr, false, grad_psf, stream);
     return ok();
+}
+
+lucem_status lucem_rl_batch_create(lucem_ctx *ctx, int32_t n, const lucem_tensor *obs, const lucem_tensor *psfs,
+                                   const lucem_rl_settings *settings, lucem_tensor *outs, lucem_workspace *ws,
+                                   void *stream, lucem_rl_batch **out) {
+    if (!ctx) return fail(LUCEM_ERR_INVALID_HANDLE, "null context");
+    if (!ws) return fail(LUCEM_ERR_INVALID_HANDLE, "a workspace is required");
+    if (!out) return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `out`: null");
+    *out = nullptr;
+    if (n < 1 || !obs || !psfs || !outs)
+        return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `n`: a batch needs at least one problem");
+    lucem_rl_settings def;
+    lucem_rl_settings_default(&def);
+    const lucem_rl_settings *s = settings ? settings : &def;
+    lucem_status st;
+    for (int i = 0; i < n; ++i) {
+        if ((st = rl_check(&obs[i], &psfs[i], &outs[i], s->num_iter, s->mode, "richardson_lucy_batch"))) return st;
+        if (obs[i].ndim != 2)
+            return fail(LUCEM_ERR_INVALID_DIMENSION, "richardson_lucy_batch takes 2-D problems, problem %d is %d-D",
+                        i, obs[i].ndim);
+        if (numel(&obs[i]) == 0)
+            return fail(LUCEM_ERR_EMPTY_INPUT, "richardson_lucy_batch: problem %d is empty", i);
+    }
+    cudaStream_t cs = static_cast<cudaStream_t>(stream);
+    std::unique_ptr<lucem_rl_batch> b(new lucem_rl_batch());
+    b->device = ctx->device;
+    b->num_iter = s->num_iter;
+    b->clip = s->clip;
+    b->mode = s->mode;
+    b->eps = rl_eps(s);
+    const int mode = s->mode;
+
+    // PSFs to the host (one synchronisation for the batch), normalised in f64.
+    std::vector<std::vector<float>> hp((size_t)n);
+    for (int i = 0; i < n; ++i) {
+        hp[(size_t)i].resize((size_t)numel(&psfs[i]));
+        CUDA_TRY(cudaMemcpyAsync(hp[(size_t)i].data(), psfs[i].data, hp[(size_t)i].size() * sizeof(float),
+                                 cudaMemcpyDeviceToHost, cs), "psf download");
+    }
+    CUDA_TRY(cudaStreamSynchronize(cs), "psf download");
+
+    std::map<int64_t, std::vector<RlRowItem>> row_groups;
+    std::map<int64_t, std::vector<RlColItem>> col_groups;
+    std::map<int64_t, const float2_ *> tw32;
+    std::vector<RlRowItem> rows_one;
+    std::vector<RlColItem> cols_one;
+    std::vector<int64_t> px_one, py_one;
+    int err = 0;
+    for (int i = 0; i < n; ++i) {
+        const int64_t Y = obs[i].dims[0], X = obs[i].dims[1], ky = psfs[i].dims[0], kx = psfs[i].dims[1];
+        const int64_t Py = batch_length(ctx, 0, rl_min_length(Y, ky, mode));
+        const int64_t Px = batch_length(ctx, 1, rl_min_length(X, kx, mode));
+        b->grids.push_back(Py);
+        b->grids.push_back(Px);
+        RlGeom g{};
+        g.ndim = 2;
+        g.Z = 1; g.Y = (int32_t)Y; g.X = (int32_t)X;
+        g.Pz = 1; g.Py = (int32_t)Py; g.Px = (int32_t)Px;
+        g.hz = 0; g.hy = (int32_t)rl_halo(ky, mode); g.hx = (int32_t)rl_halo(kx, mode);
+        g.Hx = g.Px / 2 + 1;
+        g.Hp = (g.Hx + 15) & ~15;
+        g.mode = mode;
+        const float2_ *t32[3];
+        const double *t64[3];
+        if ((st = twiddles(ctx, 1, &t32[0], &t64[0])) || (st = twiddles(ctx, Py, &t32[1], &t64[1])) ||
+            (st = twiddles(ctx, Px, &t32[2], &t64[2])))
+            return st;
+        tw32[Py] = t32[1];
+        tw32[Px] = t32[2];
+        // Transfer functions (deconvolve.rs:77-88 normalisation; centres as
+        // lucem_richardson_lucy).
+        const std::vector<float> &h = hp[(size_t)i];
+        double sum = 0.0;
+        for (float v : h) sum += (double)v;
+        const double norm = std::fabs(sum) > 1e-12 ? 1.0 / sum : 1.0;
+        std::vector<double> pn(h.size());
+        for (size_t j = 0; j < h.size(); ++j) pn[j] = (double)h[j] * norm;
+        const int32_t kdi[3] = {1, (int32_t)ky, (int32_t)kx};
+        const int32_t c_conv[3] = {0, (int32_t)(ky - 1 - ky / 2), (int32_t)(kx - 1 - kx / 2)};
+        const int32_t c_corr[3] = {0, (int32_t)(ky / 2), (int32_t)(kx / 2)};
+        const bool same = c_conv[1] == c_corr[1] && c_conv[2] == c_corr[2];
+        const size_t hbytes = (size_t)Py * g.Hp * sizeof(float2_);
+        void *h_conv = b->alloc(hbytes, &err);
+        void *h_corr = same ? h_conv : b->alloc(hbytes, &err);
+        void *s1 = b->alloc((size_t)Y * g.Hp * sizeof(float2_), &err);
+        if (!h_conv || !h_corr || !s1) return cuda_fail(err, "batch plan allocation");
+        void *psf64 = nullptr, *wa = nullptr, *wb = nullptr;
+        if ((st = ws->get("rl_psf64", pn.size() * sizeof(double), &psf64)) ||
+            (st = ws->get("rl_otf_a", (size_t)ky * g.Hp * 16, &wa)) ||
+            (st = ws->get("rl_otf_b", (size_t)Py * g.Hp * 16, &wb)))
+            return st;
+        CUDA_TRY(cudaMemcpyAsync(psf64, pn.data(), pn.size() * sizeof(double), cudaMemcpyHostToDevice, cs),
+                 "psf upload");
+        int e = rl_launch_otf(g, static_cast<const double *>(psf64), kdi, c_conv, static_cast<double *>(wa),
+                              static_cast<double *>(wb), h_conv, t64[2], t64[1], t64[0], stream);
+        if (!e && !same)
+            e = rl_launch_otf(g, static_cast<const double *>(psf64), kdi, c_corr, static_cast<double *>(wa),
+                              static_cast<double *>(wb), h_corr, t64[2], t64[1], t64[0], stream);
+        if (e) return cuda_fail(e, "transfer function launch");
+        // The scratch and the host copy are reused by the next problem.
+        CUDA_TRY(cudaStreamSynchronize(cs), "transfer function");
+
+        RlRowItem r{};
+        r.s1 = static_cast<float2_ *>(s1);
+        r.obs = static_cast<const float *>(obs[i].data);
+        r.est = static_cast<float *>(outs[i].data);
+        r.nrows = (int32_t)Y;
+        r.X = (int32_t)X;
+        r.hx = g.hx;
+        RlColItem c{};
+        c.src = static_cast<const float2_ *>(s1);
+        c.dst = static_cast<float2_ *>(s1);
+        c.H = static_cast<const float2_ *>(h_conv);
+        c.H2 = static_cast<const float2_ *>(h_corr);
+        c.src_row = c.dst_row = c.h_row = g.Hp;
+        c.ncols = g.Hx;
+        c.Hx = g.Hx;
+        c.n_img = (int32_t)Y;
+        c.halo = g.hy;
+        c.store_begin = g.hy;
+        c.store_count = (int32_t)Y;
+        row_groups[Px].push_back(r);
+        col_groups[Py].push_back(c);
+        rows_one.push_back(r);
+        cols_one.push_back(c);
+        px_one.push_back(Px);
+        py_one.push_back(Py);
+    }
+    for (auto &kv : row_groups)
+        if ((st = upload_group(b.get(), (int32_t)kv.first, kv.second, row_tile_rows((int)kv.first / 2),
+                               tw32[kv.first], &b->rows)))
+            return st;
+    for (auto &kv : col_groups)
+        if ((st = upload_group(b.get(), (int32_t)kv.first, kv.second, col_tile_width((int)kv.first),
+                               tw32[kv.first], &b->cols)))
+            return st;
+    for (int i = 0; i < n; ++i) {
+        std::vector<RlRowItem> r1{rows_one[(size_t)i]};
+        std::vector<RlColItem> c1{cols_one[(size_t)i]};
+        if ((st = upload_group(b.get(), (int32_t)px_one[(size_t)i], r1, row_tile_rows((int)px_one[(size_t)i] / 2),
+                               tw32[px_one[(size_t)i]], &b->rows1)) ||
+            (st = upload_group(b.get(), (int32_t)py_one[(size_t)i], c1, col_tile_width((int)py_one[(size_t)i]),
+                               tw32[py_one[(size_t)i]], &b->cols1)))
+            return st;
+    }
+    *out = b.release();
+    return ok();
+}
+
+lucem_status lucem_rl_batch_run(lucem_rl_batch *b, int32_t per_problem, lucem_workspace *ws, void *stream) {
+    if (!b) return fail(LUCEM_ERR_INVALID_HANDLE, "null batch plan");
+    TimerScope timer_scope(ws);
+    PassTimer *t = ws ? ws->t() : nullptr;
+    if (!per_problem) {
+        RlBatchLaunch L{b->mode, b->rows.data(), (int32_t)b->rows.size(), b->cols.data(), (int32_t)b->cols.size()};
+        int e = rl_batch_iterations(L, b->num_iter, b->clip, b->eps, stream, t);
+        return e ? cuda_fail(e, "richardson_lucy_batch launch") : ok();
+    }
+    for (size_t i = 0; i < b->rows1.size(); ++i) {
+        RlBatchLaunch L{b->mode, &b->rows1[i], 1, &b->cols1[i], 1};
+        int e = rl_batch_iterations(L, b->num_iter, b->clip, b->eps, stream, t);
+        if (e) return cuda_fail(e, "richardson_lucy_batch launch");
+    }
+    return ok();
+}
+
+lucem_status lucem_rl_batch_info(const lucem_rl_batch *b, int64_t *grids, int32_t *n_row_launches,
+                                 int32_t *n_col_launches) {
+    if (!b) return fail(LUCEM_ERR_INVALID_HANDLE, "null batch plan");
+    if (grids) std::copy(b->grids.begin(), b->grids.end(), grids);
+    if (n_row_launches) *n_row_launches = (int32_t)b->rows.size();
+    if (n_col_launches) *n_col_launches = (int32_t)b->cols.size();
+    return ok();
+}
+
+void lucem_rl_batch_destroy(lucem_rl_batch *b) { delete b; }
+
+lucem_status lucem_autotune_fft(lucem_ctx *ctx, const int64_t *lengths, int32_t n, lucem_workspace *ws,
+                                void *stream) {
+    if (!ctx) return fail(LUCEM_ERR_INVALID_HANDLE, "null context");
+    if (!ws) return fail(LUCEM_ERR_INVALID_HANDLE, "a workspace is required");
+    if (n < 0 || (n > 0 && !lengths)) return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `lengths`");
+    lucem_status st;
+    const int64_t elems = (int64_t)1 << 24;
+    for (int i = 0; i < n; ++i) {
+        const int64_t L = lengths[i];
+        if (L < 32 || L > 16384 || !good_factors(L))
+            return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `lengths`: %lld does not factor into 2, 3, 5, 7",
+                        (long long)L);
+        const float2_ *t32;
+        const double *t64;
+        if ((st = twiddles(ctx, L, &t32, &t64))) return st;
+        for (int kind = 0; kind < 2; ++kind) {
+            if (kind == 1 && (L & 1)) continue;
+            const int lines = (int)std::max<int64_t>(64, (elems / L) & ~(int64_t)15);
+            void *a = nullptr, *bb = nullptr;
+            const size_t abytes = (size_t)lines * (size_t)L * sizeof(float2_);
+            if ((st = ws->get("tune_a", abytes, &a)) || (st = ws->get("tune_b", (size_t)lines * L * sizeof(float), &bb)))
+                return st;
+            CUDA_TRY(cudaMemsetAsync(a, 0, abytes, static_cast<cudaStream_t>(stream)), "tune buffers");
+            CUDA_TRY(cudaMemsetAsync(bb, 0, (size_t)lines * L * sizeof(float), static_cast<cudaStream_t>(stream)),
+                     "tune buffers");
+            float ms = 0.f;
+            int e = rl_tune_pass(kind, (int)L, lines, a, bb, t32, 3, stream, &ms);
+            if (e) return cuda_fail(e, "autotune launch");
+            // ns per transformed element, relative to nothing: the cost model
+            // only compares lengths of one kind.
+            const double per = (double)ms * 1e6 / ((double)lines * (double)L);
+            std::lock_guard<std::mutex> lk(ctx->mu);
+            ctx->tune[{kind, L}] = per;
+        }
+    }
+    return ok();
+}
+
+lucem_status lucem_autotune_query(lucem_ctx *ctx, int32_t kind, int64_t length, double *ns_per_element) {
+    if (!ctx) return fail(LUCEM_ERR_INVALID_HANDLE, "null context");
+    if (!ns_per_element) return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `ns_per_element`: null");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    auto it = ctx->tune.find({kind, length});
+    if (it == ctx->tune.end()) {
+        *ns_per_element = 0.0;
+        return fail(LUCEM_ERR_INVALID_PARAMETER, "no autotune entry for kind %d length %lld", kind, (long long)length);
+    }
+    *ns_per_element = it->second;
+    return ok();
+}
+
+lucem_status lucem_autotune_save(lucem_ctx *ctx, const char *path) {
+    if (!ctx) return fail(LUCEM_ERR_INVALID_HANDLE, "null context");
+    if (!path) return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `path`: null");
+    FILE *f = std::fopen(path, "w");
+    if (!f) return fail(LUCEM_ERR_INVALID_PARAMETER, "cannot write %s", path);
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    std::fprintf(f, "# lucem_b200 FFT pass costs: kind (0 column, 1 row) length ns_per_element\n");
+    for (auto &kv : ctx->tune) std::fprintf(f, "%d %lld %.9g\n", kv.first.first, (long long)kv.first.second, kv.second);
+    std::fclose(f);
+    return ok();
+}
+
+lucem_status lucem_autotune_load(lucem_ctx *ctx, const char *path) {
+    if (!ctx) return fail(LUCEM_ERR_INVALID_HANDLE, "null context");
+    if (!path) return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `path`: null");
+    FILE *f = std::fopen(path, "r");
+    if (!f) return fail(LUCEM_ERR_INVALID_PARAMETER, "cannot read %s", path);
+    char line[256];
+    std::map<std::pair<int, int64_t>, double> got;
+    while (std::fgets(line, sizeof line, f)) {
+        if (line[0] == '#' || line[0] == '\n') continue;
+        int kind;
+        long long len;
+        double v;
+        if (std::sscanf(line, "%d %lld %lf", &kind, &len, &v) != 3 || (kind != 0 && kind != 1) || len < 1 ||
+            !(v > 0.0)) {
+            std::fclose(f);
+            return fail(LUCEM_ERR_INVALID_PARAMETER, "malformed autotune line in %s: %s", path, line);
+        }
+        got[{kind, (int64_t)len}] = v;
+    }
+    std::fclose(f);
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    for (auto &kv : got) ctx->tune[kv.first] = kv.second;
+    return ok();
+}
+
+lucem_status lucem_graph_begin(void *stream) {
+    if (!stream) return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `stream`: the legacy default stream cannot be captured");
+    CUDA_TRY(cudaStreamBeginCapture(static_cast<cudaStream_t>(stream), cudaStreamCaptureModeThreadLocal),
+             "stream capture");
+    return ok();
+}
+
+lucem_status lucem_graph_end(void *stream, lucem_graph **out) {
+    if (!out) return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `out`: null");
+    *out = nullptr;
+    cudaGraph_t g = nullptr;
+    CUDA_TRY(cudaStreamEndCapture(static_cast<cudaStream_t>(stream), &g), "stream capture");
+    cudaGraphExec_t x = nullptr;
+    cudaError_t e = cudaGraphInstantiate(&x, g, 0);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return cuda_fail((int)e, "graph instantiation");
+    }
+    auto *h = new lucem_graph();
+    h->graph = g;
+    h->exec = x;
+    *out = h;
+    return ok();
+}
+
+lucem_status lucem_graph_launch(lucem_graph *graph, void *stream) {
+    if (!graph) return fail(LUCEM_ERR_INVALID_HANDLE, "null graph");
+    CUDA_TRY(cudaGraphLaunch(graph->exec, static_cast<cudaStream_t>(stream)), "graph launch");
+    return ok();
+}
+
+void lucem_graph_destroy(lucem_graph *graph) {
+    if (!graph) return;
+    cudaGraphExecDestroy(graph->exec);
+    cudaGraphDestroy(graph->graph);
+    delete graph;
 }
 
 }  // extern "C"

@@ -69,6 +69,12 @@ __device__ __forceinline__ int pad_index_rt(int p, int len, int mode) {
 template <typename T>
 __device__ __forceinline__ float load_as_float(const T *p) { return static_cast<float>(__ldg(p)); }
 
+// Two consecutive samples of one load.
+template <typename T> struct Pair;
+template <> struct Pair<uint8_t> { using type = uchar2; };
+template <> struct Pair<uint16_t> { using type = ushort2; };
+template <> struct Pair<float> { using type = float2; };
+
 // Where one CTA tile sits.  Coordinates of the read box are absolute (slide
 // or plane); the pad map applies at the read box's borders.
 struct TileGeom {
@@ -184,22 +190,63 @@ __device__ void family_tile(const FamParams &p, const TileGeom &g, float *A, flo
     const int AH = kTH + 2 * R0;
     const T *in = static_cast<const T *>(p.in) + (int64_t)g.plane * p.in_plane_stride;
 
-    // Phase 0: tile + halo -> A (f32), pad map relative to the read box.  A
-    // warp stages one row at a time (row map once per row, lanes along x).
+    // Phase 0: tile + halo -> A (f32).  Each thread issues all loads of a
+    // chunk (8 per thread) before any of its shared-memory stores, so a warp
+    // has many global loads in flight instead of one row at a time.
     {
-        const int lane = tid & 31, warp = tid >> 5;
-        const int rx0 = g.ox - g.rb_x - R1;
-        for (int r = warp; r < AH; r += kThreads / 32) {
-            const int py = pad_index_rt(g.oy - g.rb_y - R0 + r, g.rb_h, p.mode);
-            float *arow = A + r * AWP;
-            if (py < 0) {
-                for (int c = lane; c < AWP; c += 32) arow[c] = p.cval;
-                continue;
+        const int wy0 = g.oy - g.rb_y - R0, wx0 = g.ox - g.rb_x - R1;  // window origin in the read box
+        const T *wbase = in + (int64_t)g.rb_y * p.in_row_pitch + g.rb_x;
+        const bool interior = wy0 >= 0 && wx0 >= 0 && wy0 + AH <= g.rb_h && wx0 + AWP <= g.rb_w;
+        const T *w0 = wbase + (int64_t)wy0 * p.in_row_pitch + wx0;
+        const bool pairs_ok = (p.in_row_pitch % 2 == 0) &&
+                              (reinterpret_cast<uintptr_t>(w0) % (2 * sizeof(T)) == 0);
+        constexpr int kChunk = NOUT == 1 ? 8 : 4;
+        if (interior && pairs_ok) {
+            // No pad map: two samples per load (AWP is even).
+            using V2 = typename Pair<T>::type;
+            const int npr = AWP / 2, total = AH * npr;
+            for (int i0 = tid; i0 < total; i0 += kThreads * kChunk) {
+                V2 v[kChunk];
+#pragma unroll
+                for (int u = 0; u < kChunk; ++u) {
+                    const int i = i0 + u * kThreads;
+                    if (i < total) {
+                        const int r = i / npr, c = i - r * npr;
+                        v[u] = __ldg(reinterpret_cast<const V2 *>(w0 + (int64_t)r * p.in_row_pitch) + c);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < kChunk; ++u) {
+                    const int i = i0 + u * kThreads;
+                    if (i < total) {
+                        const int r = i / npr, c = i - r * npr;
+                        *reinterpret_cast<float2 *>(A + r * AWP + 2 * c) =
+                            make_float2((float)v[u].x * p.in_scale, (float)v[u].y * p.in_scale);
+                    }
+                }
             }
-            const T *src = in + (int64_t)(g.rb_y + py) * p.in_row_pitch + g.rb_x;
-            for (int c = lane; c < AWP; c += 32) {
-                const int px = pad_index_rt(rx0 + c, g.rb_w, p.mode);
-                arow[c] = px < 0 ? p.cval : load_as_float(src + px) * p.in_scale;
+        } else {
+            // Pad map relative to the read box (border tiles, odd pitches).
+            const int total = AH * AWP;
+            for (int i0 = tid; i0 < total; i0 += kThreads * kChunk) {
+                float v[kChunk];
+#pragma unroll
+                for (int u = 0; u < kChunk; ++u) {
+                    const int i = i0 + u * kThreads;
+                    v[u] = p.cval;
+                    if (i < total) {
+                        const int r = i / AWP, c = i - r * AWP;
+                        const int py = pad_index_rt(wy0 + r, g.rb_h, p.mode);
+                        const int px = pad_index_rt(wx0 + c, g.rb_w, p.mode);
+                        if (py >= 0 && px >= 0)
+                            v[u] = load_as_float(wbase + (int64_t)py * p.in_row_pitch + px) * p.in_scale;
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < kChunk; ++u) {
+                    const int i = i0 + u * kThreads;
+                    if (i < total) A[i] = v[u];
+                }
             }
         }
     }

@@ -221,6 +221,49 @@ int rl_backward(const RlGeom &g, const RlBuffers &b, const RlBwdBuffers &w, cons
 // convolution centre).  Uses w.c, w.t, w.spec_e, w.spec_cbar, w.pbar1, full_*.
 int rl_convolve_backward(const RlGeom &g, const RlBuffers &b, const RlBwdBuffers &w, const float *x,
                          const float *gout, float *gx, float *gpsf, void *stream, PassTimer *timer);
+// ---- batched 2-D Richardson-Lucy -------------------------------------------
+
+// Tiles per launch unit of the column pass (columns) and of the row pass
+// (rows) for a transform length; the host uses them to lay out work lists.
+int col_tile_width(int n);
+int row_tile_rows(int M);
+
+// One problem of a batched column pass (device layout of the kernels' item).
+struct RlColItem {
+    const float2_ *src;
+    float2_ *dst;
+    const float2_ *H, *H2;        // convolution / correlation transfer functions
+    float2_ *spec_out;
+    int64_t src_outer, src_row, dst_outer, dst_row, h_outer, h_row;
+    int32_t ncols, Hx, n_img, halo, store_begin, store_count;
+    int32_t tile_begin, pad_;
+};
+// One problem of a batched row pass.
+struct RlRowItem {
+    float2_ *s1;
+    const float *obs;
+    float *est;
+    int32_t nrows, X, hx, tile_begin;
+};
+// Problems that share a transform length n: their items (device array,
+// sorted by tile_begin) and the length's twiddle table.
+struct RlBatchGroup {
+    int32_t n;
+    const void *items;
+    int32_t n_items, total_tiles;
+    const float2_ *tw;
+};
+struct RlBatchLaunch {
+    int32_t mode;
+    const RlBatchGroup *rows;     // grouped by Px
+    int32_t n_rows;
+    const RlBatchGroup *cols;     // grouped by Py
+    int32_t n_cols;
+};
+int rl_tune_pass(int kind, int n, int lines, void *a, void *b, const float2_ *tw, int reps, void *stream,
+                 float *ms);
+int rl_batch_iterations(const RlBatchLaunch &L, int num_iter, int clip, float eps, void *stream, PassTimer *timer);
+
 // OTF of the normalised PSF `psf_dev` (f64 [kz][ky][kx]) centred at `centre`,
 // scaled by 1/(Pz*Py*Px), into complex [Pz][Py][Hp] (f32).  Work buffers are
 // f64 complex of size kz*ky*Hp and kz*Py*Hp.

@@ -92,7 +92,58 @@ struct ColPass {
     FftPlan plan;
     const float2 *tw;             // e^{-2 pi i m / n}, m < n
     int32_t C, CP;
+    // Batch mode (items != null): the launch covers several problems of the
+    // same transform length; tile t belongs to the last item whose
+    // tile_begin <= t, and that item's fields replace the ones above.
+    const struct ColItem *items;
+    int32_t n_items, total_tiles, use_h2;
 };
+
+// One problem of a batched column pass (the per-problem fields of ColPass).
+struct ColItem {
+    const float2 *src;
+    float2 *dst;
+    const float2 *H, *H2;         // H2: the second transfer function (use_h2)
+    float2 *spec_out;
+    int64_t src_outer, src_row, dst_outer, dst_row, h_outer, h_row;
+    int32_t ncols, Hx, n_img, halo, store_begin, store_count;
+    int32_t tile_begin, pad_;
+};
+
+__device__ __forceinline__ ColItem col_view(const ColPass &p) {
+    ColItem v;
+    v.src = p.src; v.dst = p.dst; v.H = p.H; v.H2 = p.H; v.spec_out = p.spec_out;
+    v.src_outer = p.src_outer; v.src_row = p.src_row; v.dst_outer = p.dst_outer; v.dst_row = p.dst_row;
+    v.h_outer = p.h_outer; v.h_row = p.h_row;
+    v.ncols = p.ncols; v.Hx = p.Hx; v.n_img = p.n_img; v.halo = p.halo;
+    v.store_begin = p.store_begin; v.store_count = p.store_count;
+    v.tile_begin = 0; v.pad_ = 0;
+    return v;
+}
+
+// Largest i with tile_begin(i) <= t (items sorted by tile_begin).
+template <class Item>
+__device__ __forceinline__ int find_item(const Item *items, int n, int t) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (items[mid].tile_begin <= t) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// The problem and local tile of global tile t.
+__device__ __forceinline__ ColItem col_tile(const ColPass &p, int t, int *local) {
+    if (p.items == nullptr) {
+        *local = t;
+        return col_view(p);
+    }
+    ColItem v = p.items[find_item(p.items, p.n_items, t)];
+    if (p.use_h2) v.H = v.H2;
+    *local = t - v.tile_begin;
+    return v;
+}
 
 // Generic column pass (any 2/3/5/7-smooth length): self-sorting transform in
 // shared memory, two buffers, natural order in and out.
@@ -105,21 +156,23 @@ __global__ void __launch_bounds__(512, 1) col_pass_kernel(const __grid_constant_
     const int C = p.C, CP = p.CP, T = blockDim.x, tid = threadIdx.x;
     for (int i = tid; i < n; i += T) tws[i] = p.tw[i];
     const fft::Tw tw{tws, 1};
-    const int ntiles = (p.ncols + C - 1) / C;
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int ntiles = p.items ? p.total_tiles : (p.ncols + C - 1) / C;
+    for (int gt = blockIdx.x; gt < ntiles; gt += gridDim.x) {
+        int tile;
+        const ColItem q = col_tile(p, gt, &tile);
         const int c0 = tile * C;
         for (int it = tid; it < n * C; it += T) {
             int row = it / C, c = it - row * C;
             int col = c0 + c;
-            float2 v = make_float2(0.f, 0.f);
-            if (col < p.ncols) {
-                int outer = col / p.Hx, kx = col - outer * p.Hx;
+            float2 val = make_float2(0.f, 0.f);
+            if (col < q.ncols) {
+                int outer = col / q.Hx, kx = col - outer * q.Hx;
                 int srow;
                 if (p.mode == kColInv) srow = row;
-                else srow = row < p.n_img + 2 * p.halo ? pad_index_rt(row - p.halo, p.n_img, p.pad_mode) : -1;
-                if (srow >= 0) v = p.src[outer * p.src_outer + srow * p.src_row + kx];
+                else srow = row < q.n_img + 2 * q.halo ? pad_index_rt(row - q.halo, q.n_img, p.pad_mode) : -1;
+                if (srow >= 0) val = q.src[outer * q.src_outer + srow * q.src_row + kx];
             }
-            bufA[row * CP + c] = v;
+            bufA[row * CP + c] = val;
         }
         __syncthreads();
         float2 *buf = fft::stockham(bufA, bufB, n, C, CP, p.plan.radix, p.plan.nstages, tw, p.mode == kColInv);
@@ -127,10 +180,10 @@ __global__ void __launch_bounds__(512, 1) col_pass_kernel(const __grid_constant_
             for (int it = tid; it < n * C; it += T) {
                 int row = it / C, c = it - row * C;
                 int col = c0 + c;
-                if (col < p.ncols) {
-                    int outer = col / p.Hx, kx = col - outer * p.Hx;
-                    if (p.spec_out) p.spec_out[outer * p.h_outer + row * p.h_row + kx] = buf[row * CP + c];
-                    float2 h = p.H[outer * p.h_outer + row * p.h_row + kx];
+                if (col < q.ncols) {
+                    int outer = col / q.Hx, kx = col - outer * q.Hx;
+                    if (q.spec_out) q.spec_out[outer * q.h_outer + row * q.h_row + kx] = buf[row * CP + c];
+                    float2 h = q.H[outer * q.h_outer + row * q.h_row + kx];
                     if (p.conj_h) h.y = -h.y;
                     buf[row * CP + c] = cmul(buf[row * CP + c], h);
                 }
@@ -138,14 +191,14 @@ __global__ void __launch_bounds__(512, 1) col_pass_kernel(const __grid_constant_
             __syncthreads();
             buf = fft::stockham(buf, buf == bufA ? bufB : bufA, n, C, CP, p.plan.radix, p.plan.nstages, tw, true);
         }
-        const int rows = p.mode == kColFwd ? n : p.store_count;
-        const int r0 = p.mode == kColFwd ? 0 : p.store_begin;
+        const int rows = p.mode == kColFwd ? n : q.store_count;
+        const int r0 = p.mode == kColFwd ? 0 : q.store_begin;
         for (int it = tid; it < rows * C; it += T) {
             int row = it / C, c = it - row * C;
             int col = c0 + c;
-            if (col < p.ncols) {
-                int outer = col / p.Hx, kx = col - outer * p.Hx;
-                p.dst[outer * p.dst_outer + row * p.dst_row + kx] = buf[(r0 + row) * CP + c];
+            if (col < q.ncols) {
+                int outer = col / q.Hx, kx = col - outer * q.Hx;
+                q.dst[outer * q.dst_outer + row * q.dst_row + kx] = buf[(r0 + row) * CP + c];
             }
         }
         __syncthreads();
@@ -157,7 +210,7 @@ __global__ void __launch_bounds__(512, 1) col_pass_kernel(const __grid_constant_
 // columns: coalesced), transforms in registers with one shared-memory
 // exchange per direction, multiplies by H in registers and stores back.
 template <int N1, int N2, int C>
-__global__ void __launch_bounds__(N1 * C, 65536 / (N1 * C * 128)) col_fast_kernel(const __grid_constant__ ColPass p) {
+__global__ void __launch_bounds__(N1 * C, (N2 > 32 ? 1 : 65536 / (N1 * C * 128))) col_fast_kernel(const __grid_constant__ ColPass p) {
     using L = fftc::ColLayout<N1, N2, C>;
     using F = fftc::TwoStep<N1, N2, L>;
     constexpr int N = N1 * N2;
@@ -168,26 +221,28 @@ __global__ void __launch_bounds__(N1 * C, 65536 / (N1 * C * 128)) col_fast_kerne
     const int tid = threadIdx.x, c = tid % C, t = tid / C;
     F::build_tables(tf, ti, p.tw, 1);
     __syncthreads();
-    const int ntiles = (p.ncols + C - 1) / C;
-    const int n_ext = p.n_img + 2 * p.halo;
-    // Element offsets within one column fit 32 bits (checked by the host).
-    const int src_row = (int)p.src_row, dst_row = (int)p.dst_row, h_row = (int)p.h_row;
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int ntiles = p.items ? p.total_tiles : (p.ncols + C - 1) / C;
+    for (int gt = blockIdx.x; gt < ntiles; gt += gridDim.x) {
+        int tile;
+        const ColItem q = col_tile(p, gt, &tile);
+        const int n_ext = q.n_img + 2 * q.halo;
+        // Element offsets within one column fit 32 bits (checked by the host).
+        const int src_row = (int)q.src_row, dst_row = (int)q.dst_row, h_row = (int)q.h_row;
         const int col = tile * C + c;
-        const bool ok = col < p.ncols;
+        const bool ok = col < q.ncols;
         int outer = 0, kx = 0;
         if (ok) {
-            outer = col / p.Hx;
-            kx = col - outer * p.Hx;
+            outer = col / q.Hx;
+            kx = col - outer * q.Hx;
         }
-        const float2 *src = p.src + (outer * p.src_outer + kx);
+        const float2 *src = q.src + (outer * q.src_outer + kx);
         float2 v[N2];
         if (p.mode == kColInv) {
 #pragma unroll
             for (int j = 0; j < N2; ++j) v[j] = ok ? src[F::freq(t, j) * src_row] : make_float2(0.f, 0.f);
             F::inverse(v, t, c, xb, ti);
         } else {
-            const float2 *h = p.H + (outer * p.h_outer + kx);
+            const float2 *h = q.H + (outer * q.h_outer + kx);
             // Short transforms prefetch the transfer function with the data
             // (one memory round trip per tile instead of two).
             constexpr bool kPrefetchH = N2 <= 16;
@@ -200,17 +255,17 @@ __global__ void __launch_bounds__(N1 * C, 65536 / (N1 * C * 128)) col_fast_kerne
 #pragma unroll
             for (int i = 0; i < N2; ++i) {
                 const int row = t + N1 * i;
-                int srow = row < n_ext ? pad_index_rt(row - p.halo, p.n_img, p.pad_mode) : -1;
+                int srow = row < n_ext ? pad_index_rt(row - q.halo, q.n_img, p.pad_mode) : -1;
                 v[i] = (ok && srow >= 0) ? src[srow * src_row] : make_float2(0.f, 0.f);
             }
             F::forward(v, t, c, xb, tf);
-            if (p.mode == kColFull && p.spec_out != nullptr && ok) {
-                float2 *so = p.spec_out + (outer * p.h_outer + kx);
+            if (p.mode == kColFull && q.spec_out != nullptr && ok) {
+                float2 *so = q.spec_out + (outer * q.h_outer + kx);
 #pragma unroll
                 for (int j = 0; j < N2; ++j) so[F::freq(t, j) * h_row] = v[j];
             }
             if (p.mode == kColFwd) {
-                float2 *dst = p.dst + (outer * p.dst_outer + kx);
+                float2 *dst = q.dst + (outer * q.dst_outer + kx);
                 if (ok) {
 #pragma unroll
                     for (int j = 0; j < N2; ++j) dst[F::freq(t, j) * dst_row] = v[j];
@@ -227,12 +282,12 @@ __global__ void __launch_bounds__(N1 * C, 65536 / (N1 * C * 128)) col_fast_kerne
             }
             F::inverse(v, t, c, xb, ti);
         }
-        float2 *dst = p.dst + (outer * p.dst_outer + kx);
+        float2 *dst = q.dst + (outer * q.dst_outer + kx);
         if (ok) {
 #pragma unroll
             for (int i = 0; i < N2; ++i) {
-                const int row = t + N1 * i - p.store_begin;
-                if (row >= 0 && row < p.store_count) dst[row * dst_row] = v[i];
+                const int row = t + N1 * i - q.store_begin;
+                if (row >= 0 && row < q.store_count) dst[row * dst_row] = v[i];
             }
         }
     }
@@ -256,7 +311,31 @@ struct RowPass {
     FftPlan plan;                 // M-point
     const float2 *tw;             // table of length Px
     int32_t C, CP;
+    // Batch mode (items != null): problems of the same Px; the item's fields
+    // replace nrows, X, hx, obs, est and s1.
+    const struct RowItem *items;
+    int32_t n_items, total_tiles;
 };
+
+struct RowItem {
+    float2 *s1;
+    const float *obs;
+    float *est;
+    int32_t nrows, X, hx, tile_begin;
+};
+
+__device__ __forceinline__ RowItem row_tile(const RowPass &p, int t, int *local) {
+    if (p.items == nullptr) {
+        *local = t;
+        RowItem v;
+        v.s1 = p.s1; v.obs = p.obs; v.est = p.est;
+        v.nrows = p.nrows; v.X = p.X; v.hx = p.hx; v.tile_begin = 0;
+        return v;
+    }
+    const RowItem v = p.items[find_item(p.items, p.n_items, t)];
+    *local = t - v.tile_begin;
+    return v;
+}
 
 __global__ void __launch_bounds__(512, 1) row_pass_kernel(const __grid_constant__ RowPass p) {
     extern __shared__ float4 smem4[];
@@ -267,8 +346,10 @@ __global__ void __launch_bounds__(512, 1) row_pass_kernel(const __grid_constant_
     float2 *bufB = bufA + (M + 1) * CP;
     for (int i = tid; i < Px; i += T) tws[i] = p.tw[i];
     const fft::Tw twM{tws, 2};   // W_M^m = W_Px^{2m}
-    const int ntiles = (p.nrows + C - 1) / C;
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int ntiles = p.items ? p.total_tiles : (p.nrows + C - 1) / C;
+    for (int gt = blockIdx.x; gt < ntiles; gt += gridDim.x) {
+        int tile;
+        const RowItem pi = row_tile(p, gt, &tile);
         const int row0 = tile * C;
         float2 *buf = bufA;  // holds the natural-order real row after C2R
         __syncthreads();
@@ -278,7 +359,7 @@ __global__ void __launch_bounds__(512, 1) row_pass_kernel(const __grid_constant_
                 int c = it / (M + 1), k = it - c * (M + 1);
                 int row = row0 + c;
                 float2 v = make_float2(0.f, 0.f);
-                if (row < p.nrows) v = p.s1[(int64_t)row * p.Hp + k];
+                if (row < pi.nrows) v = pi.s1[(int64_t)row * p.Hp + k];
                 bufA[k * CP + c] = v;
             }
             __syncthreads();
@@ -307,31 +388,31 @@ __global__ void __launch_bounds__(512, 1) row_pass_kernel(const __grid_constant_
         // Epilogue on the image columns; the real sample at position i of the
         // row is component (i & 1) of packed element i >> 1.
         const bool emit = !(p.kind == kRowUpdate && p.last) && p.kind != kRowRealOut;
-        for (int it = tid; it < p.X * C; it += T) {
-            int c = it / p.X, xi = it - c * p.X;
+        for (int it = tid; it < pi.X * C; it += T) {
+            int c = it / pi.X, xi = it - c * pi.X;
             int row = row0 + c;
-            if (row >= p.nrows) continue;
-            int i = xi + p.hx;
+            if (row >= pi.nrows) continue;
+            int i = xi + pi.hx;
             float *slot = bufr + ((i >> 1) * CP + c) * 2 + (i & 1);
-            int64_t g = (int64_t)row * p.X + xi;
+            int64_t g = (int64_t)row * pi.X + xi;
             float v;
             if (p.kind == kRowInit) {
                 v = 0.5f;
             } else if (p.kind == kRowRealIn) {
-                v = p.obs[g];
+                v = pi.obs[g];
             } else if (p.kind == kRowRealOut) {
                 v = *slot;
-                p.est[g] = v;
+                pi.est[g] = v;
             } else if (p.kind == kRowRatio) {
                 float conv = *slot;
                 float d = fabsf(conv) < p.eps ? p.eps : conv;
-                v = p.obs[g] / d;
+                v = pi.obs[g] / d;
             } else {
                 float corr = *slot;
-                float old = p.est_first ? 0.5f : p.est[g];
+                float old = p.est_first ? 0.5f : pi.est[g];
                 v = old * corr;
                 if (p.last && p.clip) v = fminf(fmaxf(v, -1.0f), 1.0f);
-                p.est[g] = v;
+                pi.est[g] = v;
             }
             if (emit) *slot = v;
         }
@@ -341,12 +422,12 @@ __global__ void __launch_bounds__(512, 1) row_pass_kernel(const __grid_constant_
         // pad-mapped image samples, everything past X + 2*hx is zero.
         for (int it = tid; it < Px * C; it += T) {
             int c = it / Px, j = it - c * Px;
-            if (j >= p.hx && j < p.hx + p.X) continue;
+            if (j >= pi.hx && j < pi.hx + pi.X) continue;
             float v = 0.0f;
-            if (j < p.X + 2 * p.hx) {
-                int q = pad_index_rt(j - p.hx, p.X, p.pad_mode);
+            if (j < pi.X + 2 * pi.hx) {
+                int q = pad_index_rt(j - pi.hx, pi.X, p.pad_mode);
                 if (q >= 0) {
-                    int s = q + p.hx;
+                    int s = q + pi.hx;
                     v = bufr[((s >> 1) * CP + c) * 2 + (s & 1)];
                 }
             }
@@ -373,7 +454,7 @@ __global__ void __launch_bounds__(512, 1) row_pass_kernel(const __grid_constant_
         for (int it = tid; it < (M + 1) * C; it += T) {
             int c = it / (M + 1), k = it - c * (M + 1);
             int row = row0 + c;
-            if (row < p.nrows) p.s1[(int64_t)row * p.Hp + k] = z[k * CP + c];
+            if (row < pi.nrows) pi.s1[(int64_t)row * p.Hp + k] = z[k * CP + c];
         }
     }
 }
@@ -396,15 +477,17 @@ __global__ void __launch_bounds__(N1 * R, 65536 / (N1 * R * 128)) row_fast_kerne
     for (int i = tid; i < Px; i += N1 * R) tws[i] = p.tw[i];
     F::build_tables(tf, ti, p.tw, 2);  // W_M^m = W_Px^{2m}
     __syncthreads();
-    const int ntiles = (p.nrows + R - 1) / R;
+    const int ntiles = p.items ? p.total_tiles : (p.nrows + R - 1) / R;
     const bool emit_last = !(p.kind == kRowUpdate && p.last) && p.kind != kRowRealOut;
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    for (int gt = blockIdx.x; gt < ntiles; gt += gridDim.x) {
+        int tile;
+        const RowItem pi = row_tile(p, gt, &tile);
         const int row = tile * R + r;
-        const bool ok = row < p.nrows;
+        const bool ok = row < pi.nrows;
         float2 *spec = xb + r * SP;
         float2 v[N2];
         if (p.kind != kRowInit && p.kind != kRowRealIn) {
-            const float2 *s1 = p.s1 + (int64_t)(ok ? row : 0) * p.Hp;
+            const float2 *s1 = pi.s1 + (int64_t)(ok ? row : 0) * p.Hp;
             for (int k = t; k <= M; k += N1) spec[k] = ok ? s1[k] : make_float2(0.f, 0.f);
             __syncthreads();
             // Z[k] = (X[k] + X*[M-k]) + i (X[k] - X*[M-k]) W_Px^{-k}
@@ -429,17 +512,17 @@ __global__ void __launch_bounds__(N1 * R, 65536 / (N1 * R * 128)) row_fast_kerne
         // columns, 8 values of m at a time: all loads of a chunk are issued
         // before its stores (the image pointers do not alias).
         {
-            const int64_t gbase = (int64_t)(ok ? row : 0) * p.X;
-            const float *__restrict__ obs = p.obs;
-            float *__restrict__ est = p.est;
+            const int64_t gbase = (int64_t)(ok ? row : 0) * pi.X;
+            const float *__restrict__ obs = pi.obs;
+            float *__restrict__ est = pi.est;
             constexpr int CH = N2 < 8 ? N2 : 8;
 #pragma unroll
             for (int i0 = 0; i0 < N2; i0 += CH) {
                 float in[2 * CH];
 #pragma unroll
                 for (int q = 0; q < 2 * CH; ++q) {
-                    const int xi = 2 * (t + N1 * (i0 + q / 2)) + (q & 1) - p.hx;
-                    const bool inside = ok && xi >= 0 && xi < p.X;
+                    const int xi = 2 * (t + N1 * (i0 + q / 2)) + (q & 1) - pi.hx;
+                    const bool inside = ok && xi >= 0 && xi < pi.X;
                     in[q] = 0.0f;
                     if ((p.kind == kRowRatio || p.kind == kRowRealIn) && inside) in[q] = obs[gbase + xi];
                     if (p.kind == kRowUpdate && !p.est_first && inside) in[q] = est[gbase + xi];
@@ -447,8 +530,8 @@ __global__ void __launch_bounds__(N1 * R, 65536 / (N1 * R * 128)) row_fast_kerne
 #pragma unroll
                 for (int q = 0; q < 2 * CH; ++q) {
                     const int i = i0 + q / 2;
-                    const int xi = 2 * (t + N1 * i) + (q & 1) - p.hx;
-                    const bool inside = xi >= 0 && xi < p.X;
+                    const int xi = 2 * (t + N1 * i) + (q & 1) - pi.hx;
+                    const bool inside = xi >= 0 && xi < pi.X;
                     const float val = (q & 1) ? v[i].y : v[i].x;
                     float nv = 0.0f;
                     if (inside) {
@@ -473,14 +556,14 @@ __global__ void __launch_bounds__(N1 * R, 65536 / (N1 * R * 128)) row_fast_kerne
 #pragma unroll
                     for (int q = 0; q < 2 * CH; ++q) {
                         const int i = i0 + q / 2;
-                        const int xi = 2 * (t + N1 * i) + (q & 1) - p.hx;
-                        if (xi >= 0 && xi < p.X) est[gbase + xi] = (q & 1) ? v[i].y : v[i].x;
+                        const int xi = 2 * (t + N1 * i) + (q & 1) - pi.hx;
+                        if (xi >= 0 && xi < pi.X) est[gbase + xi] = (q & 1) ? v[i].y : v[i].x;
                     }
                 }
             }
         }
         if (!emit_last) continue;
-        if (p.hx > 0) {
+        if (pi.hx > 0) {
             // Extension along x by the pad map: positions outside
             // [hx, hx + X) take image samples, past X + 2 hx zero.
             float *real = reinterpret_cast<float *>(spec);
@@ -497,11 +580,11 @@ __global__ void __launch_bounds__(N1 * R, 65536 / (N1 * R * 128)) row_fast_kerne
 #pragma unroll
                 for (int e = 0; e < 2; ++e) {
                     const int pos = 2 * m + e;
-                    if (pos >= p.hx && pos < p.hx + p.X) continue;
+                    if (pos >= pi.hx && pos < pi.hx + pi.X) continue;
                     float nv = 0.0f;
-                    if (pos < p.X + 2 * p.hx) {
-                        int q = pad_index_rt(pos - p.hx, p.X, p.pad_mode);
-                        if (q >= 0) nv = real[q + p.hx];
+                    if (pos < pi.X + 2 * pi.hx) {
+                        int q = pad_index_rt(pos - pi.hx, pi.X, p.pad_mode);
+                        if (q >= 0) nv = real[q + pi.hx];
                     }
                     if (e) v[i].y = nv; else v[i].x = nv;
                 }
@@ -523,7 +606,7 @@ __global__ void __launch_bounds__(N1 * R, 65536 / (N1 * R * 128)) row_fast_kerne
         }
         __syncthreads();
         if (ok) {
-            float2 *s1 = p.s1 + (int64_t)row * p.Hp;
+            float2 *s1 = pi.s1 + (int64_t)row * p.Hp;
             for (int k = t; k <= M; k += N1) s1[k] = spec[k];
         }
         __syncthreads();
@@ -610,12 +693,44 @@ int sms() {
     return n > 0 ? n : 148;
 }
 
+}  // namespace
+
+// Columns per tile of the column pass for transform length n (the launch
+// shapes of launch_col below).
+int col_tile_width(int n) {
+    switch (n) {
+    case 64: case 128: case 256: case 512: return 16;
+    case 1024: case 2048: return 8;
+    default: break;
+    }
+    // Generic: two (n x (C+1)) buffers plus twiddles within ~200 KB.
+    int C = 64;
+    while (C > 2 && ((size_t)n * (1 + 2 * (size_t)(C + 1))) * sizeof(float2) > 200 * 1024) C >>= 1;
+    return C;
+}
+
+// Rows per tile of the row pass for packed length M = Px / 2.
+int row_tile_rows(int M) {
+    switch (M) {
+    case 64: case 128: return 32;
+    case 256: case 512: return 16;
+    case 1024: return 8;
+    default: break;
+    }
+    // Two (M+1) x (C+1) buffers plus the twiddles, about 100 KB at most.
+    int C = 16;
+    while (C > 2 && ((size_t)2 * M + 2 * (size_t)(M + 1) * (C + 1)) * sizeof(float2) > 110 * 1024) C >>= 1;
+    return C;
+}
+
+namespace {
+
 template <int N1, int N2, int C>
 int launch_col_fast(const ColPass &p, cudaStream_t s) {
     using L = fftc::ColLayout<N1, N2, C>;
     constexpr int N = N1 * N2;
     size_t smem = ((size_t)2 * N + (size_t)L::kBuf) * sizeof(float2);
-    int ntiles = (p.ncols + C - 1) / C;
+    int ntiles = p.items ? p.total_tiles : (p.ncols + C - 1) / C;
     int per_sm = (int)((200 * 1024) / (smem + 1024));
     per_sm = per_sm < 1 ? 1 : (per_sm > 8 ? 8 : per_sm);
     int grid = ntiles < sms() * per_sm ? ntiles : sms() * per_sm;
@@ -630,7 +745,7 @@ int launch_row_fast(const RowPass &p, cudaStream_t s) {
     constexpr int M = N1 * N2;
     constexpr int U = L::kBuf > R * (M + 1) ? L::kBuf : R * (M + 1);
     size_t smem = ((size_t)2 * M + 2 * (size_t)M + (size_t)U) * sizeof(float2);
-    int ntiles = (p.nrows + R - 1) / R;
+    int ntiles = p.items ? p.total_tiles : (p.nrows + R - 1) / R;
     int per_sm = (int)((200 * 1024) / (smem + 1024));
     per_sm = per_sm < 1 ? 1 : (per_sm > 8 ? 8 : per_sm);
     int grid = ntiles < sms() * per_sm ? ntiles : sms() * per_sm;
@@ -646,17 +761,16 @@ int launch_col(ColPass p, cudaStream_t s) {
     case 256: return launch_col_fast<16, 16, 16>(p, s);
     case 512: return launch_col_fast<16, 32, 16>(p, s);
     case 1024: return launch_col_fast<32, 32, 8>(p, s);
+    case 2048: return launch_col_fast<32, 64, 8>(p, s);
     default: break;
     }
-    // Generic: two (n x (C+1)) buffers plus twiddles within ~200 KB.
-    int C = 64;
-    while (C > 2 && ((size_t)p.plan.n * (1 + 2 * (size_t)(C + 1))) * sizeof(float2) > 200 * 1024) C >>= 1;
+    const int C = col_tile_width(p.plan.n);
     int T = (int)(((int64_t)p.plan.n * C / 8 + 31) / 32) * 32;
     T = T < 128 ? 128 : (T > 512 ? 512 : T);
     p.C = C;
     p.CP = C + 1;
     size_t smem = ((size_t)p.plan.n + 2 * (size_t)p.plan.n * p.CP) * sizeof(float2);
-    int ntiles = (p.ncols + C - 1) / C;
+    int ntiles = p.items ? p.total_tiles : (p.ncols + C - 1) / C;
     int per_sm = (int)((227 * 1024) / (smem + 1024));
     if (per_sm < 1) per_sm = 1;
     int grid = ntiles < sms() * per_sm ? ntiles : sms() * per_sm;
@@ -675,16 +789,14 @@ int launch_row(RowPass p, cudaStream_t s) {
     default: break;
     }
     const int M = p.M;
-    // Two (M+1) x (C+1) buffers plus the twiddles, about 100 KB at most.
-    int C = 16;
-    while (C > 2 && ((size_t)p.Px + 2 * (size_t)(M + 1) * (C + 1)) * sizeof(float2) > 110 * 1024) C >>= 1;
+    const int C = row_tile_rows(M);
     int T = (int)(((int64_t)M * C / 8 + 31) / 32) * 32;
     if (T < 128) T = 128;
     if (T > 512) T = 512;
     p.C = C;
     p.CP = C + 1;
     size_t smem = ((size_t)p.Px + 2 * (size_t)(M + 1) * p.CP) * sizeof(float2);
-    int ntiles = (p.nrows + C - 1) / C;
+    int ntiles = p.items ? p.total_tiles : (p.nrows + C - 1) / C;
     int per_sm = (int)((227 * 1024) / (smem + 1024));
     if (per_sm < 1) per_sm = 1;
     int grid = ntiles < sms() * per_sm ? ntiles : sms() * per_sm;
@@ -977,6 +1089,123 @@ int rl_apply(const RlGeom &g, const RlBuffers &b, const void *H, int conj, const
     RlRunner run(g, b, stream, timer);
     if (!run.ok) return (int)cudaErrorInvalidValue;
     return run.apply(H, conj, x, out, nullptr);
+}
+
+static_assert(sizeof(ColItem) == sizeof(RlColItem), "ColItem layout");
+static_assert(sizeof(RowItem) == sizeof(RlRowItem), "RowItem layout");
+
+// Batched iterations: per pass kind one launch per group of problems that
+// share the transform length (groups built by the host), in the order of
+// rl_launch_iterations.
+int rl_batch_iterations(const RlBatchLaunch &L, int num_iter, int clip, float eps, void *stream, PassTimer *timer) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    auto rows = [&](int kind, int est_first, int last) -> int {
+        for (int gi = 0; gi < L.n_rows; ++gi) {
+            const RlBatchGroup &G = L.rows[gi];
+            RowPass r{};
+            r.Px = G.n;
+            r.M = G.n / 2;
+            r.Hx = r.M + 1;
+            r.Hp = (r.Hx + 15) & ~15;
+            r.pad_mode = L.mode;
+            r.kind = kind;
+            r.est_first = est_first;
+            r.last = last;
+            r.clip = clip;
+            r.eps = eps;
+            if (!fft_make_plan(r.M, &r.plan)) return (int)cudaErrorInvalidValue;
+            r.tw = reinterpret_cast<const float2 *>(G.tw);
+            r.items = static_cast<const RowItem *>(G.items);
+            r.n_items = G.n_items;
+            r.total_tiles = G.total_tiles;
+            if (timer) timer->begin(kPassRlRow, stream);
+            int e = launch_row(r, s);
+            if (timer) timer->end(kPassRlRow, stream);
+            if (e) return e;
+        }
+        return 0;
+    };
+    auto cols = [&](int h2) -> int {
+        for (int gi = 0; gi < L.n_cols; ++gi) {
+            const RlBatchGroup &G = L.cols[gi];
+            ColPass c{};
+            c.mode = kColFull;
+            c.pad_mode = L.mode;
+            c.conj_h = h2;
+            c.use_h2 = h2;
+            if (!fft_make_plan(G.n, &c.plan)) return (int)cudaErrorInvalidValue;
+            c.tw = reinterpret_cast<const float2 *>(G.tw);
+            c.items = static_cast<const ColItem *>(G.items);
+            c.n_items = G.n_items;
+            c.total_tiles = G.total_tiles;
+            if (timer) timer->begin(kPassRlColFull, stream);
+            int e = launch_col(c, s);
+            if (timer) timer->end(kPassRlColFull, stream);
+            if (e) return e;
+        }
+        return 0;
+    };
+    int e;
+    if ((e = rows(kRowInit, 0, 0))) return e;
+    for (int it = 0; it < num_iter; ++it) {
+        if ((e = cols(0))) return e;
+        if ((e = rows(kRowRatio, 0, 0))) return e;
+        if ((e = cols(1))) return e;
+        if ((e = rows(kRowUpdate, it == 0, it + 1 == num_iter))) return e;
+    }
+    return 0;
+}
+
+// Times one column pass (kind 0: forward * H * inverse over `lines` columns)
+// or one row pass (kind 1: the ratio epilogue over `lines` rows) of length n
+// on scratch buffers; average of `reps` launches after one warm-up, in ms.
+// a: complex, n * (n/2 + 16) * lines / n elements at least (see the host),
+// b: lines * n floats.
+int rl_tune_pass(int kind, int n, int lines, void *a, void *b, const float2_ *tw, int reps, void *stream,
+                 float *ms) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess) return (int)cudaErrorUnknown;
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return (int)cudaErrorUnknown;
+    }
+    auto launch = [&]() -> int {
+        if (kind == 0) {
+            ColPass c{};
+            c.ncols = lines; c.Hx = lines;
+            c.src = static_cast<const float2 *>(a); c.src_outer = 0; c.src_row = lines;
+            c.n_img = n; c.halo = 0;
+            c.dst = static_cast<float2 *>(a); c.dst_outer = 0; c.dst_row = lines;
+            c.store_begin = 0; c.store_count = n;
+            c.mode = kColFull; c.pad_mode = LUCEM_PAD_CONSTANT;
+            c.H = static_cast<const float2 *>(a); c.h_outer = 0; c.h_row = lines;
+            if (!fft_make_plan(n, &c.plan)) return (int)cudaErrorInvalidValue;
+            c.tw = reinterpret_cast<const float2 *>(tw);
+            return launch_col(c, s);
+        }
+        RowPass r{};
+        r.nrows = lines; r.X = n; r.Px = n; r.M = n / 2; r.Hx = n / 2 + 1; r.Hp = (r.Hx + 15) & ~15; r.hx = 0;
+        r.pad_mode = LUCEM_PAD_CONSTANT; r.kind = kRowRatio; r.eps = 1e-6f;
+        r.obs = static_cast<const float *>(b);
+        r.s1 = static_cast<float2 *>(a);
+        if (!fft_make_plan(r.M, &r.plan)) return (int)cudaErrorInvalidValue;
+        r.tw = reinterpret_cast<const float2 *>(tw);
+        return launch_row(r, s);
+    };
+    int e = launch();
+    if (!e) e = (int)cudaEventRecord(e0, s);
+    for (int i = 0; i < reps && !e; ++i) e = launch();
+    if (!e) e = (int)cudaEventRecord(e1, s);
+    if (!e) e = (int)cudaEventSynchronize(e1);
+    if (!e) {
+        float t = 0.f;
+        e = (int)cudaEventElapsedTime(&t, e0, e1);
+        *ms = t / (float)reps;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return e;
 }
 
 // Reverse mode through the unrolled iterations (clip off), checkpoints every K.

@@ -28,7 +28,8 @@ __all__ = [
     "difference_of_gaussians", "gaussian_laplace", "gaussian_grad_mag", "unsharp_mask",
     "gaussian_family", "schedule", "gaussian_family_tiles", "richardson_lucy", "rl_grid",
     "gaussian_halo", "op_halo", "gaussian_blur_adjoint", "richardson_lucy_backward", "fft_convolve",
-    "fft_convolve_backward",
+    "fft_convolve_backward", "RlBatch", "richardson_lucy_batch", "autotune_fft", "autotune_query",
+    "autotune_save", "autotune_load", "Graph",
 ]
 
 
@@ -608,3 +609,147 @@ def fft_convolve_backward(x: torch.Tensor, psf: torch.Tensor, grad_out: torch.Te
     N.check(N.lib().lucem_fft_convolve_backward(ctx.handle, C.byref(ti), C.byref(tp), PadMode.CONSTANT,
                                                 _grid_arg(grid), C.byref(tg), tgx, tgp, ws.handle, _stream(x)))
     return gp, gx
+
+
+# ---------------------------------------------------------------------------
+# batched 2-D Richardson-Lucy, autotuning, graphs
+
+
+def _tensor_array(ts, name):
+    arr = (N.Tensor * len(ts))()
+    for i, t in enumerate(ts):
+        arr[i] = _tensor(t, f"{name}[{i}]")
+    return arr
+
+
+class RlBatch:
+    """A planned batch of 2-D Richardson-Lucy problems of any sizes and PSFs
+    (lucem_rl_batch_*).  The plan keeps the tensors' device pointers: keep
+    `images`, `psfs` and `outs` alive while it is used.  run() only launches
+    (one launch per pass and length group), so it can be captured in a CUDA
+    graph; run(per_problem=True) runs the same kernels image by image."""
+
+    def __init__(self, images: Sequence[torch.Tensor], psfs: Sequence[torch.Tensor], *, num_iter: int = 30,
+                 clip: bool = True, filter_epsilon: Optional[float] = None, mode="reflect",
+                 outs: Optional[Sequence[torch.Tensor]] = None, workspace: Optional[Workspace] = None):
+        if len(images) == 0 or len(images) != len(psfs):
+            raise LucemError(7, "invalid parameter `images`: one PSF per image, at least one image")
+        x0 = images[0]
+        ctx, ws = _ctx_ws(x0, workspace)
+        self.images, self.psfs = list(images), list(psfs)
+        self.outs = list(outs) if outs is not None else [torch.empty(x.shape, dtype=torch.float32, device=x.device)
+                                                        for x in images]
+        s = _rl_settings(num_iter, clip, filter_epsilon, mode, None)
+        ti = _tensor_array(self.images, "images")
+        tp = _tensor_array(self.psfs, "psfs")
+        to = _tensor_array(self.outs, "outs")
+        h = C.c_void_p()
+        N.check(N.lib().lucem_rl_batch_create(ctx.handle, len(images), ti, tp, C.byref(s), to, ws.handle,
+                                              _stream(x0), C.byref(h)))
+        self.handle = h
+        self.device = x0.device
+
+    def run(self, per_problem: bool = False, workspace: Optional[Workspace] = None):
+        ws = workspace.handle if workspace is not None else None
+        N.check(N.lib().lucem_rl_batch_run(self.handle, int(bool(per_problem)), ws,
+                                           C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)))
+        return self.outs
+
+    def info(self):
+        """(grids [(Py, Px)], launches per row pass, launches per column pass)."""
+        n = len(self.images)
+        g = (C.c_int64 * (2 * n))()
+        nr, nc = C.c_int32(), C.c_int32()
+        N.check(N.lib().lucem_rl_batch_info(self.handle, g, C.byref(nr), C.byref(nc)))
+        return [(int(g[2 * i]), int(g[2 * i + 1])) for i in range(n)], nr.value, nc.value
+
+    def close(self):
+        if getattr(self, "handle", None):
+            N.lib().lucem_rl_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def richardson_lucy_batch(images: Sequence[torch.Tensor], psfs: Sequence[torch.Tensor], **kw):
+    """richardson_lucy over a list of 2-D images of any sizes, one PSF each,
+    as one planned batch; returns the list of estimates."""
+    b = RlBatch(images, psfs, **kw)
+    try:
+        return b.run()
+    finally:
+        torch.cuda.current_stream(b.device).synchronize()
+        b.close()
+
+
+def autotune_fft(lengths, device=None, workspace: Optional[Workspace] = None):
+    """Measure the FFT pass costs at `lengths` (lucem_autotune_fft); batched
+    plans made afterwards on this device choose grids by them."""
+    dev = _device_index(device)
+    ctx = context(dev)
+    ws = workspace if workspace is not None else _default_ws(dev)
+    arr = (C.c_int64 * max(1, len(lengths)))(*[int(v) for v in lengths])
+    N.check(N.lib().lucem_autotune_fft(ctx.handle, arr, len(lengths), ws.handle,
+                                       C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)))
+
+
+def autotune_query(kind: int, length: int, device=None) -> float:
+    """ns per transformed element of the column (kind 0) or row (kind 1) pass."""
+    v = C.c_double()
+    N.check(N.lib().lucem_autotune_query(context(_device_index(device)).handle, int(kind), int(length), C.byref(v)))
+    return v.value
+
+
+def autotune_save(path: str, device=None):
+    N.check(N.lib().lucem_autotune_save(context(_device_index(device)).handle, str(path).encode()))
+
+
+def autotune_load(path: str, device=None):
+    N.check(N.lib().lucem_autotune_load(context(_device_index(device)).handle, str(path).encode()))
+
+
+class Graph:
+    """A CUDA graph of launch-only library calls (lucem_graph_*):
+
+        g = Graph(stream); with g: plan.run(); ...; g.launch()
+    """
+
+    def __init__(self, stream: Optional[torch.cuda.Stream] = None):
+        self.stream = stream if stream is not None else torch.cuda.Stream()
+        self.handle = None
+
+    def __enter__(self):
+        self._ctx = torch.cuda.stream(self.stream)
+        self._ctx.__enter__()
+        N.check(N.lib().lucem_graph_begin(C.c_void_p(self.stream.cuda_stream)))
+        return self
+
+    def __exit__(self, exc_type, exc, tb):
+        h = C.c_void_p()
+        st = N.lib().lucem_graph_end(C.c_void_p(self.stream.cuda_stream), C.byref(h))
+        self._ctx.__exit__(exc_type, exc, tb)
+        if exc_type is None:
+            N.check(st)
+            self.handle = h
+        elif h:
+            N.lib().lucem_graph_destroy(h)
+        return False
+
+    def launch(self, stream: Optional[torch.cuda.Stream] = None):
+        s = stream if stream is not None else torch.cuda.current_stream()
+        N.check(N.lib().lucem_graph_launch(self.handle, C.c_void_p(s.cuda_stream)))
+
+    def close(self):
+        if self.handle:
+            N.lib().lucem_graph_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -138,3 +138,32 @@ def blob_slide(channels=5, height=34560, width=24960, densities=(1e-4, 2.5e-4, 5
         out[c] = noisy.to(torch.int32).view(height, width).to(torch.uint16)
         del img, noisy
     return out
+
+
+def bead_batch(specs, device="cuda", density=3000 / (64 * 512 * 512), background=10.0):
+    """The uneven 2-D batch on the GPU: for each (h, w, sigma, seed) of
+    uneven_bead_batch, beads (intensity ~ U[1e3, 1e4], density per pixel as
+    the bead volume) at uniform integer positions, blurred by the normalised
+    Gaussian PSF of support 2*ceil(3 sigma) + 1 (zero padding; the library's
+    own separable blur, whose taps are that PSF's separable factors),
+    + background, + Poisson noise.  Returns (images f32, psfs f32) lists."""
+    import torch
+
+    from . import ops
+
+    images, psfs = [], []
+    for h, w, sigma, seed in specs:
+        gen = torch.Generator(device=device)
+        gen.manual_seed(int(seed))
+        n = max(1, int(round(density * h * w)))
+        img = torch.zeros(h * w, dtype=torch.float32, device=device)
+        pos = torch.randint(0, h * w, (n,), generator=gen, device=device)
+        amp = 1e3 + 9e3 * torch.rand(n, generator=gen, device=device)
+        img.index_add_(0, pos, amp)
+        r = int(np.ceil(3 * sigma))
+        blurred = ops.gaussian_blur(img.view(h, w), sigma, mode="constant", radii=r)
+        obs = torch.poisson(blurred + background, generator=gen).to(torch.float32)
+        k = 2 * r + 1
+        images.append(obs.contiguous())
+        psfs.append(torch.from_numpy(gaussian_psf((k, k), (sigma, sigma)).astype(np.float32)).to(device))
+    return images, psfs

@@ -96,10 +96,14 @@ def test_fft_lengths_and_rl_grid():
     assert lib.lucem_fft_good_length(1021, 0) == 1024
     assert lib.lucem_fft_good_length(1025, 0) == 1029  # 3 * 7^3
     assert lib.lucem_fft_good_length(1029, 1) == 1050
-    # zero padding needs n + k/2, the other modes n + 2 (k/2)
-    assert lb.rl_grid((64, 512, 512), (31, 15, 15), mode="constant") == (80, 525, 540)  # 520 = 8*5*13
+    # zero padding needs n + k/2, the other modes n + 2 (k/2); the automatic
+    # length is the cheapest m * 2^k above the need by the default pass costs
+    # (power-of-two register kernels 1; Stockham 5 for columns, 2.7 for rows)
+    assert lb.rl_grid((64, 512, 512), (31, 15, 15), mode="constant") == (128, 1024, 1024)
+    assert lb.rl_grid((40, 53), (7, 5), mode="reflect") == (64, 60)   # 60 * 2.7 < 128 * 1
+    assert lb.rl_grid((3000, 3000), (9, 9), mode="constant") == (3072, 3072)
     assert lb.rl_grid((64, 512, 512), (31, 15, 15), mode="constant", grid=(128, 1024, 1024)) == (128, 1024, 1024)
-    assert lb.rl_grid((100, 200), (9, 9), mode="reflect") == (108, 210)
+    assert lb.rl_grid((100, 200), (9, 9), mode="reflect") == (128, 256)
     with pytest.raises(N.LucemError) as e:
         lb.rl_grid((64, 512, 512), (31, 15, 15), mode="constant", grid=(64, 1024, 1024))
     assert e.value.name == "INVALID_PARAMETER"
