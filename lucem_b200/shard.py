@@ -44,3 +44,16 @@ def shard(items: Sequence[T], rank: int, world: int, cost: Callable[[T], float] 
 def block_cost(block) -> float:
     """Work estimate of one tile-walk block: its owned pixels."""
     return float(block.size[0] * block.size[1] * block.size[2])
+
+
+def allreduce_psf_grad(grad, group=None):
+    """Sum a PSF gradient over the ranks of the default (or given) process
+    group, in place: the one collective of a data-parallel PSF fit, where each
+    rank runs the reverse pass of its share of the volumes with the same PSF.
+    A no-op without an initialised process group or with one rank."""
+    import torch.distributed as dist
+
+    if not dist.is_available() or not dist.is_initialized() or dist.get_world_size(group) == 1:
+        return grad
+    dist.all_reduce(grad, op=dist.ReduceOp.SUM, group=group)
+    return grad

@@ -310,3 +310,18 @@ def test_psf_fit_configuration_gradient_on_64_taps(oracle):
     got = host(th.grad).reshape(-1)
     idx = rng.choice(theta.size, size=64, replace=False)
     oracle.assert_close(got[idx], _fd(loss64, theta, idx), FD_RTOL, "15x9x9 PSF, 20 iterations")
+
+
+@pytest.mark.parametrize("shape,kshape,T", [((40, 36), (7, 6), 8), ((12, 30, 28), (5, 7, 7), 6)])
+def test_rl_gradients_against_the_fp64_reverse_oracle(oracle, shape, kshape, T):
+    """Every PSF tap and every observation pixel against the FP64 reverse
+    pass (itself checked against central differences on the host)."""
+    rng = np.random.default_rng(sum(shape))
+    obs = rng.uniform(0.5, 2.0, shape).astype(np.float32).astype(np.float64)
+    psf = rng.uniform(0.2, 1.0, kshape).astype(np.float32).astype(np.float64)
+    w = rng.standard_normal(shape).astype(np.float32).astype(np.float64)
+    gp, gx = lb.richardson_lucy_backward(dev(obs), dev(psf), dev(w), num_iter=T, filter_epsilon=1e-6,
+                                         checkpoint_every=3)
+    wp, wx = oracle.richardson_lucy_backward_fft64(obs, psf, w, num_iter=T, filter_epsilon=1e-6)
+    oracle.assert_close(host(gp), wp, FD_RTOL, "psf gradient")
+    oracle.assert_close(host(gx), wx, FD_RTOL, "observation gradient")

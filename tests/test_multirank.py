@@ -77,3 +77,44 @@ def test_two_ranks_gloo_tile_walk_equals_whole_image(tmp_path):
     gathered = np.load(tmp_path / "gathered.npy")
     whole = np.load(tmp_path / "whole.npy")
     assert np.abs(gathered - whole).max() < 1e-3
+
+
+def _psf_fit_rank(rank, world, port, out_dir):
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, os.path.join(root, "oracle"))
+    import oracle as O
+    import torch
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        rng = np.random.default_rng(5)
+        vols = [rng.uniform(0.5, 2.0, (6, 10, 9)) for _ in range(5)]
+        ws = [rng.standard_normal((6, 10, 9)) for _ in range(5)]
+        psf = rng.uniform(0.2, 1.0, (3, 3, 3))
+        mine = shard.shard(list(range(5)), rank, world, lambda i: float(vols[i].size))
+        g = np.zeros(psf.shape)
+        for i in mine:
+            g += O.richardson_lucy_backward_fft64(vols[i], psf, ws[i], num_iter=3, filter_epsilon=1e-6)[0]
+        t = torch.from_numpy(g)
+        shard.allreduce_psf_grad(t)
+        if rank == 0:
+            np.save(os.path.join(out_dir, "dp.npy"), t.numpy())
+            whole = sum(O.richardson_lucy_backward_fft64(v, psf, w, num_iter=3, filter_epsilon=1e-6)[0]
+                        for v, w in zip(vols, ws))
+            np.save(os.path.join(out_dir, "single.npy"), whole)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_ranks_gloo_psf_gradient_allreduce(tmp_path):
+    """Data-parallel PSF fit: each rank's share of the volumes, one all-reduce
+    of the PSF gradient, equal to the single-process sum."""
+    port = _free_port()
+    mp.start_processes(_psf_fit_rank, args=(2, port, str(tmp_path)), nprocs=2, join=True, start_method="spawn")
+    dp = np.load(tmp_path / "dp.npy")
+    single = np.load(tmp_path / "single.npy")
+    assert np.allclose(dp, single, rtol=1e-12, atol=1e-15)

@@ -175,3 +175,34 @@ def test_halo_of_sigma_two_is_eight(oracle):
     """bindings/python/tests/test_runtime_io.py:28."""
     assert oracle.resolved_radius(4.0, 2.0) == 8
     assert int(np.ceil(4 * 2.0)) == 8
+
+
+@pytest.mark.parametrize("shape,kshape", [((12, 10), (3, 5)), ((11, 9), (4, 4)), ((6, 7, 8), (2, 3, 4))])
+def test_rl_backward_oracle_against_central_differences(oracle, shape, kshape):
+    """The FP64 reverse-mode oracle against FP64 central differences of the
+    FP64 RL (h 1e-5): PSF and observation gradients."""
+    rng = np.random.default_rng(sum(shape))
+    obs = rng.uniform(0.5, 2.0, shape)
+    psf = rng.uniform(0.2, 1.0, kshape)
+    w = rng.standard_normal(shape)
+    gp, gy = oracle.richardson_lucy_backward_fft64(obs, psf, w, num_iter=5, filter_epsilon=1e-6)
+
+    def loss(o, p):
+        return float(np.sum(w * oracle.richardson_lucy_fft64(o, p, num_iter=5, filter_epsilon=1e-6)))
+
+    h = 1e-5
+    fd = np.zeros(psf.size)
+    for i in range(psf.size):
+        pp = psf.copy().reshape(-1)
+        pp[i] += h
+        lp = loss(obs, pp.reshape(kshape))
+        pp[i] -= 2 * h
+        fd[i] = (lp - loss(obs, pp.reshape(kshape))) / (2 * h)
+    assert np.abs(gp.reshape(-1) - fd).max() <= 1e-7 * np.abs(fd).max()
+    for i in range(0, obs.size, max(1, obs.size // 6)):
+        oo = obs.copy().reshape(-1)
+        oo[i] += h
+        lp = loss(oo.reshape(shape), psf)
+        oo[i] -= 2 * h
+        d = (lp - loss(oo.reshape(shape), psf)) / (2 * h)
+        assert abs(gy.reshape(-1)[i] - d) <= 1e-7 * max(1.0, abs(d))
