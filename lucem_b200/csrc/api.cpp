@@ -1742,18 +1742,110 @@ lucem_status rl_prepare(lucem_ctx *ctx, const lucem_tensor *in, const lucem_tens
         su->same_centre = su->same_centre && su->c_conv[d] == su->c_corr[d];
     }
     const bool same_centre = su->same_centre;
-    const size_t hbytes = (size_t)g.Pz * g.Py * g.Hp * sizeof(float2_);
+    // A separable PSF (p = mz (x) my (x) mx / S^2 with the axis marginals, S =
+    // sum p, to 1e-6 of max |p|: the Gaussian PSFs) gets a factored transfer
+    // function built on the host: the z (3-D) or y (2-D) factor stays a
+    // vector and the pass multiplies it in, so no dense [Pz][Py][Hp] array is
+    // streamed through the passes.
+    std::vector<double> marg[3];
+    bool separable = false;
+    {
+        double S = 0.0, pmax = 0.0;
+        for (int d = 0; d < 3; ++d) marg[d].assign((size_t)kd[d], 0.0);
+        for (int64_t z = 0; z < kd[0]; ++z)
+            for (int64_t y = 0; y < kd[1]; ++y)
+                for (int64_t x = 0; x < kd[2]; ++x) {
+                    const double v = pn[(size_t)((z * kd[1] + y) * kd[2] + x)];
+                    marg[0][(size_t)z] += v;
+                    marg[1][(size_t)y] += v;
+                    marg[2][(size_t)x] += v;
+                    S += v;
+                    pmax = std::max(pmax, std::fabs(v));
+                }
+        if (std::fabs(S) > 1e-12 && pmax > 0.0) {
+            double err = 0.0;
+            for (int64_t z = 0; z < kd[0]; ++z)
+                for (int64_t y = 0; y < kd[1]; ++y)
+                    for (int64_t x = 0; x < kd[2]; ++x) {
+                        const double prod = marg[0][(size_t)z] * marg[1][(size_t)y] * marg[2][(size_t)x] / (S * S);
+                        err = std::max(err, std::fabs(pn[(size_t)((z * kd[1] + y) * kd[2] + x)] - prod));
+                    }
+            separable = err <= 1e-6 * pmax && kn > 1;
+            for (double &v : marg[2]) v /= S * S;
+        }
+    }
+    const size_t hbytes = separable ? (size_t)(nd == 3 ? g.Py : 1) * g.Hp * sizeof(float2_)
+                                    : (size_t)g.Pz * g.Py * g.Hp * sizeof(float2_);
+    const int64_t nrow = nd == 3 ? g.Pz : g.Py;
     std::string key(reinterpret_cast<const char *>(pn.data()), pn.size() * sizeof(double));
     key.append(reinterpret_cast<const char *>(kdi), sizeof kdi);
     key.append(reinterpret_cast<const char *>(grid), 3 * sizeof(int64_t));
     key.append(reinterpret_cast<const char *>(&g.Hp), sizeof g.Hp);
-    void *h_conv = nullptr, *h_corr = nullptr;
+    key.push_back(separable ? 's' : 'd');
+    void *h_conv = nullptr, *h_corr = nullptr, *r_conv = nullptr, *r_corr = nullptr;
     Slot *sl_conv = nullptr, *sl_corr = nullptr;
     if ((st = ws->get("rl_otf_conv", hbytes, &h_conv, &sl_conv))) return st;
     if (!same_centre && (st = ws->get("rl_otf_corr", hbytes, &h_corr, &sl_corr))) return st;
-    if (same_centre) h_corr = h_conv;
+    if (separable) {
+        if ((st = ws->get("rl_otf_conv_row", (size_t)nrow * sizeof(float2_), &r_conv))) return st;
+        if (!same_centre && (st = ws->get("rl_otf_corr_row", (size_t)nrow * sizeof(float2_), &r_corr))) return st;
+    }
+    if (same_centre) {
+        h_corr = h_conv;
+        r_corr = r_conv;
+    }
     const bool fresh = sl_conv->key != key || (!same_centre && sl_corr->key != key);
-    if (fresh) {
+    if (fresh && separable) {
+        // 1-D DFTs of the marginals at each centre, f64 (exact integer angle
+        // reduction), scale 1/(Pz Py Px) folded into the table.
+        auto dft = [](const std::vector<double> &m, int64_t c, int64_t P, int64_t nbins) {
+            std::vector<double> out((size_t)(2 * nbins), 0.0);
+            for (int64_t k = 0; k < nbins; ++k) {
+                double re = 0.0, im = 0.0;
+                for (int64_t s2 = 0; s2 < (int64_t)m.size(); ++s2) {
+                    const int64_t q = (((k * (s2 - c)) % P) + P) % P;
+                    const double a = 2.0 * M_PI * (double)q / (double)P;
+                    re += m[(size_t)s2] * std::cos(a);
+                    im -= m[(size_t)s2] * std::sin(a);
+                }
+                out[(size_t)(2 * k)] = re;
+                out[(size_t)(2 * k + 1)] = im;
+            }
+            return out;
+        };
+        const double scale = 1.0 / ((double)g.Pz * (double)g.Py * (double)g.Px);
+        cudaStream_t cs2 = static_cast<cudaStream_t>(stream);
+        std::vector<float> tab, rowv;
+        auto build = [&](const int32_t *cen, void *hdst, void *rdst) -> lucem_status {
+            const std::vector<double> fz = dft(marg[0], cen[0], g.Pz, g.Pz);
+            const std::vector<double> fy = dft(marg[1], cen[1], g.Py, g.Py);
+            const std::vector<double> fx = dft(marg[2], cen[2], g.Px, g.Hx);
+            const int64_t ny = nd == 3 ? g.Py : 1;
+            tab.assign((size_t)(2 * ny * g.Hp), 0.0f);
+            for (int64_t y = 0; y < ny; ++y)
+                for (int64_t x = 0; x < g.Hx; ++x) {
+                    // 3-D: Fy(y) Fx(x); 2-D: Fz(0) Fx(x) (Fz(0) = the z marginal's sum).
+                    const double ar = nd == 3 ? fy[(size_t)(2 * y)] : fz[0];
+                    const double ai = nd == 3 ? fy[(size_t)(2 * y + 1)] : fz[1];
+                    const double br = fx[(size_t)(2 * x)], bi = fx[(size_t)(2 * x + 1)];
+                    tab[(size_t)(2 * (y * g.Hp + x))] = (float)((ar * br - ai * bi) * scale);
+                    tab[(size_t)(2 * (y * g.Hp + x) + 1)] = (float)((ar * bi + ai * br) * scale);
+                }
+            const std::vector<double> &fr = nd == 3 ? fz : fy;
+            rowv.assign(fr.begin(), fr.end());
+            CUDA_TRY(cudaMemcpyAsync(hdst, tab.data(), tab.size() * sizeof(float), cudaMemcpyHostToDevice, cs2),
+                     "transfer function upload");
+            CUDA_TRY(cudaMemcpyAsync(rdst, rowv.data(), rowv.size() * sizeof(float), cudaMemcpyHostToDevice, cs2),
+                     "transfer function upload");
+            // The host tables are reused for the second centre.
+            CUDA_TRY(cudaStreamSynchronize(cs2), "transfer function upload");
+            return ok();
+        };
+        if ((st = build(su->c_conv, h_conv, r_conv))) return st;
+        if (!same_centre && (st = build(su->c_corr, h_corr, r_corr))) return st;
+        sl_conv->key = key;
+        if (sl_corr) sl_corr->key = key;
+    } else if (fresh) {
         void *psf64 = nullptr, *wa = nullptr, *wb = nullptr;
         if ((st = ws->get("rl_psf64", (size_t)kn * sizeof(double), &psf64))) return st;
         if ((st = ws->get("rl_otf_a", (size_t)kd[0] * kd[1] * g.Hp * 16, &wa))) return st;
@@ -1784,6 +1876,8 @@ lucem_status rl_prepare(lucem_ctx *ctx, const lucem_tensor *in, const lucem_tens
     b.s2 = s2;
     b.h_conv = h_conv;
     b.h_corr = h_corr;
+    b.hrow_conv = separable ? r_conv : nullptr;
+    b.hrow_corr = separable ? r_corr : nullptr;
     b.tw_x = tw32[2];
     b.tw_y = tw32[1];
     b.tw_z = tw32[0];

@@ -83,7 +83,11 @@ constexpr double sin2pi(long m, long L) {
     return q == 0 ? sp : (q == 1 ? cp : (q == 2 ? -sp : -cp));
 }
 
-__device__ __forceinline__ float2 add(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+// Complex add as one packed f32x2 instruction (sm_100; the same IEEE result
+// per component as two scalar adds).  Subtraction stays scalar: the packed
+// form needs the negated pair in extra registers and made the 128-register
+// transforms spill.
+__device__ __forceinline__ float2 add(float2 a, float2 b) { return __fadd2_rn(a, b); }
 __device__ __forceinline__ float2 sub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
 __device__ __forceinline__ float2 mul(float2 a, float2 w) {
     return make_float2(fmaf(a.x, w.x, -a.y * w.y), fmaf(a.x, w.y, a.y * w.x));

@@ -190,9 +190,10 @@ __device__ void family_tile(const FamParams &p, const TileGeom &g, float *A, flo
     const int AH = kTH + 2 * R0;
     const T *in = static_cast<const T *>(p.in) + (int64_t)g.plane * p.in_plane_stride;
 
-    // Phase 0: tile + halo -> A (f32).  Each thread issues all loads of a
-    // chunk (8 per thread) before any of its shared-memory stores, so a warp
-    // has many global loads in flight instead of one row at a time.
+    // Phase 0: tile + halo -> A (f32).  A warp stages rows warp, warp + 8,
+    // ...; each lane covers columns lane, lane + 32, ... of a row (no index
+    // division), and every lane issues the loads of 4 rows before storing
+    // any of them, so many global loads are in flight per warp.
     {
         const int wy0 = g.oy - g.rb_y - R0, wx0 = g.ox - g.rb_x - R1;  // window origin in the read box
         const T *wbase = in + (int64_t)g.rb_y * p.in_row_pitch + g.rb_x;
@@ -200,52 +201,58 @@ __device__ void family_tile(const FamParams &p, const TileGeom &g, float *A, flo
         const T *w0 = wbase + (int64_t)wy0 * p.in_row_pitch + wx0;
         const bool pairs_ok = (p.in_row_pitch % 2 == 0) &&
                               (reinterpret_cast<uintptr_t>(w0) % (2 * sizeof(T)) == 0);
-        constexpr int kChunk = NOUT == 1 ? 8 : 4;
+        const int lane = tid & 31, warp = tid >> 5;
+        constexpr int kRows = NOUT == 1 ? 4 : 2;  // rows in flight per lane
+        constexpr int kWarps = kThreads / 32;
         if (interior && pairs_ok) {
-            // No pad map: two samples per load (AWP is even).
+            // No pad map: two samples per load (AWP is even, <= 128).
             using V2 = typename Pair<T>::type;
-            const int npr = AWP / 2, total = AH * npr;
-            for (int i0 = tid; i0 < total; i0 += kThreads * kChunk) {
-                V2 v[kChunk];
+            const int npr = AWP / 2;
+            for (int r0 = warp; r0 < AH; r0 += kWarps * kRows) {
+                V2 v[kRows][2];
 #pragma unroll
-                for (int u = 0; u < kChunk; ++u) {
-                    const int i = i0 + u * kThreads;
-                    if (i < total) {
-                        const int r = i / npr, c = i - r * npr;
-                        v[u] = __ldg(reinterpret_cast<const V2 *>(w0 + (int64_t)r * p.in_row_pitch) + c);
-                    }
+                for (int k = 0; k < kRows; ++k) {
+                    const int r = r0 + kWarps * k;
+                    const V2 *src = reinterpret_cast<const V2 *>(w0 + (int64_t)r * p.in_row_pitch);
+#pragma unroll
+                    for (int h = 0; h < 2; ++h)
+                        if (r < AH && lane + 32 * h < npr) v[k][h] = __ldg(src + lane + 32 * h);
                 }
 #pragma unroll
-                for (int u = 0; u < kChunk; ++u) {
-                    const int i = i0 + u * kThreads;
-                    if (i < total) {
-                        const int r = i / npr, c = i - r * npr;
-                        *reinterpret_cast<float2 *>(A + r * AWP + 2 * c) =
-                            make_float2((float)v[u].x * p.in_scale, (float)v[u].y * p.in_scale);
-                    }
+                for (int k = 0; k < kRows; ++k) {
+                    const int r = r0 + kWarps * k;
+#pragma unroll
+                    for (int h = 0; h < 2; ++h)
+                        if (r < AH && lane + 32 * h < npr)
+                            *reinterpret_cast<float2 *>(A + r * AWP + 2 * (lane + 32 * h)) =
+                                make_float2((float)v[k][h].x * p.in_scale, (float)v[k][h].y * p.in_scale);
                 }
             }
         } else {
-            // Pad map relative to the read box (border tiles, odd pitches).
-            const int total = AH * AWP;
-            for (int i0 = tid; i0 < total; i0 += kThreads * kChunk) {
-                float v[kChunk];
+            // Pad map relative to the read box (border tiles, odd pitches):
+            // the row map once per row, the column map per element.
+            for (int r0 = warp; r0 < AH; r0 += kWarps * kRows) {
+                float v[kRows][4];
 #pragma unroll
-                for (int u = 0; u < kChunk; ++u) {
-                    const int i = i0 + u * kThreads;
-                    v[u] = p.cval;
-                    if (i < total) {
-                        const int r = i / AWP, c = i - r * AWP;
-                        const int py = pad_index_rt(wy0 + r, g.rb_h, p.mode);
-                        const int px = pad_index_rt(wx0 + c, g.rb_w, p.mode);
-                        if (py >= 0 && px >= 0)
-                            v[u] = load_as_float(wbase + (int64_t)py * p.in_row_pitch + px) * p.in_scale;
+                for (int k = 0; k < kRows; ++k) {
+                    const int r = r0 + kWarps * k;
+                    const int py = r < AH ? pad_index_rt(wy0 + r, g.rb_h, p.mode) : -1;
+#pragma unroll
+                    for (int h = 0; h < 4; ++h) {
+                        const int c = lane + 32 * h;
+                        v[k][h] = p.cval;
+                        if (py >= 0 && c < AWP) {
+                            const int px = pad_index_rt(wx0 + c, g.rb_w, p.mode);
+                            if (px >= 0) v[k][h] = load_as_float(wbase + (int64_t)py * p.in_row_pitch + px) * p.in_scale;
+                        }
                     }
                 }
 #pragma unroll
-                for (int u = 0; u < kChunk; ++u) {
-                    const int i = i0 + u * kThreads;
-                    if (i < total) A[i] = v[u];
+                for (int k = 0; k < kRows; ++k) {
+                    const int r = r0 + kWarps * k;
+#pragma unroll
+                    for (int h = 0; h < 4; ++h)
+                        if (r < AH && lane + 32 * h < AWP) A[r * AWP + lane + 32 * h] = v[k][h];
                 }
             }
         }

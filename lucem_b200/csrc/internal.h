@@ -186,6 +186,11 @@ struct RlBuffers {
     void *s2;      // complex [Z][Py][Hp] (3-D only)
     const void *h_conv;  // complex [Pz][Py][Hp]
     const void *h_corr;  // complex [Pz][Py][Hp] (may equal h_conv)
+    // Separable PSF: h_conv / h_corr hold the product of the factors of all
+    // axes but the last transformed one ([Py][Hp] in 3-D, [Hp] in 2-D) and
+    // hrow_* that factor ([Pz] in 3-D, [Py] in 2-D).  Null: dense transfer
+    // functions.
+    const void *hrow_conv, *hrow_corr;
     const float2_ *tw_x, *tw_y, *tw_z;  // twiddle tables e^{-2 pi i k / n}, n = Px, Py, Pz
 };
 

@@ -88,7 +88,11 @@ struct ColPass {
     const float2 *H;              // transfer function (kColFull)
     int64_t h_outer, h_row;
     int32_t conj_h;
-    float2 *spec_out;             // kColFull: also store the forward spectrum here (H's layout), or null
+    float2 *spec_out;             // kColFull: also store the forward spectrum here, or null:
+    int64_t spec_row;             // [outer * h_outer + row * spec_row + kx] (the dense layout)
+    const float2 *Hrow;           // kColFull, separable transfer function: the factor along the
+                                  // transformed axis (natural order); H then holds the other
+                                  // axes' product and h_row is 0.  Null: H is dense.
     FftPlan plan;
     const float2 *tw;             // e^{-2 pi i m / n}, m < n
     int32_t C, CP;
@@ -182,8 +186,9 @@ __global__ void __launch_bounds__(512, 1) col_pass_kernel(const __grid_constant_
                 int col = c0 + c;
                 if (col < q.ncols) {
                     int outer = col / q.Hx, kx = col - outer * q.Hx;
-                    if (q.spec_out) q.spec_out[outer * q.h_outer + row * q.h_row + kx] = buf[row * CP + c];
+                    if (q.spec_out) q.spec_out[outer * q.h_outer + row * p.spec_row + kx] = buf[row * CP + c];
                     float2 h = q.H[outer * q.h_outer + row * q.h_row + kx];
+                    if (p.Hrow) h = cmul(h, p.Hrow[row]);
                     if (p.conj_h) h.y = -h.y;
                     buf[row * CP + c] = cmul(buf[row * CP + c], h);
                 }
@@ -209,7 +214,7 @@ __global__ void __launch_bounds__(512, 1) col_pass_kernel(const __grid_constant_
 // each thread loads its N2 values straight from global memory (lanes along
 // columns: coalesced), transforms in registers with one shared-memory
 // exchange per direction, multiplies by H in registers and stores back.
-template <int N1, int N2, int C>
+template <int N1, int N2, int C, bool SEP>
 __global__ void __launch_bounds__(N1 * C, (N2 > 32 ? 1 : 65536 / (N1 * C * 128))) col_fast_kernel(const __grid_constant__ ColPass p) {
     using L = fftc::ColLayout<N1, N2, C>;
     using F = fftc::TwoStep<N1, N2, L>;
@@ -247,7 +252,10 @@ __global__ void __launch_bounds__(N1 * C, (N2 > 32 ? 1 : 65536 / (N1 * C * 128))
             // (one memory round trip per tile instead of two).
             constexpr bool kPrefetchH = N2 <= 16;
             float2 hv[kPrefetchH ? N2 : 1];
-            if (kPrefetchH && p.mode == kColFull) {
+            // SEP: separable transfer function (ColPass::Hrow), chosen at launch.
+            float2 hc = make_float2(0.f, 0.f);
+            if (SEP && p.mode == kColFull && ok) hc = h[0];
+            if (kPrefetchH && p.mode == kColFull && !SEP) {
 #pragma unroll
                 for (int j = 0; j < (kPrefetchH ? N2 : 1); ++j)
                     hv[j] = ok ? h[F::freq(t, j) * h_row] : make_float2(0.f, 0.f);
@@ -262,7 +270,7 @@ __global__ void __launch_bounds__(N1 * C, (N2 > 32 ? 1 : 65536 / (N1 * C * 128))
             if (p.mode == kColFull && q.spec_out != nullptr && ok) {
                 float2 *so = q.spec_out + (outer * q.h_outer + kx);
 #pragma unroll
-                for (int j = 0; j < N2; ++j) so[F::freq(t, j) * h_row] = v[j];
+                for (int j = 0; j < N2; ++j) so[F::freq(t, j) * (int)p.spec_row] = v[j];
             }
             if (p.mode == kColFwd) {
                 float2 *dst = q.dst + (outer * q.dst_outer + kx);
@@ -275,7 +283,8 @@ __global__ void __launch_bounds__(N1 * C, (N2 > 32 ? 1 : 65536 / (N1 * C * 128))
 #pragma unroll
             for (int j = 0; j < N2; ++j) {
                 float2 hj;
-                if constexpr (kPrefetchH) hj = hv[j];
+                if constexpr (SEP) hj = fftc::mul(hc, p.Hrow[F::freq(t, j)]);
+                else if constexpr (kPrefetchH) hj = hv[j];
                 else hj = ok ? h[F::freq(t, j) * h_row] : make_float2(0.f, 0.f);
                 if (p.conj_h) hj.y = -hj.y;
                 v[j] = fftc::mul(v[j], hj);
@@ -734,8 +743,13 @@ int launch_col_fast(const ColPass &p, cudaStream_t s) {
     int per_sm = (int)((200 * 1024) / (smem + 1024));
     per_sm = per_sm < 1 ? 1 : (per_sm > 8 ? 8 : per_sm);
     int grid = ntiles < sms() * per_sm ? ntiles : sms() * per_sm;
-    cudaFuncSetAttribute(col_fast_kernel<N1, N2, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    col_fast_kernel<N1, N2, C><<<grid, N1 * C, smem, s>>>(p);
+    if (p.Hrow) {
+        cudaFuncSetAttribute(col_fast_kernel<N1, N2, C, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        col_fast_kernel<N1, N2, C, true><<<grid, N1 * C, smem, s>>>(p);
+    } else {
+        cudaFuncSetAttribute(col_fast_kernel<N1, N2, C, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        col_fast_kernel<N1, N2, C, false><<<grid, N1 * C, smem, s>>>(p);
+    }
     return (int)cudaGetLastError();
 }
 
@@ -915,6 +929,10 @@ struct RlRunner {
     int pair(const void *H, int conj, float2 *spec_out) {
         float2 *s1 = static_cast<float2 *>(b.s1);
         float2 *s2 = static_cast<float2 *>(b.s2);
+        // A separable transfer function comes with its factor along the last
+        // transformed axis (z in 3-D, y in 2-D).
+        const float2 *Hrow = static_cast<const float2 *>(
+            H == b.h_conv ? b.hrow_conv : (H == b.h_corr ? b.hrow_corr : nullptr));
         if (g.ndim == 2) {
             ColPass c{};
             c.ncols = g.Hx; c.Hx = g.Hx;
@@ -923,8 +941,10 @@ struct RlRunner {
             c.dst = s1; c.dst_outer = 0; c.dst_row = g.Hp;
             c.store_begin = g.hy; c.store_count = g.Y;
             c.mode = kColFull; c.pad_mode = g.mode;
-            c.H = static_cast<const float2 *>(H); c.h_outer = 0; c.h_row = g.Hp; c.conj_h = conj;
+            c.H = static_cast<const float2 *>(H); c.h_outer = 0; c.h_row = Hrow ? 0 : g.Hp; c.conj_h = conj;
+            c.Hrow = Hrow;
             c.spec_out = spec_out;
+            c.spec_row = g.Hp;
             c.plan = py_plan; c.tw = reinterpret_cast<const float2 *>(b.tw_y);
             return col(c);
         }
@@ -937,9 +957,11 @@ struct RlRunner {
         zp.dst = s2; zp.dst_outer = g.Hp; zp.dst_row = (int64_t)g.Py * g.Hp;
         zp.store_begin = g.hz; zp.store_count = g.Z;
         zp.mode = kColFull; zp.pad_mode = g.mode;
-        zp.H = static_cast<const float2 *>(H); zp.h_outer = g.Hp; zp.h_row = (int64_t)g.Py * g.Hp;
+        zp.H = static_cast<const float2 *>(H); zp.h_outer = g.Hp; zp.h_row = Hrow ? 0 : (int64_t)g.Py * g.Hp;
         zp.conj_h = conj;
+        zp.Hrow = Hrow;
         zp.spec_out = spec_out;
+        zp.spec_row = (int64_t)g.Py * g.Hp;
         zp.plan = pz_plan; zp.tw = reinterpret_cast<const float2 *>(b.tw_z);
         if ((e = col(zp))) return e;
         return col(y_inverse(s2, (int64_t)g.Py * g.Hp));

@@ -312,13 +312,19 @@ def test_psf_fit_configuration_gradient_on_64_taps(oracle):
     oracle.assert_close(got[idx], _fd(loss64, theta, idx), FD_RTOL, "15x9x9 PSF, 20 iterations")
 
 
-@pytest.mark.parametrize("shape,kshape,T", [((40, 36), (7, 6), 8), ((12, 30, 28), (5, 7, 7), 6)])
-def test_rl_gradients_against_the_fp64_reverse_oracle(oracle, shape, kshape, T):
+@pytest.mark.parametrize("shape,kshape,T,gauss", [((40, 36), (7, 6), 8, False), ((12, 30, 28), (5, 7, 7), 6, False),
+                                                  ((40, 36), (6, 9), 8, True), ((12, 30, 28), (5, 7, 7), 6, True)])
+def test_rl_gradients_against_the_fp64_reverse_oracle(oracle, shape, kshape, T, gauss):
     """Every PSF tap and every observation pixel against the FP64 reverse
-    pass (itself checked against central differences on the host)."""
+    pass (itself checked against central differences on the host); a
+    Gaussian PSF takes the factored (separable) transfer-function path."""
     rng = np.random.default_rng(sum(shape))
     obs = rng.uniform(0.5, 2.0, shape).astype(np.float32).astype(np.float64)
-    psf = rng.uniform(0.2, 1.0, kshape).astype(np.float32).astype(np.float64)
+    if gauss:
+        psf = lb.synth.gaussian_psf(kshape, [1.3 + 0.2 * i for i in range(len(kshape))])
+    else:
+        psf = rng.uniform(0.2, 1.0, kshape)
+    psf = psf.astype(np.float32).astype(np.float64)
     w = rng.standard_normal(shape).astype(np.float32).astype(np.float64)
     gp, gx = lb.richardson_lucy_backward(dev(obs), dev(psf), dev(w), num_iter=T, filter_epsilon=1e-6,
                                          checkpoint_every=3)
