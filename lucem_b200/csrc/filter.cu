@@ -66,6 +66,17 @@ __device__ __forceinline__ int pad_index_rt(int p, int len, int mode) {
     }
 }
 
+// u8 / u16 / f32 -> f32 times `scale`.  Integers go through the float bit
+// pattern 2^23 + v (exact for v < 2^23) on the FMA pipe instead of a
+// conversion instruction: (2^23 + v) * s - 2^23 * s is v * s rounded once,
+// the same value as float(v) * s.
+__device__ __forceinline__ float to_f32_scaled(uint32_t v, float s) {
+    return fmaf(__uint_as_float(0x4B000000u | v), s, -8388608.0f * s);
+}
+__device__ __forceinline__ float to_f32_scaled(uint16_t v, float s) { return to_f32_scaled((uint32_t)v, s); }
+__device__ __forceinline__ float to_f32_scaled(uint8_t v, float s) { return to_f32_scaled((uint32_t)v, s); }
+__device__ __forceinline__ float to_f32_scaled(float v, float s) { return v * s; }
+
 template <typename T>
 __device__ __forceinline__ float load_as_float(const T *p) { return static_cast<float>(__ldg(p)); }
 
@@ -225,7 +236,7 @@ __device__ void family_tile(const FamParams &p, const TileGeom &g, float *A, flo
                     for (int h = 0; h < 2; ++h)
                         if (r < AH && lane + 32 * h < npr)
                             *reinterpret_cast<float2 *>(A + r * AWP + 2 * (lane + 32 * h)) =
-                                make_float2((float)v[k][h].x * p.in_scale, (float)v[k][h].y * p.in_scale);
+                                make_float2(to_f32_scaled(v[k][h].x, p.in_scale), to_f32_scaled(v[k][h].y, p.in_scale));
                 }
             }
         } else {
@@ -243,7 +254,7 @@ __device__ void family_tile(const FamParams &p, const TileGeom &g, float *A, flo
                         v[k][h] = p.cval;
                         if (py >= 0 && c < AWP) {
                             const int px = pad_index_rt(wx0 + c, g.rb_w, p.mode);
-                            if (px >= 0) v[k][h] = load_as_float(wbase + (int64_t)py * p.in_row_pitch + px) * p.in_scale;
+                            if (px >= 0) v[k][h] = to_f32_scaled(__ldg(wbase + (int64_t)py * p.in_row_pitch + px), p.in_scale);
                         }
                     }
                 }
