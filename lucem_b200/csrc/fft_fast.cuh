@@ -157,6 +157,30 @@ __device__ __forceinline__ void rdft(float2 *v) {
     }
 }
 
+// First decimation-in-frequency stage when the upper half of the input is
+// zero: (a, 0) -> (a, W_L^j a).
+template <int L, int... J>
+__device__ __forceinline__ void first_stage_zero_hi(float2 *v, std::integer_sequence<int, J...>) {
+    ((v[J + L / 2] = rot<L, J, false>(v[J])), ...);
+}
+
+// Decimation-in-time inverse of length L computing only the lower half of
+// the output: every stage but the last as rdft, the last one (half span
+// L/2, a single block) producing v[j] = v[j] + W^j v[j + L/2] only.
+template <int L, int... J>
+__device__ __forceinline__ void last_stage_lo(float2 *v, std::integer_sequence<int, J...>) {
+    ((v[J] = add(v[J], rot<L, J, true>(v[J + L / 2]))), ...);
+}
+template <int L, int H = 1>
+__device__ __forceinline__ void rdft_inv_lo(float2 *v) {
+    if constexpr (2 * H < L) {
+        stage<H, true, false>(v, std::make_integer_sequence<int, L / 2>{});
+        rdft_inv_lo<L, 2 * H>(v);
+    } else {
+        last_stage_lo<L>(v, std::make_integer_sequence<int, L / 2>{});
+    }
+}
+
 // Exchange-buffer layouts.  ColLayout: C sequences per CTA along columns
 // (lanes run along c); [N2][N1 * C + PAD] with PAD = C mod 16 so that a half
 // warp touches 32 distinct banks.  RowLayout: R sequences per CTA along rows
@@ -200,9 +224,17 @@ struct TwoStep {
     }
 
     // v[i] = x[t + N1 i]  ->  v[s N1 + p] = X[(t + N1 s) + N2 bitrev_N1(p)]
-    // (see freq).  Ends synchronised.
+    // (see freq).  Ends synchronised.  ZERO_HI: the input rows N/2 .. N-1
+    // are zero (v[i] = 0 for i >= N2/2; zero padding to at least twice the
+    // data), so the first butterfly stage reduces to v[i + N2/2] = W v[i].
+    template <bool ZERO_HI = false>
     __device__ __forceinline__ static void forward(float2 *v, int t, int c, float2 *xb, const float2 *tf) {
-        rdft<N2, false>(v);  // v[p] = Y[bitrev(p)]
+        if constexpr (ZERO_HI && N2 >= 4) {
+            first_stage_zero_hi<N2>(v, std::make_integer_sequence<int, N2 / 2>{});
+            rdft<N2, false, N2 / 4>(v);
+        } else {
+            rdft<N2, false>(v);  // v[p] = Y[bitrev(p)]
+        }
 #pragma unroll
         for (int p = 0; p < N2; ++p) {
             const int k2 = bitrev(p, N2);
@@ -221,6 +253,9 @@ struct TwoStep {
     }
 
     // Inverse (unnormalised) of the forward layout: v[i] = N x[t + N1 i] on return.
+    // LO_ONLY: only the rows 0 .. N/2-1 are wanted (v[i], i < N2/2); the
+    // last butterfly stage skips the upper halves, which are left undefined.
+    template <bool LO_ONLY = false>
     __device__ __forceinline__ static void inverse(float2 *v, int t, int c, float2 *xb, const float2 *ti) {
 #pragma unroll
         for (int s = 0; s < S; ++s) {
@@ -236,7 +271,8 @@ struct TwoStep {
         __syncthreads();
 #pragma unroll
         for (int k2 = 0; k2 < N2; ++k2) v[bitrev(k2, N2)] = xb[Layout::idx(k2, t, c)];
-        rdft<N2, true>(v);
+        if constexpr (LO_ONLY && N2 >= 4) rdft_inv_lo<N2>(v);
+        else rdft<N2, true>(v);
         __syncthreads();
     }
 

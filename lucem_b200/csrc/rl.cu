@@ -214,8 +214,13 @@ __global__ void __launch_bounds__(512, 1) col_pass_kernel(const __grid_constant_
 // each thread loads its N2 values straight from global memory (lanes along
 // columns: coalesced), transforms in registers with one shared-memory
 // exchange per direction, multiplies by H in registers and stores back.
-template <int N1, int N2, int C, bool SEP>
+// PR (chosen at launch for zero padding to at least twice the data):
+// bit 1, the input rows N/2 .. N-1 are zero (not loaded, first forward
+// stage pruned); bit 2, only the rows below N/2 are stored (last inverse
+// stage pruned).
+template <int N1, int N2, int C, bool SEP, int PR>
 __global__ void __launch_bounds__(N1 * C, (N2 > 32 ? 1 : 65536 / (N1 * C * 128))) col_fast_kernel(const __grid_constant__ ColPass p) {
+    constexpr bool kZeroHi = (PR & 1) != 0, kLoOnly = (PR & 2) != 0;
     using L = fftc::ColLayout<N1, N2, C>;
     using F = fftc::TwoStep<N1, N2, L>;
     constexpr int N = N1 * N2;
@@ -245,7 +250,7 @@ __global__ void __launch_bounds__(N1 * C, (N2 > 32 ? 1 : 65536 / (N1 * C * 128))
         if (p.mode == kColInv) {
 #pragma unroll
             for (int j = 0; j < N2; ++j) v[j] = ok ? src[F::freq(t, j) * src_row] : make_float2(0.f, 0.f);
-            F::inverse(v, t, c, xb, ti);
+            F::template inverse<kLoOnly>(v, t, c, xb, ti);
         } else {
             const float2 *h = q.H + (outer * q.h_outer + kx);
             // Short transforms prefetch the transfer function with the data
@@ -262,11 +267,12 @@ __global__ void __launch_bounds__(N1 * C, (N2 > 32 ? 1 : 65536 / (N1 * C * 128))
             }
 #pragma unroll
             for (int i = 0; i < N2; ++i) {
+                if (kZeroHi && i >= N2 / 2) continue;  // rows >= N/2: zero, never read
                 const int row = t + N1 * i;
                 int srow = row < n_ext ? pad_index_rt(row - q.halo, q.n_img, p.pad_mode) : -1;
                 v[i] = (ok && srow >= 0) ? src[srow * src_row] : make_float2(0.f, 0.f);
             }
-            F::forward(v, t, c, xb, tf);
+            F::template forward<kZeroHi>(v, t, c, xb, tf);
             if (p.mode == kColFull && q.spec_out != nullptr && ok) {
                 float2 *so = q.spec_out + (outer * q.h_outer + kx);
 #pragma unroll
@@ -289,12 +295,13 @@ __global__ void __launch_bounds__(N1 * C, (N2 > 32 ? 1 : 65536 / (N1 * C * 128))
                 if (p.conj_h) hj.y = -hj.y;
                 v[j] = fftc::mul(v[j], hj);
             }
-            F::inverse(v, t, c, xb, ti);
+            F::template inverse<kLoOnly>(v, t, c, xb, ti);
         }
         float2 *dst = q.dst + (outer * q.dst_outer + kx);
         if (ok) {
 #pragma unroll
             for (int i = 0; i < N2; ++i) {
+                if (kLoOnly && i >= N2 / 2) continue;  // not computed, not stored
                 const int row = t + N1 * i - q.store_begin;
                 if (row >= 0 && row < q.store_count) dst[row * dst_row] = v[i];
             }
@@ -470,7 +477,10 @@ __global__ void __launch_bounds__(512, 1) row_pass_kernel(const __grid_constant_
 
 // Fast row pass for packed lengths M = N1 * N2 (powers of two): R rows per
 // CTA, lanes along the row (coalesced), the M-point transforms in registers.
-template <int N1, int N2, int R>
+// ZP (chosen at launch): the real row's data and extension fit the first
+// half (X + 2 hx <= Px / 2), so the packed samples m >= M/2 are zero going
+// into the forward transform and unused coming out of the inverse one.
+template <int N1, int N2, int R, bool ZP>
 __global__ void __launch_bounds__(N1 * R, 65536 / (N1 * R * 128)) row_fast_kernel(const __grid_constant__ RowPass p) {
     using L = fftc::RowLayout<N1, N2, R>;
     using F = fftc::TwoStep<N1, N2, L>;
@@ -515,7 +525,7 @@ __global__ void __launch_bounds__(N1 * R, 65536 / (N1 * R * 128)) row_fast_kerne
 #pragma unroll
             for (int j = 0; j < N2; ++j) v[j] = spec[F::freq(t, j)];
             __syncthreads();
-            F::inverse(v, t, r, xb, ti);
+            F::template inverse<ZP>(v, t, r, xb, ti);
         }
         // v[i] = (x[2m], x[2m+1]), m = t + N1 i.  Epilogue on the image
         // columns, 8 values of m at a time: all loads of a chunk are issued
@@ -600,7 +610,7 @@ __global__ void __launch_bounds__(N1 * R, 65536 / (N1 * R * 128)) row_fast_kerne
             }
             __syncthreads();
         }
-        F::forward(v, t, r, xb, tf);
+        F::template forward<ZP>(v, t, r, xb, tf);
 #pragma unroll
         for (int j = 0; j < N2; ++j) spec[F::freq(t, j)] = v[j];
         __syncthreads();
@@ -743,12 +753,28 @@ int launch_col_fast(const ColPass &p, cudaStream_t s) {
     int per_sm = (int)((200 * 1024) / (smem + 1024));
     per_sm = per_sm < 1 ? 1 : (per_sm > 8 ? 8 : per_sm);
     int grid = ntiles < sms() * per_sm ? ntiles : sms() * per_sm;
+    // Pruning needs the zero rows / the unstored rows to be the upper half of
+    // every column (single problems only: a batch's items differ).
+    const int N_ = N1 * N2;
+    int pr = 0;
+    if (!p.items && p.mode != kColInv && p.n_img + 2 * p.halo <= N_ / 2) pr |= 1;
+    if (!p.items && p.mode != kColFwd && p.store_begin >= 0 && p.store_begin + p.store_count <= N_ / 2) pr |= 2;
+    auto go = [&](auto kern) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        kern<<<grid, N1 * C, smem, s>>>(p);
+    };
     if (p.Hrow) {
-        cudaFuncSetAttribute(col_fast_kernel<N1, N2, C, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        col_fast_kernel<N1, N2, C, true><<<grid, N1 * C, smem, s>>>(p);
+        // Separable products occur in the forward * H * inverse pass only,
+        // where zero padding prunes both ends or neither.
+        if (pr == 3) go(col_fast_kernel<N1, N2, C, true, 3>);
+        else go(col_fast_kernel<N1, N2, C, true, 0>);
     } else {
-        cudaFuncSetAttribute(col_fast_kernel<N1, N2, C, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        col_fast_kernel<N1, N2, C, false><<<grid, N1 * C, smem, s>>>(p);
+        switch (pr) {
+        case 0: go(col_fast_kernel<N1, N2, C, false, 0>); break;
+        case 1: go(col_fast_kernel<N1, N2, C, false, 1>); break;
+        case 2: go(col_fast_kernel<N1, N2, C, false, 2>); break;
+        default: go(col_fast_kernel<N1, N2, C, false, 3>); break;
+        }
     }
     return (int)cudaGetLastError();
 }
@@ -763,8 +789,14 @@ int launch_row_fast(const RowPass &p, cudaStream_t s) {
     int per_sm = (int)((200 * 1024) / (smem + 1024));
     per_sm = per_sm < 1 ? 1 : (per_sm > 8 ? 8 : per_sm);
     int grid = ntiles < sms() * per_sm ? ntiles : sms() * per_sm;
-    cudaFuncSetAttribute(row_fast_kernel<N1, N2, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    row_fast_kernel<N1, N2, R><<<grid, N1 * R, smem, s>>>(p);
+    // Pruning for single problems only (a batch's items differ in X).
+    if (!p.items && p.X + 2 * p.hx <= p.Px / 2) {
+        cudaFuncSetAttribute(row_fast_kernel<N1, N2, R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        row_fast_kernel<N1, N2, R, true><<<grid, N1 * R, smem, s>>>(p);
+    } else {
+        cudaFuncSetAttribute(row_fast_kernel<N1, N2, R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        row_fast_kernel<N1, N2, R, false><<<grid, N1 * R, smem, s>>>(p);
+    }
     return (int)cudaGetLastError();
 }
 
