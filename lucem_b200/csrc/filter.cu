@@ -193,10 +193,12 @@ __device__ __forceinline__ void hpass_r(int R, const float *IT, int x0, int yp, 
 // One 64 x 64 output tile: stage tile + halo (cast fused), then per filter
 // the axis-0 pass into IT and the axis-1 pass into registers, folded into
 // every response that uses the filter; responses written once at the end.
-template <typename T, int NOUT>
+template <typename T, int NOUT, int RF = -1>
 __device__ void family_tile(const FamParams &p, const TileGeom &g, float *A, float *IT) {
     const int tid = threadIdx.x;
-    const int R0 = p.rmax0, R1 = p.rmax1;
+    // RF >= 0: one filter whose two kernel radii are both RF, known at compile
+    // time (strides and tap loops become constants).
+    const int R0 = RF >= 0 ? RF : p.rmax0, R1 = RF >= 0 ? RF : p.rmax1;
     const int AWP = kTW + 2 * R1;   // even (R1 even)
     const int AH = kTH + 2 * R0;
     const T *in = static_cast<const T *>(p.in) + (int64_t)g.plane * p.in_plane_stride;
@@ -297,11 +299,13 @@ __device__ void family_tile(const FamParams &p, const TileGeom &g, float *A, flo
         }
     }
 
-    for (int f = 0; f < p.n_filters; ++f) {
-        const int r0 = p.r0[f], r1 = p.r1[f];
+    const int nf = RF >= 0 ? 1 : p.n_filters;
+    for (int f = 0; f < nf; ++f) {
+        const int r0 = RF >= 0 ? RF : p.r0[f], r1 = RF >= 0 ? RF : p.r1[f];
         const int ncols = kTW + 2 * r1;           // even
         const int cstart = R1 - r1;               // even
-        vpass_r(r0, A, AWP, R0 - r0, cstart, ncols, reinterpret_cast<const float2 *>(p.taps0[f]), IT);
+        if constexpr (RF >= 0) vpass<RF>(A, AWP, R0 - r0, cstart, ncols, reinterpret_cast<const float2 *>(p.taps0[f]), IT);
+        else vpass_r(r0, A, AWP, R0 - r0, cstart, ncols, reinterpret_cast<const float2 *>(p.taps0[f]), IT);
         __syncthreads();
         if (p.mode == LUCEM_PAD_CONSTANT) {
             // A column outside the read box is cval itself in the reference's
@@ -314,7 +318,8 @@ __device__ void family_tile(const FamParams &p, const TileGeom &g, float *A, flo
             __syncthreads();
         }
         float2 o[8];
-        hpass_r(r1, IT, xc * 8, yp, reinterpret_cast<const float2 *>(p.taps1[f]), o);
+        if constexpr (RF >= 0) hpass<RF>(IT, xc * 8, yp, reinterpret_cast<const float2 *>(p.taps1[f]), o);
+        else hpass_r(r1, IT, xc * 8, yp, reinterpret_cast<const float2 *>(p.taps1[f]), o);
         // Fold this filter into every response that uses it.
 #pragma unroll
         for (int k = 0; k < NOUT; ++k) {
@@ -375,8 +380,8 @@ __device__ void family_tile(const FamParams &p, const TileGeom &g, float *A, flo
 }
 
 // Planes launch: B planes of [H, W], each its own read and owned box.
-template <typename T, int NOUT>
-__global__ void __launch_bounds__(kThreads, 2)
+template <typename T, int NOUT, int RF = -1>
+__global__ void __launch_bounds__(kThreads, RF >= 0 ? 3 : 2)
 family_planes_kernel(const __grid_constant__ FamParams p, int tiles_y, int tiles_x) {
     extern __shared__ float4 smem4[];
     float *A = reinterpret_cast<float *>(smem4);
@@ -391,7 +396,7 @@ family_planes_kernel(const __grid_constant__ FamParams p, int tiles_y, int tiles
         g.rb_y = 0; g.rb_x = 0; g.rb_h = p.H; g.rb_w = p.W;
         g.oy = ty * kTH; g.ox = tx * kTW;
         g.th = min(kTH, p.H - g.oy); g.tw = min(kTW, p.W - g.ox);
-        family_tile<T, NOUT>(p, g, A, IT);
+        family_tile<T, NOUT, RF>(p, g, A, IT);
         __syncthreads();
     }
 }
@@ -438,10 +443,10 @@ family_work_kernel(const __grid_constant__ FamParams p, const FamWork *__restric
     }
 }
 
-template <typename T, int NOUT>
+template <typename T, int NOUT, int RF = -1>
 int dispatch_planes(const FamParams &p, size_t smem, int grid, int ty, int tx, cudaStream_t s) {
-    cudaFuncSetAttribute(family_planes_kernel<T, NOUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    family_planes_kernel<T, NOUT><<<grid, kThreads, smem, s>>>(p, ty, tx);
+    cudaFuncSetAttribute(family_planes_kernel<T, NOUT, RF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    family_planes_kernel<T, NOUT, RF><<<grid, kThreads, smem, s>>>(p, ty, tx);
     return (int)cudaGetLastError();
 }
 
@@ -455,6 +460,17 @@ int dispatch_work(const FamParams &p, size_t smem, int grid, const FamWork *work
 
 template <typename T>
 int dispatch_planes_n(const FamParams &p, size_t smem, int grid, int ty, int tx, cudaStream_t s) {
+    // A single filter with equal radii along both axes (a plain 2-D blur) runs
+    // a kernel compiled for that radius.
+    if (p.n_outputs == 1 && p.n_filters == 1 && p.r0[0] == p.r1[0] && p.rmax0 == p.r0[0] && p.rmax1 == p.r1[0]) {
+        switch (p.r0[0]) {
+#define RFCASE(r) \
+    case r: return dispatch_planes<T, 1, r>(p, smem, grid, ty, tx, s);
+            RFCASE(2) RFCASE(4) RFCASE(6) RFCASE(8) RFCASE(10) RFCASE(12) RFCASE(16)
+#undef RFCASE
+        default: break;
+        }
+    }
     return p.n_outputs == 1 ? dispatch_planes<T, 1>(p, smem, grid, ty, tx, s)
                             : dispatch_planes<T, kFamMaxOutputs>(p, smem, grid, ty, tx, s);
 }
