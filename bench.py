@@ -480,16 +480,40 @@ def run_ours(args, rank, world, local_rank):
     obs_pin = torch.from_numpy(obs_h).pin_memory()
     psf_pin = torch.from_numpy(psf_h).pin_memory()
     res_pin = torch.empty(obs_h.shape, dtype=torch.float32).pin_memory()
-    obs_d = torch.empty_like(obs)
-    psf_d = torch.empty_like(psf)
+    # Every step copies its volume and PSF in and its estimate out; the copies
+    # run on a second stream, double-buffered, so step k+1's upload and step
+    # k's download overlap the deconvolutions.
+    obs_d = [torch.empty_like(obs) for _ in range(2)]
+    psf_d = [torch.empty_like(psf) for _ in range(2)]
+    out_d = [torch.empty_like(out) for _ in range(2)]
+    cs = torch.cuda.Stream(dev)
+    ev_in = [torch.cuda.Event() for _ in range(2)]
+    ev_done = [torch.cuda.Event() for _ in range(2)]
+
+    def upload(b):
+        with torch.cuda.stream(cs):
+            obs_d[b].copy_(obs_pin, non_blocking=True)
+            psf_d[b].copy_(psf_pin, non_blocking=True)
+            ev_in[b].record(cs)
+
     torch.cuda.synchronize(dev)
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     f0.record(s)
-    for _ in range(args.steps):
-        obs_d.copy_(obs_pin, non_blocking=True)
-        psf_d.copy_(psf_pin, non_blocking=True)
-        step(obs_d, psf_d, out)
-        res_pin.copy_(out, non_blocking=True)
+    cs.wait_stream(s)
+    upload(0)
+    for k in range(args.steps):
+        b = k % 2
+        s.wait_event(ev_in[b])
+        if k + 1 < args.steps:
+            if k >= 1:
+                cs.wait_event(ev_done[1 - b])  # step k-1 is done with buffer 1-b
+            upload(1 - b)
+        step(obs_d[b], psf_d[b], out_d[b])
+        ev_done[b].record(s)
+        with torch.cuda.stream(cs):
+            cs.wait_event(ev_done[b])
+            res_pin.copy_(out_d[b], non_blocking=True)
+    s.wait_stream(cs)
     f1.record(s)
     torch.cuda.synchronize(dev)
     e2e_ms = f0.elapsed_time(f1) / args.steps

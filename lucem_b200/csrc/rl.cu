@@ -480,8 +480,11 @@ __global__ void __launch_bounds__(512, 1) row_pass_kernel(const __grid_constant_
 // ZP (chosen at launch): the real row's data and extension fit the first
 // half (X + 2 hx <= Px / 2), so the packed samples m >= M/2 are zero going
 // into the forward transform and unused coming out of the inverse one.
-template <int N1, int N2, int R, bool ZP>
+template <int N1, int N2, int R, bool ZP, int KIND>
 __global__ void __launch_bounds__(N1 * R, 65536 / (N1 * R * 128)) row_fast_kernel(const __grid_constant__ RowPass p) {
+    // KIND >= 0: the row kind fixed at compile time (the ratio and update
+    // passes of every iteration); -1: kind at run time.
+    const int kind = KIND >= 0 ? KIND : p.kind;
     using L = fftc::RowLayout<N1, N2, R>;
     using F = fftc::TwoStep<N1, N2, L>;
     constexpr int M = N1 * N2, Px = 2 * M;
@@ -497,7 +500,7 @@ __global__ void __launch_bounds__(N1 * R, 65536 / (N1 * R * 128)) row_fast_kerne
     F::build_tables(tf, ti, p.tw, 2);  // W_M^m = W_Px^{2m}
     __syncthreads();
     const int ntiles = p.items ? p.total_tiles : (p.nrows + R - 1) / R;
-    const bool emit_last = !(p.kind == kRowUpdate && p.last) && p.kind != kRowRealOut;
+    const bool emit_last = !(kind == kRowUpdate && p.last) && kind != kRowRealOut;
     for (int gt = blockIdx.x; gt < ntiles; gt += gridDim.x) {
         int tile;
         const RowItem pi = row_tile(p, gt, &tile);
@@ -505,7 +508,7 @@ __global__ void __launch_bounds__(N1 * R, 65536 / (N1 * R * 128)) row_fast_kerne
         const bool ok = row < pi.nrows;
         float2 *spec = xb + r * SP;
         float2 v[N2];
-        if (p.kind != kRowInit && p.kind != kRowRealIn) {
+        if (kind != kRowInit && kind != kRowRealIn) {
             const float2 *s1 = pi.s1 + (int64_t)(ok ? row : 0) * p.Hp;
             for (int k = t; k <= M; k += N1) spec[k] = ok ? s1[k] : make_float2(0.f, 0.f);
             __syncthreads();
@@ -543,8 +546,8 @@ __global__ void __launch_bounds__(N1 * R, 65536 / (N1 * R * 128)) row_fast_kerne
                     const int xi = 2 * (t + N1 * (i0 + q / 2)) + (q & 1) - pi.hx;
                     const bool inside = ok && xi >= 0 && xi < pi.X;
                     in[q] = 0.0f;
-                    if ((p.kind == kRowRatio || p.kind == kRowRealIn) && inside) in[q] = obs[gbase + xi];
-                    if (p.kind == kRowUpdate && !p.est_first && inside) in[q] = est[gbase + xi];
+                    if ((kind == kRowRatio || kind == kRowRealIn) && inside) in[q] = obs[gbase + xi];
+                    if (kind == kRowUpdate && !p.est_first && inside) in[q] = est[gbase + xi];
                 }
 #pragma unroll
                 for (int q = 0; q < 2 * CH; ++q) {
@@ -554,13 +557,13 @@ __global__ void __launch_bounds__(N1 * R, 65536 / (N1 * R * 128)) row_fast_kerne
                     const float val = (q & 1) ? v[i].y : v[i].x;
                     float nv = 0.0f;
                     if (inside) {
-                        if (p.kind == kRowInit) {
+                        if (kind == kRowInit) {
                             nv = 0.5f;
-                        } else if (p.kind == kRowRealIn) {
+                        } else if (kind == kRowRealIn) {
                             nv = in[q];
-                        } else if (p.kind == kRowRealOut) {
+                        } else if (kind == kRowRealOut) {
                             nv = val;
-                        } else if (p.kind == kRowRatio) {
+                        } else if (kind == kRowRatio) {
                             const float d = fabsf(val) < p.eps ? p.eps : val;
                             nv = in[q] / d;
                         } else {
@@ -571,7 +574,7 @@ __global__ void __launch_bounds__(N1 * R, 65536 / (N1 * R * 128)) row_fast_kerne
                     }
                     if (q & 1) v[i].y = nv; else v[i].x = nv;
                 }
-                if ((p.kind == kRowUpdate || p.kind == kRowRealOut) && ok) {
+                if ((kind == kRowUpdate || kind == kRowRealOut) && ok) {
 #pragma unroll
                     for (int q = 0; q < 2 * CH; ++q) {
                         const int i = i0 + q / 2;
@@ -790,12 +793,21 @@ int launch_row_fast(const RowPass &p, cudaStream_t s) {
     per_sm = per_sm < 1 ? 1 : (per_sm > 8 ? 8 : per_sm);
     int grid = ntiles < sms() * per_sm ? ntiles : sms() * per_sm;
     // Pruning for single problems only (a batch's items differ in X).
-    if (!p.items && p.X + 2 * p.hx <= p.Px / 2) {
-        cudaFuncSetAttribute(row_fast_kernel<N1, N2, R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        row_fast_kernel<N1, N2, R, true><<<grid, N1 * R, smem, s>>>(p);
+    const bool zp = !p.items && p.X + 2 * p.hx <= p.Px / 2;
+    auto go = [&](auto kern) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        kern<<<grid, N1 * R, smem, s>>>(p);
+    };
+    // The two passes of every iteration get kernels compiled for their kind.
+    if (p.kind == kRowRatio) {
+        if (zp) go(row_fast_kernel<N1, N2, R, true, kRowRatio>);
+        else go(row_fast_kernel<N1, N2, R, false, kRowRatio>);
+    } else if (p.kind == kRowUpdate) {
+        if (zp) go(row_fast_kernel<N1, N2, R, true, kRowUpdate>);
+        else go(row_fast_kernel<N1, N2, R, false, kRowUpdate>);
     } else {
-        cudaFuncSetAttribute(row_fast_kernel<N1, N2, R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        row_fast_kernel<N1, N2, R, false><<<grid, N1 * R, smem, s>>>(p);
+        if (zp) go(row_fast_kernel<N1, N2, R, true, -1>);
+        else go(row_fast_kernel<N1, N2, R, false, -1>);
     }
     return (int)cudaGetLastError();
 }
