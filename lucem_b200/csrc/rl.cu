@@ -218,9 +218,10 @@ __global__ void __launch_bounds__(512, 1) col_pass_kernel(const __grid_constant_
 // bit 1, the input rows N/2 .. N-1 are zero (not loaded, first forward
 // stage pruned); bit 2, only the rows below N/2 are stored (last inverse
 // stage pruned).
-template <int N1, int N2, int C, bool SEP, int PR>
+template <int N1, int N2, int C, bool SEP, int PR, int MODE>
 __global__ void __launch_bounds__(N1 * C, (N2 > 32 ? 1 : 65536 / (N1 * C * 128))) col_fast_kernel(const __grid_constant__ ColPass p) {
     constexpr bool kZeroHi = (PR & 1) != 0, kLoOnly = (PR & 2) != 0;
+    // MODE: the pass's ColMode (p.mode), fixed at compile time.
     using L = fftc::ColLayout<N1, N2, C>;
     using F = fftc::TwoStep<N1, N2, L>;
     constexpr int N = N1 * N2;
@@ -247,7 +248,7 @@ __global__ void __launch_bounds__(N1 * C, (N2 > 32 ? 1 : 65536 / (N1 * C * 128))
         }
         const float2 *src = q.src + (outer * q.src_outer + kx);
         float2 v[N2];
-        if (p.mode == kColInv) {
+        if (MODE == kColInv) {
 #pragma unroll
             for (int j = 0; j < N2; ++j) v[j] = ok ? src[F::freq(t, j) * src_row] : make_float2(0.f, 0.f);
             F::template inverse<kLoOnly>(v, t, c, xb, ti);
@@ -259,8 +260,8 @@ __global__ void __launch_bounds__(N1 * C, (N2 > 32 ? 1 : 65536 / (N1 * C * 128))
             float2 hv[kPrefetchH ? N2 : 1];
             // SEP: separable transfer function (ColPass::Hrow), chosen at launch.
             float2 hc = make_float2(0.f, 0.f);
-            if (SEP && p.mode == kColFull && ok) hc = h[0];
-            if (kPrefetchH && p.mode == kColFull && !SEP) {
+            if (SEP && MODE == kColFull && ok) hc = h[0];
+            if (kPrefetchH && MODE == kColFull && !SEP) {
 #pragma unroll
                 for (int j = 0; j < (kPrefetchH ? N2 : 1); ++j)
                     hv[j] = ok ? h[F::freq(t, j) * h_row] : make_float2(0.f, 0.f);
@@ -273,12 +274,12 @@ __global__ void __launch_bounds__(N1 * C, (N2 > 32 ? 1 : 65536 / (N1 * C * 128))
                 v[i] = (ok && srow >= 0) ? src[srow * src_row] : make_float2(0.f, 0.f);
             }
             F::template forward<kZeroHi>(v, t, c, xb, tf);
-            if (p.mode == kColFull && q.spec_out != nullptr && ok) {
+            if (MODE == kColFull && q.spec_out != nullptr && ok) {
                 float2 *so = q.spec_out + (outer * q.h_outer + kx);
 #pragma unroll
                 for (int j = 0; j < N2; ++j) so[F::freq(t, j) * (int)p.spec_row] = v[j];
             }
-            if (p.mode == kColFwd) {
+            if (MODE == kColFwd) {
                 float2 *dst = q.dst + (outer * q.dst_outer + kx);
                 if (ok) {
 #pragma unroll
@@ -766,18 +767,21 @@ int launch_col_fast(const ColPass &p, cudaStream_t s) {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         kern<<<grid, N1 * C, smem, s>>>(p);
     };
-    if (p.Hrow) {
-        // Separable products occur in the forward * H * inverse pass only,
-        // where zero padding prunes both ends or neither.
-        if (pr == 3) go(col_fast_kernel<N1, N2, C, true, 3>);
-        else go(col_fast_kernel<N1, N2, C, true, 0>);
+    // One instantiation per pass mode; pruning only where the mode allows it
+    // (forward: the zero input half; inverse: the unstored output half;
+    // forward * H * inverse: both or neither).
+    if (p.mode == kColFwd) {
+        if (pr & 1) go(col_fast_kernel<N1, N2, C, false, 1, kColFwd>);
+        else go(col_fast_kernel<N1, N2, C, false, 0, kColFwd>);
+    } else if (p.mode == kColInv) {
+        if (pr & 2) go(col_fast_kernel<N1, N2, C, false, 2, kColInv>);
+        else go(col_fast_kernel<N1, N2, C, false, 0, kColInv>);
+    } else if (p.Hrow) {
+        if (pr == 3) go(col_fast_kernel<N1, N2, C, true, 3, kColFull>);
+        else go(col_fast_kernel<N1, N2, C, true, 0, kColFull>);
     } else {
-        switch (pr) {
-        case 0: go(col_fast_kernel<N1, N2, C, false, 0>); break;
-        case 1: go(col_fast_kernel<N1, N2, C, false, 1>); break;
-        case 2: go(col_fast_kernel<N1, N2, C, false, 2>); break;
-        default: go(col_fast_kernel<N1, N2, C, false, 3>); break;
-        }
+        if (pr == 3) go(col_fast_kernel<N1, N2, C, false, 3, kColFull>);
+        else go(col_fast_kernel<N1, N2, C, false, 0, kColFull>);
     }
     return (int)cudaGetLastError();
 }
