@@ -307,6 +307,21 @@ lucem_status lucem_fft_convolve_backward(lucem_ctx *ctx, const lucem_tensor *x, 
                                          int32_t mode, const int64_t *grid, const lucem_tensor *grad_out,
                                          lucem_tensor *grad_x, lucem_tensor *grad_psf, lucem_workspace *ws,
                                          void *stream);
+/* A batch of separate 2-D images of any sizes, each blurred as
+ * lucem_gaussian_blur would with the isotropic sigma of its set
+ * (set_sigmas[set_ids[i]]), the same mode, cval, truncate and input scale for
+ * all: the batched counterpart of calling gaussian_blur_into per image
+ * (crates/lucem-ops/src/filter/gaussian.rs:176-237).  Per sigma set, one
+ * persistent launch walks the 64x64 tiles of all its images.  ins: n tensors
+ * of one dtype (u8, u16 or f32); outs: n f32 tensors of the same shapes.  The
+ * image list is uploaded on the first call with a given list (the stream is
+ * synchronised then); later calls with the same list only launch.  Kernel
+ * radius at most 32 (sigma 8 at truncate 4). */
+lucem_status lucem_gaussian_batch(lucem_ctx *ctx, int32_t n, const lucem_tensor *ins, lucem_tensor *outs,
+                                  const int32_t *set_ids, int32_t n_sets, const double *set_sigmas, int32_t mode,
+                                  double cval, double truncate, double input_scale, lucem_workspace *ws,
+                                  void *stream);
+
 /* ---- Batched 2-D Richardson-Lucy --------------------------------------
  * Many 2-D problems of different sizes and PSFs (the reference runs
  * richardson_lucy once per image, crates/lucem-ops/src/restore/

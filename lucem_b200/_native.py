@@ -106,6 +106,8 @@ SIGNATURES = {
     "lucem_richardson_lucy_backward": (I32, [P, TP, TP, C.POINTER(RlSettings), TP, I32, TP, TP, P, P]),
     "lucem_fft_convolve": (I32, [P, TP, TP, I32, I64P, TP, P, P]),
     "lucem_fft_convolve_backward": (I32, [P, TP, TP, I32, I64P, TP, TP, TP, P, P]),
+    "lucem_gaussian_batch": (I32, [P, I32, TP, TP, C.POINTER(I32), I32, DP, I32, C.c_double, C.c_double,
+                                    C.c_double, P, P]),
     "lucem_rl_batch_create": (I32, [P, I32, TP, TP, C.POINTER(RlSettings), TP, P, P, C.POINTER(P)]),
     "lucem_rl_batch_run": (I32, [P, I32, P, P]),
     "lucem_rl_batch_info": (I32, [P, I64P, C.POINTER(I32), C.POINTER(I32)]),

@@ -1504,6 +1504,111 @@ lucem_status lucem_gaussian_family_tiles(lucem_ctx *ctx, const lucem_tensor *sli
     return e ? cuda_fail(e, "tiled family launch") : ok();
 }
 
+lucem_status lucem_gaussian_batch(lucem_ctx *ctx, int32_t n, const lucem_tensor *ins, lucem_tensor *outs,
+                                  const int32_t *set_ids, int32_t n_sets, const double *set_sigmas, int32_t mode,
+                                  double cval, double truncate, double input_scale, lucem_workspace *ws,
+                                  void *stream) {
+    TimerScope timer_scope(ws);
+    if (!ctx) return fail(LUCEM_ERR_INVALID_HANDLE, "null context");
+    if (!ws) return fail(LUCEM_ERR_INVALID_HANDLE, "a workspace is required");
+    if (n < 1 || !ins || !outs || !set_ids)
+        return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `n`: a batch needs at least one image");
+    if (n_sets < 1 || !set_sigmas)
+        return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `n_sets`: at least one sigma set");
+    lucem_status st;
+    if ((st = check_mode(mode))) return st;
+    for (int s2 = 0; s2 < n_sets; ++s2) {
+        const double sg = set_sigmas[s2];
+        if (!std::isfinite(sg) || sg < 0.0)
+            return fail(LUCEM_ERR_INVALID_PARAMETER,
+                        "invalid parameter `sigmas`: sigma must be non-negative and finite, got %g", sg);
+        if (sg > 0.0 && radius_of(truncate, sg) > kFamMaxRadius)
+            return fail(LUCEM_ERR_INVALID_PARAMETER,
+                        "invalid parameter `sigmas`: radius %d of sigma %g exceeds the batched kernel's %d",
+                        (int)radius_of(truncate, sg), sg, kFamMaxRadius);
+    }
+    for (int i = 0; i < n; ++i) {
+        if ((st = check_in_out(&ins[i], &outs[i]))) return st;
+        if (ins[i].ndim != 2)
+            return fail(LUCEM_ERR_INVALID_DIMENSION, "gaussian_batch takes 2-D images, image %d is %d-D", i, ins[i].ndim);
+        if (ins[i].dtype != ins[0].dtype)
+            return fail(LUCEM_ERR_UNSUPPORTED_DTYPE, "gaussian_batch: every image has the first image's dtype");
+        if (set_ids[i] < 0 || set_ids[i] >= n_sets)
+            return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `set_ids`: image %d has set %d of %d", i,
+                        set_ids[i], n_sets);
+    }
+    int th = 64, tw = 64;
+    family_tile_dims(&th, &tw);
+    // Work list: images grouped by sigma set, each set's tiles numbered from 0.
+    std::vector<FamImage> items;
+    std::vector<int32_t> set_begin((size_t)n_sets + 1, 0), set_tiles((size_t)n_sets, 0);
+    for (int s2 = 0; s2 < n_sets; ++s2) {
+        set_begin[(size_t)s2] = (int32_t)items.size();
+        int64_t t = 0;
+        for (int i = 0; i < n; ++i) {
+            if (set_ids[i] != s2 || numel(&ins[i]) == 0) continue;
+            FamImage it{};
+            it.in = ins[i].data;
+            it.out = static_cast<float *>(outs[i].data);
+            it.H = (int32_t)ins[i].dims[0];
+            it.W = (int32_t)ins[i].dims[1];
+            it.in_pitch = it.W;
+            it.out_pitch = it.W;
+            it.tile_begin = (int32_t)t;
+            t += ((int64_t)(it.H + th - 1) / th) * ((it.W + tw - 1) / tw);
+            if (t > INT32_MAX) return fail(LUCEM_ERR_TOO_MANY_ELEMENTS, "gaussian_batch: too many tiles in one set");
+            items.push_back(it);
+        }
+        set_tiles[(size_t)s2] = (int32_t)t;
+    }
+    set_begin[(size_t)n_sets] = (int32_t)items.size();
+    if (items.empty()) return ok();
+    // Upload the work list once per distinct list (then calls only launch).
+    void *wdev = nullptr;
+    Slot *wslot = nullptr;
+    const size_t wbytes = items.size() * sizeof(FamImage);
+    if ((st = ws->get("gauss_batch_items", wbytes, &wdev, &wslot))) return st;
+    std::string key(reinterpret_cast<const char *>(items.data()), wbytes);
+    if (wslot->key != key) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        cudaStreamIsCapturing(static_cast<cudaStream_t>(stream), &cs);
+        if (cs != cudaStreamCaptureStatusNone)
+            return fail(LUCEM_ERR_INVALID_PARAMETER,
+                        "a new image list cannot be uploaded during stream capture: call once before capturing");
+        CUDA_TRY(cudaMemcpyAsync(wdev, items.data(), wbytes, cudaMemcpyHostToDevice, static_cast<cudaStream_t>(stream)),
+                 "uploading the image list");
+        CUDA_TRY(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)), "image list upload");
+        wslot->key = key;
+    }
+    const FamImage *idev = static_cast<const FamImage *>(wdev);
+    for (int s2 = 0; s2 < n_sets; ++s2) {
+        const int32_t b = set_begin[(size_t)s2], cnt = set_begin[(size_t)s2 + 1] - b;
+        if (cnt == 0) continue;
+        const double sg = set_sigmas[s2];
+        int e = 0;
+        if (!(sg > 0.0)) {
+            // sigma 0: the reference copies the input (gaussian.rs:102-104).
+            for (int32_t k = 0; k < cnt && !e; ++k) {
+                const FamImage &it = items[(size_t)(b + k)];
+                e = timed(kPassElementwise, stream, [&] {
+                    return launch_cast(it.in, ins[0].dtype, (float)input_scale, it.out, (int64_t)it.H * it.W, stream);
+                });
+            }
+        } else {
+            const int64_t r = (int64_t)radius_of(truncate, sg);
+            const GaussPass rows{0, sg, 0, r}, cols{1, sg, 0, r};
+            FamParams fp;
+            lucem_tensor view = ins[0];
+            gaussian_fused_params(&fp, &view, mode, cval, (float)input_scale, rows, cols, nullptr);
+            e = timed(kPassFamily, stream, [&] {
+                return launch_family_batch(fp, ins[0].dtype, idev + b, cnt, set_tiles[(size_t)s2], stream);
+            });
+        }
+        if (e) return cuda_fail(e, "gaussian_batch launch");
+    }
+    return ok();
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------------

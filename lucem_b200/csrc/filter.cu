@@ -93,6 +93,11 @@ struct TileGeom {
     int rb_y, rb_x, rb_h, rb_w;   // read box
     int oy, ox;                   // output tile origin (absolute)
     int th, tw;                   // valid rows / cols of this tile
+    // Batch of separate images: this tile's image and output (row pitches in
+    // elements) replace FamParams' input and single output.  Null otherwise.
+    const void *in;
+    float *out;
+    int64_t in_pitch, out_pitch;
 };
 
 // Axis-0 pass of one filter with kernel radius R over the staged tile A
@@ -201,7 +206,9 @@ __device__ void family_tile(const FamParams &p, const TileGeom &g, float *A, flo
     const int R0 = RF >= 0 ? RF : p.rmax0, R1 = RF >= 0 ? RF : p.rmax1;
     const int AWP = kTW + 2 * R1;   // even (R1 even)
     const int AH = kTH + 2 * R0;
-    const T *in = static_cast<const T *>(p.in) + (int64_t)g.plane * p.in_plane_stride;
+    const int64_t ipitch = g.in ? g.in_pitch : p.in_row_pitch;
+    const T *in = g.in ? static_cast<const T *>(g.in)
+                       : static_cast<const T *>(p.in) + (int64_t)g.plane * p.in_plane_stride;
 
     // Phase 0: tile + halo -> A (f32).  A warp stages rows warp, warp + 8,
     // ...; each lane covers columns lane, lane + 32, ... of a row (no index
@@ -209,10 +216,10 @@ __device__ void family_tile(const FamParams &p, const TileGeom &g, float *A, flo
     // any of them, so many global loads are in flight per warp.
     {
         const int wy0 = g.oy - g.rb_y - R0, wx0 = g.ox - g.rb_x - R1;  // window origin in the read box
-        const T *wbase = in + (int64_t)g.rb_y * p.in_row_pitch + g.rb_x;
+        const T *wbase = in + (int64_t)g.rb_y * ipitch + g.rb_x;
         const bool interior = wy0 >= 0 && wx0 >= 0 && wy0 + AH <= g.rb_h && wx0 + AWP <= g.rb_w;
-        const T *w0 = wbase + (int64_t)wy0 * p.in_row_pitch + wx0;
-        const bool pairs_ok = (p.in_row_pitch % 2 == 0) &&
+        const T *w0 = wbase + (int64_t)wy0 * ipitch + wx0;
+        const bool pairs_ok = (ipitch % 2 == 0) &&
                               (reinterpret_cast<uintptr_t>(w0) % (2 * sizeof(T)) == 0);
         const int lane = tid & 31, warp = tid >> 5;
         constexpr int kRows = NOUT == 1 ? 4 : 2;  // rows in flight per lane
@@ -226,7 +233,7 @@ __device__ void family_tile(const FamParams &p, const TileGeom &g, float *A, flo
 #pragma unroll
                 for (int k = 0; k < kRows; ++k) {
                     const int r = r0 + kWarps * k;
-                    const V2 *src = reinterpret_cast<const V2 *>(w0 + (int64_t)r * p.in_row_pitch);
+                    const V2 *src = reinterpret_cast<const V2 *>(w0 + (int64_t)r * ipitch);
 #pragma unroll
                     for (int h = 0; h < 2; ++h)
                         if (r < AH && lane + 32 * h < npr) v[k][h] = __ldg(src + lane + 32 * h);
@@ -256,7 +263,7 @@ __device__ void family_tile(const FamParams &p, const TileGeom &g, float *A, flo
                         v[k][h] = p.cval;
                         if (py >= 0 && c < AWP) {
                             const int px = pad_index_rt(wx0 + c, g.rb_w, p.mode);
-                            if (px >= 0) v[k][h] = to_f32_scaled(__ldg(wbase + (int64_t)py * p.in_row_pitch + px), p.in_scale);
+                            if (px >= 0) v[k][h] = to_f32_scaled(__ldg(wbase + (int64_t)py * ipitch + px), p.in_scale);
                         }
                     }
                 }
@@ -353,7 +360,8 @@ __device__ void family_tile(const FamParams &p, const TileGeom &g, float *A, flo
     for (int k = 0; k < NOUT; ++k) {
         if (k >= p.n_outputs) break;
         const FamOutput &oo = p.outs[k];
-        float *obase = oo.out + (int64_t)g.plane * oo.plane_stride;
+        float *obase = g.out ? g.out : oo.out + (int64_t)g.plane * oo.plane_stride;
+        const int64_t opitch = g.out ? g.out_pitch : oo.row_pitch;
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             const int y = 2 * yp + h, x = xc * 8;
@@ -365,7 +373,7 @@ __device__ void family_tile(const FamParams &p, const TileGeom &g, float *A, flo
                 if (oo.combine == (int)Combine::kHypot) v[j] = sqrtf(fmaxf(a, 0.0f)) * oo.alpha;
                 else v[j] = a + oo.bias;
             }
-            float *dst = obase + (int64_t)(g.oy + y) * oo.row_pitch + g.ox + x;
+            float *dst = obase + (int64_t)(g.oy + y) * opitch + g.ox + x;
             const bool vec_ok = (x + 8 <= g.tw) && ((reinterpret_cast<uintptr_t>(dst) & 15) == 0);
             if (vec_ok) {
                 reinterpret_cast<float4 *>(dst)[0] = make_float4(v[0], v[1], v[2], v[3]);
@@ -389,7 +397,7 @@ family_planes_kernel(const __grid_constant__ FamParams p, int tiles_y, int tiles
     const int per_plane = tiles_y * tiles_x;
     const int total = per_plane * p.B;
     for (int t = blockIdx.x; t < total; t += gridDim.x) {
-        TileGeom g;
+        TileGeom g{};
         g.plane = t / per_plane;
         int r = t - g.plane * per_plane;
         int ty = r / tiles_x, tx = r - ty * tiles_x;
@@ -432,7 +440,7 @@ family_work_kernel(const __grid_constant__ FamParams p, const FamWork *__restric
         int local = tg - w.tile_begin;
         int tiles_x = (w.own_w + kTW - 1) / kTW;
         int ty = local / tiles_x, tx = local - ty * tiles_x;
-        TileGeom g;
+        TileGeom g{};
         g.plane = w.channel;
         g.rb_y = w.read_y; g.rb_x = w.read_x; g.rb_h = w.read_h; g.rb_w = w.read_w;
         g.oy = w.own_y + ty * kTH; g.ox = w.own_x + tx * kTW;
@@ -441,6 +449,70 @@ family_work_kernel(const __grid_constant__ FamParams p, const FamWork *__restric
         __syncthreads();
         if (!counter) t += gridDim.x;
     }
+}
+
+int sm_count();
+
+// Batch of separate 2-D images sharing one filter set: tile t belongs to
+// the last item whose tile_begin <= t; each image is its own read box.
+// CTAs walk tiles blockIdx.x, +gridDim.x, ...
+template <typename T, int RF = -1>
+__global__ void __launch_bounds__(kThreads, RF >= 0 ? 3 : 2)
+family_batch_kernel(const __grid_constant__ FamParams p, const FamImage *__restrict__ items, int n_items,
+                    int n_tiles) {
+    extern __shared__ float4 smem4[];
+    float *A = reinterpret_cast<float *>(smem4);
+    float *IT = A + (kTH + 2 * p.rmax0) * (kTW + 2 * p.rmax1);
+    for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+        int lo = 0, hi = n_items - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (items[mid].tile_begin <= t) lo = mid; else hi = mid - 1;
+        }
+        const FamImage it = items[lo];
+        const int local = t - it.tile_begin;
+        const int tiles_x = (it.W + kTW - 1) / kTW;
+        const int ty = local / tiles_x, tx = local - ty * tiles_x;
+        TileGeom g{};
+        g.plane = 0;
+        g.rb_y = 0; g.rb_x = 0; g.rb_h = it.H; g.rb_w = it.W;
+        g.oy = ty * kTH; g.ox = tx * kTW;
+        g.th = min(kTH, it.H - g.oy); g.tw = min(kTW, it.W - g.ox);
+        g.in = it.in;
+        g.out = it.out;
+        g.in_pitch = it.in_pitch;
+        g.out_pitch = it.out_pitch;
+        family_tile<T, 1, RF>(p, g, A, IT);
+        __syncthreads();
+    }
+}
+
+template <typename T, int RF = -1>
+int dispatch_batch(const FamParams &p, size_t smem, const FamImage *items, int n_items, int n_tiles,
+                   cudaStream_t s) {
+    cudaFuncSetAttribute(family_batch_kernel<T, RF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, family_batch_kernel<T, RF>, kThreads, smem);
+    if (per_sm < 1) per_sm = 1;
+    const int slots = sm_count() * per_sm;
+    const int grid = n_tiles < slots ? n_tiles : slots;
+    family_batch_kernel<T, RF><<<grid, kThreads, smem, s>>>(p, items, n_items, n_tiles);
+    return (int)cudaGetLastError();
+}
+
+template <typename T>
+int dispatch_batch_r(const FamParams &p, size_t smem, const FamImage *items, int n_items, int n_tiles,
+                     cudaStream_t s) {
+    if (p.n_filters == 1 && p.r0[0] == p.r1[0] && p.rmax0 == p.r0[0] && p.rmax1 == p.r1[0]) {
+        switch (p.r0[0]) {
+#define RFCASE(r) \
+    case r: return dispatch_batch<T, r>(p, smem, items, n_items, n_tiles, s);
+            RFCASE(2) RFCASE(4) RFCASE(6) RFCASE(8) RFCASE(10) RFCASE(12) RFCASE(16)
+#undef RFCASE
+        default: break;
+        }
+    }
+    return dispatch_batch<T>(p, smem, items, n_items, n_tiles, s);
 }
 
 template <typename T, int NOUT, int RF = -1>
@@ -519,6 +591,19 @@ int launch_family_planes(const FamParams &p, int in_dtype, void *stream) {
     case LUCEM_U8: return dispatch_planes_n<uint8_t>(p, smem, grid, ty, tx, s);
     case LUCEM_U16: return dispatch_planes_n<uint16_t>(p, smem, grid, ty, tx, s);
     case LUCEM_F32: return dispatch_planes_n<float>(p, smem, grid, ty, tx, s);
+    default: return (int)cudaErrorInvalidValue;
+    }
+}
+
+int launch_family_batch(const FamParams &p, int in_dtype, const FamImage *items_dev, int32_t n_items,
+                        int32_t n_tiles, void *stream) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (n_tiles == 0) return 0;
+    const size_t smem = family_smem_bytes(p.rmax0, p.rmax1);
+    switch (in_dtype) {
+    case LUCEM_U8: return dispatch_batch_r<uint8_t>(p, smem, items_dev, n_items, n_tiles, s);
+    case LUCEM_U16: return dispatch_batch_r<uint16_t>(p, smem, items_dev, n_items, n_tiles, s);
+    case LUCEM_F32: return dispatch_batch_r<float>(p, smem, items_dev, n_items, n_tiles, s);
     default: return (int)cudaErrorInvalidValue;
     }
 }

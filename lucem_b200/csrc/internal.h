@@ -77,10 +77,24 @@ struct FamWork {
     int32_t tile_begin;   // first CTA tile index of this item in the flattened list
 };
 
+// One image of a batch of separate 2-D images (lucem_gaussian_batch).
+struct FamImage {
+    const void *in;               // [H][in_pitch] of the input dtype
+    float *out;                   // [H][out_pitch]
+    int64_t in_pitch, out_pitch;  // elements
+    int32_t H, W;
+    int32_t tile_begin;           // first 64x64 tile of this image in the batch
+    int32_t pad_;
+};
+
 // Launchers (filter.cu).  All return cudaGetLastError() as int.
 int launch_family_planes(const FamParams &p, int in_dtype, void *stream);
 // Tiles [tile_base, tile_base + n_tiles) of the work list (global tile
 // indices); with counter_dev the launch is persistent (persistent_ctas CTAs).
+// Every 64x64 tile of n_items images with the same filter set (p's filters,
+// one output: combine, alpha, bias from p.outs[0]; its pointer unused).
+int launch_family_batch(const FamParams &p, int in_dtype, const FamImage *items_dev, int32_t n_items,
+                        int32_t n_tiles, void *stream);
 int launch_family_work(const FamParams &p, int in_dtype, const FamWork *work_dev, int32_t n_work,
                        int32_t n_tiles, int32_t tile_base, int32_t *counter_dev,
                        int32_t persistent_ctas, void *stream);

@@ -29,7 +29,7 @@ __all__ = [
     "gaussian_family", "schedule", "gaussian_family_tiles", "richardson_lucy", "rl_grid",
     "gaussian_halo", "op_halo", "gaussian_blur_adjoint", "richardson_lucy_backward", "fft_convolve",
     "fft_convolve_backward", "RlBatch", "richardson_lucy_batch", "autotune_fft", "autotune_query",
-    "autotune_save", "autotune_load", "Graph",
+    "autotune_save", "autotune_load", "Graph", "gaussian_batch",
 ]
 
 
@@ -753,3 +753,31 @@ class Graph:
             self.close()
         except Exception:
             pass
+
+
+def gaussian_batch(images: Sequence[torch.Tensor], sigmas, *, mode="reflect", cval=0.0, truncate=4.0,
+                   input_scale=1.0, outs: Optional[Sequence[torch.Tensor]] = None,
+                   workspace: Optional[Workspace] = None):
+    """gaussian_blur of each 2-D image with its own isotropic sigma
+    (`sigmas`: one per image, or one for all) in one launch per distinct sigma
+    (lucem_gaussian_batch); returns the list of f32 outputs."""
+    images = list(images)
+    if len(images) == 0:
+        return []
+    if np.isscalar(sigmas):
+        sigmas = [sigmas] * len(images)
+    sigmas = [float(v) for v in sigmas]
+    if len(sigmas) != len(images):
+        raise LucemError(7, "invalid parameter `sigmas`: one per image")
+    uniq = sorted(set(sigmas))
+    ids = (C.c_int32 * len(images))(*[uniq.index(v) for v in sigmas])
+    sets = (C.c_double * len(uniq))(*uniq)
+    ctx, ws = _ctx_ws(images[0], workspace)
+    outs = list(outs) if outs is not None else [torch.empty(x.shape, dtype=torch.float32, device=x.device)
+                                                for x in images]
+    ti = _tensor_array(images, "images")
+    to = _tensor_array(outs, "outs")
+    N.check(N.lib().lucem_gaussian_batch(ctx.handle, len(images), ti, to, ids, len(uniq), sets, PadMode.parse(mode),
+                                         float(cval), float(truncate), float(input_scale), ws.handle,
+                                         _stream(images[0])))
+    return outs
