@@ -290,13 +290,21 @@ __global__ void __launch_bounds__(N1 * C, (N2 > 32 ? 1 : 65536 / (N1 * C * 128))
 #pragma unroll
             for (int j = 0; j < N2; ++j) {
                 float2 hj;
-                if constexpr (SEP) hj = fftc::mul(hc, p.Hrow[F::freq(t, j)]);
+                // Separable: the row factor here, the column's constant factor
+                // after the inverse, on the stored values only (it commutes).
+                if constexpr (SEP) hj = p.Hrow[F::freq(t, j)];
                 else if constexpr (kPrefetchH) hj = hv[j];
                 else hj = ok ? h[F::freq(t, j) * h_row] : make_float2(0.f, 0.f);
                 if (p.conj_h) hj.y = -hj.y;
                 v[j] = fftc::mul(v[j], hj);
             }
             F::template inverse<kLoOnly>(v, t, c, xb, ti);
+            if constexpr (SEP) {
+                if (p.conj_h) hc.y = -hc.y;
+#pragma unroll
+                for (int i = 0; i < N2; ++i)
+                    if (!(kLoOnly && i >= N2 / 2)) v[i] = fftc::mul(v[i], hc);
+            }
         }
         float2 *dst = q.dst + (outer * q.dst_outer + kx);
         if (ok) {
