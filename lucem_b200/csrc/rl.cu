@@ -730,7 +730,8 @@ int sms() {
 // shapes of launch_col below).
 int col_tile_width(int n) {
     switch (n) {
-    case 64: case 128: case 256: case 512: return 16;
+    case 128: return 8;
+    case 64: case 256: case 512: return 16;
     case 1024: case 2048: return 8;
     default: break;
     }
@@ -827,7 +828,7 @@ int launch_row_fast(const RowPass &p, cudaStream_t s) {
 int launch_col(ColPass p, cudaStream_t s) {
     switch (p.plan.n) {
     case 64: return launch_col_fast<8, 8, 16>(p, s);
-    case 128: return launch_col_fast<8, 16, 16>(p, s);
+    case 128: return launch_col_fast<8, 16, 8>(p, s);
     case 256: return launch_col_fast<16, 16, 16>(p, s);
     case 512: return launch_col_fast<16, 32, 16>(p, s);
     case 1024: return launch_col_fast<32, 32, 8>(p, s);
