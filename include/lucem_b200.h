@@ -369,10 +369,15 @@ lucem_status lucem_graph_end(void *stream, lucem_graph **out);
 lucem_status lucem_graph_launch(lucem_graph *graph, void *stream);
 void lucem_graph_destroy(lucem_graph *graph);
 
-/* The grid lucem_richardson_lucy would use (host only). */
+/* The grid lucem_richardson_lucy uses (host only), before any autotuning of
+ * the context: per axis the requested length, or the cheapest m * 2^k
+ * (m in {1,3,5,7,9,15,21,25,27}) at least the padding's need, by length
+ * times pass cost (the register-resident power-of-two kernels 1, the
+ * Stockham kernels 5 for columns and 2.7 for rows). */
 lucem_status lucem_rl_grid(const int64_t *dims, const int64_t *kdims, int32_t ndim, int32_t mode,
                            const int64_t *requested, int64_t *grid_out);
-/* Smallest length >= n that the FFT kernels support (host only). */
+/* Smallest 2/3/5/7-smooth length >= n (even when `even`): the shortest
+ * length the FFT kernels support (host only). */
 int64_t lucem_fft_good_length(int64_t n, int32_t even);
 
 #ifdef __cplusplus
