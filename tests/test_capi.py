@@ -130,3 +130,18 @@ def test_library_is_built_for_sm100a():
 
     assert build.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
     assert os.path.exists(N.LIB_PATH)
+
+
+def test_header_compiles_as_c99_and_cpp():
+    """include/lucem_b200.h is plain C: a C99 and a C++ translation unit
+    include it without warnings."""
+    import shutil
+    import subprocess
+
+    hdr = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "lucem_b200.h")
+    for cc, args in (("gcc", ["-x", "c", "-std=c99"]), ("g++", ["-x", "c++", "-std=c++17"])):
+        if shutil.which(cc) is None:
+            pytest.skip(f"{cc} not available")
+        r = subprocess.run([cc, "-fsyntax-only", "-Wall", "-Wextra", "-Werror", *args, hdr],
+                           capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
