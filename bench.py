@@ -113,7 +113,8 @@ def nvsmi_id(dev):
 
 
 # ---------------------------------------------------------------------------
-# algorithmic bytes per launch ("Measurement")
+# Algorithmic bytes per launch of each RL pass kernel: the arrays each pass
+# must read and write once (complex64 spectra, f32 volumes).
 
 
 def psf_is_separable(psf):
@@ -597,7 +598,7 @@ def run_ours(args, rank, world, local_rank):
                 "frac": achieved / peak if achieved else None, "traffic": profile_traffic(dominant),
                 "kernel": dominant, "launches_per_step": cnt, "us_per_launch": per_launch_ms * 1e3,
                 "algorithmic_bytes_per_launch": alg, "peak_source": ("measured (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
-                                else "fallback: 6.65 TB/s, an earlier copy measurement on this pool (MEASURED_PEAKS.json absent)")}
+                                else "fallback: 6.65 TB/s, a copy bandwidth measured earlier on B200 (MEASURED_PEAKS.json absent)")}
     step_kernels = {k: {"launches": c, "ms": t, "share": t / sum(v[1] for v in kinds.values())}
                     for k, (c, t) in kinds.items()}
     cpu = None

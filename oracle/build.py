@@ -1,7 +1,7 @@
 """Builds the oracle's C restatement into oracle/_build/liblucem_oracle.so.
 
 Test infrastructure: the parity tests, the smoke check and the benchmark's
-CPU-baseline leg load this library as the checker.  Plain gcc, OpenMP, no
+CPU-baseline leg load this library to check results.  Plain gcc, OpenMP, no
 -ffast-math (the restatement must keep the reference's f32 rounding).
 """
 from __future__ import annotations

@@ -1,7 +1,7 @@
 /*
  * lucem_oracle.h -- CPU restatement of lucem-ops' separable Gaussian family and
  * Richardson-Lucy deconvolution.  TEST INFRASTRUCTURE ONLY: the parity tests,
- * the smoke check and the benchmark's CPU-baseline leg call it as the checker.
+ * the smoke check and the benchmark's CPU-baseline leg call it to check results.
  * The product (lucem_b200) never links or calls anything in this directory.
  *
  * Parity status: the reference (Rust + CubeCL 0.11.4, not vendored) cannot be

@@ -2,7 +2,7 @@
 an FP64 FFT Richardson-Lucy in numpy.
 
 TEST INFRASTRUCTURE ONLY.  The parity tests, the smoke check and the
-benchmark's CPU-baseline leg use it as the checker; the product never imports
+benchmark's CPU-baseline leg use it to check results; the product never imports
 it.  Parity status: pinned to the reference's own known-answer tests and to
 scipy.ndimage fixtures, not to bit-level CubeCL output (the reference cannot be
 built here); see lucem_oracle.h.

@@ -1,5 +1,5 @@
 """The multi-rank path on CPU: world_size 2 over gloo.  Each rank filters its
-share of the blocks of a tile walk (through the oracle, as the checker) and
+share of the blocks of a tile walk (through the oracle, as the reference result) and
 the gathered result equals the whole-image filter: the work list shards with
 no collective on the data path."""
 import os
