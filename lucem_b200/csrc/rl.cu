@@ -320,7 +320,13 @@ __global__ void __launch_bounds__(N1 * C, (N2 > 32 ? 1 : 65536 / (N1 * C * 128))
 
 // Row pass kinds: the RL iteration's three (start from the constant 0.5,
 // ratio, update) and the plain transforms (a real array in, or out).
-enum RowKind : int { kRowInit = 0, kRowRatio = 1, kRowUpdate = 2, kRowRealIn = 3, kRowRealOut = 4 };
+// The reverse pass adds two fused kinds: RatioKeep (the ratio pass that also
+// stores the convolution c into est) and Cbar (rbar in: cbar = -rbar y /
+// guard(c)^2, 0 where guarded, out to the transform; ybar += rbar / guard(c)
+// when aux2 is given; c from aux, y from obs).
+enum RowKind : int {
+    kRowInit = 0, kRowRatio = 1, kRowUpdate = 2, kRowRealIn = 3, kRowRealOut = 4, kRowRatioKeep = 5, kRowCbar = 6
+};
 
 // The x axis: C2R, the Richardson-Lucy epilogue on the image columns, the x
 // extension and R2C, for C rows per tile.
@@ -336,6 +342,8 @@ struct RowPass {
     FftPlan plan;                 // M-point
     const float2 *tw;             // table of length Px
     int32_t C, CP;
+    const float *aux;             // [nrows][X]: c (Cbar)
+    float *aux2;                  // [nrows][X]: ybar, accumulated (Cbar; may be null)
     // Batch mode (items != null): problems of the same Px; the item's fields
     // replace nrows, X, hx, obs, est and s1.
     const struct RowItem *items;
@@ -428,10 +436,17 @@ __global__ void __launch_bounds__(512, 1) row_pass_kernel(const __grid_constant_
             } else if (p.kind == kRowRealOut) {
                 v = *slot;
                 pi.est[g] = v;
-            } else if (p.kind == kRowRatio) {
+            } else if (p.kind == kRowRatio || p.kind == kRowRatioKeep) {
                 float conv = *slot;
                 float d = fabsf(conv) < p.eps ? p.eps : conv;
                 v = pi.obs[g] / d;
+                if (p.kind == kRowRatioKeep) pi.est[g] = conv;
+            } else if (p.kind == kRowCbar) {
+                const float rb = *slot, ci = p.aux[g];
+                const bool gd = fabsf(ci) < p.eps;
+                const float d = gd ? p.eps : ci;
+                v = gd ? 0.0f : -rb * pi.obs[g] / (d * d);
+                if (p.aux2) p.aux2[g] += rb / d;
             } else {
                 float corr = *slot;
                 float old = p.est_first ? 0.5f : pi.est[g];
@@ -555,7 +570,9 @@ __global__ void __launch_bounds__(N1 * R, 65536 / (N1 * R * 128)) row_fast_kerne
                     const int xi = 2 * (t + N1 * (i0 + q / 2)) + (q & 1) - pi.hx;
                     const bool inside = ok && xi >= 0 && xi < pi.X;
                     in[q] = 0.0f;
-                    if ((kind == kRowRatio || kind == kRowRealIn) && inside) in[q] = obs[gbase + xi];
+                    if ((kind == kRowRatio || kind == kRowRealIn || KIND == kRowRatioKeep || KIND == kRowCbar) &&
+                        inside)
+                        in[q] = obs[gbase + xi];
                     if (kind == kRowUpdate && !p.est_first && inside) in[q] = est[gbase + xi];
                 }
 #pragma unroll
@@ -575,6 +592,16 @@ __global__ void __launch_bounds__(N1 * R, 65536 / (N1 * R * 128)) row_fast_kerne
                         } else if (kind == kRowRatio) {
                             const float d = fabsf(val) < p.eps ? p.eps : val;
                             nv = in[q] / d;
+                        } else if (KIND == kRowRatioKeep) {
+                            const float d = fabsf(val) < p.eps ? p.eps : val;
+                            nv = in[q] / d;
+                            if (ok) est[gbase + xi] = val;
+                        } else if (KIND == kRowCbar) {
+                            const float ci = p.aux[gbase + xi];
+                            const bool gd = fabsf(ci) < p.eps;
+                            const float d = gd ? p.eps : ci;
+                            nv = gd ? 0.0f : -val * in[q] / (d * d);
+                            if (p.aux2 && ok) p.aux2[gbase + xi] += val / d;
                         } else {
                             const float old = p.est_first ? 0.5f : in[q];
                             nv = old * val;
@@ -818,6 +845,12 @@ int launch_row_fast(const RowPass &p, cudaStream_t s) {
     } else if (p.kind == kRowUpdate) {
         if (zp) go(row_fast_kernel<N1, N2, R, true, kRowUpdate>);
         else go(row_fast_kernel<N1, N2, R, false, kRowUpdate>);
+    } else if (p.kind == kRowRatioKeep) {
+        if (zp) go(row_fast_kernel<N1, N2, R, true, kRowRatioKeep>);
+        else go(row_fast_kernel<N1, N2, R, false, kRowRatioKeep>);
+    } else if (p.kind == kRowCbar) {
+        if (zp) go(row_fast_kernel<N1, N2, R, true, kRowCbar>);
+        else go(row_fast_kernel<N1, N2, R, false, kRowCbar>);
     } else {
         if (zp) go(row_fast_kernel<N1, N2, R, true, -1>);
         else go(row_fast_kernel<N1, N2, R, false, -1>);
@@ -941,11 +974,14 @@ struct RlRunner {
         return e;
     }
 
-    int row(int kind, const float *in_real, float *out_real, int est_first, int last, int clip, float eps) {
+    int row(int kind, const float *in_real, float *out_real, int est_first, int last, int clip, float eps,
+            const float *aux = nullptr, float *aux2 = nullptr) {
         RowPass r = rp;
         r.kind = kind;
         r.obs = in_real;
         r.est = out_real;
+        r.aux = aux;
+        r.aux2 = aux2;
         r.est_first = est_first;
         r.last = last;
         r.clip = clip;
@@ -1073,34 +1109,10 @@ struct RlRunner {
 
 // ---- elementwise kernels of the backward pass --------------------------
 
-// r = y / guard(c), guard(c) = eps where |c| < eps (deconvolve.rs:127-131).
-__global__ void rl_ratio_kernel(const float *__restrict__ c, const float *__restrict__ y, float *__restrict__ r,
-                                int64_t n, float eps) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const float d = fabsf(c[i]) < eps ? eps : c[i];
-        r[i] = y[i] / d;
-    }
-}
-
 __global__ void rl_mul_kernel(const float *__restrict__ a, const float *__restrict__ b, float *__restrict__ out,
                               int64_t n) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         out[i] = a[i] * b[i];
-}
-
-// cbar = d(loss)/d(c) through r = y / guard(c): zero where the guard holds;
-// ybar += rbar / guard(c) when ybar is given.
-__global__ void rl_cbar_kernel(const float *__restrict__ rbar, const float *__restrict__ y,
-                               const float *__restrict__ c, float *__restrict__ cbar, float *__restrict__ ybar,
-                               int64_t n, float eps) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const float ci = c[i];
-        const bool guarded = fabsf(ci) < eps;
-        const float d = guarded ? eps : ci;
-        const float rb = rbar[i];
-        cbar[i] = guarded ? 0.0f : -rb * y[i] / (d * d);
-        if (ybar) ybar[i] += rb / d;
-    }
 }
 
 // ebar = ebar * a + t
@@ -1335,13 +1347,21 @@ int rl_backward(const RlGeom &g, const RlBuffers &b, const RlBwdBuffers &w, cons
         }
         for (int k = k1 - 1; k >= k0; --k) {
             const float *ek = w.seg + (int64_t)(k - k0) * V;
-            if ((e = run.apply(b.h_conv, 0, ek, w.c, spec_e))) return e;
-            rl_ratio_kernel<<<grid, 256, 0, s>>>(w.c, y, w.r, V, eps);
-            if ((e = run.apply(b.h_corr, 1, w.r, w.a, spec_r))) return e;
+            // c = A e_k (kept), r = y / guard(c) straight into the correlation,
+            // a = B r: the ratio is fused into the row pass between them.
+            if ((e = run.row(kRowRealIn, ek, nullptr, 0, 0, 0, eps))) return e;
+            if ((e = run.pair(b.h_conv, 0, spec_e))) return e;
+            if ((e = run.row(kRowRatioKeep, y, w.c, 0, 0, 0, eps))) return e;
+            if ((e = run.pair(b.h_corr, 1, spec_r))) return e;
+            if ((e = run.row(kRowRealOut, nullptr, w.a, 0, 0, 0, eps))) return e;
             rl_mul_kernel<<<grid, 256, 0, s>>>(w.ebar, ek, w.abar, V);
-            if ((e = run.apply(b.h_corr, 0, w.abar, w.rbar, spec_abar))) return e;
-            rl_cbar_kernel<<<grid, 256, 0, s>>>(w.rbar, y, w.c, w.cbar, ybar, V, eps);
-            if ((e = run.apply(b.h_conv, 1, w.cbar, w.t, spec_cbar))) return e;
+            // rbar = B^T abar, then cbar (and ybar) fused into the row pass that
+            // starts t = A^T cbar.
+            if ((e = run.row(kRowRealIn, w.abar, nullptr, 0, 0, 0, eps))) return e;
+            if ((e = run.pair(b.h_corr, 0, spec_abar))) return e;
+            if ((e = run.row(kRowCbar, y, nullptr, 0, 0, 0, eps, w.c, ybar))) return e;
+            if ((e = run.pair(b.h_conv, 1, spec_cbar))) return e;
+            if ((e = run.row(kRowRealOut, nullptr, w.t, 0, 0, 0, eps))) return e;
             rl_ebar_kernel<<<grid, 256, 0, s>>>(w.ebar, w.a, w.t, V);
             if (pbar2) {
                 spec_mac_kernel<<<sg, 256, 0, s>>>(pbar1, spec_cbar, spec_e, nullptr, nullptr, nspec);
