@@ -320,12 +320,15 @@ __global__ void __launch_bounds__(N1 * C, (N2 > 32 ? 1 : 65536 / (N1 * C * 128))
 
 // Row pass kinds: the RL iteration's three (start from the constant 0.5,
 // ratio, update) and the plain transforms (a real array in, or out).
-// The reverse pass adds two fused kinds: RatioKeep (the ratio pass that also
-// stores the convolution c into est) and Cbar (rbar in: cbar = -rbar y /
-// guard(c)^2, 0 where guarded, out to the transform; ybar += rbar / guard(c)
-// when aux2 is given; c from aux, y from obs).
+// The reverse pass adds four fused kinds:
+//   RatioKeep  c in: store c (est), r = y / guard(c) out (y from obs);
+//   Cbar       rbar in: cbar = -rbar y / guard(c)^2 (0 where guarded) out,
+//              ybar += rbar / guard(c) when aux2 is given (c from aux);
+//   Abar       a in: store a (est), abar = ebar * e out (ebar from aux, e from obs);
+//   Ebar       t in: ebar = ebar * a + t in place (ebar aux2, a aux), nothing out.
 enum RowKind : int {
-    kRowInit = 0, kRowRatio = 1, kRowUpdate = 2, kRowRealIn = 3, kRowRealOut = 4, kRowRatioKeep = 5, kRowCbar = 6
+    kRowInit = 0, kRowRatio = 1, kRowUpdate = 2, kRowRealIn = 3, kRowRealOut = 4, kRowRatioKeep = 5, kRowCbar = 6,
+    kRowAbar = 7, kRowEbar = 8
 };
 
 // The x axis: C2R, the Richardson-Lucy epilogue on the image columns, the x
@@ -420,7 +423,7 @@ __global__ void __launch_bounds__(512, 1) row_pass_kernel(const __grid_constant_
         float *bufr = reinterpret_cast<float *>(buf);
         // Epilogue on the image columns; the real sample at position i of the
         // row is component (i & 1) of packed element i >> 1.
-        const bool emit = !(p.kind == kRowUpdate && p.last) && p.kind != kRowRealOut;
+        const bool emit = !(p.kind == kRowUpdate && p.last) && p.kind != kRowRealOut && p.kind != kRowEbar;
         for (int it = tid; it < pi.X * C; it += T) {
             int c = it / pi.X, xi = it - c * pi.X;
             int row = row0 + c;
@@ -447,6 +450,12 @@ __global__ void __launch_bounds__(512, 1) row_pass_kernel(const __grid_constant_
                 const float d = gd ? p.eps : ci;
                 v = gd ? 0.0f : -rb * pi.obs[g] / (d * d);
                 if (p.aux2) p.aux2[g] += rb / d;
+            } else if (p.kind == kRowAbar) {
+                pi.est[g] = *slot;
+                v = p.aux[g] * pi.obs[g];
+            } else if (p.kind == kRowEbar) {
+                v = fmaf(p.aux2[g], p.aux[g], *slot);
+                p.aux2[g] = v;
             } else {
                 float corr = *slot;
                 float old = p.est_first ? 0.5f : pi.est[g];
@@ -524,7 +533,7 @@ __global__ void __launch_bounds__(N1 * R, 65536 / (N1 * R * 128)) row_fast_kerne
     F::build_tables(tf, ti, p.tw, 2);  // W_M^m = W_Px^{2m}
     __syncthreads();
     const int ntiles = p.items ? p.total_tiles : (p.nrows + R - 1) / R;
-    const bool emit_last = !(kind == kRowUpdate && p.last) && kind != kRowRealOut;
+    const bool emit_last = !(kind == kRowUpdate && p.last) && kind != kRowRealOut && KIND != kRowEbar;
     for (int gt = blockIdx.x; gt < ntiles; gt += gridDim.x) {
         int tile;
         const RowItem pi = row_tile(p, gt, &tile);
@@ -570,7 +579,8 @@ __global__ void __launch_bounds__(N1 * R, 65536 / (N1 * R * 128)) row_fast_kerne
                     const int xi = 2 * (t + N1 * (i0 + q / 2)) + (q & 1) - pi.hx;
                     const bool inside = ok && xi >= 0 && xi < pi.X;
                     in[q] = 0.0f;
-                    if ((kind == kRowRatio || kind == kRowRealIn || KIND == kRowRatioKeep || KIND == kRowCbar) &&
+                    if ((kind == kRowRatio || kind == kRowRealIn || KIND == kRowRatioKeep || KIND == kRowCbar ||
+                         KIND == kRowAbar) &&
                         inside)
                         in[q] = obs[gbase + xi];
                     if (kind == kRowUpdate && !p.est_first && inside) in[q] = est[gbase + xi];
@@ -602,6 +612,12 @@ __global__ void __launch_bounds__(N1 * R, 65536 / (N1 * R * 128)) row_fast_kerne
                             const float d = gd ? p.eps : ci;
                             nv = gd ? 0.0f : -val * in[q] / (d * d);
                             if (p.aux2 && ok) p.aux2[gbase + xi] += val / d;
+                        } else if (KIND == kRowAbar) {
+                            if (ok) est[gbase + xi] = val;
+                            nv = p.aux[gbase + xi] * in[q];
+                        } else if (KIND == kRowEbar) {
+                            nv = fmaf(p.aux2[gbase + xi], p.aux[gbase + xi], val);
+                            if (ok) p.aux2[gbase + xi] = nv;
                         } else {
                             const float old = p.est_first ? 0.5f : in[q];
                             nv = old * val;
@@ -851,6 +867,12 @@ int launch_row_fast(const RowPass &p, cudaStream_t s) {
     } else if (p.kind == kRowCbar) {
         if (zp) go(row_fast_kernel<N1, N2, R, true, kRowCbar>);
         else go(row_fast_kernel<N1, N2, R, false, kRowCbar>);
+    } else if (p.kind == kRowAbar) {
+        if (zp) go(row_fast_kernel<N1, N2, R, true, kRowAbar>);
+        else go(row_fast_kernel<N1, N2, R, false, kRowAbar>);
+    } else if (p.kind == kRowEbar) {
+        if (zp) go(row_fast_kernel<N1, N2, R, true, kRowEbar>);
+        else go(row_fast_kernel<N1, N2, R, false, kRowEbar>);
     } else {
         if (zp) go(row_fast_kernel<N1, N2, R, true, -1>);
         else go(row_fast_kernel<N1, N2, R, false, -1>);
@@ -1109,19 +1131,6 @@ struct RlRunner {
 
 // ---- elementwise kernels of the backward pass --------------------------
 
-__global__ void rl_mul_kernel(const float *__restrict__ a, const float *__restrict__ b, float *__restrict__ out,
-                              int64_t n) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        out[i] = a[i] * b[i];
-}
-
-// ebar = ebar * a + t
-__global__ void rl_ebar_kernel(float *__restrict__ ebar, const float *__restrict__ a, const float *__restrict__ t,
-                               int64_t n) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        ebar[i] = fmaf(ebar[i], a[i], t[i]);
-}
-
 // acc += x * conj(y) (+ u * conj(v) when u is given), over n complex values.
 __global__ void spec_mac_kernel(float2 *__restrict__ acc, const float2 *__restrict__ x, const float2 *__restrict__ y,
                                 const float2 *__restrict__ u, const float2 *__restrict__ v, int64_t n) {
@@ -1318,7 +1327,7 @@ int rl_backward(const RlGeom &g, const RlBuffers &b, const RlBwdBuffers &w, cons
     const int64_t V = (int64_t)g.Z * g.Y * g.X;
     const size_t vb = (size_t)V * sizeof(float);
     const int64_t nspec = (int64_t)g.Pz * g.Py * g.Hp;
-    const int grid = ew_grid_rl(V), sg = ew_grid_rl(nspec);
+    const int sg = ew_grid_rl(nspec);
     int e;
     if (K < 1) K = 1;
     const int nseg = (T + K - 1) / K;
@@ -1353,16 +1362,14 @@ int rl_backward(const RlGeom &g, const RlBuffers &b, const RlBwdBuffers &w, cons
             if ((e = run.pair(b.h_conv, 0, spec_e))) return e;
             if ((e = run.row(kRowRatioKeep, y, w.c, 0, 0, 0, eps))) return e;
             if ((e = run.pair(b.h_corr, 1, spec_r))) return e;
-            if ((e = run.row(kRowRealOut, nullptr, w.a, 0, 0, 0, eps))) return e;
-            rl_mul_kernel<<<grid, 256, 0, s>>>(w.ebar, ek, w.abar, V);
-            // rbar = B^T abar, then cbar (and ybar) fused into the row pass that
-            // starts t = A^T cbar.
-            if ((e = run.row(kRowRealIn, w.abar, nullptr, 0, 0, 0, eps))) return e;
+            // a out (kept) and abar = ebar * e_k in, in one row pass; rbar =
+            // B^T abar; cbar (and ybar) fused into the row pass that starts
+            // t = A^T cbar; ebar = ebar * a + t fused into the last one.
+            if ((e = run.row(kRowAbar, ek, w.a, 0, 0, 0, eps, w.ebar))) return e;
             if ((e = run.pair(b.h_corr, 0, spec_abar))) return e;
             if ((e = run.row(kRowCbar, y, nullptr, 0, 0, 0, eps, w.c, ybar))) return e;
             if ((e = run.pair(b.h_conv, 1, spec_cbar))) return e;
-            if ((e = run.row(kRowRealOut, nullptr, w.t, 0, 0, 0, eps))) return e;
-            rl_ebar_kernel<<<grid, 256, 0, s>>>(w.ebar, w.a, w.t, V);
+            if ((e = run.row(kRowEbar, nullptr, nullptr, 0, 0, 0, eps, w.a, w.ebar))) return e;
             if (pbar2) {
                 spec_mac_kernel<<<sg, 256, 0, s>>>(pbar1, spec_cbar, spec_e, nullptr, nullptr, nspec);
                 spec_mac_kernel<<<sg, 256, 0, s>>>(pbar2, spec_r, spec_abar, nullptr, nullptr, nspec);
