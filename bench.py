@@ -459,6 +459,17 @@ def rl_batch_secondary(dev, peak, reps=3):
     ms_graph = timed(g.launch, reps)
     ms_batched = timed(plan.run, reps)
     ms_per_image = timed(lambda: plan.run(per_problem=True), 1)
+    # The same images through the public single-image call, one after another.
+    api_outs = [torch.empty_like(x) for x in images]
+
+    def per_image_api():
+        for x, k, o in zip(images, psfs, api_outs):
+            lb.richardson_lucy(x, k, num_iter=T, clip=False, filter_epsilon=1e-6, mode="constant", out=o,
+                               workspace=ws)
+
+    per_image_api()
+    ms_api = timed(per_image_api, 1)
+    del api_outs
     px = sum(int(x.numel()) for x in images)
     # Algorithmic bytes per iteration: two convolution passes, each
     # 12 HW + 32 H Pw' + 24 Ph Pw' bytes (real in/out, row spectra, column
@@ -478,7 +489,8 @@ def rl_batch_secondary(dev, peak, reps=3):
                       "30 iterations)",
             "value": px * T / (best * 1e-3) / 1e9, "unit": "Gpx-iter/s", "ms_per_batch": best,
             "ms_graph_replay": ms_graph, "ms_batched_launches": ms_batched, "ms_per_image_launches": ms_per_image,
-            "batched_vs_per_image": ms_per_image / best, "pixels": px,
+            "batched_vs_per_image": ms_per_image / best,
+            "ms_per_image_api_calls": ms_api, "batched_vs_per_image_api_calls": ms_api / best, "pixels": px,
             "launch_groups": {"row": n_row, "column": n_col},
             "launches_batched": 1 * n_row + T * (2 * n_row + 2 * n_col),
             "launches_per_image": len(grids) * (1 + 4 * T),
