@@ -218,9 +218,37 @@ __global__ void __launch_bounds__(512, 1) col_pass_kernel(const __grid_constant_
 // bit 1, the input rows N/2 .. N-1 are zero (not loaded, first forward
 // stage pruned); bit 2, only the rows below N/2 are stored (last inverse
 // stage pruned).
+// The input rows of global tile gt held by thread (c, t) in value slots
+// i < N2 (i < N2 / 2 when the upper half is zero), padded per the pass.
+template <int N1, int N2, int C, bool ZERO_HI>
+__device__ __forceinline__ void col_load_input(const ColPass &p, int gt, int t, int c, float2 *v) {
+    int tile;
+    const ColItem q = col_tile(p, gt, &tile);
+    const int col = tile * C + c;
+    const bool ok = col < q.ncols;
+    int outer = 0, kx = 0;
+    if (ok) {
+        outer = col / q.Hx;
+        kx = col - outer * q.Hx;
+    }
+    const float2 *src = q.src + (outer * q.src_outer + kx);
+    const int n_ext = q.n_img + 2 * q.halo, src_row = (int)q.src_row;
+#pragma unroll
+    for (int i = 0; i < N2; ++i) {
+        if (ZERO_HI && i >= N2 / 2) continue;
+        const int row = t + N1 * i;
+        int srow = row < n_ext ? pad_index_rt(row - q.halo, q.n_img, p.pad_mode) : -1;
+        v[i] = (ok && srow >= 0) ? src[srow * src_row] : make_float2(0.f, 0.f);
+    }
+}
+
+// PR bit 4 (with bit 1, forward and full modes): the next tile's input rows
+// are loaded into registers before the current tile's transforms, so their
+// memory latency overlaps the arithmetic.
 template <int N1, int N2, int C, bool SEP, int PR, int MODE>
 __global__ void __launch_bounds__(N1 * C, (N2 > 32 ? 1 : 65536 / (N1 * C * 128))) col_fast_kernel(const __grid_constant__ ColPass p) {
     constexpr bool kZeroHi = (PR & 1) != 0, kLoOnly = (PR & 2) != 0;
+    constexpr bool kPrefetch = (PR & 4) != 0 && kZeroHi && MODE != kColInv;
     // MODE: the pass's ColMode (p.mode), fixed at compile time.
     using L = fftc::ColLayout<N1, N2, C>;
     using F = fftc::TwoStep<N1, N2, L>;
@@ -233,6 +261,10 @@ __global__ void __launch_bounds__(N1 * C, (N2 > 32 ? 1 : 65536 / (N1 * C * 128))
     F::build_tables(tf, ti, p.tw, 1);
     __syncthreads();
     const int ntiles = p.items ? p.total_tiles : (p.ncols + C - 1) / C;
+    float2 nx[kPrefetch ? N2 / 2 : 1];
+    if constexpr (kPrefetch) {
+        if (blockIdx.x < ntiles) col_load_input<N1, N2, C, true>(p, blockIdx.x, t, c, nx);
+    }
     for (int gt = blockIdx.x; gt < ntiles; gt += gridDim.x) {
         int tile;
         const ColItem q = col_tile(p, gt, &tile);
@@ -266,12 +298,18 @@ __global__ void __launch_bounds__(N1 * C, (N2 > 32 ? 1 : 65536 / (N1 * C * 128))
                 for (int j = 0; j < (kPrefetchH ? N2 : 1); ++j)
                     hv[j] = ok ? h[F::freq(t, j) * h_row] : make_float2(0.f, 0.f);
             }
+            if constexpr (kPrefetch) {
 #pragma unroll
-            for (int i = 0; i < N2; ++i) {
-                if (kZeroHi && i >= N2 / 2) continue;  // rows >= N/2: zero, never read
-                const int row = t + N1 * i;
-                int srow = row < n_ext ? pad_index_rt(row - q.halo, q.n_img, p.pad_mode) : -1;
-                v[i] = (ok && srow >= 0) ? src[srow * src_row] : make_float2(0.f, 0.f);
+                for (int i = 0; i < N2 / 2; ++i) v[i] = nx[i];
+                if (gt + (int)gridDim.x < ntiles) col_load_input<N1, N2, C, true>(p, gt + gridDim.x, t, c, nx);
+            } else {
+#pragma unroll
+                for (int i = 0; i < N2; ++i) {
+                    if (kZeroHi && i >= N2 / 2) continue;  // rows >= N/2: zero, never read
+                    const int row = t + N1 * i;
+                    int srow = row < n_ext ? pad_index_rt(row - q.halo, q.n_img, p.pad_mode) : -1;
+                    v[i] = (ok && srow >= 0) ? src[srow * src_row] : make_float2(0.f, 0.f);
+                }
             }
             F::template forward<kZeroHi>(v, t, c, xb, tf);
             if (MODE == kColFull && q.spec_out != nullptr && ok) {
@@ -829,8 +867,16 @@ int launch_col_fast(const ColPass &p, cudaStream_t s) {
         if (pr & 2) go(col_fast_kernel<N1, N2, C, false, 2, kColInv>);
         else go(col_fast_kernel<N1, N2, C, false, 0, kColInv>);
     } else if (p.Hrow) {
-        if (pr == 3) go(col_fast_kernel<N1, N2, C, true, 3, kColFull>);
-        else go(col_fast_kernel<N1, N2, C, true, 0, kColFull>);
+        // The 128-point separable full pass loads the next tile ahead (PR
+        // bit 4): 238 against 246 us per launch on the 64x512x512 volume.
+        // The same prefetch in the forward pass measured slower; the other
+        // lengths keep the plain loads.
+        if (pr == 3) {
+            if constexpr (N1 * N2 == 128) go(col_fast_kernel<N1, N2, C, true, 7, kColFull>);
+            else go(col_fast_kernel<N1, N2, C, true, 3, kColFull>);
+        } else {
+            go(col_fast_kernel<N1, N2, C, true, 0, kColFull>);
+        }
     } else {
         if (pr == 3) go(col_fast_kernel<N1, N2, C, false, 3, kColFull>);
         else go(col_fast_kernel<N1, N2, C, false, 0, kColFull>);
