@@ -140,11 +140,18 @@ def rl_kernel_bytes(shape, grid, separable=False):
     # times a [Pz] vector, read from L2 rather than HBM: not counted.
     h = 0 if separable else Pz * Py * Hx * c
     v = Z * Y * X * 4
+    # Row passes of one step: the initial one (writes S1), then per iteration
+    # ratio (read S1 + obs, write S1) and update (read S1 + est, write S1 +
+    # est; the last one writes est only): the average per launch.
+    it = ITERS
+    row_total = s1 + it * (2 * s1 + v) + (it - 1) * (2 * s1 + 2 * v) + (s1 + 2 * v)
     return {
         "rl_col_full": s2 + h + s2,           # z pass: read S2, read H, write S2
         "rl_col_forward": s1 + s2,            # y forward: read S1, write S2
         "rl_col_inverse": s2 + s1,            # y inverse: read S2, write S1
-        "rl_row_pass": s1 + v + s1,           # ratio pass: read S1 + obs, write S1 (update: + est)
+        "rl_col_y": 2 * s1,                   # separable: y convolution, S1 in place
+        "rl_col_z": 2 * s1,                   # separable: z convolution, S1 in place
+        "rl_row_pass": row_total / (1 + 2 * it),
     }
 
 
@@ -169,6 +176,43 @@ def cpu_sample_rate(num_threads=0):
     return int(np.prod(CPU_SAMPLE)) / dt / 1e9, dt, O.get_threads()
 
 
+def cpu_fft_sample_rate(num_iter=1):
+    """The same workload on the host through FFTs (the oracle's f32 FFT
+    restatement on scipy.fft, complex64 spectra, all host cores), full volume
+    and grid, `num_iter` iterations: returns (Gvox-iter/s, seconds, threads)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O  # the CPU restatement (baseline leg only)
+
+    from lucem_b200 import synth
+
+    obs, psf = synth.bead_volume(shape=SHAPE, psf_shape=PSF_SHAPE)
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    O.richardson_lucy_fft(obs, psf, num_iter=num_iter, clip=False, filter_epsilon=EPS, grid=GRID,
+                          dtype=np.float32, workers=threads)
+    dt = time.perf_counter() - t0
+    return int(np.prod(SHAPE)) * num_iter / dt / 1e9, dt, threads
+
+
+def fp64_crosscheck():
+    """tests/fp64_cufft.py: FP64 Richardson-Lucy through cuFFT (float64), the
+    cross-check the parity tests pin to the host FP64 oracle."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import fp64_cufft
+
+    return fp64_cufft
+
+
+def perturbed_psf(psf, seed=0x6C7563656D + 11, amount=1e-3):
+    """The Gaussian PSF plus a seeded non-negative term that grows along x:
+    not a product of per-axis factors (the dense transfer-function path);
+    the same PSF as tests/test_rl_fullsize_gpu.py."""
+    rng = np.random.default_rng(seed)
+    p = psf.astype(np.float64)
+    p = p + amount * p.max() * rng.uniform(0.0, 1.0, p.shape) * (np.arange(p.shape[2]) / p.shape[2])[None, None, :]
+    return (p / p.sum()).astype(np.float32)
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -189,6 +233,58 @@ def run_reference(args, rank, world):
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def rl3d_dense_secondary(dev, peak, steps=3):
+    """The headline volume with a non-separable PSF (the Gaussian plus a 1e-3
+    asymmetric perturbation): the general path with a dense transfer function
+    streamed through the z pass.  Same grid, iterations and settings."""
+    import torch
+
+    import lucem_b200 as lb
+
+    obs_h, psf_h = lb.synth.bead_volume(shape=SHAPE, psf_shape=PSF_SHAPE)
+    p_h = perturbed_psf(psf_h)
+    obs = torch.from_numpy(obs_h).to(dev)
+    psf = torch.from_numpy(p_h).to(dev)
+    out = torch.empty_like(obs)
+    ws = lb.Workspace(dev.index)
+    s = torch.cuda.current_stream(dev)
+
+    def step():
+        lb.richardson_lucy(obs, psf, num_iter=ITERS, clip=False, filter_epsilon=EPS, mode="constant", grid=GRID,
+                           out=out, workspace=ws)
+
+    step()
+    torch.cuda.synchronize(dev)
+    ws.set_timing(True)
+    step()
+    kinds = ws.timings()
+    ws.set_timing(False)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    a.record(s)
+    for _ in range(steps):
+        step()
+    b.record(s)
+    torch.cuda.synchronize(dev)
+    ms = a.elapsed_time(b) / steps
+    nbytes = rl_kernel_bytes(SHAPE, GRID, separable=False)
+    dominant = max(kinds, key=lambda k: kinds[k][1])
+    cnt, tot = kinds[dominant]
+    alg = nbytes.get(dominant)
+    achieved = alg / (tot / cnt * 1e-3) / 1e9 if alg else None
+    F = fp64_crosscheck()
+    err = F.max_rel_err(out, F.richardson_lucy(obs, p_h, ITERS, EPS, GRID))
+    torch.cuda.empty_cache()
+    return {"metric": "RL Gvox-iter/s, dense transfer function (64x512x512 bead volume, non-separable 31x15x15 "
+                      "PSF, 50 iterations, grid 128x1024x1024)",
+            "value": int(np.prod(SHAPE)) * ITERS / (ms * 1e-3) / 1e9, "unit": UNIT, "ms_per_step": ms,
+            "step_kernels": {k: {"launches": c, "ms": t} for k, (c, t) in kinds.items()},
+            "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak if achieved else None, "us_per_launch": tot / cnt * 1e3,
+                         "algorithmic_bytes_per_launch": alg, "traffic": profile_traffic(dominant + "_dense")},
+            "parity": {"max_rel_err_vs_fp64": err, "tolerance": 1e-4}}
 
 
 def gaussian_secondary(dev, peak):
@@ -319,7 +415,9 @@ def psf_fit_secondary(dev, steps=2):
                                  seed=500 + b)[0] for b in range(B)]
     obs = torch.from_numpy(np.stack(vols)).to(dev)
     obs = obs / obs.max()
-    theta = torch.zeros(kshape, dtype=torch.float32, device=dev, requires_grad=True)
+    # Initial PSF: Gaussian sigma_z 4, sigma_xy 2, through the inverse softplus.
+    g0 = lb.synth.gaussian_psf(kshape, (4.0, 2.0, 2.0))
+    theta = torch.from_numpy(np.log(np.expm1(g0)).astype(np.float32)).to(dev).requires_grad_(True)
     ws = lb.Workspace(dev)
     s = torch.cuda.current_stream(dev)
 
@@ -481,6 +579,13 @@ def rl_batch_secondary(dev, peak, reps=3):
         it_bytes += 2 * (12 * h * w + 32 * h * pw + 24 * py * pw)
     best = min(ms_graph, ms_batched)
     achieved = it_bytes * T / (best * 1e-3) / 1e9
+    # Parity of every 8th image of the last run against FP64 on its grid.
+    plan.run()
+    F = fp64_crosscheck()
+    torch.cuda.synchronize(dev)
+    worst = 0.0
+    for i in range(0, len(images), 8):
+        worst = max(worst, F.max_rel_err(plan.outs[i], F.richardson_lucy(images[i], psfs[i], T, 1e-6, grids[i])))
     g.close()
     plan.close()
     del images, psfs
@@ -492,6 +597,8 @@ def rl_batch_secondary(dev, peak, reps=3):
             "batched_vs_per_image": ms_per_image / best,
             "ms_per_image_api_calls": ms_api, "batched_vs_per_image_api_calls": ms_api / best, "pixels": px,
             "launch_groups": {"row": n_row, "column": n_col},
+            "parity": {"max_rel_err_vs_fp64": worst, "tolerance": 1e-4,
+                       "sample": "every 8th image (32 of 256); all 256 in tests/test_rl_fullsize_gpu.py"},
             "launches_batched": 1 * n_row + T * (2 * n_row + 2 * n_col),
             "launches_per_image": len(grids) * (1 + 4 * T),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -613,20 +720,36 @@ def run_ours(args, rank, world, local_rank):
                                 else "fallback: 6.65 TB/s, a copy bandwidth measured earlier on B200 (MEASURED_PEAKS.json absent)")}
     step_kernels = {k: {"launches": c, "ms": t, "share": t / sum(v[1] for v in kinds.values())}
                     for k, (c, t) in kinds.items()}
-    cpu = None
+    # Parity of the timed result (the last step's estimate) against FP64.
+    F = fp64_crosscheck()
+    parity = {"max_rel_err_vs_fp64": F.max_rel_err(out, F.richardson_lucy(obs, psf_h, ITERS, EPS, GRID)),
+              "tolerance": 1e-4,
+              "fp64": "cuFFT float64 on the device (tests/fp64_cufft.py), pinned to the host scipy FP64 oracle "
+                      "on this grid by tests/test_rl_fullsize_gpu.py",
+              "vs_f32_restatement": None,
+              "note": "the f32 direct restatement of the reference is checked at reduced sizes in tests/; at "
+                      "this size it would take days on the host"}
+    torch.cuda.empty_cache()
+    cpu = cpu_fft = None
     if world == 1:
         r, dt, threads = cpu_sample_rate()
         cpu = {"value": r, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"direct-correlation RL (reference algorithm) on a {CPU_SAMPLE[0]}x{CPU_SAMPLE[1]}x"
                          f"{CPU_SAMPLE[2]} sub-volume, full PSF, 1 iteration ({dt:.2f} s)"}
+        r, dt, threads = cpu_fft_sample_rate()
+        cpu_fft = {"value": r, "unit": UNIT, "cores": threads, "kind": "port-fft",
+                   "sample": f"f32 FFT restatement (scipy.fft, complex64) on the full 64x512x512 volume and "
+                             f"128x1024x1024 grid, 1 iteration ({dt:.2f} s)"}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "l2": "working set ~0.95 GB per step (spectra + transfer function) > 126 MB L2; no flush"},
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "roofline": roofline, "cpu_baseline": cpu, "cpu_baseline_fft": cpu_fft, "parity": parity, "e2e": e2e,
             "gpu_launches": launches_per_step * args.steps, "clocks": clocks, "step_kernels": step_kernels,
             "secondary": {"gaussian_2048": gaussian_secondary(dev, peak)}}
+    if args.dense:
+        line["secondary"]["rl3d_dense"] = rl3d_dense_secondary(dev, peak)
     if args.tiles:
         line["secondary"]["gaussian_tiles"] = tiles_secondary(dev, peak)
     if args.psf_fit:
@@ -646,6 +769,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--iters", type=int, default=ITERS, help="Richardson-Lucy iterations per step (metric: 50)")
+    ap.add_argument("--dense", type=int, default=1, help="also measure the headline with a non-separable PSF")
     ap.add_argument("--tiles", type=int, default=1, help="also measure the tiled-slide Gaussian family walk")
     ap.add_argument("--psf-fit", type=int, default=1, help="also measure the differentiable blind PSF fit")
     ap.add_argument("--rl-batch", type=int, default=1, help="also measure the batched uneven 2-D RL")

@@ -62,7 +62,7 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> str:
         return LIB
     os.makedirs(BUILD, exist_ok=True)
     srcs = sources()
-    with cf.ThreadPoolExecutor(max_workers=min(8, len(srcs))) as ex:
+    with cf.ThreadPoolExecutor(max_workers=max(1, min(os.cpu_count() or 8, len(srcs)))) as ex:
         objs = list(ex.map(lambda s: _compile(s, verbose_ptxas), srcs))
     tmp = LIB + ".tmp"
     cmd = [_nvcc(), *ARCH, "-shared", "-Xcompiler", "-fPIC", "-o", tmp, *objs, "-cudart", "static"]

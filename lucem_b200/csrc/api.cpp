@@ -211,7 +211,7 @@ namespace lucem {
 const char *pass_name(int kind) {
     static const char *names[kPassCount] = {"rl_row_pass", "rl_col_forward", "rl_col_full", "rl_col_inverse",
                                             "rl_transfer_function", "gaussian_family", "correlate_1d",
-                                            "elementwise"};
+                                            "elementwise", "rl_col_y", "rl_col_z"};
     return kind >= 0 && kind < kPassCount ? names[kind] : "?";
 }
 }  // namespace lucem
@@ -1887,17 +1887,29 @@ lucem_status rl_prepare(lucem_ctx *ctx, const lucem_tensor *in, const lucem_tens
     key.append(reinterpret_cast<const char *>(grid), 3 * sizeof(int64_t));
     key.append(reinterpret_cast<const char *>(&g.Hp), sizeof g.Hp);
     key.push_back(separable ? 's' : 'd');
+    key.push_back((char)('0' + nd));
     void *h_conv = nullptr, *h_corr = nullptr, *r_conv = nullptr, *r_corr = nullptr;
     Slot *sl_conv = nullptr, *sl_corr = nullptr;
     if ((st = ws->get("rl_otf_conv", hbytes, &h_conv, &sl_conv))) return st;
     if (!same_centre && (st = ws->get("rl_otf_corr", hbytes, &h_corr, &sl_corr))) return st;
+    void *y_conv = nullptr, *y_corr = nullptr, *x_conv = nullptr, *x_corr = nullptr;
     if (separable) {
         if ((st = ws->get("rl_otf_conv_row", (size_t)nrow * sizeof(float2_), &r_conv))) return st;
         if (!same_centre && (st = ws->get("rl_otf_corr_row", (size_t)nrow * sizeof(float2_), &r_corr))) return st;
+        if (nd == 3) {
+            if ((st = ws->get("rl_otf_conv_y", (size_t)g.Py * sizeof(float2_), &y_conv))) return st;
+            if ((st = ws->get("rl_otf_conv_x", (size_t)g.Hp * sizeof(float2_), &x_conv))) return st;
+            if (!same_centre) {
+                if ((st = ws->get("rl_otf_corr_y", (size_t)g.Py * sizeof(float2_), &y_corr))) return st;
+                if ((st = ws->get("rl_otf_corr_x", (size_t)g.Hp * sizeof(float2_), &x_corr))) return st;
+            }
+        }
     }
     if (same_centre) {
         h_corr = h_conv;
         r_corr = r_conv;
+        y_corr = y_conv;
+        x_corr = x_conv;
     }
     const bool fresh = sl_conv->key != key || (!same_centre && sl_corr->key != key);
     if (fresh && separable) {
@@ -1920,8 +1932,8 @@ lucem_status rl_prepare(lucem_ctx *ctx, const lucem_tensor *in, const lucem_tens
         };
         const double scale = 1.0 / ((double)g.Pz * (double)g.Py * (double)g.Px);
         cudaStream_t cs2 = static_cast<cudaStream_t>(stream);
-        std::vector<float> tab, rowv;
-        auto build = [&](const int32_t *cen, void *hdst, void *rdst) -> lucem_status {
+        std::vector<float> tab, rowv, yv, xv;
+        auto build = [&](const int32_t *cen, void *hdst, void *rdst, void *ydst, void *xdst) -> lucem_status {
             const std::vector<double> fz = dft(marg[0], cen[0], g.Pz, g.Pz);
             const std::vector<double> fy = dft(marg[1], cen[1], g.Py, g.Py);
             const std::vector<double> fx = dft(marg[2], cen[2], g.Px, g.Hx);
@@ -1942,12 +1954,25 @@ lucem_status rl_prepare(lucem_ctx *ctx, const lucem_tensor *in, const lucem_tens
                      "transfer function upload");
             CUDA_TRY(cudaMemcpyAsync(rdst, rowv.data(), rowv.size() * sizeof(float), cudaMemcpyHostToDevice, cs2),
                      "transfer function upload");
+            if (ydst) {
+                // Per-axis factors of the 3-D table: Fy alone, Fx with the scale.
+                yv.assign(fy.begin(), fy.end());
+                xv.assign((size_t)(2 * g.Hp), 0.0f);
+                for (int64_t x = 0; x < g.Hx; ++x) {
+                    xv[(size_t)(2 * x)] = (float)(fx[(size_t)(2 * x)] * scale);
+                    xv[(size_t)(2 * x + 1)] = (float)(fx[(size_t)(2 * x + 1)] * scale);
+                }
+                CUDA_TRY(cudaMemcpyAsync(ydst, yv.data(), yv.size() * sizeof(float), cudaMemcpyHostToDevice, cs2),
+                         "transfer function upload");
+                CUDA_TRY(cudaMemcpyAsync(xdst, xv.data(), xv.size() * sizeof(float), cudaMemcpyHostToDevice, cs2),
+                         "transfer function upload");
+            }
             // The host tables are reused for the second centre.
             CUDA_TRY(cudaStreamSynchronize(cs2), "transfer function upload");
             return ok();
         };
-        if ((st = build(su->c_conv, h_conv, r_conv))) return st;
-        if (!same_centre && (st = build(su->c_corr, h_corr, r_corr))) return st;
+        if ((st = build(su->c_conv, h_conv, r_conv, y_conv, x_conv))) return st;
+        if (!same_centre && (st = build(su->c_corr, h_corr, r_corr, y_corr, x_corr))) return st;
         sl_conv->key = key;
         if (sl_corr) sl_corr->key = key;
     } else if (fresh) {
@@ -1983,6 +2008,10 @@ lucem_status rl_prepare(lucem_ctx *ctx, const lucem_tensor *in, const lucem_tens
     b.h_corr = h_corr;
     b.hrow_conv = separable ? r_conv : nullptr;
     b.hrow_corr = separable ? r_corr : nullptr;
+    b.hy_conv = y_conv;
+    b.hy_corr = y_corr;
+    b.hx_conv = x_conv;
+    b.hx_corr = x_corr;
     b.tw_x = tw32[2];
     b.tw_y = tw32[1];
     b.tw_z = tw32[0];

@@ -158,6 +158,8 @@ enum PassKind : int {
     kPassFamily,         // fused 2-D Gaussian family
     kPassCorrelate,      // per-axis correlation
     kPassElementwise,    // combine / cast / fill
+    kPassRlColY,         // separable PSF: y convolution on the row spectra (forward * Hy * inverse)
+    kPassRlColZ,         // separable PSF: z convolution on the row spectra (forward * Hz * inverse)
     kPassCount
 };
 const char *pass_name(int kind);
@@ -205,6 +207,11 @@ struct RlBuffers {
     // hrow_* that factor ([Pz] in 3-D, [Py] in 2-D).  Null: dense transfer
     // functions.
     const void *hrow_conv, *hrow_corr;
+    // Separable 3-D PSF, per-axis factors: y ([Py]) and x times 1/(Pz Py Px)
+    // ([Hp]).  With them a convolution without a spectrum output runs as a
+    // y convolution and a z convolution on s1 (no s2 round trip).  Null
+    // otherwise.
+    const void *hy_conv, *hy_corr, *hx_conv, *hx_corr;
     const float2_ *tw_x, *tw_y, *tw_z;  // twiddle tables e^{-2 pi i k / n}, n = Px, Py, Pz
 };
 

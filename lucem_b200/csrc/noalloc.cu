@@ -17,7 +17,12 @@
 //
 // Set-up: the first call on a device (with that device current) resolves the
 // array's device address with cudaGetSymbolAddress, once per device; that
-// first call should come before any stream capture on the device.
+// first call should come before any stream capture on the device.  The address
+// is kept for the life of the process: after a cudaDeviceReset the array is
+// reloaded elsewhere and this entry point must not be called again.
+//
+// Taps reach the array through kernel parameters (put_taps below), so a call
+// makes no host-to-device copy.
 //
 // Sharing: every call uses the same array and it keeps the previous call's
 // contents.  Nothing here needs to start at zero (each pass overwrites what
@@ -26,6 +31,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -68,6 +74,32 @@ lucem_status scratch_base(float **out) {
     }
     *out = d.base;
     return LUCEM_OK;
+}
+
+// Taps travel to the device inside the parameters of a small kernel, not
+// through a host-to-device copy: a launch copies its parameters when it is
+// issued (and a captured launch keeps its own copy), so no host buffer has to
+// outlive the call and nothing is staged through pageable memory.
+constexpr int kTapsPerLaunch = 1000;  // 4,004 bytes of parameters
+struct TapsChunk {
+    int32_t n;
+    float w[kTapsPerLaunch];
+};
+
+__global__ void put_taps_kernel(float *__restrict__ dst, const TapsChunk chunk) {
+    for (int i = threadIdx.x; i < chunk.n; i += blockDim.x) dst[i] = chunk.w[i];
+}
+
+int put_taps(float *dst, const std::vector<float> &w, cudaStream_t s) {
+    for (size_t off = 0; off < w.size(); off += kTapsPerLaunch) {
+        TapsChunk c;
+        c.n = (int32_t)std::min(w.size() - off, (size_t)kTapsPerLaunch);
+        std::memcpy(c.w, w.data() + off, (size_t)c.n * sizeof(float));
+        put_taps_kernel<<<1, 256, 0, s>>>(dst + off, c);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return (int)e;
+    }
+    return 0;
 }
 
 int64_t numel_of(const lucem_tensor *t) {
@@ -127,10 +159,9 @@ extern "C" lucem_status lucem_gaussian_blur_noalloc(const lucem_tensor *in, cons
     int64_t tap_off = 0;
     for (size_t i = 0; i < n_generic; ++i) {
         const lucem::GaussPass &p = passes[i];
-        std::vector<float> w = lucem::gaussian_pass_taps(p);
-        cudaError_t ce = cudaMemcpyAsync(taps + tap_off, w.data(), w.size() * sizeof(float),
-                                         cudaMemcpyHostToDevice, cs);
-        if (ce != cudaSuccess) return lucem::set_error(LUCEM_ERR_CUDA, cudaGetErrorString(ce));
+        const std::vector<float> w = lucem::gaussian_pass_taps(p);
+        if (int e = put_taps(taps + tap_off, w, cs))
+            return lucem::set_error(LUCEM_ERR_CUDA, cudaGetErrorString((cudaError_t)e));
         const bool last = !fuse && i + 1 == n_generic;
         float *dst = last ? dst_final : bufs[ping];
         int64_t outer = 1, inner = 1;

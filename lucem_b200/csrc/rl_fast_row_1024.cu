@@ -1,0 +1,11 @@
+// rl_fast_row_1024.cu -- instantiations of the register-resident Richardson-Lucy passes
+// (rl_pass.cuh) for packed row length 1024, in a translation unit of their own.
+#include "rl_pass.cuh"
+
+namespace lucem {
+namespace rlp {
+
+int launch_row_1024(const RowPass &p, cudaStream_t s) { return launch_row_fast<32, 32, 8>(p, s); }
+
+}  // namespace rlp
+}  // namespace lucem

@@ -279,7 +279,16 @@ def richardson_lucy_fft64(obs, psf, num_iter=30, clip=False, filter_epsilon=None
     """FP64 Richardson-Lucy with zero padding (PadMode::Constant, cval 0) computed
     through FFTs on `grid` (>= dims + k - 1 per axis).  Mathematically equal to
     the reference's direct Constant-mode iteration (deconvolve.rs:109-147)."""
-    obs = np.asarray(obs, np.float64)
+    return richardson_lucy_fft(obs, psf, num_iter, clip, filter_epsilon, grid, np.float64)
+
+
+def richardson_lucy_fft(obs, psf, num_iter=30, clip=False, filter_epsilon=None, grid=None, dtype=np.float64,
+                        workers=-1):
+    """richardson_lucy_fft64 in `dtype` (float64, or float32 with complex64
+    spectra: the host FFT restatement the benchmark times), on `workers`
+    threads (-1: all host cores).  The transfer functions are built in FP64
+    and rounded once to `dtype`."""
+    obs = np.asarray(obs, dtype)
     psf = np.asarray(psf, np.float64)
     nd = obs.ndim
     if grid is None:
@@ -290,18 +299,20 @@ def richardson_lucy_fft64(obs, psf, num_iter=30, clip=False, filter_epsilon=None
     k = psf.shape
     # correlate(src, flipped psf) == convolution with p centred at k-1-k//2;
     # correlate(src, p) == correlation with p centred at k//2 (convolve.rs:144-145).
-    h_conv = centred_otf(p, grid, [k[d] - 1 - k[d] // 2 for d in range(nd)])
-    h_corr = np.conj(centred_otf(p, grid, [k[d] // 2 for d in range(nd)]))
-    eps = rl_epsilon(filter_epsilon)
+    cdt = np.complex128 if dtype == np.float64 else np.complex64
+    h_conv = centred_otf(p, grid, [k[d] - 1 - k[d] // 2 for d in range(nd)]).astype(cdt, copy=False)
+    h_corr = np.conj(centred_otf(p, grid, [k[d] // 2 for d in range(nd)])).astype(cdt, copy=False)
+    eps = dtype(rl_epsilon(filter_epsilon))
     sl = tuple(slice(0, n) for n in obs.shape)
-    est = np.full(obs.shape, 0.5)
+    est = np.full(obs.shape, 0.5, dtype)
     for it in range(num_iter):
         ax = tuple(range(nd))
-        conv = sfft.irfftn(sfft.rfftn(est, grid, axes=ax, workers=-1) * h_conv, grid, axes=ax, workers=-1)[sl]
+        conv = sfft.irfftn(sfft.rfftn(est, grid, axes=ax, workers=workers) * h_conv, grid, axes=ax,
+                           workers=workers)[sl]
         safe = np.where(np.abs(conv) < eps, eps, conv)
         ratio = obs / safe
-        corr = sfft.irfftn(sfft.rfftn(ratio, grid, axes=ax, workers=-1) * h_corr, grid, axes=ax,
-                           workers=-1)[sl]
+        corr = sfft.irfftn(sfft.rfftn(ratio, grid, axes=ax, workers=workers) * h_corr, grid, axes=ax,
+                           workers=workers)[sl]
         est = est * corr
         if clip and it + 1 == num_iter:
             est = np.clip(est, -1.0, 1.0)

@@ -54,6 +54,51 @@ def test_two_calls_in_a_row_match_the_allocating_entry_point(oracle):
     oracle.assert_close(got_b.cpu().numpy(), want_b.cpu().numpy().astype(np.float64), RTOL, "second call")
 
 
+def test_three_generic_passes_use_both_halves_of_the_scratch(oracle):
+    """A radius beyond the fused 2-D kernel on every axis of a volume: three
+    generic passes, input -> first half -> second half -> output."""
+    rng = np.random.default_rng(23)
+    x = torch.from_numpy(rng.standard_normal((40, 70, 90)).astype(np.float32)).cuda()
+    for sig in ([9.0], [9.5, 10.0, 11.0]):
+        got = noalloc_blur(x, sig, mode="wrap")
+        want = lb.gaussian_blur(x, sig, mode="wrap")
+        torch.cuda.synchronize()
+        oracle.assert_close(got.cpu().numpy(), want.cpu().numpy().astype(np.float64), RTOL, f"sigma {sig}")
+
+
+def test_repeated_calls_leave_device_memory_unchanged():
+    """After one call of each kind (kernels loaded), further calls with new
+    data take no device memory: free memory before and after is equal."""
+    rng = np.random.default_rng(29)
+    a = torch.from_numpy(rng.integers(0, 4000, (12, 150, 260)).astype(np.uint16)).cuda()
+    b = torch.from_numpy(rng.standard_normal((300, 410)).astype(np.float32)).cuda()
+    full = torch.ones((2, 1024, 2048), dtype=torch.float32, device="cuda")  # exactly the maximum
+    calls = [(a, [1.5, 2.0, 2.5]), (b, [9.0]), (full, [1.0, 2.0, 2.0])]
+    outs = [torch.empty(x.shape, dtype=torch.float32, device="cuda") for x, _ in calls]
+
+    def run_all():
+        for (x, sig), o in zip(calls, outs):
+            s = N.GaussianSettings()
+            N.lib().lucem_gaussian_settings_default(C.byref(s))
+            arr = (C.c_double * len(sig))(*sig)
+            ti, to = _tensor(x, "input"), _tensor(o, "output")
+            stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+            N.check(N.lib().lucem_gaussian_blur_noalloc(C.byref(ti), arr, len(sig), C.byref(s), C.byref(to), stream))
+
+    a2 = torch.from_numpy(rng.integers(0, 4000, a.shape).astype(np.uint16)).cuda()
+    b2 = torch.from_numpy(rng.standard_normal(b.shape).astype(np.float32)).cuda()
+    run_all()
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    a.copy_(a2)
+    b.copy_(b2)
+    for _ in range(3):
+        run_all()
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, f"free device memory changed by {free0 - free1} bytes"
+
+
 def test_sizes_beyond_the_static_scratch_are_refused():
     x = torch.zeros((MAX_ELEMS + 1,), dtype=torch.float32, device="cuda")
     with pytest.raises(N.LucemError) as e:
