@@ -102,6 +102,17 @@ size_t lucem_workspace_capacity_bytes(const lucem_workspace *ws);
 lucem_status lucem_workspace_set_timing(lucem_workspace *ws, int32_t enable);
 lucem_status lucem_workspace_timings(lucem_workspace *ws, char *names, double *ms, int64_t *launches,
                                      int32_t cap, int32_t *n_out);
+/* Bounded device waits.  No counterpart in the reference (it has no device
+ * waits).  The TMA-staged plain 2-D blur (the fused kernel for launches of at
+ * least 12 tiles per SM) waits for each tile's tensor copy at most `ns`
+ * nanoseconds (default one second; 0: give up at once, for tests), then loads
+ * that tile directly: results are the same either way.  A CTA never exits
+ * with a copy still in flight into its shared memory (it waits for it, at
+ * most two seconds more).  lucem_workspace_wait_status synchronises `stream`,
+ * returns the number of waits that gave up since the last call in *gave_up
+ * and clears it; LUCEM_ERR_DEVICE_TIMEOUT when that number is not zero. */
+lucem_status lucem_workspace_set_wait_limit(lucem_workspace *ws, int64_t ns);
+lucem_status lucem_workspace_wait_status(lucem_workspace *ws, void *stream, int64_t *gave_up);
 /* Parses a pad-mode name with the reference's aliases
  * (crates/lucem-ops/src/core/pad.rs:46-56); LUCEM_ERR_UNKNOWN_PAD_MODE else. */
 lucem_status lucem_pad_mode_parse(const char *name, int32_t *mode_out);

@@ -80,6 +80,8 @@ SIGNATURES = {
     "lucem_workspace_destroy": (None, [P]),
     "lucem_workspace_capacity_bytes": (C.c_size_t, [P]),
     "lucem_workspace_set_timing": (I32, [P, I32]),
+    "lucem_workspace_set_wait_limit": (I32, [P, I64]),
+    "lucem_workspace_wait_status": (I32, [P, P, I64P]),
     "lucem_workspace_timings": (I32, [P, C.c_char_p, DP, I64P, I32, C.POINTER(I32)]),
     "lucem_pad_mode_parse": (I32, [C.c_char_p, C.POINTER(I32)]),
     "lucem_gaussian_kernel_1d": (I32, [D, C.c_uint32, I64, DP]),

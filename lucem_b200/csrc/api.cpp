@@ -333,6 +333,7 @@ struct lucem_workspace {
     std::map<std::string, Slot> slots;
     std::unique_ptr<EventTimer> timer;  // set while timing is enabled
     PassTimer *t() { return timer.get(); }
+    int64_t wait_limit_ns = -1;         // bounded device waits: -1 the default (one second)
     // crates/lucem-core/src/memory/workspace.rs:28-37: grow-only, budget checked.
     lucem_status get(const char *name, size_t bytes, void **out, Slot **slot_out = nullptr) {
         Slot &s = slots[name];
@@ -423,6 +424,31 @@ lucem_status lucem_workspace_set_timing(lucem_workspace *ws, int32_t enable) {
         ws->timer.reset();
     }
     return ok();
+}
+
+lucem_status lucem_workspace_set_wait_limit(lucem_workspace *ws, int64_t ns) {
+    if (!ws) return fail(LUCEM_ERR_INVALID_HANDLE, "null workspace");
+    if (ns < 0) return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `ns`: a wait limit cannot be negative");
+    ws->wait_limit_ns = ns;
+    return ok();
+}
+
+lucem_status lucem_workspace_wait_status(lucem_workspace *ws, void *stream, int64_t *gave_up) {
+    if (!ws || !gave_up) return fail(LUCEM_ERR_INVALID_HANDLE, "null workspace or output");
+    *gave_up = 0;
+    auto it = ws->slots.find("device_status");
+    if (it == ws->slots.end() || !it->second.ptr) return ok();
+    cudaStream_t cs = static_cast<cudaStream_t>(stream);
+    int32_t n = 0;
+    CUDA_TRY(cudaMemcpyAsync(&n, it->second.ptr, sizeof n, cudaMemcpyDeviceToHost, cs), "status read");
+    CUDA_TRY(cudaStreamSynchronize(cs), "status read");
+    if (n == 0) return ok();
+    CUDA_TRY(cudaMemsetAsync(it->second.ptr, 0, sizeof n, cs), "status reset");
+    CUDA_TRY(cudaStreamSynchronize(cs), "status reset");
+    *gave_up = n;
+    return fail(LUCEM_ERR_DEVICE_TIMEOUT,
+                "%d bounded device wait(s) gave up (tensor copies of the staged blur; those tiles were loaded "
+                "directly, results are unaffected)", (int)n);
 }
 
 lucem_status lucem_workspace_timings(lucem_workspace *ws, char *names, double *ms, int64_t *launches,
@@ -670,6 +696,23 @@ void init_fam(FamParams *fp, const lucem_tensor *in, int mode, double cval, doub
     fp->in_scale = (float)scale;
 }
 
+// The workspace's bounded-wait settings and give-up counter for a family
+// launch (a 64-byte "device_status" slot, zeroed when first allocated).
+lucem_status fam_waits(lucem_workspace *ws, FamParams *fp, void *stream) {
+    if (!ws) return ok();
+    void *p = nullptr;
+    Slot *sl = nullptr;
+    lucem_status st = ws->get("device_status", 64, &p, &sl);
+    if (st) return st;
+    if (sl->key.empty()) {
+        CUDA_TRY(cudaMemsetAsync(p, 0, 64, static_cast<cudaStream_t>(stream)), "status reset");
+        sl->key = "zeroed";
+    }
+    fp->wait_status = static_cast<int32_t *>(p);
+    fp->wait_ns = ws->wait_limit_ns < 0 ? 0 : (ws->wait_limit_ns == 0 ? -1 : ws->wait_limit_ns);
+    return ok();
+}
+
 // Executes a pass list from `in` into `out` (f32): the reference's
 // separable::run (crates/lucem-ops/src/core/separable.rs:20-61), with the
 // last two passes fused into one launch when they are the two innermost axes
@@ -735,6 +778,7 @@ lucem_status run_passes(lucem_ctx *ctx, const lucem_tensor *in, const std::vecto
         o.alpha = 1.0f;
         o.beta = 0.0f;
         o.bias = 0.0f;
+        if (lucem_status ws_st = fam_waits(ws, &fp, stream)) return ws_st;
         int e = timed(kPassFamily, stream, [&] { return launch_family_planes(fp, src_dtype, stream); });
         if (e) return cuda_fail(e, "gaussian family launch");
     }
@@ -1127,6 +1171,7 @@ lucem_status family_impl(lucem_ctx *ctx, const lucem_tensor *in, const lucem_res
             fp.outs[k].plane_stride = (int64_t)fp.H * fp.W;
             fp.outs[k].row_pitch = fp.W;
         }
+        if ((st = fam_waits(ws, &fp, stream))) return st;
         int e = timed(kPassFamily, stream, [&] { return launch_family_planes(fp, in->dtype, stream); });
         return e ? cuda_fail(e, "gaussian family launch") : ok();
     }

@@ -83,12 +83,17 @@ constexpr double sin2pi(long m, long L) {
     return q == 0 ? sp : (q == 1 ? cp : (q == 2 ? -sp : -cp));
 }
 
-// Complex add as one packed f32x2 instruction (sm_100; the same IEEE result
-// per component as two scalar adds).  Subtraction stays scalar: the packed
-// form needs the negated pair in extra registers and made the 128-register
-// transforms spill.
+// Complex add and subtract as one packed f32x2 instruction each (sm_100
+// add.f32x2 / sub.f32x2; the same IEEE result per component as two scalar
+// operations).  The subtraction is written in PTX (no CUDA intrinsic for it),
+// so it needs no negated copy of its operand.
 __device__ __forceinline__ float2 add(float2 a, float2 b) { return __fadd2_rn(a, b); }
-__device__ __forceinline__ float2 sub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 sub(float2 a, float2 b) {
+    float2 r;
+    asm("{\n .reg .b64 ra, rb, rd;\n mov.b64 ra, {%2, %3};\n mov.b64 rb, {%4, %5};\n sub.rn.f32x2 rd, ra, rb;\n mov.b64 {%0, %1}, rd;\n}"
+        : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return r;
+}
 __device__ __forceinline__ float2 mul(float2 a, float2 w) {
     return make_float2(fmaf(a.x, w.x, -a.y * w.y), fmaf(a.x, w.y, a.y * w.x));
 }

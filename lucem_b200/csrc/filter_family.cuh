@@ -521,23 +521,38 @@ int dispatch_batch_r(const FamParams &p, size_t smem, const FamImage *items, int
 // (pad maps) and any wait that gives up use the load path of family_tile.
 // No multicast: every copy reads this GPU's own input.
 
-// Times a CTA gave up waiting for a tensor copy and fell back to plain loads.
-__device__ int g_tma_fallbacks;
-
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-// Bounded wait on an mbarrier phase (about a second at most); uniform over
-// the block (all threads agree on the result).
-__device__ __forceinline__ bool mbar_wait_all(uint32_t mbar, uint32_t phase) {
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait on an mbarrier phase: polls until the phase completes or
+// `limit_ns` nanoseconds of %globaltimer have passed (limit_ns < 0: no
+// polling at all).  Uniform over the block: every thread returns the same
+// answer (true only if every thread saw the phase complete).
+__device__ __forceinline__ bool mbar_wait_all(uint32_t mbar, uint32_t phase, int64_t limit_ns) {
     bool done = false;
-    for (int i = 0; i < (1 << 20) && !done; ++i) {
-        uint32_t ok = 0;
-        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-                     : "=r"(ok) : "r"(mbar), "r"(phase) : "memory");
-        done = ok != 0;
+    if (limit_ns >= 0) {
+        const uint64_t t0 = global_ns();
+        for (;;) {
+            uint32_t ok = 0;
+            asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+                         : "=r"(ok) : "r"(mbar), "r"(phase) : "memory");
+            if (ok) {
+                done = true;
+                break;
+            }
+            if ((int64_t)(global_ns() - t0) >= limit_ns) break;
+        }
     }
     return __syncthreads_and(done) != 0;
 }
+
+constexpr int64_t kTmaWaitDefaultNs = 1000000000;  // one second
+constexpr int64_t kTmaDrainNs = 2000000000;        // before exit, for a copy given up on
 
 template <typename T, int RF>
 __global__ void __launch_bounds__(kThreads, 3)
@@ -584,8 +599,13 @@ family_planes_tma_kernel(const __grid_constant__ FamParams p, const __grid_const
                 : "memory");
         }
     };
+    const int64_t limit = p.wait_ns == 0 ? kTmaWaitDefaultNs : p.wait_ns;
     bool tma = true;
     uint32_t phase = 0;
+    // A copy given up on is still in flight into `raw`: its phase is waited
+    // for (with kTmaDrainNs) before the CTA exits.
+    bool lost = false;
+    uint32_t lost_phase = 0;
     int t = blockIdx.x;
     bool pending = false;
     if (t < total && interior(geom(t))) {
@@ -596,7 +616,7 @@ family_planes_tma_kernel(const __grid_constant__ FamParams p, const __grid_const
         const TileGeom g = geom(t);
         bool staged = false;
         if (pending) {
-            if (mbar_wait_all(mb, phase)) {
+            if (mbar_wait_all(mb, phase, limit)) {
                 const int n2 = AWP * AH / 2;
                 using V2 = typename Pair<T>::type;
                 const V2 *r2 = reinterpret_cast<const V2 *>(raw);
@@ -608,7 +628,9 @@ family_planes_tma_kernel(const __grid_constant__ FamParams p, const __grid_const
                 staged = true;
             } else {
                 tma = false;  // never reuse raw after a copy that did not arrive
-                if (threadIdx.x == 0) atomicAdd(&g_tma_fallbacks, 1);
+                lost = true;
+                lost_phase = phase;
+                if (threadIdx.x == 0 && p.wait_status) atomicAdd(p.wait_status, 1);
             }
             phase ^= 1u;
             __syncthreads();
@@ -620,6 +642,11 @@ family_planes_tma_kernel(const __grid_constant__ FamParams p, const __grid_const
         else family_tile<T, 1, RF, false>(p, g, A, IT);
         __syncthreads();
     }
+    // No CTA leaves with a tensor copy still writing into its shared memory:
+    // wait (bounded) for the one given up on; count it again if even that
+    // wait runs out.
+    if (lost && !mbar_wait_all(mb, lost_phase, kTmaDrainNs) && threadIdx.x == 0 && p.wait_status)
+        atomicAdd(p.wait_status, 1);
 }
 
 // Tensor map of the input planes for family_planes_tma_kernel, when every

@@ -66,6 +66,11 @@ struct FamParams {
     // zero padded from the filter's own radius to its kernel radius.
     float2_ taps0[kFamMaxFilters][kFamTapStride];
     float2_ taps1[kFamMaxFilters][kFamTapStride];
+    // Bounded waits of the TMA-staged blur: give up on a tensor copy after
+    // wait_ns nanoseconds (0: the default, one second; -1: at once, without
+    // polling), count each give-up in *wait_status (may be null).
+    int32_t *wait_status;
+    int64_t wait_ns;
 };
 
 // One tile of a batched walk: the read box of one channel and the owned box

@@ -365,7 +365,13 @@ __global__ void __launch_bounds__(N1 * R, 65536 / (N1 * R * 128)) row_fast_kerne
         float2 v[N2];
         if (kind != kRowInit && kind != kRowRealIn) {
             const float2 *s1 = pi.s1 + (int64_t)(ok ? row : 0) * p.Hp;
-            for (int k = t; k <= M; k += N1) spec[k] = ok ? s1[k] : make_float2(0.f, 0.f);
+            // Every load of the row's half spectrum issued before any store.
+#pragma unroll
+            for (int j = 0; j < N2; ++j) v[j] = ok ? s1[t + N1 * j] : make_float2(0.f, 0.f);
+            const float2 vm = (ok && t == 0) ? s1[M] : make_float2(0.f, 0.f);
+#pragma unroll
+            for (int j = 0; j < N2; ++j) spec[t + N1 * j] = v[j];
+            if (t == 0) spec[M] = vm;
             __syncthreads();
             // Z[k] = (X[k] + X*[M-k]) + i (X[k] - X*[M-k]) W_Px^{-k}
             for (int k = t; 2 * k <= M; k += N1) {

@@ -102,6 +102,26 @@ class Workspace:
         (restarts the totals)."""
         N.check(N.lib().lucem_workspace_set_timing(self.handle, int(bool(enable))))
 
+    def set_wait_limit(self, ns: int):
+        """Bounded device waits of this workspace's calls: give up on a tensor
+        copy after `ns` nanoseconds (0: at once; the default is one second)."""
+        N.check(N.lib().lucem_workspace_set_wait_limit(self.handle, int(ns)))
+
+    def wait_status(self, stream=None) -> int:
+        """Synchronises the stream and returns (and clears) the number of
+        device waits that gave up; raises LucemError DEVICE_TIMEOUT when it is
+        not zero, with the count in the exception's `gave_up`."""
+        st = stream if stream is not None else torch.cuda.current_stream()
+        n = C.c_int64()
+        rc = N.lib().lucem_workspace_wait_status(self.handle, C.c_void_p(st.cuda_stream), C.byref(n))
+        if rc != 0:
+            try:
+                N.check(rc)
+            except LucemError as e:
+                e.gave_up = n.value
+                raise
+        return n.value
+
     def timings(self) -> dict:
         """{kernel kind: (launches, total device ms)} since timing was enabled;
         synchronises on the recorded events."""

@@ -53,3 +53,28 @@ def test_tile_walk_persistent_equals_per_block_launches(dtype):
     torch.cuda.synchronize()
     for k, (u, v) in enumerate(zip(a, b)):
         assert torch.equal(u, v), f"response {k}"
+
+
+def test_wait_that_gives_up_falls_back_and_is_reported(oracle):
+    """With a wait limit of zero every tensor copy is given up on at once: the
+    tiles are loaded directly (same result), each CTA waits for its copy in
+    flight before it exits, and the workspace reports the give-ups as
+    DEVICE_TIMEOUT; with the default limit nothing is reported."""
+    rng = np.random.default_rng(31)
+    x = torch.from_numpy(rng.integers(0, 4000, (2560, 3072)).astype(np.uint16)).cuda()
+    ws = lb.Workspace()
+    want = lb.gaussian_blur(x, 2.0, workspace=ws)
+    assert ws.wait_status() == 0
+    ws.set_wait_limit(0)
+    got = lb.gaussian_blur(x, 2.0, workspace=ws)
+    with pytest.raises(lb.LucemError) as e:
+        ws.wait_status()
+    assert e.value.name == "DEVICE_TIMEOUT" and e.value.gave_up > 0
+    assert torch.equal(got, want)
+    assert ws.wait_status() == 0  # cleared by the read
+    ws.set_wait_limit(1_000_000_000)
+    again = lb.gaussian_blur(x, 2.0, workspace=ws)
+    assert ws.wait_status() == 0
+    assert torch.equal(again, want)
+    with pytest.raises(lb.LucemError):
+        ws.set_wait_limit(-1)
