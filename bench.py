@@ -426,7 +426,7 @@ def psf_fit_secondary(dev, steps=2):
         psf = sp / sp.sum()
         est = lb.autograd.richardson_lucy(obs, psf, num_iter=T, filter_epsilon=1e-6, checkpoint_every=K,
                                           workspace=ws)
-        reblur = torch.stack([lb.autograd.fft_convolve(est[b], psf) for b in range(B)])
+        reblur = lb.autograd.fft_convolve(est, psf)
         return ((reblur - obs) ** 2).mean()
 
     def step():

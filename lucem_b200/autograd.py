@@ -162,37 +162,20 @@ class _RichardsonLucy(torch.autograd.Function):
         psf = psf.contiguous()
         ctx.kw = kw
         ctx.save_for_backward(x, psf)
-        batched = x.dim() == psf.dim() + 1
-        ctx.batched = batched
-        f = lambda xi: ops.richardson_lucy(xi, psf, num_iter=kw["num_iter"], clip=False,
-                                           filter_epsilon=kw["filter_epsilon"], mode="constant",
-                                           grid=kw["grid"], workspace=kw["workspace"])
-        if batched:
-            return torch.stack([f(xi) for xi in x])
-        return f(x)
+        # A leading batch axis goes to the library as it is: one call, the
+        # volumes in the same launches.
+        return ops.richardson_lucy(x, psf, num_iter=kw["num_iter"], clip=False, filter_epsilon=kw["filter_epsilon"],
+                                   mode="constant", grid=kw["grid"], workspace=kw["workspace"])
 
     @staticmethod
     def backward(ctx, g):
         x, psf = ctx.saved_tensors
         kw = ctx.kw
         need_x, need_p = ctx.needs_input_grad[0], ctx.needs_input_grad[1]
-        g = g.contiguous()
-
-        def one(xi, gi):
-            return ops.richardson_lucy_backward(xi, psf, gi, num_iter=kw["num_iter"],
-                                                filter_epsilon=kw["filter_epsilon"], grid=kw["grid"],
-                                                checkpoint_every=kw["checkpoint_every"], need_psf=need_p,
-                                                need_input=need_x, workspace=kw["workspace"])
-
-        if ctx.batched:
-            gp_sum, gxs = None, []
-            for xi, gi in zip(x, g):
-                gp, gx = one(xi, gi)
-                if need_p:
-                    gp_sum = gp if gp_sum is None else gp_sum + gp
-                gxs.append(gx)
-            return (torch.stack(gxs) if need_x else None), gp_sum, None
-        gp, gx = one(x, g)
+        gp, gx = ops.richardson_lucy_backward(x, psf, g.contiguous(), num_iter=kw["num_iter"],
+                                              filter_epsilon=kw["filter_epsilon"], grid=kw["grid"],
+                                              checkpoint_every=kw["checkpoint_every"], need_psf=need_p,
+                                              need_input=need_x, workspace=kw["workspace"])
         return gx, gp, None
 
 

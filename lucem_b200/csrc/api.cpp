@@ -1799,10 +1799,14 @@ lucem_status rl_check(const lucem_tensor *in, const lucem_tensor *psf, const luc
         return st;
     if ((st = same_shape("input", in, "output", out))) return st;
     if ((st = not_aliased(in, out))) return st;
-    if (in->ndim != 2 && in->ndim != 3)
+    // A leading batch axis on the input (one more axis than the PSF): the
+    // images or volumes share the PSF.
+    const bool batched = in->ndim == psf->ndim + 1 && (psf->ndim == 2 || psf->ndim == 3);
+    const int nd = batched ? psf->ndim : in->ndim;
+    if (nd != 2 && nd != 3)
         return fail(LUCEM_ERR_INVALID_DIMENSION, "%s input expects 2 or 3-D array, got %d-D shape %s", what,
                     in->ndim, dims_str(in).c_str());
-    if (psf->ndim != in->ndim)
+    if (!batched && psf->ndim != in->ndim)
         return fail(LUCEM_ERR_INVALID_DIMENSION, "%s psf expects %d-D array, got %d-D shape %s", what, in->ndim,
                     psf->ndim, dims_str(psf).c_str());
     if (numel(psf) == 0) return fail(LUCEM_ERR_INVALID_WEIGHTS, "psf: PSF cannot be empty");
@@ -1839,12 +1843,14 @@ lucem_status rl_prepare(lucem_ctx *ctx, const lucem_tensor *in, const lucem_tens
                         const int64_t *grid_req, bool normalise, lucem_workspace *ws, void *stream, RlSetup *su) {
     lucem_status st;
     cudaStream_t cs = static_cast<cudaStream_t>(stream);
-    const int nd = in->ndim;
+    // in: [nb,] + the PSF's rank (rl_check); the nb volumes share the PSF.
+    const int nd = psf->ndim, boff = in->ndim - nd;
     int64_t dims[3] = {1, 1, 1};
     for (int d = 0; d < nd; ++d) {
-        dims[3 - nd + d] = in->dims[d];
+        dims[3 - nd + d] = in->dims[boff + d];
         su->kd[3 - nd + d] = psf->dims[d];
     }
+    const int64_t nb = boff ? in->dims[0] : 1;
     int64_t req[3] = {0, 0, 0};
     for (int d = 0; d < nd; ++d) req[3 - nd + d] = grid_req ? grid_req[d] : 0;
     if ((st = rl_grid_impl(dims + (3 - nd), su->kd + (3 - nd), nd, mode, req + (3 - nd), su->grid + (3 - nd),
@@ -1861,6 +1867,7 @@ lucem_status rl_prepare(lucem_ctx *ctx, const lucem_tensor *in, const lucem_tens
     g.Hx = g.Px / 2 + 1;
     g.Hp = (g.Hx + 15) & ~15;
     g.mode = mode;
+    g.nb = (int32_t)nb;
 
     const int64_t kn = numel(psf);
     su->kn = kn;
@@ -2044,8 +2051,8 @@ lucem_status rl_prepare(lucem_ctx *ctx, const lucem_tensor *in, const lucem_tens
     }
 
     void *s1 = nullptr, *s2 = nullptr;
-    if ((st = ws->get("rl_s1", (size_t)g.Z * g.Y * g.Hp * sizeof(float2_), &s1))) return st;
-    if (nd == 3 && (st = ws->get("rl_s2", (size_t)g.Z * g.Py * g.Hp * sizeof(float2_), &s2))) return st;
+    if ((st = ws->get("rl_s1", (size_t)nb * g.Z * g.Y * g.Hp * sizeof(float2_), &s1))) return st;
+    if (nd == 3 && (st = ws->get("rl_s2", (size_t)nb * g.Z * g.Py * g.Hp * sizeof(float2_), &s2))) return st;
     RlBuffers &b = su->b;
     b.s1 = s1;
     b.s2 = s2;
@@ -2068,7 +2075,10 @@ lucem_status rl_prepare(lucem_ctx *ctx, const lucem_tensor *in, const lucem_tens
 lucem_status rl_bwd_buffers(const RlSetup &su, int T, int K, bool full_rl, lucem_workspace *ws, RlBwdBuffers *w) {
     lucem_status st;
     const RlGeom &g = su.g;
-    const size_t vb = (size_t)g.Z * g.Y * g.X * sizeof(float);
+    // Volumes and per-volume spectra hold every volume of a batch; the
+    // accumulated cross-spectra (pbar) and the full-grid buffers one.
+    const size_t nb = g.nb > 1 ? (size_t)g.nb : 1;
+    const size_t vb = nb * g.Z * g.Y * g.X * sizeof(float);
     const size_t sb = (size_t)g.Pz * g.Py * g.Hp * sizeof(float2_);
     std::memset(w, 0, sizeof *w);
     void *p = nullptr;
@@ -2077,8 +2087,8 @@ lucem_status rl_bwd_buffers(const RlSetup &su, int T, int K, bool full_rl, lucem
         if (!s2) *dst = static_cast<float *>(p);
         return s2;
     };
-    auto spec = [&](const char *name, float2_ **dst) -> lucem_status {
-        lucem_status s2 = ws->get(name, sb, &p);
+    auto spec = [&](const char *name, float2_ **dst, size_t count = 1) -> lucem_status {
+        lucem_status s2 = ws->get(name, sb * count, &p);
         if (!s2) *dst = static_cast<float2_ *>(p);
         return s2;
     };
@@ -2089,12 +2099,12 @@ lucem_status rl_bwd_buffers(const RlSetup &su, int T, int K, bool full_rl, lucem
         float **dst[8] = {&w->c, &w->r, &w->a, &w->abar, &w->rbar, &w->cbar, &w->t, &w->ebar};
         for (int i = 0; i < 8; ++i)
             if ((st = vol(names[i], 1, dst[i]))) return st;
-        if ((st = spec("rlb_spec_r", &w->spec_r)) || (st = spec("rlb_spec_abar", &w->spec_abar))) return st;
+        if ((st = spec("rlb_spec_r", &w->spec_r, nb)) || (st = spec("rlb_spec_abar", &w->spec_abar, nb))) return st;
         if (!su.same_centre && (st = spec("rlb_pbar2", &w->pbar2))) return st;
     } else {
         if ((st = vol("rlb_c", 1, &w->c)) || (st = vol("rlb_t", 1, &w->t))) return st;
     }
-    if ((st = spec("rlb_spec_e", &w->spec_e)) || (st = spec("rlb_spec_cbar", &w->spec_cbar)) ||
+    if ((st = spec("rlb_spec_e", &w->spec_e, nb)) || (st = spec("rlb_spec_cbar", &w->spec_cbar, nb)) ||
         (st = spec("rlb_pbar1", &w->pbar1)))
         return st;
     const size_t fz = g.ndim == 3 ? (size_t)g.Pz : 1;
@@ -2281,7 +2291,7 @@ lucem_status lucem_fft_convolve(lucem_ctx *ctx, const lucem_tensor *x, const luc
     if (numel(x) == 0) return ok();
     int64_t req[3] = {0, 0, 0};
     if (grid)
-        for (int d = 0; d < x->ndim; ++d) req[d] = grid[d];
+        for (int d = 0; d < psf->ndim && d < 3; ++d) req[d] = grid[d];
     RlSetup su;
     if ((st = rl_prepare(ctx, x, psf, mode, req, false, ws, stream, &su))) return st;
     int e = rl_apply(su.g, su.b, su.b.h_conv, 0, static_cast<const float *>(x->data), static_cast<float *>(out->data),
@@ -2313,7 +2323,7 @@ lucem_status lucem_fft_convolve_backward(lucem_ctx *ctx, const lucem_tensor *x, 
     if (numel(x) == 0) return ok();
     int64_t req[3] = {0, 0, 0};
     if (grid)
-        for (int d = 0; d < x->ndim; ++d) req[d] = grid[d];
+        for (int d = 0; d < psf->ndim && d < 3; ++d) req[d] = grid[d];
     RlSetup su;
     if ((st = rl_prepare(ctx, x, psf, mode, req, false, ws, stream, &su))) return st;
     RlBwdBuffers w;

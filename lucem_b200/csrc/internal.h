@@ -200,6 +200,7 @@ struct RlGeom {
     int32_t Hx;              // Px/2 + 1
     int32_t Hp;              // spectrum row pitch (complex elements)
     int32_t mode;
+    int32_t nb;              // volumes sharing the PSF, stored one after another (0 or 1: one)
 };
 
 struct RlBuffers {

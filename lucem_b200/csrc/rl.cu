@@ -61,10 +61,11 @@ __global__ void __launch_bounds__(512, 1) col_pass_kernel(const __grid_constant_
             float2 val = make_float2(0.f, 0.f);
             if (col < q.ncols) {
                 int outer = col / q.Hx, kx = col - outer * q.Hx;
+                const ColOffsets off = col_offsets(p, q, outer);
                 int srow;
                 if (p.mode == kColInv) srow = row;
                 else srow = row < q.n_img + 2 * q.halo ? pad_index_rt(row - q.halo, q.n_img, p.pad_mode) : -1;
-                if (srow >= 0) val = q.src[outer * q.src_outer + srow * q.src_row + kx];
+                if (srow >= 0) val = q.src[off.src + srow * q.src_row + kx];
             }
             bufA[row * CP + c] = val;
         }
@@ -76,8 +77,9 @@ __global__ void __launch_bounds__(512, 1) col_pass_kernel(const __grid_constant_
                 int col = c0 + c;
                 if (col < q.ncols) {
                     int outer = col / q.Hx, kx = col - outer * q.Hx;
-                    if (q.spec_out) q.spec_out[outer * q.h_outer + row * p.spec_row + kx] = buf[row * CP + c];
-                    float2 h = q.H ? q.H[outer * q.h_outer + row * q.h_row + kx] : make_float2(1.f, 0.f);
+                    const ColOffsets off = col_offsets(p, q, outer);
+                    if (q.spec_out) q.spec_out[off.spec + row * p.spec_row + kx] = buf[row * CP + c];
+                    float2 h = q.H ? q.H[off.h + row * q.h_row + kx] : make_float2(1.f, 0.f);
                     if (p.Hrow) h = cmul(h, p.Hrow[row]);
                     if (p.conj_h) h.y = -h.y;
                     buf[row * CP + c] = cmul(buf[row * CP + c], h);
@@ -93,7 +95,7 @@ __global__ void __launch_bounds__(512, 1) col_pass_kernel(const __grid_constant_
             int col = c0 + c;
             if (col < q.ncols) {
                 int outer = col / q.Hx, kx = col - outer * q.Hx;
-                q.dst[outer * q.dst_outer + row * q.dst_row + kx] = buf[(r0 + row) * CP + c];
+                q.dst[col_offsets(p, q, outer).dst + row * q.dst_row + kx] = buf[(r0 + row) * CP + c];
             }
         }
         __syncthreads();
@@ -426,11 +428,13 @@ struct RlRunner {
     PassTimer *timer;
     RowPass rp{};
     FftPlan py_plan{}, pz_plan{};
+    int nb = 1;  // volumes sharing the PSF (RlGeom::nb)
     bool ok = true;
 
     RlRunner(const RlGeom &g_, const RlBuffers &b_, void *stream_, PassTimer *timer_)
         : g(g_), b(b_), s(static_cast<cudaStream_t>(stream_)), stream(stream_), timer(timer_) {
-        rp.nrows = g.Z * g.Y;
+        nb = g.nb > 1 ? g.nb : 1;
+        rp.nrows = nb * g.Z * g.Y;
         rp.X = g.X;
         rp.Px = g.Px;
         rp.M = g.Px / 2;
@@ -472,7 +476,7 @@ struct RlRunner {
 
     ColPass y_forward(float2 *dst, int64_t dst_outer) const {
         ColPass c{};
-        c.ncols = g.Z * g.Hx; c.Hx = g.Hx;
+        c.ncols = nb * g.Z * g.Hx; c.Hx = g.Hx;
         c.src = static_cast<const float2 *>(b.s1); c.src_outer = (int64_t)g.Y * g.Hp; c.src_row = g.Hp;
         c.n_img = g.Y; c.halo = g.hy;
         c.dst = dst; c.dst_outer = dst_outer; c.dst_row = g.Hp;
@@ -483,7 +487,7 @@ struct RlRunner {
 
     ColPass y_inverse(const float2 *src, int64_t src_outer) const {
         ColPass c{};
-        c.ncols = g.Z * g.Hx; c.Hx = g.Hx;
+        c.ncols = nb * g.Z * g.Hx; c.Hx = g.Hx;
         c.src = src; c.src_outer = src_outer; c.src_row = g.Hp;
         c.n_img = g.Py; c.halo = 0;
         c.dst = static_cast<float2 *>(b.s1); c.dst_outer = (int64_t)g.Y * g.Hp; c.dst_row = g.Hp;
@@ -506,10 +510,13 @@ struct RlRunner {
             H == b.h_conv ? b.hrow_conv : (H == b.h_corr ? b.hrow_corr : nullptr));
         if (g.ndim == 2) {
             ColPass c{};
-            c.ncols = g.Hx; c.Hx = g.Hx;
+            c.ncols = nb * g.Hx; c.Hx = g.Hx;
             c.src = s1; c.src_outer = 0; c.src_row = g.Hp;
             c.n_img = g.Y; c.halo = g.hy;
             c.dst = s1; c.dst_outer = 0; c.dst_row = g.Hp;
+            // One column block per image: image v at v * Y * Hp, its spectrum
+            // at v * Py * Hp.
+            c.bdiv = 1; c.src_b = c.dst_b = (int64_t)g.Y * g.Hp; c.spec_b = (int64_t)g.Py * g.Hp;
             c.store_begin = g.hy; c.store_count = g.Y;
             c.mode = kColFull; c.pad_mode = g.mode;
             c.H = static_cast<const float2 *>(H); c.h_outer = 0; c.h_row = Hrow ? 0 : g.Hp; c.conj_h = conj;
@@ -529,7 +536,7 @@ struct RlRunner {
             const void *fy = H == b.h_conv ? b.hy_conv : b.hy_corr;
             const void *fx = H == b.h_conv ? b.hx_conv : b.hx_corr;
             ColPass yc{};
-            yc.ncols = g.Z * g.Hx; yc.Hx = g.Hx;
+            yc.ncols = nb * g.Z * g.Hx; yc.Hx = g.Hx;
             yc.src = s1; yc.src_outer = (int64_t)g.Y * g.Hp; yc.src_row = g.Hp;
             yc.n_img = g.Y; yc.halo = g.hy;
             yc.dst = s1; yc.dst_outer = (int64_t)g.Y * g.Hp; yc.dst_row = g.Hp;
@@ -540,10 +547,11 @@ struct RlRunner {
             yc.plan = py_plan; yc.tw = reinterpret_cast<const float2 *>(b.tw_y);
             if ((e = col(yc, kPassRlColY))) return e;
             ColPass zc{};
-            zc.ncols = g.Y * g.Hx; zc.Hx = g.Hx;
+            zc.ncols = nb * g.Y * g.Hx; zc.Hx = g.Hx;
             zc.src = s1; zc.src_outer = g.Hp; zc.src_row = (int64_t)g.Y * g.Hp;
             zc.n_img = g.Z; zc.halo = g.hz;
             zc.dst = s1; zc.dst_outer = g.Hp; zc.dst_row = (int64_t)g.Y * g.Hp;
+            zc.bdiv = g.Y; zc.src_b = zc.dst_b = (int64_t)g.Z * g.Y * g.Hp;
             zc.store_begin = g.hz; zc.store_count = g.Z;
             zc.mode = kColFull; zc.pad_mode = g.mode;
             zc.H = nullptr; zc.h_outer = 0; zc.h_row = 0; zc.conj_h = conj;
@@ -553,10 +561,11 @@ struct RlRunner {
         }
         if ((e = col(y_forward(s2, (int64_t)g.Py * g.Hp)))) return e;
         ColPass zp{};
-        zp.ncols = g.Py * g.Hx; zp.Hx = g.Hx;
+        zp.ncols = nb * g.Py * g.Hx; zp.Hx = g.Hx;
         zp.src = s2; zp.src_outer = g.Hp; zp.src_row = (int64_t)g.Py * g.Hp;
         zp.n_img = g.Z; zp.halo = g.hz;
         zp.dst = s2; zp.dst_outer = g.Hp; zp.dst_row = (int64_t)g.Py * g.Hp;
+        zp.bdiv = g.Py; zp.src_b = zp.dst_b = (int64_t)g.Z * g.Py * g.Hp; zp.spec_b = (int64_t)g.Pz * g.Py * g.Hp;
         zp.store_begin = g.hz; zp.store_count = g.Z;
         zp.mode = kColFull; zp.pad_mode = g.mode;
         zp.H = static_cast<const float2 *>(H); zp.h_outer = g.Hp; zp.h_row = Hrow ? 0 : (int64_t)g.Py * g.Hp;
@@ -618,18 +627,22 @@ struct RlRunner {
 
 // ---- elementwise kernels of the backward pass --------------------------
 
-// acc += x * conj(y) (+ u * conj(v) when u is given), over n complex values.
+// acc += sum over nb volumes of x * conj(y) (+ u * conj(v) when u is given),
+// over n complex values per volume (volumes n apart; volumes in order).
 __global__ void spec_mac_kernel(float2 *__restrict__ acc, const float2 *__restrict__ x, const float2 *__restrict__ y,
-                                const float2 *__restrict__ u, const float2 *__restrict__ v, int64_t n) {
+                                const float2 *__restrict__ u, const float2 *__restrict__ v, int64_t n, int nb) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         float2 a = acc[i];
-        const float2 p = x[i], q = y[i];
-        a.x += p.x * q.x + p.y * q.y;
-        a.y += p.y * q.x - p.x * q.y;
-        if (u) {
-            const float2 s = u[i], t = v[i];
-            a.x += s.x * t.x + s.y * t.y;
-            a.y += s.y * t.x - s.x * t.y;
+        for (int b = 0; b < nb; ++b) {
+            const int64_t j = i + b * n;
+            const float2 p = x[j], q = y[j];
+            a.x += p.x * q.x + p.y * q.y;
+            a.y += p.y * q.x - p.x * q.y;
+            if (u) {
+                const float2 s = u[j], t = v[j];
+                a.x += s.x * t.x + s.y * t.y;
+                a.y += s.y * t.x - s.x * t.y;
+            }
         }
         acc[i] = a;
     }
@@ -655,6 +668,7 @@ int ew_grid_rl(int64_t n) {
 // accumulated cross-spectrum back to lags.
 RlGeom full_geom(const RlGeom &g) {
     RlGeom gf = g;
+    gf.nb = 1;
     gf.Z = g.ndim == 3 ? g.Pz : 1;
     gf.Y = g.Py;
     gf.X = g.Px;
@@ -811,7 +825,10 @@ int rl_backward(const RlGeom &g, const RlBuffers &b, const RlBwdBuffers &w, cons
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     RlRunner run(g, b, stream, timer);
     if (!run.ok) return (int)cudaErrorInvalidValue;
-    const int64_t V = (int64_t)g.Z * g.Y * g.X;
+    // V: every volume of the batch (the state arrays hold nb volumes each);
+    // nspec: one volume's spectrum (the cross-spectra are summed over volumes).
+    const int nb = g.nb > 1 ? g.nb : 1;
+    const int64_t V = (int64_t)nb * g.Z * g.Y * g.X;
     const size_t vb = (size_t)V * sizeof(float);
     const int64_t nspec = (int64_t)g.Pz * g.Py * g.Hp;
     const int sg = ew_grid_rl(nspec);
@@ -858,10 +875,10 @@ int rl_backward(const RlGeom &g, const RlBuffers &b, const RlBwdBuffers &w, cons
             if ((e = run.pair(b.h_conv, 1, spec_cbar))) return e;
             if ((e = run.row(kRowEbar, nullptr, nullptr, 0, 0, 0, eps, w.a, w.ebar))) return e;
             if (pbar2) {
-                spec_mac_kernel<<<sg, 256, 0, s>>>(pbar1, spec_cbar, spec_e, nullptr, nullptr, nspec);
-                spec_mac_kernel<<<sg, 256, 0, s>>>(pbar2, spec_r, spec_abar, nullptr, nullptr, nspec);
+                spec_mac_kernel<<<sg, 256, 0, s>>>(pbar1, spec_cbar, spec_e, nullptr, nullptr, nspec, nb);
+                spec_mac_kernel<<<sg, 256, 0, s>>>(pbar2, spec_r, spec_abar, nullptr, nullptr, nspec, nb);
             } else {
-                spec_mac_kernel<<<sg, 256, 0, s>>>(pbar1, spec_cbar, spec_e, spec_r, spec_abar, nspec);
+                spec_mac_kernel<<<sg, 256, 0, s>>>(pbar1, spec_cbar, spec_e, spec_r, spec_abar, nspec, nb);
             }
             if ((e = (int)cudaGetLastError())) return e;
         }
@@ -902,7 +919,8 @@ int rl_convolve_backward(const RlGeom &g, const RlBuffers &b, const RlBwdBuffers
     if ((e = run.apply(b.h_conv, 0, x, w.c, spec_x))) return e;
     const int64_t nspec = (int64_t)g.Pz * g.Py * g.Hp;
     if ((e = (int)cudaMemsetAsync(pbar, 0, nspec * sizeof(float2), s))) return e;
-    spec_mac_kernel<<<ew_grid_rl(nspec), 256, 0, s>>>(pbar, spec_g, spec_x, nullptr, nullptr, nspec);
+    spec_mac_kernel<<<ew_grid_rl(nspec), 256, 0, s>>>(pbar, spec_g, spec_x, nullptr, nullptr, nspec,
+                                                      g.nb > 1 ? g.nb : 1);
     const RlGeom gf = full_geom(g);
     RlBuffers bf = b;
     bf.s1 = w.full_s1;

@@ -72,6 +72,12 @@ struct ColPass {
     FftPlan plan;
     const float2 *tw;             // e^{-2 pi i m / n}, m < n
     int32_t C, CP;
+    // Volumes sharing one transfer function (bdiv > 0): outer index o splits
+    // into volume v = o / bdiv and o' = o % bdiv; src, dst and spec_out are
+    // offset by v times src_b, dst_b, spec_b and o' takes the place of o.
+    // bdiv == 0: one volume.
+    int32_t bdiv;
+    int64_t src_b, dst_b, spec_b;
     // Batch mode (items != null): the launch covers several problems of the
     // same transform length; tile t belongs to the last item whose
     // tile_begin <= t, and that item's fields replace the ones above.
@@ -113,6 +119,25 @@ __device__ __forceinline__ int find_item(const Item *items, int n, int t) {
     return lo;
 }
 
+// Element offsets of column `outer` (before kx and the row term): source,
+// destination, transfer function and spectrum output.
+struct ColOffsets {
+    int64_t src, dst, h, spec;
+};
+__device__ __forceinline__ ColOffsets col_offsets(const ColPass &p, const ColItem &q, int outer) {
+    int v = 0, o = outer;
+    if (p.bdiv > 0) {
+        v = outer / p.bdiv;
+        o = outer - v * p.bdiv;
+    }
+    ColOffsets r;
+    r.src = v * p.src_b + o * q.src_outer;
+    r.dst = v * p.dst_b + o * q.dst_outer;
+    r.h = o * q.h_outer;
+    r.spec = v * p.spec_b + o * q.h_outer;
+    return r;
+}
+
 // The problem and local tile of global tile t.
 __device__ __forceinline__ ColItem col_tile(const ColPass &p, int t, int *local) {
     if (p.items == nullptr) {
@@ -146,7 +171,7 @@ __device__ __forceinline__ void col_load_input(const ColPass &p, int gt, int t, 
         outer = col / q.Hx;
         kx = col - outer * q.Hx;
     }
-    const float2 *src = q.src + (outer * q.src_outer + kx);
+    const float2 *src = q.src + (col_offsets(p, q, outer).src + kx);
     const int n_ext = q.n_img + 2 * q.halo, src_row = (int)q.src_row;
 #pragma unroll
     for (int i = 0; i < N2; ++i) {
@@ -193,14 +218,15 @@ __global__ void __launch_bounds__(N1 * C, (N2 > 32 ? 1 : 65536 / (N1 * C * 128))
             outer = col / q.Hx;
             kx = col - outer * q.Hx;
         }
-        const float2 *src = q.src + (outer * q.src_outer + kx);
+        const ColOffsets off = col_offsets(p, q, outer);
+        const float2 *src = q.src + (off.src + kx);
         float2 v[N2];
         if (MODE == kColInv) {
 #pragma unroll
             for (int j = 0; j < N2; ++j) v[j] = ok ? src[F::freq(t, j) * src_row] : make_float2(0.f, 0.f);
             F::template inverse<kLoOnly>(v, t, c, xb, ti);
         } else {
-            const float2 *h = q.H + (outer * q.h_outer + kx);
+            const float2 *h = q.H + (off.h + kx);
             // Short transforms prefetch the transfer function with the data
             // (one memory round trip per tile instead of two).
             constexpr bool kPrefetchH = N2 <= 16;
@@ -230,12 +256,12 @@ __global__ void __launch_bounds__(N1 * C, (N2 > 32 ? 1 : 65536 / (N1 * C * 128))
             }
             F::template forward<kZeroHi>(v, t, c, xb, tf);
             if (MODE == kColFull && q.spec_out != nullptr && ok) {
-                float2 *so = q.spec_out + (outer * q.h_outer + kx);
+                float2 *so = q.spec_out + (off.spec + kx);
 #pragma unroll
                 for (int j = 0; j < N2; ++j) so[F::freq(t, j) * (int)p.spec_row] = v[j];
             }
             if (MODE == kColFwd) {
-                float2 *dst = q.dst + (outer * q.dst_outer + kx);
+                float2 *dst = q.dst + (off.dst + kx);
                 if (ok) {
 #pragma unroll
                     for (int j = 0; j < N2; ++j) dst[F::freq(t, j) * dst_row] = v[j];
@@ -263,7 +289,7 @@ __global__ void __launch_bounds__(N1 * C, (N2 > 32 ? 1 : 65536 / (N1 * C * 128))
                 }
             }
         }
-        float2 *dst = q.dst + (outer * q.dst_outer + kx);
+        float2 *dst = q.dst + (off.dst + kx);
         if (ok) {
 #pragma unroll
             for (int i = 0; i < N2; ++i) {

@@ -573,7 +573,9 @@ def richardson_lucy(x: torch.Tensor, psf: torch.Tensor, *, num_iter: int = 30, c
                     filter_epsilon: Optional[float] = None, mode="reflect", grid=None,
                     out: Optional[torch.Tensor] = None, workspace: Optional[Workspace] = None) -> torch.Tensor:
     """richardson_lucy (crates/lucem-ops/src/restore/deconvolve.rs:45-162) for
-    2-D and 3-D inputs, on FFT convolution.  `grid` overrides the FFT lengths."""
+    2-D and 3-D inputs, on FFT convolution.  `grid` overrides the FFT lengths.
+    `x` may carry one leading batch axis (one axis more than `psf`): the
+    images or volumes share the PSF and run in the same launches."""
     ctx, ws = _ctx_ws(x, workspace)
     out = _out_like(x, out)
     s = _rl_settings(num_iter, clip, filter_epsilon, mode, grid)
@@ -590,7 +592,8 @@ def richardson_lucy_backward(x: torch.Tensor, psf: torch.Tensor, grad_out: torch
     """(d loss / d psf, d loss / d x) of richardson_lucy(x, psf, clip=False,
     mode="constant", ...) given d loss / d (its output); either is None when
     not asked for.  The iterations are recomputed from checkpoints kept every
-    `checkpoint_every` iterations.  No counterpart in the reference."""
+    `checkpoint_every` iterations.  With a leading batch axis on `x` the PSF
+    gradient is summed over the batch.  No counterpart in the reference."""
     ctx, ws = _ctx_ws(x, workspace)
     s = _rl_settings(num_iter, False, filter_epsilon, "constant", grid)
     gp = torch.empty(psf.shape, dtype=torch.float32, device=x.device) if need_psf else None
@@ -607,7 +610,8 @@ def fft_convolve(x: torch.Tensor, psf: torch.Tensor, *, grid=None, out: Optional
                  workspace: Optional[Workspace] = None) -> torch.Tensor:
     """The forward model of richardson_lucy (deconvolve.rs:120, correlation
     with the flipped PSF): convolution centred at k-1-k//2 per axis, zero
-    padding, the PSF as given, on the FFT grid."""
+    padding, the PSF as given, on the FFT grid.  `x` may carry one leading
+    batch axis (one PSF for the batch)."""
     ctx, ws = _ctx_ws(x, workspace)
     out = _out_like(x, out)
     ti, tp, to = _tensor(x, "x"), _tensor(psf, "psf"), _tensor(out, "output")

@@ -331,3 +331,23 @@ def test_rl_gradients_against_the_fp64_reverse_oracle(oracle, shape, kshape, T, 
     wp, wx = oracle.richardson_lucy_backward_fft64(obs, psf, w, num_iter=T, filter_epsilon=1e-6)
     oracle.assert_close(host(gp), wp, FD_RTOL, "psf gradient")
     oracle.assert_close(host(gx), wx, FD_RTOL, "observation gradient")
+
+
+@pytest.mark.parametrize("gauss", [False, True])
+def test_batched_rl_backward_sums_the_psf_gradient(gauss):
+    """One call over a batch of volumes (one PSF): the observation gradients
+    equal the single-volume calls' bit for bit, the PSF gradient is their sum
+    (1e-5: the batch is summed inside the cross-spectrum accumulation)."""
+    rng = np.random.default_rng(41 + gauss)
+    obs = rng.uniform(0.5, 2.0, (3, 8, 20, 18)).astype(np.float32)
+    kshape = (3, 5, 5)
+    psf = (lb.synth.gaussian_psf(kshape, (1.0, 1.3, 1.1)) if gauss else rng.uniform(0.2, 1.0, kshape)).astype(np.float32)
+    w = rng.standard_normal(obs.shape).astype(np.float32)
+    kw = dict(num_iter=6, filter_epsilon=1e-6, checkpoint_every=2)
+    gp, gx = lb.richardson_lucy_backward(dev(obs), dev(psf), dev(w), **kw)
+    gp_sum = np.zeros(kshape)
+    for b in range(obs.shape[0]):
+        gpb, gxb = lb.richardson_lucy_backward(dev(obs[b]), dev(psf), dev(w[b]), **kw)
+        np.testing.assert_array_equal(host(gx)[b], host(gxb))
+        gp_sum += host(gpb)
+    np.testing.assert_allclose(host(gp), gp_sum, rtol=1e-5, atol=1e-5 * np.abs(gp_sum).max())
