@@ -380,6 +380,48 @@ lucem_status lucem_graph_end(void *stream, lucem_graph **out);
 lucem_status lucem_graph_launch(lucem_graph *graph, void *stream);
 void lucem_graph_destroy(lucem_graph *graph);
 
+/* ---- spectral operators -------------------------------------------- */
+
+/* crates/lucem-ops/src/core/fft.rs:55-100 fft_nd_into: N-D forward
+ * (inverse = 0, unnormalised) or inverse (inverse scaled by 1/len per axis)
+ * DFT over every axis of a split complex f32 array (re_in, im_in) into
+ * (re_out, im_out), axes in order, ping/pong through the workspace.  The
+ * reference evaluates each axis as a direct O(len^2) DFT (dft_axis_kernel,
+ * core/kernels/fft.rs:9-47); here: shared-memory Stockham transforms for
+ * 2,3,5,7-smooth lengths up to 8192, four-step beyond, Bluestein for other
+ * lengths up to 4096, a direct DFT above that.  0-D or empty arrays are
+ * copied. */
+lucem_status lucem_fft_nd(lucem_ctx *ctx, const lucem_tensor *re_in, const lucem_tensor *im_in,
+                          lucem_tensor *re_out, lucem_tensor *im_out, int32_t inverse, lucem_workspace *ws,
+                          void *stream);
+/* crates/lucem-ops/src/core/fft.rs:14-53 fft_1d_into: the same along one
+ * axis (negative axes count from the end).  The workspace may be NULL except
+ * for smooth lengths above 8192 (four-step scratch). */
+lucem_status lucem_fft_1d(lucem_ctx *ctx, const lucem_tensor *re_in, const lucem_tensor *im_in,
+                          lucem_tensor *re_out, lucem_tensor *im_out, int32_t axis, int32_t inverse,
+                          lucem_workspace *ws, void *stream);
+/* crates/lucem-ops/src/core/fft.rs:104-138 complex_mul_into: out = a * b, or
+ * a * conj(b) when conj_b, split complex f32. */
+lucem_status lucem_complex_mul(const lucem_tensor *a_re, const lucem_tensor *a_im, const lucem_tensor *b_re,
+                               const lucem_tensor *b_im, lucem_tensor *out_re, lucem_tensor *out_im, int32_t conj_b,
+                               void *stream);
+
+/* crates/lucem-ops/src/restore/deconvolve.rs:163-183 WienerDeconvolve. */
+typedef struct lucem_wiener_settings {
+    double balance;            /* 0.1; regularisation weight, finite and >= 0 */
+    int32_t clip;              /* 1: clamp the result to [-1, 1] */
+} lucem_wiener_settings;
+void lucem_wiener_settings_default(lucem_wiener_settings *s);
+/* crates/lucem-ops/src/restore/deconvolve.rs:210-295 wiener_deconvolve_into:
+ * X = conj(H) Y / max(|H|^2 + balance |L|^2, 1e-12) with Y the FFT of the
+ * 2-D f32 input, H that of the PSF centred at (kh/2, kw/2) on the image grid
+ * (circular), L that of the discrete Laplacian; out = Re(IFFT(X)), clipped
+ * when asked.  Same checks and error kinds as the reference; every FFT is
+ * lucem_fft_nd's. */
+lucem_status lucem_wiener_deconvolve(lucem_ctx *ctx, const lucem_tensor *in, const lucem_tensor *psf,
+                                     const lucem_wiener_settings *settings, lucem_tensor *out, lucem_workspace *ws,
+                                     void *stream);
+
 /* The grid lucem_richardson_lucy uses (host only), before any autotuning of
  * the context: per axis the requested length, or the cheapest m * 2^k
  * (m in {1,3,5,7,9,15,21,25,27}) at least the padding's need, by length

@@ -62,6 +62,10 @@ class RlSettings(C.Structure):
                 ("filter_epsilon", C.c_double), ("mode", C.c_int32), ("grid", C.c_int64 * 3)]
 
 
+class WienerSettings(C.Structure):
+    _fields_ = [("balance", C.c_double), ("clip", C.c_int32)]
+
+
 # name -> (restype, argtypes); every function include/lucem_b200.h declares.
 P = C.c_void_p
 PP = C.POINTER(C.c_void_p)
@@ -81,6 +85,11 @@ SIGNATURES = {
     "lucem_workspace_capacity_bytes": (C.c_size_t, [P]),
     "lucem_workspace_set_timing": (I32, [P, I32]),
     "lucem_workspace_set_wait_limit": (I32, [P, I64]),
+    "lucem_fft_nd": (I32, [P, TP, TP, TP, TP, I32, P, P]),
+    "lucem_fft_1d": (I32, [P, TP, TP, TP, TP, I32, I32, P, P]),
+    "lucem_complex_mul": (I32, [TP, TP, TP, TP, TP, TP, I32, P]),
+    "lucem_wiener_settings_default": (None, [C.POINTER(WienerSettings)]),
+    "lucem_wiener_deconvolve": (I32, [P, TP, TP, C.POINTER(WienerSettings), TP, P, P]),
     "lucem_workspace_wait_status": (I32, [P, P, I64P]),
     "lucem_workspace_timings": (I32, [P, C.c_char_p, DP, I64P, I32, C.POINTER(I32)]),
     "lucem_pad_mode_parse": (I32, [C.c_char_p, C.POINTER(I32)]),

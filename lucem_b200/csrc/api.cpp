@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <complex>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -211,7 +212,7 @@ namespace lucem {
 const char *pass_name(int kind) {
     static const char *names[kPassCount] = {"rl_row_pass", "rl_col_forward", "rl_col_full", "rl_col_inverse",
                                             "rl_transfer_function", "gaussian_family", "correlate_1d",
-                                            "elementwise", "rl_col_y", "rl_col_z"};
+                                            "elementwise", "rl_col_y", "rl_col_z", "fft"};
     return kind >= 0 && kind < kPassCount ? names[kind] : "?";
 }
 }  // namespace lucem
@@ -2638,6 +2639,433 @@ void lucem_graph_destroy(lucem_graph *graph) {
     cudaGraphExecDestroy(graph->exec);
     cudaGraphDestroy(graph->graph);
     delete graph;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// The general complex FFT (crates/lucem-ops/src/core/fft.rs:14-100) and the
+// spectral operators on it.
+
+namespace {
+
+using cd = std::complex<double>;
+
+// Forward DFT of a 2,3,5,7-smooth length in FP64 (recursive decimation in
+// time on the smallest factor; host tables only).
+void host_fft64(std::vector<cd> &a) {
+    const size_t n = a.size();
+    if (n <= 1) return;
+    size_t p = 0;
+    for (size_t f : {2, 3, 5, 7})
+        if (n % f == 0) {
+            p = f;
+            break;
+        }
+    const size_t m = n / p;
+    std::vector<std::vector<cd>> sub(p, std::vector<cd>(m));
+    for (size_t r = 0; r < p; ++r)
+        for (size_t j = 0; j < m; ++j) sub[r][j] = a[j * p + r];
+    for (auto &v : sub) host_fft64(v);
+    for (size_t k = 0; k < n; ++k) {
+        cd acc = 0.0;
+        for (size_t r = 0; r < p; ++r) {
+            const size_t q = (r * k) % n;
+            const double ang = -2.0 * M_PI * (double)q / (double)n;
+            acc += sub[r][k % m] * cd(std::cos(ang), std::sin(ang));
+        }
+        a[k] = acc;
+    }
+}
+
+// Bluestein tables of length len on a smooth M >= 2 len - 1 (device, cached
+// in the context): the chirp c[k] = e^{-i pi k^2 / len} (exact phase
+// k^2 mod 2 len) and the spectrum of the conjugate chirp filter divided by M.
+lucem_status bluestein_tables(lucem_ctx *ctx, int64_t len, int64_t M, const float2_ **chirp, const float2_ **filt) {
+    std::string kc = "bluestein-chirp-" + std::to_string(len);
+    std::string kf = "bluestein-filter-" + std::to_string(len) + "-" + std::to_string(M);
+    std::vector<float> c((size_t)(2 * len));
+    std::vector<cd> b((size_t)M, cd(0.0, 0.0));
+    for (int64_t k = 0; k < len; ++k) {
+        const int64_t q = (k * k) % (2 * len);
+        const double ang = M_PI * (double)q / (double)len;
+        c[(size_t)(2 * k)] = (float)std::cos(ang);
+        c[(size_t)(2 * k + 1)] = (float)-std::sin(ang);
+        const cd conjc(std::cos(ang), std::sin(ang));
+        b[(size_t)k] = conjc;
+        if (k > 0) b[(size_t)(M - k)] = conjc;
+    }
+    int err = 0;
+    void *pc = ctx->get_or_upload(kc, c.data(), c.size() * sizeof(float), &err);
+    if (!pc) return cuda_fail(err, "chirp upload");
+    void *pf = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        auto it = ctx->cache.find(kf);
+        if (it != ctx->cache.end()) pf = it->second;
+    }
+    if (!pf) {
+        host_fft64(b);
+        std::vector<float> f((size_t)(2 * M));
+        for (int64_t k = 0; k < M; ++k) {
+            f[(size_t)(2 * k)] = (float)(b[(size_t)k].real() / (double)M);
+            f[(size_t)(2 * k + 1)] = (float)(b[(size_t)k].imag() / (double)M);
+        }
+        pf = ctx->get_or_upload(kf, f.data(), f.size() * sizeof(float), &err);
+        if (!pf) return cuda_fail(err, "chirp filter upload");
+    }
+    *chirp = static_cast<const float2_ *>(pc);
+    *filt = static_cast<const float2_ *>(pf);
+    return ok();
+}
+
+// One side of an axis pass: split (re, im) or interleaved (c).
+struct FftSide {
+    const float *re = nullptr;
+    const float *im = nullptr;
+    float2_ *c = nullptr;
+    float *wre = nullptr, *wim = nullptr;  // destination split
+};
+
+// Largest smooth divisor n1 <= kFftLinesMax of n with n / n1 <= kFftLinesMax.
+int64_t four_step_split(int64_t n) {
+    int64_t best = 0;
+    for (int64_t d = 1; d * d <= n; ++d) {
+        if (n % d) continue;
+        for (int64_t n1 : {d, n / d}) {
+            const int64_t n2 = n / n1;
+            FftPlan a, b;
+            if (n1 <= kFftLinesMax && n2 <= kFftLinesMax && fft_make_plan(n1, &a) && fft_make_plan(n2, &b))
+                if (best == 0 || std::llabs(n1 - n2) < std::llabs(best - n / best)) best = n1;
+        }
+    }
+    return best;
+}
+
+// The transform along one axis of an [outer, len, inner] array: src -> dst,
+// inverse scaled by 1 / len as the reference's dft_axis_kernel
+// (crates/lucem-ops/src/core/kernels/fft.rs:41-43).  `scratch` (outer * len *
+// inner complex) is needed for smooth lengths above kFftLinesMax.
+lucem_status fft_axis(lucem_ctx *ctx, const FftSide &src, const FftSide &dst, int64_t outer, int64_t len,
+                      int64_t inner, bool inverse, int clip, float2_ *scratch, void *stream) {
+    FftLines p{};
+    p.sre = src.re;
+    p.sim = src.im;
+    p.sc = src.c;
+    p.dre = dst.wre;
+    p.dim = dst.wim;
+    p.dc = dst.c;
+    p.n_outer = outer;
+    p.inner = inner;
+    p.s_os_hi = p.d_os_hi = len * inner;
+    p.s_rs = p.d_rs = inner;
+    p.scale = inverse ? (float)(1.0 / (double)len) : 1.0f;
+    p.clip = clip;
+    lucem_status st;
+    const float2_ *tw32 = nullptr;
+    const double *tw64 = nullptr;
+    FftPlan plan;
+    const bool smooth = fft_make_plan(len, &plan);
+    if (smooth && len <= kFftLinesMax) {
+        if ((st = twiddles(ctx, len, &tw32, &tw64))) return st;
+        p.n = (int32_t)len;
+        p.src_rows = p.dst_rows = (int32_t)len;
+        p.inverse = inverse;
+        p.plan = plan;
+        p.tw = tw32;
+        int e = timed(kPassFft, stream, [&] { return launch_fft_lines(p, stream); });
+        return e ? cuda_fail(e, "fft launch") : ok();
+    }
+    if (smooth) {
+        // Four-step: n = n1 n2, element m1 n2 + m2 -> X[k1 + n1 k2].
+        const int64_t n1 = four_step_split(len), n2 = n1 ? len / n1 : 0;
+        if (!n1 || !scratch) return fail(LUCEM_ERR_INVALID_PARAMETER, "fft: no four-step split for length %lld",
+                                        (long long)len);
+        const float2_ *tw_n = nullptr, *tw_1 = nullptr, *tw_2 = nullptr;
+        if ((st = twiddles(ctx, len, &tw_n, &tw64)) || (st = twiddles(ctx, n1, &tw_1, &tw64)) ||
+            (st = twiddles(ctx, n2, &tw_2, &tw64)))
+            return st;
+        FftLines a = p;
+        a.dre = a.dim = nullptr;
+        a.dc = scratch;
+        a.inner = n2 * inner;
+        a.s_rs = a.d_rs = n2 * inner;
+        a.n = (int32_t)n1;
+        a.src_rows = a.dst_rows = (int32_t)n1;
+        a.inverse = inverse;
+        fft_make_plan(n1, &a.plan);
+        a.tw = tw_1;
+        a.twiddle_n = (int32_t)len;
+        a.tw_big = tw_n;
+        a.tw_div = inner;
+        a.scale = 1.0f;
+        a.clip = 0;
+        int e = timed(kPassFft, stream, [&] { return launch_fft_lines(a, stream); });
+        if (e) return cuda_fail(e, "fft launch");
+        FftLines b = p;
+        b.sre = b.sim = nullptr;
+        b.sc = scratch;
+        b.n_outer = outer * n1;
+        b.inner = inner;
+        b.s_os_hi = n2 * inner;
+        b.s_rs = inner;
+        b.d_odiv = (int32_t)n1;
+        b.d_os_hi = len * inner;
+        b.d_os_lo = inner;
+        b.d_rs = n1 * inner;
+        b.n = (int32_t)n2;
+        b.src_rows = b.dst_rows = (int32_t)n2;
+        b.inverse = inverse;
+        fft_make_plan(n2, &b.plan);
+        b.tw = tw_2;
+        e = timed(kPassFft, stream, [&] { return launch_fft_lines(b, stream); });
+        return e ? cuda_fail(e, "fft launch") : ok();
+    }
+    const int64_t M = fft_good_length(2 * len - 1, false);
+    if (M <= kFftLinesMax) {
+        // Bluestein: X = c (.) ((x c) (*) conj(c)), the circular convolution on
+        // M points; the inverse transform through conjugation.
+        const float2_ *chirp = nullptr, *filt = nullptr;
+        if ((st = bluestein_tables(ctx, len, M, &chirp, &filt))) return st;
+        if ((st = twiddles(ctx, M, &tw32, &tw64))) return st;
+        p.n = (int32_t)M;
+        p.src_rows = p.dst_rows = (int32_t)len;
+        p.inverse = 0;
+        fft_make_plan(M, &p.plan);
+        p.tw = tw32;
+        p.pre = chirp;
+        p.mid = filt;
+        p.post = chirp;
+        p.conj_in = p.conj_out = inverse;
+        int e = timed(kPassFft, stream, [&] { return launch_fft_lines(p, stream); });
+        return e ? cuda_fail(e, "fft launch") : ok();
+    }
+    // Longer lengths without a smooth factorisation: the direct DFT.
+    if ((st = twiddles(ctx, len, &tw32, &tw64))) return st;
+    p.n = (int32_t)len;
+    p.src_rows = p.dst_rows = (int32_t)len;
+    p.inverse = inverse;
+    p.tw = tw32;
+    int e = timed(kPassFft, stream, [&] { return launch_dft_direct(p, stream); });
+    return e ? cuda_fail(e, "dft launch") : ok();
+}
+
+// N-D transform across all axes in order (fft_nd_into, core/fft.rs:55-100):
+// axis 0 src -> ping, the middle axes between ping and pong, the last one
+// into dst.  dims: the array's shape.
+lucem_status fft_nd(lucem_ctx *ctx, const int64_t *dims, int nd, const FftSide &src, const FftSide &dst,
+                    bool inverse, int clip, lucem_workspace *ws, void *stream) {
+    int64_t n = 1;
+    for (int d = 0; d < nd; ++d) n *= dims[d];
+    bool four = false;
+    for (int d = 0; d < nd; ++d) {
+        FftPlan pl;
+        four = four || (dims[d] > kFftLinesMax && fft_make_plan(dims[d], &pl));
+    }
+    lucem_status st;
+    void *scr = nullptr, *ping = nullptr, *pong = nullptr;
+    if (four && (st = ws->get("fft_four_step", (size_t)n * sizeof(float2_), &scr))) return st;
+    if (nd >= 2 && (st = ws->get("fft_ping", (size_t)n * sizeof(float2_), &ping))) return st;
+    if (nd >= 3 && (st = ws->get("fft_pong", (size_t)n * sizeof(float2_), &pong))) return st;
+    float2_ *scratch = static_cast<float2_ *>(scr);
+    FftSide cur = src;
+    float2_ *bufs[2] = {static_cast<float2_ *>(ping), static_cast<float2_ *>(pong)};
+    int which = 0;
+    for (int d = 0; d < nd; ++d) {
+        int64_t outer = 1, inner = 1;
+        for (int i = 0; i < d; ++i) outer *= dims[i];
+        for (int i = d + 1; i < nd; ++i) inner *= dims[i];
+        FftSide out;
+        const bool last = d + 1 == nd;
+        if (last) {
+            out = dst;
+        } else {
+            out.c = bufs[which];
+        }
+        if ((st = fft_axis(ctx, cur, out, outer, dims[d], inner, inverse, last ? clip : 0, scratch, stream)))
+            return st;
+        if (!last) {
+            cur = FftSide{};
+            cur.c = bufs[which];
+            which ^= 1;
+        }
+    }
+    return ok();
+}
+
+lucem_status fft_check(const lucem_tensor *re_in, const lucem_tensor *im_in, const lucem_tensor *re_out,
+                       const lucem_tensor *im_out) {
+    lucem_status st;
+    if ((st = check_tensor("re_in", re_in)) || (st = check_tensor("im_in", im_in)) ||
+        (st = check_tensor("re_out", re_out)) || (st = check_tensor("im_out", im_out)))
+        return st;
+    if ((st = same_shape("re_in", re_in, "im_in", im_in)) || (st = same_shape("re_in", re_in, "re_out", re_out)) ||
+        (st = same_shape("re_in", re_in, "im_out", im_out)))
+        return st;
+    if ((st = not_aliased(re_in, re_out)) || (st = not_aliased(im_in, im_out))) return st;
+    for (const lucem_tensor *t : {re_in, im_in, re_out, im_out})
+        if (t->dtype != LUCEM_F32) return fail(LUCEM_ERR_UNSUPPORTED_DTYPE, "fft takes f32 arrays");
+    return ok();
+}
+
+}  // namespace
+
+extern "C" {
+
+lucem_status lucem_fft_nd(lucem_ctx *ctx, const lucem_tensor *re_in, const lucem_tensor *im_in,
+                          lucem_tensor *re_out, lucem_tensor *im_out, int32_t inverse, lucem_workspace *ws,
+                          void *stream) {
+    TimerScope timer_scope(ws);
+    if (!ctx) return fail(LUCEM_ERR_INVALID_HANDLE, "null context");
+    if (!ws) return fail(LUCEM_ERR_INVALID_HANDLE, "a workspace is required");
+    lucem_status st;
+    if ((st = fft_check(re_in, im_in, re_out, im_out))) return st;
+    const int64_t n = numel(re_in);
+    cudaStream_t cs = static_cast<cudaStream_t>(stream);
+    if (re_in->ndim == 0 || n == 0) {
+        // fft.rs:69-72: copies.
+        if (n > 0) {
+            CUDA_TRY(cudaMemcpyAsync(re_out->data, re_in->data, (size_t)n * 4, cudaMemcpyDeviceToDevice, cs), "copy");
+            CUDA_TRY(cudaMemcpyAsync(im_out->data, im_in->data, (size_t)n * 4, cudaMemcpyDeviceToDevice, cs), "copy");
+        }
+        return ok();
+    }
+    FftSide src, dst;
+    src.re = static_cast<const float *>(re_in->data);
+    src.im = static_cast<const float *>(im_in->data);
+    dst.wre = static_cast<float *>(re_out->data);
+    dst.wim = static_cast<float *>(im_out->data);
+    return fft_nd(ctx, re_in->dims, re_in->ndim, src, dst, inverse != 0, 0, ws, stream);
+}
+
+lucem_status lucem_fft_1d(lucem_ctx *ctx, const lucem_tensor *re_in, const lucem_tensor *im_in,
+                          lucem_tensor *re_out, lucem_tensor *im_out, int32_t axis, int32_t inverse,
+                          lucem_workspace *ws, void *stream) {
+    TimerScope timer_scope(ws);
+    if (!ctx) return fail(LUCEM_ERR_INVALID_HANDLE, "null context");
+    lucem_status st;
+    if ((st = fft_check(re_in, im_in, re_out, im_out))) return st;
+    const int nd = re_in->ndim;
+    const int ax = axis < 0 ? axis + nd : axis;
+    if (nd == 0 || ax < 0 || ax >= nd)
+        return fail(LUCEM_ERR_INVALID_DIMENSION, "axis %d is out of range for a %d-D array", (int)axis, nd);
+    if (numel(re_in) == 0) return ok();
+    int64_t outer = 1, inner = 1;
+    for (int i = 0; i < ax; ++i) outer *= re_in->dims[i];
+    for (int i = ax + 1; i < nd; ++i) inner *= re_in->dims[i];
+    const int64_t len = re_in->dims[ax];
+    void *scr = nullptr;
+    FftPlan pl;
+    if (len > kFftLinesMax && fft_make_plan(len, &pl)) {
+        if (!ws) return fail(LUCEM_ERR_INVALID_HANDLE, "a workspace is required for lengths above %d", kFftLinesMax);
+        if ((st = ws->get("fft_four_step", (size_t)numel(re_in) * sizeof(float2_), &scr))) return st;
+    }
+    FftSide src, dst;
+    src.re = static_cast<const float *>(re_in->data);
+    src.im = static_cast<const float *>(im_in->data);
+    dst.wre = static_cast<float *>(re_out->data);
+    dst.wim = static_cast<float *>(im_out->data);
+    return fft_axis(ctx, src, dst, outer, len, inner, inverse != 0, 0, static_cast<float2_ *>(scr), stream);
+}
+
+lucem_status lucem_complex_mul(const lucem_tensor *a_re, const lucem_tensor *a_im, const lucem_tensor *b_re,
+                               const lucem_tensor *b_im, lucem_tensor *out_re, lucem_tensor *out_im, int32_t conj_b,
+                               void *stream) {
+    lucem_status st;
+    if ((st = check_tensor("a_re", a_re)) || (st = check_tensor("a_im", a_im)) || (st = check_tensor("b_re", b_re)) ||
+        (st = check_tensor("b_im", b_im)) || (st = check_tensor("out_re", out_re)) ||
+        (st = check_tensor("out_im", out_im)))
+        return st;
+    if ((st = same_shape("a_re", a_re, "b_re", b_re)) || (st = same_shape("a_re", a_re, "out_re", out_re)) ||
+        (st = same_shape("a_re", a_re, "a_im", a_im)) || (st = same_shape("a_re", a_re, "b_im", b_im)) ||
+        (st = same_shape("a_re", a_re, "out_im", out_im)))
+        return st;
+    for (const lucem_tensor *t : {a_re, a_im, b_re, b_im, (const lucem_tensor *)out_re, (const lucem_tensor *)out_im})
+        if (t->dtype != LUCEM_F32) return fail(LUCEM_ERR_UNSUPPORTED_DTYPE, "complex_mul takes f32 arrays");
+    const int64_t n = numel(a_re);
+    if (n == 0) return ok();
+    int e = launch_complex_mul(static_cast<const float *>(a_re->data), static_cast<const float *>(a_im->data),
+                               static_cast<const float *>(b_re->data), static_cast<const float *>(b_im->data),
+                               static_cast<float *>(out_re->data), static_cast<float *>(out_im->data), n, conj_b,
+                               stream);
+    return e ? cuda_fail(e, "complex_mul launch") : ok();
+}
+
+void lucem_wiener_settings_default(lucem_wiener_settings *s) {
+    s->balance = 0.1;
+    s->clip = 1;
+}
+
+lucem_status lucem_wiener_deconvolve(lucem_ctx *ctx, const lucem_tensor *in, const lucem_tensor *psf,
+                                     const lucem_wiener_settings *settings, lucem_tensor *out, lucem_workspace *ws,
+                                     void *stream) {
+    TimerScope timer_scope(ws);
+    if (!ctx) return fail(LUCEM_ERR_INVALID_HANDLE, "null context");
+    if (!ws) return fail(LUCEM_ERR_INVALID_HANDLE, "a workspace is required");
+    lucem_wiener_settings def;
+    lucem_wiener_settings_default(&def);
+    const lucem_wiener_settings *s = settings ? settings : &def;
+    lucem_status st;
+    // restore/deconvolve.rs:218-244, same order.
+    if ((st = check_tensor("input", in)) || (st = check_tensor("output", out)) || (st = check_tensor("psf", psf)))
+        return st;
+    if ((st = same_shape("input", in, "output", out)) || (st = not_aliased(in, out))) return st;
+    if (in->ndim != 2)
+        return fail(LUCEM_ERR_INVALID_DIMENSION, "wiener_deconvolve input expects 2-D array, got %d-D shape %s",
+                    in->ndim, dims_str(in).c_str());
+    if (psf->ndim != 2)
+        return fail(LUCEM_ERR_INVALID_DIMENSION, "wiener_deconvolve psf expects 2-D array, got %d-D shape %s",
+                    psf->ndim, dims_str(psf).c_str());
+    if (numel(psf) == 0) return fail(LUCEM_ERR_INVALID_WEIGHTS, "psf: PSF cannot be empty");
+    if (!std::isfinite(s->balance) || s->balance < 0.0)
+        return fail(LUCEM_ERR_INVALID_PARAMETER,
+                    "invalid parameter `balance`: balance must be non-negative and finite, got %g", s->balance);
+    if (in->dtype != LUCEM_F32 || psf->dtype != LUCEM_F32 || out->dtype != LUCEM_F32)
+        return fail(LUCEM_ERR_UNSUPPORTED_DTYPE, "wiener_deconvolve takes f32 input, psf and output");
+    if (numel(in) == 0) return ok();
+    const int64_t H = in->dims[0], W = in->dims[1];
+    if (psf->dims[0] > H || psf->dims[1] > W)
+        return fail(LUCEM_ERR_INVALID_WEIGHTS, "psf: PSF dimensions must not exceed image dimensions");
+    const int64_t n = H * W;
+    void *bufs[4] = {};
+    const char *names[4] = {"wiener_y", "wiener_h", "wiener_l", "wiener_x"};
+    for (int i = 0; i < 4; ++i)
+        if ((st = ws->get(names[i], (size_t)n * sizeof(float2_), &bufs[i]))) return st;
+    float2_ *Y = static_cast<float2_ *>(bufs[0]), *Hk = static_cast<float2_ *>(bufs[1]);
+    float2_ *Lk = static_cast<float2_ *>(bufs[2]), *X = static_cast<float2_ *>(bufs[3]);
+    // Y = FFT(input).
+    FftSide src, dst;
+    src.re = static_cast<const float *>(in->data);
+    dst.c = Y;
+    if ((st = fft_nd(ctx, in->dims, 2, src, dst, false, 0, ws, stream))) return st;
+    // H = FFT of the PSF centred at (kh/2, kw/2); X stages it.
+    auto centred_fft = [&](const float *k, int kh, int kw, float2_ *dst_c) -> lucem_status {
+        int e = launch_centre_kernel(k, kh, kw, X, (int)H, (int)W, stream);
+        if (e) return cuda_fail(e, "kernel centring");
+        FftSide a, b;
+        a.c = X;
+        b.c = dst_c;
+        return fft_nd(ctx, in->dims, 2, a, b, false, 0, ws, stream);
+    };
+    if ((st = centred_fft(static_cast<const float *>(psf->data), (int)psf->dims[0], (int)psf->dims[1], Hk))) return st;
+    // The discrete Laplacian [0 -1 0; -1 4 -1; 0 -1 0] (a 1 x 1 one below
+    // 3 x 3 images), as deconvolve.rs:250-262.
+    const bool lap3 = H >= 3 && W >= 3;
+    const float lap[9] = {0, -1, 0, -1, 4, -1, 0, -1, 0}, one = 1.0f;
+    int err = 0;
+    void *lapd = ctx->get_or_upload(lap3 ? "wiener-laplacian-3x3" : "wiener-laplacian-1x1", lap3 ? lap : &one,
+                                    lap3 ? sizeof lap : sizeof one, &err);
+    if (!lapd) return cuda_fail(err, "laplacian upload");
+    if ((st = centred_fft(static_cast<const float *>(lapd), lap3 ? 3 : 1, lap3 ? 3 : 1, Lk))) return st;
+    int e = timed(kPassElementwise, stream, [&] {
+        return launch_wiener_filter(Y, Hk, Lk, X, n, (float)s->balance, 1.0e-12f, stream);
+    });
+    if (e) return cuda_fail(e, "wiener filter launch");
+    // out = Re(IFFT(X)), clipped to [-1, 1] when asked (deconvolve.rs:285-292).
+    FftSide xs, os;
+    xs.c = X;
+    os.wre = static_cast<float *>(out->data);
+    return fft_nd(ctx, in->dims, 2, xs, os, true, s->clip ? 1 : 0, ws, stream);
 }
 
 }  // extern "C"

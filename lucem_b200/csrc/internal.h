@@ -165,6 +165,7 @@ enum PassKind : int {
     kPassElementwise,    // combine / cast / fill
     kPassRlColY,         // separable PSF: y convolution on the row spectra (forward * Hy * inverse)
     kPassRlColZ,         // separable PSF: z convolution on the row spectra (forward * Hz * inverse)
+    kPassFft,            // general complex FFT along one axis
     kPassCount
 };
 const char *pass_name(int kind);
@@ -188,6 +189,44 @@ struct FftPlan {
 
 bool fft_make_plan(int64_t n, FftPlan *plan);
 int64_t fft_good_length(int64_t n, bool even);
+
+// One axis pass of the general complex FFT (spectral.cu): every line (O, k),
+// O < n_outer, k < inner, of length n.  Element `row` of line (O, k) sits at
+// base(O) + k + row * rs with base(O) = (O / odiv) os_hi + (O % odiv) os_lo
+// (odiv <= 1: O os_hi), for the source (s_*) and the destination (d_*).
+// Source: split (sre, sim; sim null: zero imaginary part) or interleaved sc.
+// Destination: split (dre, dim; dim null: imaginary part dropped) or dc.
+// src_rows / dst_rows: rows read (the rest zero) / written.  Options: pre
+// (per input row), mid (between a forward and a backward transform, the
+// Bluestein filter), post (per output row), twiddle W_twiddle_n^(m2 row) with
+// m2 = k / tw_div (four-step), conjugation in / out, scale, clip to [-1, 1]
+// (split real output).  C, CP: set by the launcher.
+constexpr int kFftLinesMax = 8192;  // longest line transformed in shared memory
+struct FftLines {
+    const float *sre, *sim;
+    const float2_ *sc;
+    float *dre, *dim;
+    float2_ *dc;
+    int64_t n_outer, inner;
+    int32_t s_odiv, d_odiv;
+    int64_t s_os_hi, s_os_lo, s_rs;
+    int64_t d_os_hi, d_os_lo, d_rs;
+    int32_t n, src_rows, dst_rows, inverse;
+    FftPlan plan;
+    const float2_ *tw, *pre, *mid, *post, *tw_big;
+    int32_t twiddle_n;
+    int64_t tw_div;
+    float scale;
+    int32_t conj_in, conj_out, clip;
+    int32_t C, CP;
+};
+int launch_fft_lines(FftLines p, void *stream);
+int launch_dft_direct(const FftLines &p, void *stream);
+int launch_wiener_filter(const float2_ *y, const float2_ *h, const float2_ *l, float2_ *x, int64_t n, float balance,
+                         float eps, void *stream);
+int launch_complex_mul(const float *ar, const float *ai, const float *br, const float *bi, float *outr, float *outi,
+                       int64_t n, int conj_b, void *stream);
+int launch_centre_kernel(const float *k, int kh, int kw, float2_ *out, int H, int W, void *stream);
 
 
 // Geometry of one RL problem on its FFT grid.  Axes are (z, y, x); 2-D inputs

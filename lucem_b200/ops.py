@@ -29,7 +29,8 @@ __all__ = [
     "gaussian_family", "schedule", "gaussian_family_tiles", "richardson_lucy", "rl_grid",
     "gaussian_halo", "op_halo", "gaussian_blur_adjoint", "richardson_lucy_backward", "fft_convolve",
     "fft_convolve_backward", "RlBatch", "richardson_lucy_batch", "autotune_fft", "autotune_query",
-    "autotune_save", "autotune_load", "Graph", "gaussian_batch",
+    "autotune_save", "autotune_load", "Graph", "gaussian_batch", "fft_nd", "fft_1d", "complex_mul",
+    "wiener_deconvolve", "from_dlpack",
 ]
 
 
@@ -165,9 +166,39 @@ def _default_ws(device: int) -> Workspace:
 # helpers
 
 
+def from_dlpack(obj) -> torch.Tensor:
+    """A torch view of any DLPack producer (an object with __dlpack__: CuPy,
+    JAX, NumPy, ...), zero-copy; torch tensors pass through.  Every operator
+    here accepts such objects in place of tensors and returns torch tensors,
+    which are DLPack producers themselves (``cupy.from_dlpack(out)``)."""
+    if isinstance(obj, torch.Tensor):
+        return obj
+    if hasattr(obj, "__dlpack__"):
+        return torch.from_dlpack(obj)
+    raise TypeError(f"expected a torch.Tensor or a DLPack producer, got {type(obj).__name__}")
+
+
+def _dlpack_args(fn):
+    """Converts DLPack producers among the positional arguments and the
+    `out` / `outs` keywords to torch views before calling `fn`."""
+    import functools
+
+    @functools.wraps(fn)
+    def wrapped(*args, **kw):
+        args = tuple(from_dlpack(a) if (not isinstance(a, torch.Tensor) and hasattr(a, "__dlpack__")) else a
+                     for a in args)
+        if kw.get("out") is not None:
+            kw["out"] = from_dlpack(kw["out"])
+        return fn(*args, **kw)
+
+    return wrapped
+
+
 def _tensor(t: torch.Tensor, name: str) -> N.Tensor:
+    if not isinstance(t, torch.Tensor) and hasattr(t, "__dlpack__"):
+        t = from_dlpack(t)
     if not isinstance(t, torch.Tensor):
-        raise TypeError(f"{name} must be a torch.Tensor")
+        raise TypeError(f"{name} must be a torch.Tensor or a DLPack producer")
     if not t.is_cuda:
         raise LucemError(7, f"invalid parameter `{name}`: must be a CUDA tensor")
     if t.dtype not in _DTYPES:
@@ -203,6 +234,9 @@ def _doubles(v) -> tuple:
 
 
 def _ctx_ws(x: torch.Tensor, workspace: Optional[Workspace]):
+    if not isinstance(x, torch.Tensor) or not x.is_cuda:
+        raise LucemError(7, "invalid parameter `input`: must be a CUDA tensor (or a DLPack producer of device "
+                            "memory)")
     dev = x.device.index if x.device.index is not None else torch.cuda.current_device()
     ctx = context(dev)
     ws = workspace if workspace is not None else _default_ws(dev)
@@ -290,6 +324,7 @@ def op_halo(op: str, sigma: float = 0.0, low_sigma: float = 0.0, high_sigma: flo
 # filters
 
 
+@_dlpack_args
 def gaussian_blur(x: torch.Tensor, sigmas, *, orders=None, mode="reflect", cval=0.0, truncate=4.0, radii=None,
                   axes=None, channel_axis=None, input_scale=1.0, out: Optional[torch.Tensor] = None,
                   workspace: Optional[Workspace] = None) -> torch.Tensor:
@@ -305,6 +340,7 @@ def gaussian_blur(x: torch.Tensor, sigmas, *, orders=None, mode="reflect", cval=
     return out
 
 
+@_dlpack_args
 def gaussian_blur_adjoint(g: torch.Tensor, sigmas, *, orders=None, mode="reflect", truncate=4.0, radii=None,
                           axes=None, channel_axis=None, input_scale=1.0, out: Optional[torch.Tensor] = None,
                           workspace: Optional[Workspace] = None) -> torch.Tensor:
@@ -322,6 +358,7 @@ def gaussian_blur_adjoint(g: torch.Tensor, sigmas, *, orders=None, mode="reflect
     return out
 
 
+@_dlpack_args
 def gaussian_1d(x: torch.Tensor, sigma: float, *, axis=-1, order=0, mode="reflect", cval=0.0, truncate=4.0,
                 radius=None, out: Optional[torch.Tensor] = None) -> torch.Tensor:
     """gaussian_1d / gaussian_1d_into (crates/lucem-ops/src/filter/gaussian.rs:66-130)."""
@@ -337,6 +374,7 @@ def gaussian_1d(x: torch.Tensor, sigma: float, *, axis=-1, order=0, mode="reflec
     return out
 
 
+@_dlpack_args
 def correlate_1d(x: torch.Tensor, weights, *, axis=-1, mode="reflect", cval=0.0, origin=0,
                  out: Optional[torch.Tensor] = None) -> torch.Tensor:
     """correlate_1d (crates/lucem-ops/src/filter/convolve.rs:40-92)."""
@@ -351,6 +389,7 @@ def correlate_1d(x: torch.Tensor, weights, *, axis=-1, mode="reflect", cval=0.0,
     return out
 
 
+@_dlpack_args
 def convolve_1d(x: torch.Tensor, weights, *, axis=-1, mode="reflect", cval=0.0, origin=0,
                 out: Optional[torch.Tensor] = None) -> torch.Tensor:
     """convolve_1d (crates/lucem-ops/src/filter/convolve.rs:95-109): correlation
@@ -366,6 +405,7 @@ def convolve_1d(x: torch.Tensor, weights, *, axis=-1, mode="reflect", cval=0.0, 
     return correlate_1d(x, w[::-1].copy(), axis=axis, mode=mode, cval=cval, origin=mirrored, out=out)
 
 
+@_dlpack_args
 def difference_of_gaussians(x: torch.Tensor, low_sigmas, high_sigmas, *, mode="reflect", cval=0.0, truncate=4.0,
                             axes=None, channel_axis=None, input_scale=1.0, out: Optional[torch.Tensor] = None,
                             workspace: Optional[Workspace] = None) -> torch.Tensor:
@@ -382,6 +422,7 @@ def difference_of_gaussians(x: torch.Tensor, low_sigmas, high_sigmas, *, mode="r
     return out
 
 
+@_dlpack_args
 def gaussian_laplace(x: torch.Tensor, sigmas, *, mode="reflect", cval=0.0, truncate=4.0,
                      out: Optional[torch.Tensor] = None, workspace: Optional[Workspace] = None) -> torch.Tensor:
     """gaussian_laplace (crates/lucem-ops/src/filter/gaussian.rs:255-303)."""
@@ -394,6 +435,7 @@ def gaussian_laplace(x: torch.Tensor, sigmas, *, mode="reflect", cval=0.0, trunc
     return out
 
 
+@_dlpack_args
 def gaussian_grad_mag(x: torch.Tensor, sigmas, *, mode="reflect", cval=0.0, truncate=4.0,
                       out: Optional[torch.Tensor] = None, workspace: Optional[Workspace] = None) -> torch.Tensor:
     """gaussian_grad_mag (crates/lucem-ops/src/filter/gaussian.rs:307-371)."""
@@ -406,6 +448,7 @@ def gaussian_grad_mag(x: torch.Tensor, sigmas, *, mode="reflect", cval=0.0, trun
     return out
 
 
+@_dlpack_args
 def unsharp_mask(x: torch.Tensor, sigmas, amount: float, *, mode="reflect", cval=0.0, truncate=4.0, axes=None,
                  channel_axis=None, input_scale=1.0, out: Optional[torch.Tensor] = None,
                  workspace: Optional[Workspace] = None) -> torch.Tensor:
@@ -440,6 +483,7 @@ def _responses(specs, outs):
     return arr
 
 
+@_dlpack_args
 def gaussian_family(x: torch.Tensor, responses: Sequence[tuple], *, mode="reflect", cval=0.0, truncate=4.0,
                     input_scale=1.0, outs: Optional[Sequence[torch.Tensor]] = None,
                     workspace: Optional[Workspace] = None):
@@ -569,6 +613,7 @@ def _grid_arg(grid):
     return (C.c_int64 * 3)(*(g + [0] * (3 - len(g))))
 
 
+@_dlpack_args
 def richardson_lucy(x: torch.Tensor, psf: torch.Tensor, *, num_iter: int = 30, clip: bool = True,
                     filter_epsilon: Optional[float] = None, mode="reflect", grid=None,
                     out: Optional[torch.Tensor] = None, workspace: Optional[Workspace] = None) -> torch.Tensor:
@@ -606,6 +651,7 @@ def richardson_lucy_backward(x: torch.Tensor, psf: torch.Tensor, grad_out: torch
     return gp, gx
 
 
+@_dlpack_args
 def fft_convolve(x: torch.Tensor, psf: torch.Tensor, *, grid=None, out: Optional[torch.Tensor] = None,
                  workspace: Optional[Workspace] = None) -> torch.Tensor:
     """The forward model of richardson_lucy (deconvolve.rs:120, correlation
@@ -633,6 +679,72 @@ def fft_convolve_backward(x: torch.Tensor, psf: torch.Tensor, grad_out: torch.Te
     N.check(N.lib().lucem_fft_convolve_backward(ctx.handle, C.byref(ti), C.byref(tp), PadMode.CONSTANT,
                                                 _grid_arg(grid), C.byref(tg), tgx, tgp, ws.handle, _stream(x)))
     return gp, gx
+
+
+# ---------------------------------------------------------------------------
+# spectral operators (crates/lucem-ops/src/core/fft.rs, restore/deconvolve.rs)
+
+
+def _zeros_like_f32(t):
+    return torch.zeros(t.shape, dtype=torch.float32, device=t.device)
+
+
+def fft_nd(re: torch.Tensor, im: Optional[torch.Tensor] = None, *, inverse: bool = False,
+           workspace: Optional[Workspace] = None):
+    """fft_nd_into (crates/lucem-ops/src/core/fft.rs:55-100): the N-D DFT of
+    the split complex f32 array (re, im) over every axis, forward
+    unnormalised, inverse scaled by 1/len per axis.  Returns (re, im)."""
+    re = from_dlpack(re)
+    im = _zeros_like_f32(re) if im is None else from_dlpack(im)
+    ctx, ws = _ctx_ws(re, workspace)
+    ore, oim = torch.empty_like(re), torch.empty_like(re)
+    a, b, c, d = _tensor(re, "re_in"), _tensor(im, "im_in"), _tensor(ore, "re_out"), _tensor(oim, "im_out")
+    N.check(N.lib().lucem_fft_nd(ctx.handle, C.byref(a), C.byref(b), C.byref(c), C.byref(d), int(bool(inverse)),
+                                 ws.handle, _stream(re)))
+    return ore, oim
+
+
+def fft_1d(re: torch.Tensor, im: Optional[torch.Tensor] = None, *, axis: int = -1, inverse: bool = False,
+           workspace: Optional[Workspace] = None):
+    """fft_1d_into (crates/lucem-ops/src/core/fft.rs:14-53): the DFT along one
+    axis of the split complex f32 array (re, im).  Returns (re, im)."""
+    re = from_dlpack(re)
+    im = _zeros_like_f32(re) if im is None else from_dlpack(im)
+    ctx, ws = _ctx_ws(re, workspace)
+    ore, oim = torch.empty_like(re), torch.empty_like(re)
+    a, b, c, d = _tensor(re, "re_in"), _tensor(im, "im_in"), _tensor(ore, "re_out"), _tensor(oim, "im_out")
+    N.check(N.lib().lucem_fft_1d(ctx.handle, C.byref(a), C.byref(b), C.byref(c), C.byref(d), int(axis),
+                                 int(bool(inverse)), ws.handle, _stream(re)))
+    return ore, oim
+
+
+def complex_mul(a_re, a_im, b_re, b_im, *, conj_b: bool = False):
+    """complex_mul_into (crates/lucem-ops/src/core/fft.rs:104-138): (a_re +
+    i a_im) (b_re + i b_im), or times conj(b).  Returns (re, im)."""
+    a_re, a_im, b_re, b_im = (from_dlpack(t) for t in (a_re, a_im, b_re, b_im))
+    ore, oim = torch.empty_like(a_re), torch.empty_like(a_re)
+    ts = [_tensor(t, n) for t, n in ((a_re, "a_re"), (a_im, "a_im"), (b_re, "b_re"), (b_im, "b_im"),
+                                     (ore, "out_re"), (oim, "out_im"))]
+    N.check(N.lib().lucem_complex_mul(*[C.byref(t) for t in ts], int(bool(conj_b)), _stream(a_re)))
+    return ore, oim
+
+
+@_dlpack_args
+def wiener_deconvolve(x: torch.Tensor, psf: torch.Tensor, *, balance: float = 0.1, clip: bool = True,
+                      out: Optional[torch.Tensor] = None, workspace: Optional[Workspace] = None) -> torch.Tensor:
+    """wiener_deconvolve (crates/lucem-ops/src/restore/deconvolve.rs:210-309):
+    regularised frequency-domain Wiener deconvolution of a 2-D f32 image,
+    X = conj(H) Y / max(|H|^2 + balance |L|^2, 1e-12), on the FFTs of fft_nd."""
+    ctx, ws = _ctx_ws(x, workspace)
+    out = _out_like(x, out)
+    s = N.WienerSettings()
+    N.lib().lucem_wiener_settings_default(C.byref(s))
+    s.balance = float(balance)
+    s.clip = int(bool(clip))
+    ti, tp, to = _tensor(x, "input"), _tensor(psf, "psf"), _tensor(out, "output")
+    N.check(N.lib().lucem_wiener_deconvolve(ctx.handle, C.byref(ti), C.byref(tp), C.byref(s), C.byref(to),
+                                            ws.handle, _stream(x)))
+    return out
 
 
 # ---------------------------------------------------------------------------

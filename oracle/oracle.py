@@ -409,3 +409,79 @@ def richardson_lucy_backward_fft64(obs, psf, grad_out, num_iter=30, filter_epsil
     gn = lags(pb_conv, cc) + lags(pb_corr, cr)
     gp = norm * (gn - np.sum(gn * p)) if abs(ssum) > 1e-12 else gn
     return gp, ybar
+
+
+# ---------------------------------------------------------------------------
+# Spectral operators (test infrastructure, FP64).
+
+
+def dft_axis(re, im, axis, inverse=False):
+    """The reference's direct DFT along `axis` (dft_axis_kernel,
+    crates/lucem-ops/src/core/kernels/fft.rs:9-47) in FP64: X[f] = sum_n
+    x[n] e^{-+2 pi i f n / len}, the inverse scaled by 1/len.  Phases reduced
+    exactly ((f n) mod len)."""
+    x = np.asarray(re, np.float64) + 1j * np.asarray(im, np.float64)
+    x = np.moveaxis(x, axis, -1)
+    n = x.shape[-1]
+    k = np.arange(n)
+    ph = (np.outer(k, k) % n).astype(np.float64)
+    sign = 1.0 if inverse else -1.0
+    w = np.exp(sign * 2j * np.pi * ph / n)
+    y = x @ w.T
+    if inverse:
+        y = y / n
+    y = np.moveaxis(y, -1, axis)
+    return y.real, y.imag
+
+
+def dft_nd(re, im, inverse=False):
+    """fft_nd_into (crates/lucem-ops/src/core/fft.rs:55-100): dft_axis over
+    axes 0, 1, ... in order."""
+    r, i = np.asarray(re, np.float64), np.asarray(im, np.float64)
+    for ax in range(r.ndim):
+        r, i = dft_axis(r, i, ax, inverse)
+    return r, i
+
+
+def centred_kernel_2d(k, shape):
+    """fft_shift_2d_kernel (restore/kernels/deconvolve.rs:79-99): tap (ky, kx)
+    at ((ky - kh/2) mod H, (kx - kw/2) mod W) of a zero [H, W] array."""
+    out = np.zeros(shape, np.float64)
+    kh, kw = k.shape
+    for ky in range(kh):
+        for kx in range(kw):
+            out[(ky - kh // 2) % shape[0], (kx - kw // 2) % shape[1]] += float(k[ky, kx])
+    return out
+
+
+def wiener_deconvolve(img, psf, balance=0.1, clip=True, fft=None):
+    """wiener_deconvolve_into (crates/lucem-ops/src/restore/deconvolve.rs:
+    210-295) in FP64: Y = DFT(img), H = DFT(centred psf), L = DFT(centred
+    Laplacian [0 -1 0; -1 4 -1; 0 -1 0], a 1x1 one below 3x3 images),
+    X = conj(H) Y / max(|H|^2 + balance |L|^2, 1e-12), out = Re(IDFT(X)),
+    clipped to [-1, 1] when `clip`.  `fft`: the N-D transform to use (default
+    dft_nd; numpy.fft for sizes where the direct DFT is too slow)."""
+    img = np.asarray(img, np.float64)
+    shape = img.shape
+    if fft is None:
+        def fft(x, inverse=False):
+            r, i = dft_nd(x.real, x.imag, inverse)
+            return r + 1j * i
+    y = fft(img + 0j)
+    h = fft(centred_kernel_2d(np.asarray(psf, np.float64), shape) + 0j)
+    if shape[0] >= 3 and shape[1] >= 3:
+        lap = np.array([[0, -1, 0], [-1, 4, -1], [0, -1, 0]], np.float64)
+    else:
+        lap = np.ones((1, 1))
+    l = fft(centred_kernel_2d(lap, shape) + 0j)
+    l2 = (l * np.conj(l)).real
+    den = np.maximum(np.abs(h) ** 2 + balance * l2, 1e-12)
+    x = np.conj(h) * y / den
+    out = fft(x, inverse=True).real
+    return np.clip(out, -1.0, 1.0) if clip else out
+
+
+def numpy_fft(x, inverse=False):
+    """numpy's FP64 FFT with fft_nd_into's scaling (pinned to dft_nd in the
+    oracle tests)."""
+    return np.fft.ifftn(x) if inverse else np.fft.fftn(x)
