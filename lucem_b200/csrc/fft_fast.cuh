@@ -282,8 +282,25 @@ struct TwoStep {
     }
 
     // Frequency held in value slot j of thread t (forward output layout).
-    __device__ __forceinline__ static int freq(int t, int j) {
+    __host__ __device__ __forceinline__ static constexpr int freq(int t, int j) {
         return (t + N1 * (j / N1)) + N2 * bitrev(j % N1, N1);
+    }
+
+    // The slot holding frequency N - freq(t, j) in thread N1 - t, the same
+    // for every t >= 1 (mirror pairs of a real transform's packing).
+    static constexpr int mirror_slot(int j) {
+        const int target = N - freq(1, j);
+        for (int q = 0; q < N2; ++q)
+            if (freq(N1 - 1, q) == target) return q;
+        return -1;
+    }
+    // Thread 0: the slot holding frequency (N - freq(0, j)) mod N in thread 0
+    // itself (j = 0: frequency 0, its own slot).
+    static constexpr int mirror_slot0(int j) {
+        const int target = (N - freq(0, j)) % N;
+        for (int q = 0; q < N2; ++q)
+            if (freq(0, q) == target) return q;
+        return -1;
     }
 };
 

@@ -391,30 +391,33 @@ __global__ void __launch_bounds__(N1 * R, 65536 / (N1 * R * 128)) row_fast_kerne
         float2 v[N2];
         if (kind != kRowInit && kind != kRowRealIn) {
             const float2 *s1 = pi.s1 + (int64_t)(ok ? row : 0) * p.Hp;
-            // Every load of the row's half spectrum issued before any store.
+            // The half spectrum straight into the inverse transform's layout
+            // (slot j of thread t holds bin freq(t, j); lanes along t:
+            // coalesced), every load issued before any use.  The merge
+            //   Z[k] = (X[k] + X*[M-k]) + i (X[k] - X*[M-k]) W_Px^{-k}
+            // takes X[M-k] from the mirror thread N1 - t of the same row
+            // (a shuffle within the warp), thread 0 from its own slots and
+            // X[M] (one more load).
 #pragma unroll
-            for (int j = 0; j < N2; ++j) v[j] = ok ? s1[t + N1 * j] : make_float2(0.f, 0.f);
-            const float2 vm = (ok && t == 0) ? s1[M] : make_float2(0.f, 0.f);
+            for (int j = 0; j < N2; ++j) v[j] = ok ? s1[F::freq(t, j)] : make_float2(0.f, 0.f);
+            const float2 xM = (ok && t == 0) ? s1[M] : make_float2(0.f, 0.f);
+            const unsigned lane = threadIdx.x & 31u, src = (lane & ~(unsigned)(N1 - 1)) | ((N1 - t) & (N1 - 1));
+            float2 z[N2];
 #pragma unroll
-            for (int j = 0; j < N2; ++j) spec[t + N1 * j] = v[j];
-            if (t == 0) spec[M] = vm;
-            __syncthreads();
-            // Z[k] = (X[k] + X*[M-k]) + i (X[k] - X*[M-k]) W_Px^{-k}
-            for (int k = t; 2 * k <= M; k += N1) {
-                float2 xk = spec[k], xm = spec[M - k];
-                float2 xmc = fftc::conjf2(xm), xkc = fftc::conjf2(xk);
-                float2 e = fftc::add(xk, xmc), d = fftc::mul(fftc::sub(xk, xmc), fftc::conjf2(tws[k]));
-                float2 zk = make_float2(e.x - d.y, e.y + d.x);
-                if (k != 0 && 2 * k != M) {
-                    float2 e2 = fftc::add(xm, xkc), d2 = fftc::mul(fftc::sub(xm, xkc), fftc::conjf2(tws[M - k]));
-                    spec[M - k] = make_float2(e2.x - d2.y, e2.y + d2.x);
-                }
-                spec[k] = zk;
+            for (int j = 0; j < N2; ++j) {
+                const int jm = F::mirror_slot(j), j0 = F::mirror_slot0(j);
+                float2 xm;
+                xm.x = __shfl_sync(0xffffffffu, v[jm].x, src);
+                xm.y = __shfl_sync(0xffffffffu, v[jm].y, src);
+                if (t == 0) xm = j == 0 ? xM : v[j0];
+                const int k = F::freq(t, j);
+                const float2 xk = v[j];
+                const float2 xmc = fftc::conjf2(xm);
+                const float2 e = fftc::add(xk, xmc), d = fftc::mul(fftc::sub(xk, xmc), fftc::conjf2(tws[k]));
+                z[j] = make_float2(e.x - d.y, e.y + d.x);
             }
-            __syncthreads();
 #pragma unroll
-            for (int j = 0; j < N2; ++j) v[j] = spec[F::freq(t, j)];
-            __syncthreads();
+            for (int j = 0; j < N2; ++j) v[j] = z[j];
             F::template inverse<ZP>(v, t, r, xb, ti);
         }
         // v[i] = (x[2m], x[2m+1]), m = t + N1 i.  Epilogue on the image
@@ -520,24 +523,34 @@ __global__ void __launch_bounds__(N1 * R, 65536 / (N1 * R * 128)) row_fast_kerne
             __syncthreads();
         }
         F::template forward<ZP>(v, t, r, xb, tf);
+        // Split, in registers: X[k] = 1/2 (Z[k] + Z*[M-k]) - i/2 W_Px^k
+        // (Z[k] - Z*[M-k]) with Z[M] = Z[0]; Z[M-k] from the mirror thread
+        // (thread 0: its own slots), X[M] from Z[0] by thread 0.
+        {
+            const unsigned lane = threadIdx.x & 31u, src = (lane & ~(unsigned)(N1 - 1)) | ((N1 - t) & (N1 - 1));
+            float2 *s1 = pi.s1 + (int64_t)(ok ? row : 0) * p.Hp;
+            float2 xM = make_float2(0.f, 0.f);
 #pragma unroll
-        for (int j = 0; j < N2; ++j) spec[F::freq(t, j)] = v[j];
-        __syncthreads();
-        // X[k] = 1/2 (Z[k] + Z*[M-k]) - i/2 W_Px^k (Z[k] - Z*[M-k]);  Z[M] = Z[0].
-        for (int k = t; 2 * k <= M; k += N1) {
-            float2 zk = spec[k], zm = spec[k == 0 ? 0 : M - k];
-            float2 zmc = fftc::conjf2(zm), zkc = fftc::conjf2(zk);
-            float2 e = fftc::add(zk, zmc), d = fftc::mul(fftc::sub(zk, zmc), tws[k]);
-            float2 e2 = fftc::add(zm, zkc), d2 = fftc::mul(fftc::sub(zm, zkc), tws[M - k]);
-            spec[k] = make_float2(0.5f * (e.x + d.y), 0.5f * (e.y - d.x));
-            if (2 * k != M) spec[M - k] = make_float2(0.5f * (e2.x + d2.y), 0.5f * (e2.y - d2.x));
+            for (int j = 0; j < N2; ++j) {
+                const int jm = F::mirror_slot(j), j0 = F::mirror_slot0(j);
+                float2 zm;
+                zm.x = __shfl_sync(0xffffffffu, v[jm].x, src);
+                zm.y = __shfl_sync(0xffffffffu, v[jm].y, src);
+                if (t == 0) zm = v[j0];
+                const int k = F::freq(t, j);
+                const float2 zk = v[j];
+                const float2 zmc = fftc::conjf2(zm);
+                const float2 e = fftc::add(zk, zmc), d = fftc::mul(fftc::sub(zk, zmc), tws[k]);
+                if (j == 0 && t == 0) {
+                    // X[M] = 1/2 (Z[0] + Z*[0]) - i/2 W_Px^M (Z[0] - Z*[0]).
+                    const float2 zkc = fftc::conjf2(zk);
+                    const float2 e2 = fftc::add(zk, zkc), d2 = fftc::mul(fftc::sub(zk, zkc), tws[M]);
+                    xM = make_float2(0.5f * (e2.x + d2.y), 0.5f * (e2.y - d2.x));
+                }
+                if (ok) s1[k] = make_float2(0.5f * (e.x + d.y), 0.5f * (e.y - d.x));
+            }
+            if (ok && t == 0) s1[M] = xM;
         }
-        __syncthreads();
-        if (ok) {
-            float2 *s1 = pi.s1 + (int64_t)row * p.Hp;
-            for (int k = t; k <= M; k += N1) s1[k] = spec[k];
-        }
-        __syncthreads();
     }
     (void)U;
 }
