@@ -64,6 +64,8 @@ __global__ void __launch_bounds__(512, 1) col_pass_kernel(const __grid_constant_
                 const ColOffsets off = col_offsets(p, q, outer);
                 int srow;
                 if (p.mode == kColInv) srow = row;
+                else if (p.pad_mode == LUCEM_PAD_CONSTANT)  // zero padding: a range check, no pad map
+                    srow = (unsigned)(row - q.halo) < (unsigned)q.n_img ? row - q.halo : -1;
                 else srow = row < q.n_img + 2 * q.halo ? pad_index_rt(row - q.halo, q.n_img, p.pad_mode) : -1;
                 if (srow >= 0) val = q.src[off.src + srow * q.src_row + kx];
             }

@@ -158,8 +158,36 @@ __device__ __forceinline__ ColItem col_tile(const ColPass &p, int t, int *local)
 // bit 1, the input rows N/2 .. N-1 are zero (not loaded, first forward
 // stage pruned); bit 2, only the rows below N/2 are stored (last inverse
 // stage pruned).
-// The input rows of global tile gt held by thread (c, t) in value slots
-// i < N2 (i < N2 / 2 when the upper half is zero), padded per the pass.
+// Rows t + N1 i (i < N2; i < N2 / 2 when the upper half is zero) of one
+// column, extended by the pass's pad map: row j holds source row
+// pad(j - halo) for j < n_img + 2 halo, zero beyond.  Zero padding takes a
+// branch of its own outside the unrolled loop (one unsigned range check per
+// row): the pad map's mode switch per element made up 15% of the 128-point
+// pass's instructions.
+template <int N1, int N2, bool ZERO_HI>
+__device__ __forceinline__ void col_load_rows(const ColPass &p, const ColItem &q, const float2 *src, int t, bool ok,
+                                              float2 *v) {
+    const int src_row = (int)q.src_row;
+    if (p.pad_mode == LUCEM_PAD_CONSTANT) {
+#pragma unroll
+        for (int i = 0; i < N2; ++i) {
+            if (ZERO_HI && i >= N2 / 2) continue;  // rows >= N/2: zero, never read
+            const int sr = t + N1 * i - q.halo;
+            v[i] = (ok && (unsigned)sr < (unsigned)q.n_img) ? src[sr * src_row] : make_float2(0.f, 0.f);
+        }
+        return;
+    }
+    const int n_ext = q.n_img + 2 * q.halo;
+#pragma unroll
+    for (int i = 0; i < N2; ++i) {
+        if (ZERO_HI && i >= N2 / 2) continue;
+        const int row = t + N1 * i;
+        const int srow = row < n_ext ? pad_index_rt(row - q.halo, q.n_img, p.pad_mode) : -1;
+        v[i] = (ok && srow >= 0) ? src[srow * src_row] : make_float2(0.f, 0.f);
+    }
+}
+
+// The input rows of global tile gt held by thread (c, t) (col_load_rows).
 template <int N1, int N2, int C, bool ZERO_HI>
 __device__ __forceinline__ void col_load_input(const ColPass &p, int gt, int t, int c, float2 *v) {
     int tile;
@@ -172,14 +200,7 @@ __device__ __forceinline__ void col_load_input(const ColPass &p, int gt, int t, 
         kx = col - outer * q.Hx;
     }
     const float2 *src = q.src + (col_offsets(p, q, outer).src + kx);
-    const int n_ext = q.n_img + 2 * q.halo, src_row = (int)q.src_row;
-#pragma unroll
-    for (int i = 0; i < N2; ++i) {
-        if (ZERO_HI && i >= N2 / 2) continue;
-        const int row = t + N1 * i;
-        int srow = row < n_ext ? pad_index_rt(row - q.halo, q.n_img, p.pad_mode) : -1;
-        v[i] = (ok && srow >= 0) ? src[srow * src_row] : make_float2(0.f, 0.f);
-    }
+    col_load_rows<N1, N2, ZERO_HI>(p, q, src, t, ok, v);
 }
 
 // PR bit 4 (with bit 1, forward and full modes): the next tile's input rows
@@ -197,8 +218,13 @@ __global__ void __launch_bounds__(N1 * C, (N2 > 32 ? 1 : 65536 / (N1 * C * 128))
     float2 *tf = reinterpret_cast<float2 *>(smem4);
     float2 *ti = tf + N;
     float2 *xb = ti + N;
+    // Separable full pass: the axis factor (N complex, natural order) staged
+    // once per CTA after the exchange buffer (launch_col_fast sizes it).
+    float2 *hrs = xb + L::kBuf;
     const int tid = threadIdx.x, c = tid % C, t = tid / C;
     F::build_tables(tf, ti, p.tw, 1);
+    if (SEP && MODE == kColFull)
+        for (int i = tid; i < N; i += N1 * C) hrs[i] = p.Hrow[i];
     __syncthreads();
     const int ntiles = p.items ? p.total_tiles : (p.ncols + C - 1) / C;
     float2 nx[kPrefetch ? N2 / 2 : 1];
@@ -208,7 +234,6 @@ __global__ void __launch_bounds__(N1 * C, (N2 > 32 ? 1 : 65536 / (N1 * C * 128))
     for (int gt = blockIdx.x; gt < ntiles; gt += gridDim.x) {
         int tile;
         const ColItem q = col_tile(p, gt, &tile);
-        const int n_ext = q.n_img + 2 * q.halo;
         // Element offsets within one column fit 32 bits (checked by the host).
         const int src_row = (int)q.src_row, dst_row = (int)q.dst_row, h_row = (int)q.h_row;
         const int col = tile * C + c;
@@ -246,13 +271,7 @@ __global__ void __launch_bounds__(N1 * C, (N2 > 32 ? 1 : 65536 / (N1 * C * 128))
                 for (int i = 0; i < N2 / 2; ++i) v[i] = nx[i];
                 if (gt + (int)gridDim.x < ntiles) col_load_input<N1, N2, C, true>(p, gt + gridDim.x, t, c, nx);
             } else {
-#pragma unroll
-                for (int i = 0; i < N2; ++i) {
-                    if (kZeroHi && i >= N2 / 2) continue;  // rows >= N/2: zero, never read
-                    const int row = t + N1 * i;
-                    int srow = row < n_ext ? pad_index_rt(row - q.halo, q.n_img, p.pad_mode) : -1;
-                    v[i] = (ok && srow >= 0) ? src[srow * src_row] : make_float2(0.f, 0.f);
-                }
+                col_load_rows<N1, N2, kZeroHi>(p, q, src, t, ok, v);
             }
             F::template forward<kZeroHi>(v, t, c, xb, tf);
             if (MODE == kColFull && q.spec_out != nullptr && ok) {
@@ -273,7 +292,7 @@ __global__ void __launch_bounds__(N1 * C, (N2 > 32 ? 1 : 65536 / (N1 * C * 128))
                 float2 hj;
                 // Separable: the row factor here, the column's constant factor
                 // after the inverse, on the stored values only (it commutes).
-                if constexpr (SEP) hj = p.Hrow[F::freq(t, j)];
+                if constexpr (SEP) hj = hrs[F::freq(t, j)];
                 else if constexpr (kPrefetchH) hj = hv[j];
                 else hj = ok ? h[F::freq(t, j) * h_row] : make_float2(0.f, 0.f);
                 if (p.conj_h) hj.y = -hj.y;
@@ -291,11 +310,19 @@ __global__ void __launch_bounds__(N1 * C, (N2 > 32 ? 1 : 65536 / (N1 * C * 128))
         }
         float2 *dst = q.dst + (off.dst + kx);
         if (ok) {
+            constexpr int kRows = kLoOnly ? N / 2 : N;  // rows computed
+            if (q.store_begin == 0 && q.store_count == kRows) {
+                // Every computed row is stored: no per-row range checks.
 #pragma unroll
-            for (int i = 0; i < N2; ++i) {
-                if (kLoOnly && i >= N2 / 2) continue;  // not computed, not stored
-                const int row = t + N1 * i - q.store_begin;
-                if (row >= 0 && row < q.store_count) dst[row * dst_row] = v[i];
+                for (int i = 0; i < N2; ++i)
+                    if (!(kLoOnly && i >= N2 / 2)) dst[(t + N1 * i) * dst_row] = v[i];
+            } else {
+#pragma unroll
+                for (int i = 0; i < N2; ++i) {
+                    if (kLoOnly && i >= N2 / 2) continue;  // not computed, not stored
+                    const int row = t + N1 * i - q.store_begin;
+                    if (row >= 0 && row < q.store_count) dst[row * dst_row] = v[i];
+                }
             }
         }
     }
@@ -566,7 +593,9 @@ template <int N1, int N2, int C>
 int launch_col_fast(const ColPass &p, cudaStream_t s) {
     using L = fftc::ColLayout<N1, N2, C>;
     constexpr int N = N1 * N2;
-    size_t smem = ((size_t)2 * N + (size_t)L::kBuf) * sizeof(float2);
+    // Twiddle tables, the exchange buffer and (separable full pass) the axis factor.
+    const size_t hrow = (p.Hrow && p.mode == kColFull) ? (size_t)N : 0;
+    size_t smem = ((size_t)2 * N + (size_t)L::kBuf + hrow) * sizeof(float2);
     int ntiles = p.items ? p.total_tiles : (p.ncols + C - 1) / C;
     int per_sm = (int)((200 * 1024) / (smem + 1024));
     per_sm = per_sm < 1 ? 1 : (per_sm > 8 ? 8 : per_sm);
