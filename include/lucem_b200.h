@@ -422,6 +422,73 @@ lucem_status lucem_wiener_deconvolve(lucem_ctx *ctx, const lucem_tensor *in, con
                                      const lucem_wiener_settings *settings, lucem_tensor *out, lucem_workspace *ws,
                                      void *stream);
 
+/* crates/lucem-ops/src/filter/spectral.rs:21-63 fourier_gaussian_into: the
+ * split complex f32 spectrum (re, im) times exp(-2 pi^2 sigma_d^2 f_d^2) per
+ * axis d in place (f_d: the bin's signed normalised frequency); `values`
+ * broadcast per axis (1 or ndim values).  All axes in one pass over the
+ * array, applied in axis order with the reference's f32 products. */
+lucem_status lucem_fourier_gaussian(lucem_ctx *ctx, lucem_tensor *re, lucem_tensor *im, const double *sigmas,
+                                    int32_t n_sigmas, void *stream);
+/* crates/lucem-ops/src/filter/spectral.rs:66-108 fourier_box_into: times
+ * sinc(pi size_d f_d) per axis (1 where |pi size_d f_d| < 1e-12). */
+lucem_status lucem_fourier_box(lucem_ctx *ctx, lucem_tensor *re, lucem_tensor *im, const double *sizes,
+                               int32_t n_sizes, void *stream);
+/* crates/lucem-ops/src/filter/spectral.rs:112-164 fourier_shift_into: times
+ * exp(-i 2 pi shift_d f_d) per axis. */
+lucem_status lucem_fourier_shift(lucem_ctx *ctx, lucem_tensor *re, lucem_tensor *im, const double *shifts,
+                                 int32_t n_shifts, void *stream);
+/* crates/lucem-ops/src/filter/spectral.rs:168-213 butterworth: N-D f32 input
+ * -> out = Re(IFFT(FFT(in) w)), w = 1 / (1 + (|f| / cutoff_ratio)^(2 order))
+ * (low pass) or 1 - that (high_pass); cutoff_ratio in (0, 0.5].  The
+ * reference builds w on the host; here it is evaluated per bin in FP64 inside
+ * the product kernel. */
+lucem_status lucem_butterworth(lucem_ctx *ctx, const lucem_tensor *in, double cutoff_ratio, int32_t high_pass,
+                               double order, lucem_tensor *out, lucem_workspace *ws, void *stream);
+
+/* crates/lucem-ops/src/register/phase.rs:18-37 PhaseCorrelation. */
+typedef struct lucem_phase_correlation_settings {
+    int64_t upsample_factor;   /* 1: integer-pixel; > 1: 1/upsample_factor pixel */
+    int32_t normalize_phase;   /* 1: R / |R| (phase correlation); 0: plain cross-correlation */
+} lucem_phase_correlation_settings;
+void lucem_phase_correlation_settings_default(lucem_phase_correlation_settings *s);
+/* crates/lucem-ops/src/register/phase.rs:39-48 PhaseCorrelationResult. */
+typedef struct lucem_phase_correlation_result {
+    double shift[LUCEM_MAX_DIMS]; /* per axis, the shift registering `moving` onto `reference` */
+    double error;                 /* translation-invariant normalised RMS error in [0, 1] */
+    double phasediff;             /* global phase difference at the peak, radians */
+} lucem_phase_correlation_result;
+/* crates/lucem-ops/src/register/phase.rs:51-255 phase_correlation: N-D f32
+ * reference and moving images of one shape.  Cross-power spectrum of their
+ * FFTs, the |cc|^2 argmax of its inverse (first index on ties), then (when
+ * upsample_factor > 1) the reference's coordinate-wise candidate search,
+ * two passes, each candidate's sum over the whole spectrum an FP64
+ * reduction on the device, and the snap to the 1/upsample_factor grid.
+ * Synchronises on `stream` (the result is host data). */
+lucem_status lucem_phase_correlation(lucem_ctx *ctx, const lucem_tensor *reference, const lucem_tensor *moving,
+                                     const lucem_phase_correlation_settings *settings,
+                                     lucem_phase_correlation_result *result, lucem_workspace *ws, void *stream);
+
+/* crates/lucem-ops/src/restore/deconvolve.rs:330-354 UnsupervisedWiener. */
+typedef struct lucem_unsupervised_wiener_settings {
+    int64_t num_iter;          /* 30 */
+    int64_t burnin;            /* 10; < num_iter */
+    int32_t clip;              /* 1: clamp the result to [-1, 1] */
+    uint64_t seed;             /* 0: the balance jitter's PCG seed */
+} lucem_unsupervised_wiener_settings;
+void lucem_unsupervised_wiener_settings_default(lucem_unsupervised_wiener_settings *s);
+/* crates/lucem-ops/src/restore/deconvolve.rs:357-509 unsupervised_wiener:
+ * 2-D f32 input and PSF; the empirical-Bayes chain of the reference (balance
+ * from 0.05, per iteration the residual, prior and trace sums at the current
+ * balance, the variance update and the PCG jitter), the posterior mean of the
+ * spectrum after the burn-in, out = Re(IFFT(mean)) (clipped when asked).
+ * Every sum is an FP64 reduction on the device and the balance update runs on
+ * the device, so the chain needs no host round trip; `balance_chain` (host,
+ * num_iter doubles, may be NULL) receives the balances.  Synchronises on
+ * `stream` when balance_chain is given. */
+lucem_status lucem_unsupervised_wiener(lucem_ctx *ctx, const lucem_tensor *in, const lucem_tensor *psf,
+                                       const lucem_unsupervised_wiener_settings *settings, lucem_tensor *out,
+                                       double *balance_chain, lucem_workspace *ws, void *stream);
+
 /* The grid lucem_richardson_lucy uses (host only), before any autotuning of
  * the context: per axis the requested length, or the cheapest m * 2^k
  * (m in {1,3,5,7,9,15,21,25,27}) at least the padding's need, by length

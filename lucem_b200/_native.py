@@ -66,6 +66,18 @@ class WienerSettings(C.Structure):
     _fields_ = [("balance", C.c_double), ("clip", C.c_int32)]
 
 
+class PhaseCorrelationSettings(C.Structure):
+    _fields_ = [("upsample_factor", C.c_int64), ("normalize_phase", C.c_int32)]
+
+
+class PhaseCorrelationResult(C.Structure):
+    _fields_ = [("shift", C.c_double * MAX_DIMS), ("error", C.c_double), ("phasediff", C.c_double)]
+
+
+class UnsupervisedWienerSettings(C.Structure):
+    _fields_ = [("num_iter", C.c_int64), ("burnin", C.c_int64), ("clip", C.c_int32), ("seed", C.c_uint64)]
+
+
 # name -> (restype, argtypes); every function include/lucem_b200.h declares.
 P = C.c_void_p
 PP = C.POINTER(C.c_void_p)
@@ -90,6 +102,15 @@ SIGNATURES = {
     "lucem_complex_mul": (I32, [TP, TP, TP, TP, TP, TP, I32, P]),
     "lucem_wiener_settings_default": (None, [C.POINTER(WienerSettings)]),
     "lucem_wiener_deconvolve": (I32, [P, TP, TP, C.POINTER(WienerSettings), TP, P, P]),
+    "lucem_fourier_gaussian": (I32, [P, TP, TP, DP, I32, P]),
+    "lucem_fourier_box": (I32, [P, TP, TP, DP, I32, P]),
+    "lucem_fourier_shift": (I32, [P, TP, TP, DP, I32, P]),
+    "lucem_butterworth": (I32, [P, TP, D, I32, D, TP, P, P]),
+    "lucem_phase_correlation_settings_default": (None, [C.POINTER(PhaseCorrelationSettings)]),
+    "lucem_phase_correlation": (I32, [P, TP, TP, C.POINTER(PhaseCorrelationSettings),
+                                      C.POINTER(PhaseCorrelationResult), P, P]),
+    "lucem_unsupervised_wiener_settings_default": (None, [C.POINTER(UnsupervisedWienerSettings)]),
+    "lucem_unsupervised_wiener": (I32, [P, TP, TP, C.POINTER(UnsupervisedWienerSettings), TP, DP, P, P]),
     "lucem_workspace_wait_status": (I32, [P, P, I64P]),
     "lucem_workspace_timings": (I32, [P, C.c_char_p, DP, I64P, I32, C.POINTER(I32)]),
     "lucem_pad_mode_parse": (I32, [C.c_char_p, C.POINTER(I32)]),

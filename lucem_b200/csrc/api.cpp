@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cfloat>
 #include <cstdarg>
 #include <cstdio>
 #include <complex>
@@ -3069,6 +3070,384 @@ lucem_status lucem_wiener_deconvolve(lucem_ctx *ctx, const lucem_tensor *in, con
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Spectral filters, Butterworth, phase correlation and unsupervised Wiener
+// (kernels in spectral_ops.cu).
+
+namespace {
+
+// Bins of a C-contiguous array (< 2^32 elements, checked by the caller).
+SpecAxes spec_axes(const lucem_tensor *t) {
+    SpecAxes a{};
+    a.ndim = t->ndim;
+    uint32_t inner = 1;
+    for (int d = t->ndim - 1; d >= 0; --d) {
+        a.len[d] = (uint32_t)t->dims[d];
+        a.inner[d] = inner;
+        inner *= (uint32_t)t->dims[d];
+    }
+    return a;
+}
+
+// The signed normalised frequency of bin k on an n-point axis, as the
+// reference's host tables (filter/spectral.rs:38-41).
+double bin_freq(int64_t k, int64_t n) {
+    return k <= n / 2 ? (double)k / (double)n : (double)(k - n) / (double)n;
+}
+
+enum class SpecKind { kGaussian, kBox, kShift };
+
+// fourier_{gaussian,box,shift}_into (filter/spectral.rs:21-164): per axis a
+// table of the transfer function (FP64 on the host, cast to f32 as
+// cast_all), all axes applied in one pass (spectral_axes_kernel).
+lucem_status spectral_filter(lucem_ctx *ctx, lucem_tensor *re, lucem_tensor *im, const double *vals, int32_t n_vals,
+                             SpecKind kind, const char *name, void *stream) {
+    if (!ctx) return fail(LUCEM_ERR_INVALID_HANDLE, "null context");
+    lucem_status st;
+    if ((st = check_tensor("re", re)) || (st = check_tensor("im", im))) return st;
+    if ((st = same_shape("re", re, "im", im))) return st;
+    if (re->dtype != LUCEM_F32 || im->dtype != LUCEM_F32)
+        return fail(LUCEM_ERR_UNSUPPORTED_DTYPE, "spectral filters take f32 arrays");
+    if ((st = not_aliased(re, im))) return st;
+    const int nd = re->ndim;
+    if (n_vals > 0 && !vals) return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `%s`: null values", name);
+    std::vector<double> per;
+    if ((st = broadcast(name, vals, n_vals, nd, &per))) return st;
+    const int64_t n = numel(re);
+    if (n == 0 || nd == 0) return ok();
+    SpecAxes a = spec_axes(re);
+    a.phase = kind == SpecKind::kShift ? 1 : 0;
+    std::vector<float> tab;
+    char buf[64];
+    std::string key = kind == SpecKind::kGaussian ? "fgauss" : kind == SpecKind::kBox ? "fbox" : "fshift";
+    for (int d = 0; d < nd; ++d) {
+        const int64_t len = re->dims[d];
+        const double v = per[(size_t)d];
+        snprintf(buf, sizeof buf, "-%lld:%.17g", (long long)len, v);
+        key += buf;
+        a.off[d] = (uint32_t)tab.size();
+        std::vector<float> c((size_t)len), sn;
+        if (kind == SpecKind::kShift) sn.resize((size_t)len);
+        for (int64_t k = 0; k < len; ++k) {
+            const double f = bin_freq(k, len);
+            if (kind == SpecKind::kGaussian) {
+                c[(size_t)k] = (float)std::exp(-2.0 * M_PI * M_PI * v * v * f * f);
+            } else if (kind == SpecKind::kBox) {
+                const double x = M_PI * v * f;
+                c[(size_t)k] = (float)(std::fabs(x) < 1e-12 ? 1.0 : std::sin(x) / x);
+            } else {
+                c[(size_t)k] = (float)std::cos(-2.0 * M_PI * v * f);
+                sn[(size_t)k] = (float)std::sin(-2.0 * M_PI * v * f);
+            }
+        }
+        tab.insert(tab.end(), c.begin(), c.end());
+        tab.insert(tab.end(), sn.begin(), sn.end());
+    }
+    int err = 0;
+    void *dtab = ctx->get_or_upload(key, tab.data(), tab.size() * sizeof(float), &err);
+    if (!dtab) return cuda_fail(err, "spectral table upload");
+    int e = launch_spectral_axes(static_cast<float *>(re->data), static_cast<float *>(im->data), n,
+                                 static_cast<const float *>(dtab), a, stream);
+    return e ? cuda_fail(e, "spectral filter launch") : ok();
+}
+
+}  // namespace
+
+extern "C" {
+
+lucem_status lucem_fourier_gaussian(lucem_ctx *ctx, lucem_tensor *re, lucem_tensor *im, const double *sigmas,
+                                    int32_t n_sigmas, void *stream) {
+    return spectral_filter(ctx, re, im, sigmas, n_sigmas, SpecKind::kGaussian, "sigmas", stream);
+}
+
+lucem_status lucem_fourier_box(lucem_ctx *ctx, lucem_tensor *re, lucem_tensor *im, const double *sizes,
+                               int32_t n_sizes, void *stream) {
+    return spectral_filter(ctx, re, im, sizes, n_sizes, SpecKind::kBox, "sizes", stream);
+}
+
+lucem_status lucem_fourier_shift(lucem_ctx *ctx, lucem_tensor *re, lucem_tensor *im, const double *shifts,
+                                 int32_t n_shifts, void *stream) {
+    return spectral_filter(ctx, re, im, shifts, n_shifts, SpecKind::kShift, "shifts", stream);
+}
+
+// filter/spectral.rs:168-213.
+lucem_status lucem_butterworth(lucem_ctx *ctx, const lucem_tensor *in, double cutoff_ratio, int32_t high_pass,
+                               double order, lucem_tensor *out, lucem_workspace *ws, void *stream) {
+    TimerScope timer_scope(ws);
+    if (!ctx) return fail(LUCEM_ERR_INVALID_HANDLE, "null context");
+    if (!ws) return fail(LUCEM_ERR_INVALID_HANDLE, "a workspace is required");
+    if (!(cutoff_ratio > 0.0 && cutoff_ratio <= 0.5))
+        return fail(LUCEM_ERR_INVALID_PARAMETER,
+                    "invalid parameter `cutoff_ratio`: cutoff_ratio must be in (0.0, 0.5], got %g", cutoff_ratio);
+    lucem_status st;
+    if ((st = check_tensor("input", in)) || (st = check_tensor("output", out))) return st;
+    if ((st = same_shape("input", in, "output", out)) || (st = not_aliased(in, out))) return st;
+    if (in->dtype != LUCEM_F32 || out->dtype != LUCEM_F32)
+        return fail(LUCEM_ERR_UNSUPPORTED_DTYPE, "butterworth takes f32 input and output");
+    const int64_t n = numel(in);
+    if (n == 0) return ok();
+    cudaStream_t cs = static_cast<cudaStream_t>(stream);
+    if (in->ndim == 0) {
+        // fft_nd of a 0-D array copies; w = 1 / (1 + 0) (low pass) or 0.
+        if (high_pass) CUDA_TRY(cudaMemsetAsync(out->data, 0, 4, cs), "fill");
+        else CUDA_TRY(cudaMemcpyAsync(out->data, in->data, 4, cudaMemcpyDeviceToDevice, cs), "copy");
+        return ok();
+    }
+    void *xb = nullptr;
+    if ((st = ws->get("bw_spectrum", (size_t)n * sizeof(float2_), &xb))) return st;
+    float2_ *X = static_cast<float2_ *>(xb);
+    FftSide src, dst;
+    src.re = static_cast<const float *>(in->data);
+    dst.c = X;
+    if ((st = fft_nd(ctx, in->dims, in->ndim, src, dst, false, 0, ws, stream))) return st;
+    int e = timed(kPassElementwise, stream,
+                  [&] { return launch_butterworth(X, n, spec_axes(in), cutoff_ratio, order, high_pass ? 1 : 0, stream); });
+    if (e) return cuda_fail(e, "butterworth launch");
+    FftSide xs, os;
+    xs.c = X;
+    os.wre = static_cast<float *>(out->data);
+    return fft_nd(ctx, in->dims, in->ndim, xs, os, true, 0, ws, stream);
+}
+
+void lucem_phase_correlation_settings_default(lucem_phase_correlation_settings *s) {
+    s->upsample_factor = 1;
+    s->normalize_phase = 1;
+}
+
+// register/phase.rs:51-255.
+lucem_status lucem_phase_correlation(lucem_ctx *ctx, const lucem_tensor *reference, const lucem_tensor *moving,
+                                     const lucem_phase_correlation_settings *settings,
+                                     lucem_phase_correlation_result *result, lucem_workspace *ws, void *stream) {
+    TimerScope timer_scope(ws);
+    if (!ctx) return fail(LUCEM_ERR_INVALID_HANDLE, "null context");
+    if (!ws) return fail(LUCEM_ERR_INVALID_HANDLE, "a workspace is required");
+    if (!result) return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `result`: null");
+    lucem_phase_correlation_settings def;
+    lucem_phase_correlation_settings_default(&def);
+    const lucem_phase_correlation_settings *s = settings ? settings : &def;
+    lucem_status st;
+    if ((st = check_tensor("reference", reference)) || (st = check_tensor("moving", moving))) return st;
+    if ((st = same_shape("reference", reference, "moving", moving))) return st;
+    if (reference->dtype != LUCEM_F32 || moving->dtype != LUCEM_F32)
+        return fail(LUCEM_ERR_UNSUPPORTED_DTYPE, "phase_correlation takes f32 images");
+    const int64_t n = numel(reference);
+    if (n == 0) return fail(LUCEM_ERR_EMPTY_INPUT, "phase_correlation: empty input");
+    if (s->upsample_factor < 1)
+        return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `upsample_factor`: upsample_factor must be >= 1");
+    // A 0-D array is one sample: the same as a 1-D array of length 1.
+    lucem_tensor view = *reference;
+    if (view.ndim == 0) {
+        view.ndim = 1;
+        view.dims[0] = 1;
+    }
+    const int nd = view.ndim;
+    const double u = (double)s->upsample_factor;
+    const int half_span = (int)std::ceil(1.5 * u);
+    const int max_cand = 2 * (half_span > 2 ? half_span : 2) + 1;
+    int64_t max_len = 1;
+    for (int d = 0; d < nd; ++d) max_len = std::max(max_len, view.dims[d]);
+    const size_t cbytes = (size_t)n * sizeof(float2_);
+    void *pa = nullptr, *pb = nullptr, *pr = nullptr, *pc = nullptr, *po = nullptr, *pt = nullptr, *pp = nullptr,
+         *pv = nullptr, *pi = nullptr, *ps = nullptr;
+    const size_t part_bytes = std::max((size_t)max_cand * kCandBlocks * sizeof(double2), (size_t)4 * kRedBlocks * sizeof(double));
+    if ((st = ws->get("pc_a", cbytes, &pa)) || (st = ws->get("pc_b", cbytes, &pb)) ||
+        (st = ws->get("pc_r", cbytes, &pr)) || (st = ws->get("pc_cc", cbytes, &pc)) ||
+        (st = ws->get("pc_part", part_bytes, &pp)) || (st = ws->get("pc_pv", kRedBlocks * sizeof(float), &pv)) ||
+        (st = ws->get("pc_pi", kRedBlocks * sizeof(uint32_t), &pi)) ||
+        (st = ws->get("pc_state", sizeof(PcState) + 4 * sizeof(double), &ps)))
+        return st;
+    if (s->upsample_factor > 1 &&
+        ((st = ws->get("pc_other", (size_t)n * sizeof(double2), &po)) ||
+         (st = ws->get("pc_axis", (size_t)max_cand * (size_t)max_len * sizeof(double2), &pt))))
+        return st;
+    float2_ *A = static_cast<float2_ *>(pa), *B = static_cast<float2_ *>(pb);
+    float2_ *R = static_cast<float2_ *>(pr), *CC = static_cast<float2_ *>(pc);
+    PcState *dst_state = static_cast<PcState *>(ps);
+    double *dsums = reinterpret_cast<double *>(static_cast<char *>(ps) + sizeof(PcState));
+    const SpecAxes axes = spec_axes(&view);
+    // F_ref, F_mov (phase.rs:81-82), R (:85-102), cc = IFFT(R) (:104-106).
+    FftSide src, dst;
+    src.re = static_cast<const float *>(reference->data);
+    dst.c = A;
+    if ((st = fft_nd(ctx, view.dims, nd, src, dst, false, 0, ws, stream))) return st;
+    src.re = static_cast<const float *>(moving->data);
+    dst.c = B;
+    if ((st = fft_nd(ctx, view.dims, nd, src, dst, false, 0, ws, stream))) return st;
+    int e = timed(kPassElementwise, stream,
+                  [&] { return launch_phase_cross_power(A, B, R, n, s->normalize_phase ? 1 : 0, stream); });
+    if (e) return cuda_fail(e, "cross-power spectrum launch");
+    FftSide rs, cs;
+    rs.c = R;
+    cs.c = CC;
+    if ((st = fft_nd(ctx, view.dims, nd, rs, cs, true, 0, ws, stream))) return st;
+    // Integer peak (:108-131).
+    e = timed(kPassElementwise, stream, [&] {
+        return launch_phase_argmax(CC, n, axes, static_cast<float *>(pv), static_cast<uint32_t *>(pi), dst_state,
+                                   stream);
+    });
+    if (e) return cuda_fail(e, "argmax launch");
+    // Subpixel refinement (:134-227): two passes, coordinate-wise.
+    if (s->upsample_factor > 1) {
+        for (int pass = 0; pass < 2; ++pass) {
+            const int radius = pass == 0 ? half_span : 2;
+            const double step = pass == 0 ? 1.0 / u : 0.25 / u;
+            for (int ax = 0; ax < nd; ++ax) {
+                e = timed(kPassElementwise, stream, [&] {
+                    return launch_phase_refine_axis(R, n, axes, ax, radius, step, static_cast<double2 *>(po),
+                                                    static_cast<double2 *>(pt), static_cast<double2 *>(pp),
+                                                    dst_state, stream);
+                });
+                if (e) return cuda_fail(e, "refinement launch");
+            }
+        }
+    }
+    // Error terms (:231-253).
+    e = timed(kPassElementwise, stream, [&] {
+        return launch_phase_error_terms(static_cast<const float *>(reference->data),
+                                        static_cast<const float *>(moving->data), A, B, n, axes, dst_state,
+                                        s->normalize_phase ? 1 : 0, static_cast<double *>(pp), dsums, stream);
+    });
+    if (e) return cuda_fail(e, "error terms launch");
+    PcState hs;
+    double sums[4];
+    cudaStream_t cst = static_cast<cudaStream_t>(stream);
+    CUDA_TRY(cudaMemcpyAsync(&hs, dst_state, sizeof hs, cudaMemcpyDeviceToHost, cst), "state download");
+    CUDA_TRY(cudaMemcpyAsync(sums, dsums, sizeof sums, cudaMemcpyDeviceToHost, cst), "sums download");
+    CUDA_TRY(cudaStreamSynchronize(cst), "synchronise");
+    for (int d = 0; d < LUCEM_MAX_DIMS; ++d) result->shift[d] = 0.0;
+    for (int d = 0; d < reference->ndim; ++d) {
+        double v = hs.shift[d];
+        if (s->upsample_factor > 1) v = std::round(v * u) / u;  // :224-226
+        result->shift[d] = v;
+    }
+    result->phasediff = std::atan2(hs.peak_im, hs.peak_re);
+    const double nn = (double)n, denom = sums[0] * sums[1];
+    if (denom <= DBL_EPSILON) {
+        result->error = 0.0;
+    } else {
+        double amp2;
+        if (!s->normalize_phase) {
+            amp2 = (hs.peak_re * hs.peak_re + hs.peak_im * hs.peak_im) * nn * nn;
+        } else {
+            const double ur = sums[2] / nn, ui = sums[3] / nn;
+            amp2 = (ur * ur + ui * ui) * nn * nn;
+        }
+        result->error = std::sqrt(1.0 - std::min(std::max(amp2 / denom, 0.0), 1.0));
+    }
+    return ok();
+}
+
+void lucem_unsupervised_wiener_settings_default(lucem_unsupervised_wiener_settings *s) {
+    s->num_iter = 30;
+    s->burnin = 10;
+    s->clip = 1;
+    s->seed = 0;
+}
+
+// restore/deconvolve.rs:357-509.
+lucem_status lucem_unsupervised_wiener(lucem_ctx *ctx, const lucem_tensor *in, const lucem_tensor *psf,
+                                       const lucem_unsupervised_wiener_settings *settings, lucem_tensor *out,
+                                       double *balance_chain, lucem_workspace *ws, void *stream) {
+    TimerScope timer_scope(ws);
+    if (!ctx) return fail(LUCEM_ERR_INVALID_HANDLE, "null context");
+    if (!ws) return fail(LUCEM_ERR_INVALID_HANDLE, "a workspace is required");
+    lucem_unsupervised_wiener_settings def;
+    lucem_unsupervised_wiener_settings_default(&def);
+    const lucem_unsupervised_wiener_settings *s = settings ? settings : &def;
+    lucem_status st;
+    if ((st = check_tensor("input", in)) || (st = check_tensor("psf", psf)) || (st = check_tensor("output", out)))
+        return st;
+    // deconvolve.rs:363-381, same order.
+    if (in->ndim != 2)
+        return fail(LUCEM_ERR_INVALID_DIMENSION,
+                    "unsupervised_wiener input expects 2-D array, got %d-D shape %s", in->ndim, dims_str(in).c_str());
+    if (psf->ndim != 2)
+        return fail(LUCEM_ERR_INVALID_DIMENSION,
+                    "unsupervised_wiener psf expects 2-D array, got %d-D shape %s", psf->ndim, dims_str(psf).c_str());
+    if (numel(psf) == 0) return fail(LUCEM_ERR_INVALID_WEIGHTS, "psf: PSF cannot be empty");
+    if (s->num_iter <= 0 || s->burnin < 0 || s->burnin >= s->num_iter)
+        return fail(LUCEM_ERR_INVALID_PARAMETER,
+                    "invalid parameter `num_iter`: num_iter (%lld) must be > burnin (%lld) and >= 1",
+                    (long long)s->num_iter, (long long)s->burnin);
+    if ((st = same_shape("input", in, "output", out)) || (st = not_aliased(in, out))) return st;
+    if (in->dtype != LUCEM_F32 || psf->dtype != LUCEM_F32 || out->dtype != LUCEM_F32)
+        return fail(LUCEM_ERR_UNSUPPORTED_DTYPE, "unsupervised_wiener takes f32 input, psf and output");
+    if (numel(in) == 0) return ok();
+    const int64_t H = in->dims[0], W = in->dims[1], n = H * W;
+    // The PSF is placed on the image grid by its centre (as wiener_deconvolve).
+    if (psf->dims[0] > H || psf->dims[1] > W)
+        return fail(LUCEM_ERR_INVALID_WEIGHTS, "psf: PSF dimensions must not exceed image dimensions");
+    void *bufs[4] = {};
+    const char *names[4] = {"wiener_y", "wiener_h", "wiener_l", "wiener_x"};
+    for (int i = 0; i < 4; ++i)
+        if ((st = ws->get(names[i], (size_t)n * sizeof(float2_), &bufs[i]))) return st;
+    float2_ *Y = static_cast<float2_ *>(bufs[0]), *Hk = static_cast<float2_ *>(bufs[1]);
+    float2_ *Lk = static_cast<float2_ *>(bufs[2]), *X = static_cast<float2_ *>(bufs[3]);
+    void *pp = nullptr, *pm = nullptr, *ppart = nullptr, *pst = nullptr, *pch = nullptr;
+    if ((st = ws->get("uw_spec", (size_t)n * sizeof(float4_), &pp)) ||
+        (st = ws->get("uw_mean", (size_t)n * sizeof(double2), &pm)) ||
+        (st = ws->get("uw_part", (size_t)(3 * kRedBlocks + 2) * sizeof(double), &ppart)) ||
+        (st = ws->get("uw_state", sizeof(UwState), &pst)) ||
+        (st = ws->get("uw_chain", (size_t)s->num_iter * sizeof(double), &pch)))
+        return st;
+    // Y, H and L as in wiener_deconvolve (deconvolve.rs:383-420).
+    FftSide src, dst;
+    src.re = static_cast<const float *>(in->data);
+    dst.c = Y;
+    if ((st = fft_nd(ctx, in->dims, 2, src, dst, false, 0, ws, stream))) return st;
+    auto centred_fft = [&](const float *k, int kh, int kw, float2_ *dst_c) -> lucem_status {
+        int e = launch_centre_kernel(k, kh, kw, X, (int)H, (int)W, stream);
+        if (e) return cuda_fail(e, "kernel centring");
+        FftSide a, b;
+        a.c = X;
+        b.c = dst_c;
+        return fft_nd(ctx, in->dims, 2, a, b, false, 0, ws, stream);
+    };
+    if ((st = centred_fft(static_cast<const float *>(psf->data), (int)psf->dims[0], (int)psf->dims[1], Hk))) return st;
+    const bool lap3 = H >= 3 && W >= 3;
+    const float lap[9] = {0, -1, 0, -1, 4, -1, 0, -1, 0}, one = 1.0f;
+    int err = 0;
+    void *lapd = ctx->get_or_upload(lap3 ? "wiener-laplacian-3x3" : "wiener-laplacian-1x1", lap3 ? lap : &one,
+                                    lap3 ? sizeof lap : sizeof one, &err);
+    if (!lapd) return cuda_fail(err, "laplacian upload");
+    if ((st = centred_fft(static_cast<const float *>(lapd), lap3 ? 3 : 1, lap3 ? 3 : 1, Lk))) return st;
+    // The chain (deconvolve.rs:433-483), on the device.
+    float4_ *P = static_cast<float4_ *>(pp);
+    double2 *mean = static_cast<double2 *>(pm);
+    double *part = static_cast<double *>(ppart), *chain = static_cast<double *>(pch);
+    UwState *ust = static_cast<UwState *>(pst);
+    int e = timed(kPassElementwise, stream, [&] {
+        return launch_uw_setup(static_cast<const float *>(in->data), Y, Hk, Lk, P, n, s->seed, part, ust, mean,
+                               stream);
+    });
+    if (e) return cuda_fail(e, "unsupervised wiener setup");
+    for (int64_t it = 0; it < s->num_iter; ++it) {
+        e = timed(kPassElementwise, stream, [&] {
+            return launch_uw_iteration(Y, Hk, P, n, it >= s->burnin ? 1 : 0, mean, part, ust, chain, (int)it, stream);
+        });
+        if (e) return cuda_fail(e, "unsupervised wiener iteration");
+    }
+    const int64_t count = s->num_iter - s->burnin;
+    e = timed(kPassElementwise, stream,
+              [&] { return launch_uw_mean(mean, n, 1.0 / (double)(count > 0 ? count : 1), X, stream); });
+    if (e) return cuda_fail(e, "posterior mean");
+    FftSide xs, os;
+    xs.c = X;
+    os.wre = static_cast<float *>(out->data);
+    if ((st = fft_nd(ctx, in->dims, 2, xs, os, true, s->clip ? 1 : 0, ws, stream))) return st;
+    if (balance_chain) {
+        cudaStream_t cst = static_cast<cudaStream_t>(stream);
+        CUDA_TRY(cudaMemcpyAsync(balance_chain, chain, (size_t)s->num_iter * sizeof(double), cudaMemcpyDeviceToHost,
+                                 cst),
+                 "chain download");
+        CUDA_TRY(cudaStreamSynchronize(cst), "synchronise");
+    }
+    return ok();
+}
+
+}  // extern "C"
+
 
 // ---------------------------------------------------------------------------
 // Helpers shared with other translation units (internal.h).

@@ -228,6 +228,47 @@ int launch_complex_mul(const float *ar, const float *ai, const float *br, const 
                        int64_t n, int conj_b, void *stream);
 int launch_centre_kernel(const float *k, int kh, int kw, float2_ *out, int H, int W, void *stream);
 
+// spectral_ops.cu: per-axis spectral filters, Butterworth, phase
+// correlation and unsupervised Wiener on the FFTs above.
+constexpr int kRedBlocks = 148 * 8;  // most blocks of one reduction launch
+constexpr int kCandBlocks = 148;     // blocks per candidate of the phase-correlation refinement sums
+struct float4_ { float x, y, z, w; };
+// Axes of a C-contiguous array of < 2^32 elements: bin k_d = (e / inner[d])
+// % len[d]; off[d]: the axis's table in a concatenated f32 table (phase: the
+// cos table, then the sin table).
+struct SpecAxes {
+    int32_t ndim, phase;
+    uint32_t len[8], inner[8], off[8];
+};
+// Device state of one phase correlation: shift per axis, the peak's
+// cross-correlation value and flat index.
+struct PcState {
+    double shift[8];
+    double peak_re, peak_im;
+    uint32_t max_idx, pad_;
+};
+// Device state of one unsupervised Wiener chain.
+struct UwState {
+    double balance, img_var;
+    uint64_t rng;
+};
+int launch_spectral_axes(float *re, float *im, int64_t n, const float *tab, const SpecAxes &a, void *stream);
+int launch_butterworth(float2_ *X, int64_t n, const SpecAxes &a, double cutoff, double order, int high_pass,
+                       void *stream);
+int launch_phase_cross_power(const float2_ *A, const float2_ *B, float2_ *R, int64_t n, int normalize, void *stream);
+int launch_phase_argmax(const float2_ *X, int64_t n, const SpecAxes &a, float *pv, uint32_t *pi, PcState *st,
+                        void *stream);
+int launch_phase_refine_axis(const float2_ *R, int64_t n, const SpecAxes &a, int ax, int radius, double step,
+                             double2 *oth, double2 *axt, double2 *part, PcState *st, void *stream);
+int launch_phase_error_terms(const float *ref, const float *mov, const float2_ *A, const float2_ *B, int64_t n,
+                             const SpecAxes &a, const PcState *st, int want_cc, double *part, double *out,
+                             void *stream);
+int launch_uw_setup(const float *in, const float2_ *Y, const float2_ *H, const float2_ *L, float4_ *P, int64_t n,
+                    uint64_t seed, double *part, UwState *st, double2 *mean, void *stream);
+int launch_uw_iteration(const float2_ *Y, const float2_ *H, const float4_ *P, int64_t n, int accumulate,
+                        double2 *mean, double *part, UwState *st, double *chain, int it, void *stream);
+int launch_uw_mean(const double2 *mean, int64_t n, double inv_count, float2_ *X, void *stream);
+
 
 // Geometry of one RL problem on its FFT grid.  Axes are (z, y, x); 2-D inputs
 // have Z = Pz = 1.

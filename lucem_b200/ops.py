@@ -30,7 +30,8 @@ __all__ = [
     "gaussian_halo", "op_halo", "gaussian_blur_adjoint", "richardson_lucy_backward", "fft_convolve",
     "fft_convolve_backward", "RlBatch", "richardson_lucy_batch", "autotune_fft", "autotune_query",
     "autotune_save", "autotune_load", "Graph", "gaussian_batch", "fft_nd", "fft_1d", "complex_mul",
-    "wiener_deconvolve", "from_dlpack",
+    "wiener_deconvolve", "from_dlpack", "fourier_gaussian", "fourier_box", "fourier_shift", "butterworth",
+    "PhaseCorrelationResult", "phase_correlation", "unsupervised_wiener",
 ]
 
 
@@ -745,6 +746,99 @@ def wiener_deconvolve(x: torch.Tensor, psf: torch.Tensor, *, balance: float = 0.
     N.check(N.lib().lucem_wiener_deconvolve(ctx.handle, C.byref(ti), C.byref(tp), C.byref(s), C.byref(to),
                                             ws.handle, _stream(x)))
     return out
+
+
+def _spectral_filter(fn, re, im, vals):
+    re, im = from_dlpack(re), from_dlpack(im)
+    ctx, _ = _ctx_ws(re, None)
+    arr, n = _doubles(vals)
+    a, b = _tensor(re, "re"), _tensor(im, "im")
+    N.check(fn(ctx.handle, C.byref(a), C.byref(b), arr, n, _stream(re)))
+    return re, im
+
+
+def fourier_gaussian(re, im, sigmas):
+    """fourier_gaussian_into (crates/lucem-ops/src/filter/spectral.rs:21-63):
+    the split complex spectrum (re, im) times exp(-2 pi^2 sigma^2 f^2) per
+    axis, in place.  Returns (re, im)."""
+    return _spectral_filter(N.lib().lucem_fourier_gaussian, re, im, sigmas)
+
+
+def fourier_box(re, im, sizes):
+    """fourier_box_into (filter/spectral.rs:66-108): times sinc(pi size f)
+    per axis, in place.  Returns (re, im)."""
+    return _spectral_filter(N.lib().lucem_fourier_box, re, im, sizes)
+
+
+def fourier_shift(re, im, shifts):
+    """fourier_shift_into (filter/spectral.rs:112-164): times
+    exp(-i 2 pi shift f) per axis, in place.  Returns (re, im)."""
+    return _spectral_filter(N.lib().lucem_fourier_shift, re, im, shifts)
+
+
+@_dlpack_args
+def butterworth(x: torch.Tensor, cutoff_ratio: float, high_pass: bool = False, order: float = 2.0, *,
+                out: Optional[torch.Tensor] = None, workspace: Optional[Workspace] = None) -> torch.Tensor:
+    """butterworth (crates/lucem-ops/src/filter/spectral.rs:168-213): N-D
+    frequency-domain Butterworth low-pass (or high-pass) filter of an f32
+    array, cutoff_ratio in (0, 0.5]."""
+    ctx, ws = _ctx_ws(x, workspace)
+    out = _out_like(x, out)
+    ti, to = _tensor(x, "input"), _tensor(out, "output")
+    N.check(N.lib().lucem_butterworth(ctx.handle, C.byref(ti), float(cutoff_ratio), int(bool(high_pass)),
+                                      float(order), C.byref(to), ws.handle, _stream(x)))
+    return out
+
+
+@dataclass
+class PhaseCorrelationResult:
+    """crates/lucem-ops/src/register/phase.rs:39-48."""
+
+    shift: list
+    error: float
+    phasediff: float
+
+
+@_dlpack_args
+def phase_correlation(reference: torch.Tensor, moving: torch.Tensor, *, upsample_factor: int = 1,
+                      normalize_phase: bool = True,
+                      workspace: Optional[Workspace] = None) -> PhaseCorrelationResult:
+    """phase_correlation (crates/lucem-ops/src/register/phase.rs:51-255): the
+    N-D shift registering `moving` onto `reference` (1 / upsample_factor
+    pixel precision), its normalised RMS error and the global phase
+    difference.  Synchronises (the result is host data)."""
+    ctx, ws = _ctx_ws(reference, workspace)
+    s = N.PhaseCorrelationSettings()
+    N.lib().lucem_phase_correlation_settings_default(C.byref(s))
+    s.upsample_factor = int(upsample_factor)
+    s.normalize_phase = int(bool(normalize_phase))
+    r = N.PhaseCorrelationResult()
+    a, b = _tensor(reference, "reference"), _tensor(moving, "moving")
+    N.check(N.lib().lucem_phase_correlation(ctx.handle, C.byref(a), C.byref(b), C.byref(s), C.byref(r),
+                                            ws.handle, _stream(reference)))
+    return PhaseCorrelationResult([float(r.shift[d]) for d in range(reference.dim())], float(r.error),
+                                  float(r.phasediff))
+
+
+@_dlpack_args
+def unsupervised_wiener(x: torch.Tensor, psf: torch.Tensor, *, num_iter: int = 30, burnin: int = 10,
+                        clip: bool = True, seed: int = 0, out: Optional[torch.Tensor] = None,
+                        workspace: Optional[Workspace] = None):
+    """unsupervised_wiener (crates/lucem-ops/src/restore/deconvolve.rs:357-509):
+    Wiener deconvolution of a 2-D f32 image with the regularisation balance
+    estimated by the reference's empirical-Bayes chain.  Returns
+    (deconvolved, balance_chain); synchronises to return the chain."""
+    ctx, ws = _ctx_ws(x, workspace)
+    out = _out_like(x, out)
+    s = N.UnsupervisedWienerSettings()
+    N.lib().lucem_unsupervised_wiener_settings_default(C.byref(s))
+    s.num_iter, s.burnin, s.clip, s.seed = int(num_iter), int(burnin), int(bool(clip)), int(seed) & (2 ** 64 - 1)
+    chain = (C.c_double * max(1, int(num_iter)))()
+    ti, tp, to = _tensor(x, "input"), _tensor(psf, "psf"), _tensor(out, "output")
+    N.check(N.lib().lucem_unsupervised_wiener(ctx.handle, C.byref(ti), C.byref(tp), C.byref(s), C.byref(to), chain,
+                                              ws.handle, _stream(x)))
+    n = int(num_iter) if x.numel() else 0
+    return out, [float(chain[i]) for i in range(n)]
 
 
 # ---------------------------------------------------------------------------

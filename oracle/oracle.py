@@ -485,3 +485,162 @@ def numpy_fft(x, inverse=False):
     """numpy's FP64 FFT with fft_nd_into's scaling (pinned to dft_nd in the
     oracle tests)."""
     return np.fft.ifftn(x) if inverse else np.fft.fftn(x)
+
+
+def bin_freq(n):
+    """Signed normalised frequency of every bin of an n-point axis
+    (crates/lucem-ops/src/filter/spectral.rs:38-41)."""
+    k = np.arange(n)
+    return np.where(k <= n // 2, k, k - n).astype(np.float64) / n
+
+
+def _axis_view(v, d, ndim):
+    shape = [1] * ndim
+    shape[d] = -1
+    return v.reshape(shape)
+
+
+def fourier_filter(re, im, values, kind):
+    """fourier_gaussian_into / fourier_box_into / fourier_shift_into
+    (crates/lucem-ops/src/filter/spectral.rs:21-164): per axis in order, the
+    f32 spectrum times the axis's f32 table (FP64 values cast once, as
+    cast_all), with the reference kernels' f32 products
+    (filter/kernels/spectral.rs:10-51)."""
+    re = np.array(re, np.float32)
+    im = np.array(im, np.float32)
+    per = broadcast_per_axis("values", values, re.ndim)
+    for d, v in enumerate(per):
+        f = bin_freq(re.shape[d])
+        if kind == "gaussian":
+            w = np.exp(-2.0 * np.pi * np.pi * v * v * f * f).astype(np.float32)
+            re, im = re * _axis_view(w, d, re.ndim), im * _axis_view(w, d, re.ndim)
+        elif kind == "box":
+            x = np.pi * v * f
+            with np.errstate(invalid="ignore", divide="ignore"):
+                w = np.where(np.abs(x) < 1e-12, 1.0, np.sin(x) / np.where(x == 0, 1.0, x)).astype(np.float32)
+            re, im = re * _axis_view(w, d, re.ndim), im * _axis_view(w, d, re.ndim)
+        else:
+            c = _axis_view(np.cos(-2.0 * np.pi * v * f).astype(np.float32), d, re.ndim)
+            s = _axis_view(np.sin(-2.0 * np.pi * v * f).astype(np.float32), d, re.ndim)
+            re, im = (re * c - im * s).astype(np.float32), (re * s + im * c).astype(np.float32)
+    return re, im
+
+
+def butterworth_weights(shape, cutoff_ratio, high_pass=False, order=2.0):
+    """The Butterworth transfer function of filter/spectral.rs:185-199 (FP64,
+    cast to f32 as the reference's host array)."""
+    r2 = np.zeros(shape, np.float64)
+    for d, n in enumerate(shape):
+        r2 = r2 + _axis_view((bin_freq(n) / cutoff_ratio) ** 2, d, len(shape))
+    lp = 1.0 / (1.0 + np.sqrt(r2) ** (2.0 * order))
+    return (1.0 - lp if high_pass else lp).astype(np.float32)
+
+
+def butterworth(x, cutoff_ratio, high_pass=False, order=2.0):
+    """butterworth (filter/spectral.rs:168-213) in FP64 on numpy's FFT:
+    Re(IFFT(FFT(x) w))."""
+    x = np.asarray(x, np.float64)
+    w = butterworth_weights(x.shape, cutoff_ratio, high_pass, order).astype(np.float64)
+    return np.fft.ifftn(np.fft.fftn(x) * w).real
+
+
+def phase_correlation(ref, mov, upsample_factor=1, normalize_phase=True):
+    """phase_correlation (crates/lucem-ops/src/register/phase.rs:51-255) in
+    FP64: cross-power spectrum, |cc|^2 argmax (first index), the two-pass
+    coordinate-wise candidate search (every candidate's sum over the whole
+    spectrum), the snap to 1/upsample_factor, phasediff and the RMS error.
+    Returns (shift, error, phasediff)."""
+    ref = np.asarray(ref, np.float64)
+    mov = np.asarray(mov, np.float64)
+    shape, nd, n = ref.shape, ref.ndim, ref.size
+    A, B = np.fft.fftn(ref), np.fft.fftn(mov)
+    R = A * np.conj(B)
+    if normalize_phase:
+        mag = np.abs(R)
+        R = np.where(mag > 1e-12, R / np.where(mag > 1e-12, mag, 1.0), 0.0)
+    cc = np.fft.ifftn(R)
+    mi = int(np.argmax(np.abs(cc) ** 2))
+    idx = np.unravel_index(mi, shape)
+    shift = [float(k if k <= shape[d] // 2 else k - shape[d]) for d, k in enumerate(idx)]
+    peak = complex(cc.flat[mi])
+    if upsample_factor > 1:
+        u = float(upsample_factor)
+        half = int(np.ceil(1.5 * u))
+        freqs = [bin_freq(s) for s in shape]
+        for ps in range(2):
+            radius, step = (half, 1.0 / u) if ps == 0 else (2, 0.25 / u)
+            for ax in range(nd):
+                other = np.zeros(shape)
+                for d in range(nd):
+                    if d != ax:
+                        other = other + 2.0 * np.pi * _axis_view(freqs[d], d, nd) * shift[d]
+                oth = np.exp(1j * other)
+                center, best, bs, bp = shift[ax], -1.0, shift[ax], peak
+                for m in range(-radius, radius + 1):
+                    cs = center + m * step
+                    tot = (R * oth * _axis_view(np.exp(1j * 2.0 * np.pi * freqs[ax] * cs), ax, nd)).sum() / n
+                    mag2 = abs(tot) ** 2
+                    if mag2 > best:
+                        best, bs, bp = mag2, cs, tot
+                shift[ax], peak = bs, bp
+        # f64::round: half away from zero (not Python's round-half-even).
+        shift = [float(np.copysign(np.floor(abs(s * u) + 0.5), s * u)) / u for s in shift]
+    phasediff = float(np.arctan2(peak.imag, peak.real))
+    denom = float((ref ** 2).sum() * (mov ** 2).sum())
+    if denom <= np.finfo(np.float64).eps:
+        error = 0.0
+    else:
+        if normalize_phase:
+            peak_u = np.fft.ifftn(A * np.conj(B)).flat[mi]
+        else:
+            peak_u = peak
+        amp2 = abs(peak_u) ** 2 * n * n
+        error = float(np.sqrt(1.0 - min(max(amp2 / denom, 0.0), 1.0)))
+    return shift, error, phasediff
+
+
+def unsupervised_wiener(img, psf, num_iter=30, burnin=10, clip=True, seed=0):
+    """unsupervised_wiener (crates/lucem-ops/src/restore/deconvolve.rs:357-509):
+    the spectra as f32 arrays (FP64 FFTs rounded once; the reference's device
+    arrays are f32), their products in f32 as complex_mul_into, the chain in
+    FP64 with the reference's update and PCG jitter.  Returns (out, chain)."""
+    img = np.asarray(img, np.float64)
+    shape, n = img.shape, float(img.size)
+    c64 = lambda z: (z.real.astype(np.float32), z.imag.astype(np.float32))  # noqa: E731
+    yr, yi = c64(np.fft.fftn(img))
+    hr, hi = c64(np.fft.fftn(centred_kernel_2d(np.asarray(psf, np.float64), shape)))
+    if shape[0] >= 3 and shape[1] >= 3:
+        lap = np.array([[0, -1, 0], [-1, 4, -1], [0, -1, 0]], np.float64)
+    else:
+        lap = np.ones((1, 1))
+    lr, li = c64(np.fft.fftn(centred_kernel_2d(lap, shape)))
+    f = lambda a: a.astype(np.float64)  # noqa: E731
+    hm2 = f(hr * hr - hi * (np.float32(0) - hi))
+    lm2 = f(lr * lr - li * (np.float32(0) - li))
+    hyr = f(yr * hr - yi * (np.float32(0) - hi))
+    hyi = f(yr * (np.float32(0) - hi) + yi * hr)
+    img_var = float(np.asarray(img, np.float32).astype(np.float64).var())
+    balance, chain = 0.05, []
+    mean = np.zeros(shape, np.complex128)
+    rng = (int(seed) + 0x9E3779B97F4A7C15) % (1 << 64)
+    for it in range(num_iter):
+        den = np.maximum(hm2 + balance * lm2, 1e-12)
+        xr, xi = hyr / den, hyi / den
+        hxr, hxi = f(hr) * xr - f(hi) * xi, f(hr) * xi + f(hi) * xr
+        dr, di = f(yr) - hxr, f(yi) - hxi
+        rss = float(((dr * dr + di * di) / n).sum())
+        reg = float((lm2 * ((xr * xr + xi * xi) / n)).sum())
+        tr = float((hm2 / den).sum())
+        if it >= burnin:
+            mean += xr + 1j * xi
+        eff = max(n - tr, 1.0)
+        sn2 = max(rss / eff, 1e-8 * max(img_var, 1e-6))
+        sx2 = max(reg / max(tr, 1.0), 1e-8)
+        rng = (rng * 6364136223846793005 + 1) % (1 << 64)
+        u = (rng >> 33) / float(1 << 31) - 0.5
+        balance = min(max(sn2 / sx2 * np.exp(u * (2.0 / np.sqrt(n))), 1e-6), 1e3)
+        chain.append(balance)
+    mean /= max(num_iter - burnin, 1)
+    m32 = mean.real.astype(np.float32).astype(np.float64) + 1j * mean.imag.astype(np.float32).astype(np.float64)
+    out = np.fft.ifftn(m32).real
+    return (np.clip(out, -1.0, 1.0) if clip else out), chain

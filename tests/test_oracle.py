@@ -240,3 +240,55 @@ def test_wiener_oracle_recovers_a_delta_psf_image(oracle):
     oracle.assert_close(out, img, 1e-3, "delta psf")
     fast = oracle.wiener_deconvolve(img, psf, balance=1e-7, clip=False, fft=oracle.numpy_fft)
     np.testing.assert_allclose(fast, out, rtol=1e-12, atol=1e-12)
+
+
+def _fourier_shifted(img, shift):
+    f = np.fft.fftn(img)
+    for d, s in enumerate(shift):
+        n = img.shape[d]
+        k = np.arange(n)
+        sh = [1] * img.ndim
+        sh[d] = -1
+        f = f * np.exp(-2j * np.pi * s * (np.where(k <= n // 2, k, k - n) / n)).reshape(sh)
+    return np.fft.ifftn(f).real
+
+
+def test_phase_correlation_oracle_reference_cases(oracle):
+    """crates/lucem-ops/src/register/phase.rs:262-296: a 16x16 sample image
+    shifted by (2.25, -1.5), upsample 20, recovered as (-2.25, 1.5) within
+    0.1; an integer roll is recovered exactly with zero error."""
+    i = np.arange(256, dtype=np.int64)
+    base = (((i * 6151 + 49_999) % 1013).astype(np.float64) * 0.1 + 0.1).reshape(16, 16)
+    shift, err, _ = oracle.phase_correlation(base, _fourier_shifted(base, (2.25, -1.5)), 20, True)
+    assert abs(shift[0] + 2.25) < 0.1 and abs(shift[1] - 1.5) < 0.1
+    shift, err, pd = oracle.phase_correlation(base, np.roll(base, (3, -4), (0, 1)), 1, True)
+    assert shift == [-3.0, 4.0] and err < 1e-6 and abs(pd) < 1e-9
+
+
+def test_fourier_filter_oracle_reference_cases(oracle):
+    """filter/spectral.rs:272-281 (a zero shift leaves the spectrum unchanged);
+    a Gaussian of sigma 0 and a box of size 0 are the identity; the
+    Butterworth low and high passes sum to one, the low pass keeps DC."""
+    re, im = np.ones((4, 4), np.float32), np.zeros((4, 4), np.float32)
+    for kind in ("shift", "gaussian", "box"):
+        r, i = oracle.fourier_filter(re, im, [0.0], kind)
+        assert np.array_equal(r, re) and np.array_equal(i, im)
+    lp = oracle.butterworth_weights((9, 12), 0.2, False, 2.0).astype(np.float64)
+    hp = oracle.butterworth_weights((9, 12), 0.2, True, 2.0).astype(np.float64)
+    np.testing.assert_allclose(lp + hp, 1.0, atol=1e-7)
+    assert lp[0, 0] == 1.0
+
+
+def test_unsupervised_wiener_oracle_reference_case(oracle):
+    """crates/lucem-ops/src/restore/deconvolve.rs:551-575: the 8x8 spot blurred
+    by a 3x3 box, 12 iterations, burn-in 4, seed 7: a chain of 12 balances in
+    [1e-6, 1e3] and an 8x8 image; the chain depends on the seed."""
+    spot = np.full((8, 8), 0.1)
+    spot[4, 4] = 0.9
+    box = np.full((3, 3), 1.0 / 9.0)
+    blurred = oracle.correlate_nd(spot.astype(np.float32), box.astype(np.float32), mode="reflect")
+    out, chain = oracle.unsupervised_wiener(blurred, box, 12, 4, True, 7)
+    assert len(chain) == 12 and out.shape == (8, 8)
+    assert all(1e-6 <= b <= 1e3 for b in chain)
+    _, other = oracle.unsupervised_wiener(blurred, box, 12, 4, True, 8)
+    assert other != chain
