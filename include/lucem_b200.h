@@ -489,6 +489,60 @@ lucem_status lucem_unsupervised_wiener(lucem_ctx *ctx, const lucem_tensor *in, c
                                        const lucem_unsupervised_wiener_settings *settings, lucem_tensor *out,
                                        double *balance_chain, lucem_workspace *ws, void *stream);
 
+/* ---- Gaussian-consumer operators ------------------------------------------
+ * 2-D input (u8, u16 or f32), f32 outputs of its shape.  Each scale's three
+ * Hessian filters (Gaussian derivatives of orders (2,0), (1,1), (0,2),
+ * truncate 4) run from one staged tile in one launch of the fused family
+ * kernel, with the per-pixel tensor math in its epilogue; filters of radius
+ * above 32 take per-axis passes and the same math elementwise. */
+
+/* crates/lucem-ops/src/feature/structure.rs:16-54 hessian_matrix. */
+lucem_status lucem_hessian_matrix(lucem_ctx *ctx, const lucem_tensor *in, double sigma, int32_t mode, double cval,
+                                  lucem_tensor *hrr, lucem_tensor *hrc, lucem_tensor *hcc, lucem_workspace *ws,
+                                  void *stream);
+/* crates/lucem-ops/src/feature/structure.rs:57-83 hessian_det: H_rr H_cc - H_rc^2. */
+lucem_status lucem_hessian_det(lucem_ctx *ctx, const lucem_tensor *in, double sigma, int32_t mode, double cval,
+                               lucem_tensor *out, lucem_workspace *ws, void *stream);
+/* crates/lucem-ops/src/feature/structure.rs:86-97 hessian_eigvals: l1 >= l2. */
+lucem_status lucem_hessian_eigvals(lucem_ctx *ctx, const lucem_tensor *in, double sigma, int32_t mode, double cval,
+                                   lucem_tensor *eig1, lucem_tensor *eig2, lucem_workspace *ws, void *stream);
+/* crates/lucem-ops/src/feature/structure.rs:164-191 shape_index (Koenderink). */
+lucem_status lucem_shape_index(lucem_ctx *ctx, const lucem_tensor *in, double sigma, int32_t mode, double cval,
+                               lucem_tensor *out, lucem_workspace *ws, void *stream);
+/* crates/lucem-ops/src/feature/structure.rs:102-147 structure_tensor: Sobel
+ * gradients, their outer products and a Gaussian window of sigma.  Both
+ * gradients and the three products in one launch (into the workspace), then
+ * the three windows. */
+lucem_status lucem_structure_tensor(lucem_ctx *ctx, const lucem_tensor *in, double sigma, int32_t mode, double cval,
+                                    lucem_tensor *arr, lucem_tensor *arc, lucem_tensor *acc, lucem_workspace *ws,
+                                    void *stream);
+/* crates/lucem-ops/src/feature/structure.rs:150-161 structure_tensor_eigvals
+ * (f32 components in, l1 >= l2 out). */
+lucem_status lucem_structure_tensor_eigvals(const lucem_tensor *arr, const lucem_tensor *arc, const lucem_tensor *acc,
+                                            lucem_tensor *eig1, lucem_tensor *eig2, void *stream);
+
+/* crates/lucem-ops/src/filter/ridge.rs:13-40 RidgeFilter. */
+typedef struct lucem_ridge_settings {
+    const double *sigmas; int32_t n_sigmas; /* NULL: {1, 3, 5, 7, 9} */
+    int32_t black_ridges;                   /* 1: dark ridges on a bright background */
+    int32_t mode;                           /* lucem_pad_mode (reflect) */
+    double cval;
+    double beta;                            /* 0.5 (Frangi) */
+    double gamma;                           /* 15 (Frangi) */
+} lucem_ridge_settings;
+void lucem_ridge_settings_default(lucem_ridge_settings *s);
+/* crates/lucem-ops/src/filter/ridge.rs:87-133 frangi_into: per scale the
+ * Hessian eigenvalues, the vesselness and the running maximum, in the
+ * scale's one launch. */
+lucem_status lucem_frangi(lucem_ctx *ctx, const lucem_tensor *in, const lucem_ridge_settings *settings,
+                          lucem_tensor *out, lucem_workspace *ws, void *stream);
+/* crates/lucem-ops/src/filter/ridge.rs:148-185 sato_into. */
+lucem_status lucem_sato(lucem_ctx *ctx, const lucem_tensor *in, const lucem_ridge_settings *settings,
+                        lucem_tensor *out, lucem_workspace *ws, void *stream);
+/* crates/lucem-ops/src/filter/ridge.rs:199-235 meijering_into. */
+lucem_status lucem_meijering(lucem_ctx *ctx, const lucem_tensor *in, const lucem_ridge_settings *settings,
+                             lucem_tensor *out, lucem_workspace *ws, void *stream);
+
 /* The grid lucem_richardson_lucy uses (host only), before any autotuning of
  * the context: per axis the requested length, or the cheapest m * 2^k
  * (m in {1,3,5,7,9,15,21,25,27}) at least the padding's need, by length

@@ -74,6 +74,11 @@ class PhaseCorrelationResult(C.Structure):
     _fields_ = [("shift", C.c_double * MAX_DIMS), ("error", C.c_double), ("phasediff", C.c_double)]
 
 
+class RidgeSettings(C.Structure):
+    _fields_ = [("sigmas", C.POINTER(C.c_double)), ("n_sigmas", C.c_int32), ("black_ridges", C.c_int32),
+                ("mode", C.c_int32), ("cval", C.c_double), ("beta", C.c_double), ("gamma", C.c_double)]
+
+
 class UnsupervisedWienerSettings(C.Structure):
     _fields_ = [("num_iter", C.c_int64), ("burnin", C.c_int64), ("clip", C.c_int32), ("seed", C.c_uint64)]
 
@@ -109,6 +114,16 @@ SIGNATURES = {
     "lucem_phase_correlation_settings_default": (None, [C.POINTER(PhaseCorrelationSettings)]),
     "lucem_phase_correlation": (I32, [P, TP, TP, C.POINTER(PhaseCorrelationSettings),
                                       C.POINTER(PhaseCorrelationResult), P, P]),
+    "lucem_hessian_matrix": (I32, [P, TP, D, I32, D, TP, TP, TP, P, P]),
+    "lucem_hessian_det": (I32, [P, TP, D, I32, D, TP, P, P]),
+    "lucem_hessian_eigvals": (I32, [P, TP, D, I32, D, TP, TP, P, P]),
+    "lucem_shape_index": (I32, [P, TP, D, I32, D, TP, P, P]),
+    "lucem_structure_tensor": (I32, [P, TP, D, I32, D, TP, TP, TP, P, P]),
+    "lucem_structure_tensor_eigvals": (I32, [TP, TP, TP, TP, TP, P]),
+    "lucem_ridge_settings_default": (None, [C.POINTER(RidgeSettings)]),
+    "lucem_frangi": (I32, [P, TP, C.POINTER(RidgeSettings), TP, P, P]),
+    "lucem_sato": (I32, [P, TP, C.POINTER(RidgeSettings), TP, P, P]),
+    "lucem_meijering": (I32, [P, TP, C.POINTER(RidgeSettings), TP, P, P]),
     "lucem_unsupervised_wiener_settings_default": (None, [C.POINTER(UnsupervisedWienerSettings)]),
     "lucem_unsupervised_wiener": (I32, [P, TP, TP, C.POINTER(UnsupervisedWienerSettings), TP, DP, P, P]),
     "lucem_workspace_wait_status": (I32, [P, P, I64P]),

@@ -3499,3 +3499,337 @@ void gaussian_fused_params(FamParams *fp, const lucem_tensor *view, int mode, do
 lucem_status set_error(lucem_status st, const char *msg) { return fail(st, "%s", msg); }
 
 }  // namespace lucem
+
+// ---------------------------------------------------------------------------
+// Gaussian-consumer operators: Hessian, shape index, structure tensor and
+// the ridge filters (crates/lucem-ops/src/feature/structure.rs,
+// filter/ridge.rs).  Every scale's three Hessian filters run from one staged
+// tile in one launch of the fused family kernel, the per-pixel tensor math
+// (tensor_ops.cuh) in its epilogue; filters wider than the fused kernel take
+// the per-axis passes and the same math elementwise.
+
+namespace {
+
+// Outputs of one fused launch with a tensor epilogue (or none).
+struct TensorOuts {
+    float *o[3] = {nullptr, nullptr, nullptr};
+};
+
+lucem_status check_2d(const char *op, const lucem_tensor *in) {
+    if (in->ndim != 2)
+        return fail(LUCEM_ERR_INVALID_DIMENSION, "%s expects 2-D array, got %d-D shape %s", op, in->ndim,
+                    dims_str(in).c_str());
+    return ok();
+}
+
+lucem_status check_sigma(double sigma) {
+    // gaussian.rs:96-101 (the blurs these operators run).
+    if (!std::isfinite(sigma) || sigma < 0.0)
+        return fail(LUCEM_ERR_INVALID_PARAMETER,
+                    "invalid parameter `sigma`: sigma must be finite and non-negative, got %g", sigma);
+    return ok();
+}
+
+// The three Hessian filters of one scale, orders (2,0), (1,1), (0,2) at
+// sigma (structure.rs:26-51): written as (a, b, c) into outs when tensor is
+// kTensorNone, else through the epilogue `tensor` into outs.
+lucem_status hessian_scale(lucem_ctx *ctx, const lucem_tensor *in, double sigma, int mode, double cval, int tensor,
+                           float p0, float p1, int black, int first, const TensorOuts &outs, lucem_workspace *ws,
+                           void *stream) {
+    const int64_t n = numel(in), H = in->dims[0], W = in->dims[1];
+    if (n == 0) return ok();
+    const int64_t r = sigma > 0.0 ? (int64_t)radius_of(4.0, sigma) : 0;
+    const uint32_t ords[3][2] = {{2, 0}, {1, 1}, {0, 2}};
+    if (r <= kFamMaxRadius && H < (1 << 30) && W < (1 << 30)) {
+        FamParams fp;
+        init_fam(&fp, in, mode, cval, 1.0);
+        fp.n_filters = 3;
+        for (int f = 0; f < 3; ++f) {
+            Pass a{0, sigma, ords[f][0], r}, b{1, sigma, ords[f][1], r};
+            // sigma 0: the reference drops the axis (a copy, orders ignored).
+            fill_filter_taps(&fp, f, sigma > 0.0 ? &a : nullptr, sigma > 0.0 ? &b : nullptr);
+            fp.rmax0 = std::max(fp.rmax0, fp.r0[f]);
+            fp.rmax1 = std::max(fp.rmax1, fp.r1[f]);
+        }
+        fp.n_outputs = 3;
+        for (int k = 0; k < 3; ++k) {
+            FamOutput &o = fp.outs[k];
+            o.out = outs.o[k];
+            o.plane_stride = H * W;
+            o.row_pitch = W;
+            o.combine = (int)Combine::kLinear;
+            o.fa = k;
+            o.fb = -1;
+            o.alpha = 1.0f;
+        }
+        fp.tensor = tensor;
+        fp.tensor_black = black;
+        fp.tensor_first = first;
+        fp.tensor_p0 = p0;
+        fp.tensor_p1 = p1;
+        if (lucem_status st = fam_waits(ws, &fp, stream)) return st;
+        int e = timed(kPassFamily, stream, [&] { return launch_family_planes(fp, in->dtype, stream); });
+        return e ? cuda_fail(e, "hessian family launch") : ok();
+    }
+    // Wider filters: the components by the per-axis passes, then the epilogue.
+    float *comp[3] = {outs.o[0], outs.o[1], outs.o[2]};
+    if (tensor != kTensorNone) {
+        if (!ws) return fail(LUCEM_ERR_INVALID_HANDLE, "a workspace is required");
+        const char *names[3] = {"hessian_a", "hessian_b", "hessian_c"};
+        for (int k = 0; k < 3; ++k) {
+            void *p = nullptr;
+            if (lucem_status st = ws->get(names[k], (size_t)n * sizeof(float), &p)) return st;
+            comp[k] = static_cast<float *>(p);
+        }
+    }
+    for (int f = 0; f < 3; ++f) {
+        std::vector<Pass> passes = {Pass{0, sigma, ords[f][0], r}, Pass{1, sigma, ords[f][1], r}};
+        if (lucem_status st = run_passes(ctx, in, passes, mode, cval, 1.0, comp[f], ws, stream)) return st;
+    }
+    if (tensor == kTensorNone) return ok();
+    int e = timed(kPassElementwise, stream, [&] {
+        return launch_tensor_elementwise(comp[0], comp[1], comp[2], outs.o[0], outs.o[1], outs.o[2], n, tensor, p0, p1,
+                                         black, first, stream);
+    });
+    return e ? cuda_fail(e, "tensor epilogue launch") : ok();
+}
+
+// Checks of the single-scale Hessian operators: 2-D input, f32 outputs of
+// its shape, none aliasing the input or another output.
+lucem_status check_hessian_io(const char *op, const lucem_tensor *in, double sigma, int32_t mode,
+                              std::initializer_list<const lucem_tensor *> outs) {
+    lucem_status st;
+    if ((st = check_tensor("input", in))) return st;
+    if ((st = check_2d(op, in)) || (st = check_mode(mode)) || (st = check_sigma(sigma))) return st;
+    for (const lucem_tensor *o : outs) {
+        if ((st = check_tensor("output", o)) || (st = same_shape("input", in, "output", o)) ||
+            (st = not_aliased(in, o)) || (st = require_f32_out(o)))
+            return st;
+        for (const lucem_tensor *o2 : outs)
+            if (o2 != o && (st = not_aliased(o, o2))) return st;
+    }
+    return ok();
+}
+
+}  // namespace
+
+extern "C" {
+
+// structure.rs:16-54.
+lucem_status lucem_hessian_matrix(lucem_ctx *ctx, const lucem_tensor *in, double sigma, int32_t mode, double cval,
+                                  lucem_tensor *hrr, lucem_tensor *hrc, lucem_tensor *hcc, lucem_workspace *ws,
+                                  void *stream) {
+    TimerScope timer_scope(ws);
+    if (!ctx) return fail(LUCEM_ERR_INVALID_HANDLE, "null context");
+    lucem_status st;
+    if ((st = check_hessian_io("hessian_matrix", in, sigma, mode, {hrr, hrc, hcc}))) return st;
+    TensorOuts o;
+    o.o[0] = static_cast<float *>(hrr->data);
+    o.o[1] = static_cast<float *>(hrc->data);
+    o.o[2] = static_cast<float *>(hcc->data);
+    return hessian_scale(ctx, in, sigma, mode, cval, kTensorNone, 0.f, 0.f, 0, 1, o, ws, stream);
+}
+
+// structure.rs:57-83.
+lucem_status lucem_hessian_det(lucem_ctx *ctx, const lucem_tensor *in, double sigma, int32_t mode, double cval,
+                               lucem_tensor *out, lucem_workspace *ws, void *stream) {
+    TimerScope timer_scope(ws);
+    if (!ctx) return fail(LUCEM_ERR_INVALID_HANDLE, "null context");
+    lucem_status st;
+    if ((st = check_hessian_io("hessian_matrix", in, sigma, mode, {out}))) return st;
+    TensorOuts o;
+    o.o[0] = static_cast<float *>(out->data);
+    return hessian_scale(ctx, in, sigma, mode, cval, kTensorDet, 0.f, 0.f, 0, 1, o, ws, stream);
+}
+
+// structure.rs:86-97.
+lucem_status lucem_hessian_eigvals(lucem_ctx *ctx, const lucem_tensor *in, double sigma, int32_t mode, double cval,
+                                   lucem_tensor *eig1, lucem_tensor *eig2, lucem_workspace *ws, void *stream) {
+    TimerScope timer_scope(ws);
+    if (!ctx) return fail(LUCEM_ERR_INVALID_HANDLE, "null context");
+    lucem_status st;
+    if ((st = check_hessian_io("hessian_matrix", in, sigma, mode, {eig1, eig2}))) return st;
+    TensorOuts o;
+    o.o[0] = static_cast<float *>(eig1->data);
+    o.o[1] = static_cast<float *>(eig2->data);
+    return hessian_scale(ctx, in, sigma, mode, cval, kTensorEigvals, 0.f, 0.f, 0, 1, o, ws, stream);
+}
+
+// structure.rs:164-191.
+lucem_status lucem_shape_index(lucem_ctx *ctx, const lucem_tensor *in, double sigma, int32_t mode, double cval,
+                               lucem_tensor *out, lucem_workspace *ws, void *stream) {
+    TimerScope timer_scope(ws);
+    if (!ctx) return fail(LUCEM_ERR_INVALID_HANDLE, "null context");
+    lucem_status st;
+    if ((st = check_hessian_io("hessian_matrix", in, sigma, mode, {out}))) return st;
+    TensorOuts o;
+    o.o[0] = static_cast<float *>(out->data);
+    return hessian_scale(ctx, in, sigma, mode, cval, kTensorShapeIndex, 0.f, 0.f, 0, 1, o, ws, stream);
+}
+
+// structure.rs:102-147: Sobel gradients (gradient.rs:71-107: [-1, 0, 1] along
+// the derivative axis, [1, 2, 1] across), their outer products, each
+// smoothed by the Gaussian window.  Here: both gradients and the three
+// products in one fused launch (into the workspace), then the three planes'
+// Gaussian blurs.
+lucem_status lucem_structure_tensor(lucem_ctx *ctx, const lucem_tensor *in, double sigma, int32_t mode, double cval,
+                                    lucem_tensor *arr, lucem_tensor *arc, lucem_tensor *acc, lucem_workspace *ws,
+                                    void *stream) {
+    TimerScope timer_scope(ws);
+    if (!ctx) return fail(LUCEM_ERR_INVALID_HANDLE, "null context");
+    if (!ws) return fail(LUCEM_ERR_INVALID_HANDLE, "a workspace is required");
+    lucem_status st;
+    if ((st = check_hessian_io("structure_tensor", in, sigma, mode, {arr, arc, acc}))) return st;
+    const int64_t n = numel(in), H = in->dims[0], W = in->dims[1];
+    if (n == 0) return ok();
+    if (H >= (1 << 30) || W >= (1 << 30))
+        return fail(LUCEM_ERR_TOO_MANY_ELEMENTS, "structure_tensor: a side of 2^30 or more");
+    void *prods = nullptr;
+    if ((st = ws->get("structure_products", (size_t)3 * n * sizeof(float), &prods))) return st;
+    float *P = static_cast<float *>(prods);
+    FamParams fp;
+    init_fam(&fp, in, mode, cval, 1.0);
+    fp.n_filters = 2;
+    const float deriv[3] = {-1.0f, 0.0f, 1.0f}, smooth[3] = {1.0f, 2.0f, 1.0f};
+    for (int f = 0; f < 2; ++f) {
+        std::memset(fp.taps0[f], 0, sizeof fp.taps0[f]);
+        std::memset(fp.taps1[f], 0, sizeof fp.taps1[f]);
+        // Kernel radius 2 (the fused kernel's even radii): taps at 1..3.
+        const float *t0 = f == 0 ? deriv : smooth, *t1 = f == 0 ? smooth : deriv;
+        for (int i = 0; i < 3; ++i) {
+            fp.taps0[f][i + 1] = float2_{t0[i], t0[i]};
+            fp.taps1[f][i + 1] = float2_{t1[i], t1[i]};
+        }
+        fp.r0[f] = fp.r1[f] = fam_kernel_radius(1);
+    }
+    fp.rmax0 = fp.rmax1 = fam_kernel_radius(1);
+    fp.n_outputs = 3;
+    for (int k = 0; k < 3; ++k) {
+        FamOutput &o = fp.outs[k];
+        o.out = P + (size_t)k * n;
+        o.plane_stride = n;
+        o.row_pitch = W;
+        o.combine = (int)Combine::kLinear;
+        o.fa = k < 2 ? k : -1;
+        o.fb = -1;
+        o.alpha = 1.0f;
+    }
+    fp.tensor = kTensorOuter;
+    if ((st = fam_waits(ws, &fp, stream))) return st;
+    int e = timed(kPassFamily, stream, [&] { return launch_family_planes(fp, in->dtype, stream); });
+    if (e) return cuda_fail(e, "structure tensor gradient launch");
+    // The Gaussian window over each product (gaussian_blur_into, orders 0).
+    const int64_t r = sigma > 0.0 ? (int64_t)radius_of(4.0, sigma) : 0;
+    std::vector<Pass> passes;
+    if (sigma > 0.0) passes = {Pass{0, sigma, 0, r}, Pass{1, sigma, 0, r}};
+    lucem_tensor* outs[3] = {arr, arc, acc};
+    for (int k = 0; k < 3; ++k) {
+        lucem_tensor view = *in;
+        view.data = P + (size_t)k * n;
+        view.dtype = LUCEM_F32;
+        if ((st = run_passes(ctx, &view, passes, mode, cval, 1.0, static_cast<float *>(outs[k]->data), ws, stream)))
+            return st;
+    }
+    return ok();
+}
+
+// structure.rs:150-161 (symmetric_eigenvalues_2x2_into, core/eigen.rs).
+lucem_status lucem_structure_tensor_eigvals(const lucem_tensor *arr, const lucem_tensor *arc, const lucem_tensor *acc,
+                                            lucem_tensor *eig1, lucem_tensor *eig2, void *stream) {
+    lucem_status st;
+    const lucem_tensor *ins[3] = {arr, arc, acc};
+    for (const lucem_tensor *t : ins)
+        if ((st = check_tensor("input", t))) return st;
+    if ((st = check_tensor("eig1", eig1)) || (st = check_tensor("eig2", eig2))) return st;
+    for (const lucem_tensor *t : {arc, acc, (const lucem_tensor *)eig1, (const lucem_tensor *)eig2})
+        if ((st = same_shape("arr", arr, "other", t))) return st;
+    for (const lucem_tensor *t : {arr, arc, acc, (const lucem_tensor *)eig1, (const lucem_tensor *)eig2})
+        if (t->dtype != LUCEM_F32) return fail(LUCEM_ERR_UNSUPPORTED_DTYPE, "structure_tensor_eigvals takes f32 arrays");
+    for (const lucem_tensor *t : ins)
+        if ((st = not_aliased(t, eig1)) || (st = not_aliased(t, eig2))) return st;
+    if ((st = not_aliased(eig1, eig2))) return st;
+    const int64_t n = numel(arr);
+    int e = launch_tensor_elementwise(static_cast<const float *>(arr->data), static_cast<const float *>(arc->data),
+                                      static_cast<const float *>(acc->data), static_cast<float *>(eig1->data),
+                                      static_cast<float *>(eig2->data), nullptr, n, kTensorEigvals, 0.f, 0.f, 0, 1,
+                                      stream);
+    return e ? cuda_fail(e, "eigenvalue launch") : ok();
+}
+
+void lucem_ridge_settings_default(lucem_ridge_settings *s) {
+    s->sigmas = nullptr;
+    s->n_sigmas = 0;
+    s->black_ridges = 1;
+    s->mode = LUCEM_PAD_REFLECT;
+    s->cval = 0.0;
+    s->beta = 0.5;
+    s->gamma = 15.0;
+}
+
+}  // extern "C"
+
+namespace {
+
+// frangi_into / sato_into / meijering_into (ridge.rs:87-245): per scale the
+// Hessian eigenvalues and the scale's response folded into the running
+// maximum, all in the scale's one fused launch.
+lucem_status ridge_filter(lucem_ctx *ctx, const char *op, int tensor, const lucem_tensor *in,
+                          const lucem_ridge_settings *settings, lucem_tensor *out, lucem_workspace *ws, void *stream) {
+    TimerScope timer_scope(ws);
+    if (!ctx) return fail(LUCEM_ERR_INVALID_HANDLE, "null context");
+    lucem_ridge_settings def;
+    lucem_ridge_settings_default(&def);
+    const lucem_ridge_settings *s = settings ? settings : &def;
+    static const double kDefaultSigmas[5] = {1.0, 3.0, 5.0, 7.0, 9.0};
+    const double *sig = s->sigmas ? s->sigmas : kDefaultSigmas;
+    const int ns = s->sigmas ? s->n_sigmas : 5;
+    lucem_status st;
+    if ((st = check_tensor("input", in)) || (st = check_tensor("output", out))) return st;
+    if ((st = check_2d(op, in)) || (st = same_shape("input", in, "output", out)) || (st = not_aliased(in, out)))
+        return st;
+    if ((st = require_f32_out(out)) || (st = check_mode(s->mode))) return st;
+    if (tensor == kTensorFrangi && ns <= 0)
+        return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `sigmas`: at least one sigma scale is required");
+    for (int i = 0; i < ns; ++i)
+        if ((st = check_sigma(sig[i]))) return st;
+    const int64_t n = numel(in);
+    if (n == 0) return ok();
+    if (ns <= 0) {
+        // The output starts at zero (ridge.rs:165-166) and no scale raises it.
+        CUDA_TRY(cudaMemsetAsync(out->data, 0, (size_t)n * sizeof(float), static_cast<cudaStream_t>(stream)), "fill");
+        return ok();
+    }
+    const float p1 = (float)(1.0 / (2.0 * std::max(s->gamma * s->gamma, 1e-12)));
+    TensorOuts o;
+    o.o[0] = static_cast<float *>(out->data);
+    for (int i = 0; i < ns; ++i) {
+        float p0 = 0.0f;
+        if (tensor == kTensorFrangi) p0 = (float)(1.0 / (2.0 * std::max(s->beta * s->beta, 1e-12)));
+        if (tensor == kTensorSato) p0 = (float)(sig[i] * sig[i]);
+        if ((st = hessian_scale(ctx, in, sig[i], s->mode, s->cval, tensor, p0, p1, s->black_ridges ? 1 : 0,
+                                i == 0 ? 1 : 0, o, ws, stream)))
+            return st;
+    }
+    return ok();
+}
+
+}  // namespace
+
+extern "C" {
+
+lucem_status lucem_frangi(lucem_ctx *ctx, const lucem_tensor *in, const lucem_ridge_settings *settings,
+                          lucem_tensor *out, lucem_workspace *ws, void *stream) {
+    return ridge_filter(ctx, "frangi", kTensorFrangi, in, settings, out, ws, stream);
+}
+
+lucem_status lucem_sato(lucem_ctx *ctx, const lucem_tensor *in, const lucem_ridge_settings *settings,
+                        lucem_tensor *out, lucem_workspace *ws, void *stream) {
+    return ridge_filter(ctx, "sato", kTensorSato, in, settings, out, ws, stream);
+}
+
+lucem_status lucem_meijering(lucem_ctx *ctx, const lucem_tensor *in, const lucem_ridge_settings *settings,
+                             lucem_tensor *out, lucem_workspace *ws, void *stream) {
+    return ridge_filter(ctx, "meijering", kTensorMeijering, in, settings, out, ws, stream);
+}
+
+}  // extern "C"

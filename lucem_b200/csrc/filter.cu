@@ -325,6 +325,31 @@ int launch_adjoint_fold(const float *g, float scale, float *out, int64_t outer, 
     return (int)cudaGetLastError();
 }
 
+namespace {
+// The tensor epilogue (tensor_ops.cuh) over stored components: the path of
+// filters too wide for the fused kernel, and structure_tensor_eigvals.
+__global__ void tensor_elementwise_kernel(const float *__restrict__ a, const float *__restrict__ b,
+                                          const float *__restrict__ c, float *o0, float *o1, float *o2, int64_t n,
+                                          int mode, float p0, float p1, int black, int first) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float prev = first ? 0.0f : o0[i];
+        float v0, v1 = 0.0f, v2 = 0.0f;
+        const int k = tens::apply(mode, a[i], b[i], c ? c[i] : 0.0f, prev, p0, p1, black != 0, &v0, &v1, &v2);
+        o0[i] = v0;
+        if (k > 1) o1[i] = v1;
+        if (k > 2) o2[i] = v2;
+    }
+}
+}  // namespace
+
+int launch_tensor_elementwise(const float *a, const float *b, const float *c, float *o0, float *o1, float *o2,
+                              int64_t n, int mode, float p0, float p1, int black, int first, void *stream) {
+    if (n == 0) return 0;
+    tensor_elementwise_kernel<<<ew_grid(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(a, b, c, o0, o1, o2, n,
+                                                                                          mode, p0, p1, black, first);
+    return (int)cudaGetLastError();
+}
+
 int launch_linear_comb(const float *a, const float *b, float *out, int64_t n, float alpha,
                        float beta, float bias, void *stream) {
     if (n == 0) return 0;

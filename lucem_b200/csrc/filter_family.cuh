@@ -11,6 +11,7 @@
 #include <cstdint>
 
 #include "internal.h"
+#include "tensor_ops.cuh"
 
 namespace lucem {
 namespace famk {
@@ -188,6 +189,64 @@ __device__ __forceinline__ void hpass_r(int R, const float *IT, int x0, int yp, 
     }
 }
 
+// Eight consecutive outputs of row y from column x of a tile (two 16-byte
+// stores where aligned and inside the tile).
+__device__ __forceinline__ void store_row8(float *obase, int64_t opitch, const TileGeom &g, int y, int x,
+                                           const float *v) {
+    float *dst = obase + (int64_t)(g.oy + y) * opitch + g.ox + x;
+    if ((x + 8 <= g.tw) && ((reinterpret_cast<uintptr_t>(dst) & 15) == 0)) {
+        reinterpret_cast<float4 *>(dst)[0] = make_float4(v[0], v[1], v[2], v[3]);
+        reinterpret_cast<float4 *>(dst)[1] = make_float4(v[4], v[5], v[6], v[7]);
+    } else {
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+            if (x + j < g.tw) dst[j] = v[j];
+    }
+}
+
+// Tensor epilogue: the first three filters' responses per pixel through
+// tens::apply into outs[0..2] (the ridge modes read their running maximum
+// from outs[0] first, unless tensor_first).
+template <int NOUT>
+__device__ __forceinline__ void tensor_epilogue(const FamParams &p, const TileGeom &g, const float2 (&acc)[NOUT][8],
+                                                int yp, int xc) {
+    float *ob[3];
+    int64_t op[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        ob[k] = g.out ? g.out : p.outs[k].out + (int64_t)g.plane * p.outs[k].plane_stride;
+        op[k] = g.out ? g.out_pitch : p.outs[k].row_pitch;
+    }
+    const bool ridge = p.tensor >= kTensorFrangi && p.tensor <= kTensorMeijering;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int y = 2 * yp + h, x = xc * 8;
+        if (y >= g.th) continue;
+        float prev[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) prev[j] = 0.0f;
+        if (ridge && !p.tensor_first) {
+            const float *src = ob[0] + (int64_t)(g.oy + y) * op[0] + g.ox + x;
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+                if (x + j < g.tw) prev[j] = src[j];
+        }
+        float v0[8], v1[8], v2[8];
+        int nout = 1;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const float a = h ? acc[0][j].y : acc[0][j].x;
+            const float b = h ? acc[1][j].y : acc[1][j].x;
+            const float c = h ? acc[2][j].y : acc[2][j].x;
+            nout = tens::apply(p.tensor, a, b, c, prev[j], p.tensor_p0, p.tensor_p1, p.tensor_black != 0, &v0[j],
+                               &v1[j], &v2[j]);
+        }
+        store_row8(ob[0], op[0], g, y, x, v0);
+        if (nout > 1) store_row8(ob[1], op[1], g, y, x, v1);
+        if (nout > 2) store_row8(ob[2], op[2], g, y, x, v2);
+    }
+}
+
 // One 64 x 64 output tile: stage tile + halo (cast fused), then per filter
 // the axis-0 pass into IT and the axis-1 pass into registers, folded into
 // every response that uses the filter; responses written once at the end.
@@ -348,6 +407,12 @@ __device__ void family_tile(const FamParams &p, const TileGeom &g, float *A, flo
         __syncthreads();  // IT is rewritten by the next filter
     }
 
+    if constexpr (NOUT >= 3) {
+        if (p.tensor != kTensorNone) {
+            tensor_epilogue<NOUT>(p, g, acc, yp, xc);
+            return;
+        }
+    }
     // Epilogue: bias / sqrt, then two 32-byte row segments per thread.
 #pragma unroll
     for (int k = 0; k < NOUT; ++k) {

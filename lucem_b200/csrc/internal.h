@@ -46,6 +46,19 @@ struct FamOutput {
     // fa or fb == -2 names the input sample itself (unsharp).
 };
 
+// Epilogue modes of FamParams::tensor (tensor_ops.cuh); 0: none, the
+// linear outputs.
+enum TensorMode : int32_t {
+    kTensorNone = 0,
+    kTensorDet = 1,        // out0 = a c - b^2
+    kTensorEigvals = 2,    // out0 = l1, out1 = l2 (l1 >= l2)
+    kTensorShapeIndex = 3, // out0 = shape index of (l1, l2)
+    kTensorFrangi = 4,     // out0 = max(out0, frangi(l1, l2)); p0 = 1/(2 beta^2), p1 = 1/(2 c^2)
+    kTensorSato = 5,       // out0 = max(out0, sato(l1 sigma^2, l2 sigma^2)); p0 = sigma^2
+    kTensorMeijering = 6,  // out0 = max(out0, meijering(l1, l2))
+    kTensorOuter = 7,      // (a, b) = (g_r, g_c): out0 = a a, out1 = a b, out2 = b b
+};
+
 // One launch of the fused 2-D family kernel over B planes of [H, W] (or over
 // work items of a slide, see FamWork).
 struct FamParams {
@@ -71,6 +84,13 @@ struct FamParams {
     // polling), count each give-up in *wait_status (may be null).
     int32_t *wait_status;
     int64_t wait_ns;
+    // Tensor epilogue (tensor_ops.cuh TensorMode; 0: none): the first three
+    // filters' responses (a, b, c) are combined per pixel into outs[0..2]
+    // instead of the linear outputs.  tensor_black: the ridge modes' dark
+    // ridges; tensor_first: the ridge modes start their running maximum at 0
+    // instead of reading the output.
+    int32_t tensor, tensor_black, tensor_first;
+    float tensor_p0, tensor_p1;
 };
 
 // One tile of a batched walk: the read box of one channel and the owned box
@@ -125,6 +145,11 @@ int launch_sqrt_scale(const float *acc, float *out, int64_t n, float scale, void
 // out = (float)in * scale (u8/u16/f32 -> f32)
 int launch_cast(const void *in, int in_dtype, float scale, float *out, int64_t n, void *stream);
 int launch_fill(float *out, int64_t n, float v, void *stream);
+// tens::apply (tensor_ops.cuh) per element: (a, b, c) -> o0 (o1, o2), mode a
+// TensorMode; c may be null (outer products); first: the ridge modes'
+// running maximum starts at 0 instead of o0.
+int launch_tensor_elementwise(const float *a, const float *b, const float *c, float *o0, float *o1, float *o2,
+                              int64_t n, int mode, float p0, float p1, int black, int first, void *stream);
 
 // ---- Gaussian planning shared by the entry points (api.cpp) ---------------
 

@@ -31,7 +31,9 @@ __all__ = [
     "fft_convolve_backward", "RlBatch", "richardson_lucy_batch", "autotune_fft", "autotune_query",
     "autotune_save", "autotune_load", "Graph", "gaussian_batch", "fft_nd", "fft_1d", "complex_mul",
     "wiener_deconvolve", "from_dlpack", "fourier_gaussian", "fourier_box", "fourier_shift", "butterworth",
-    "PhaseCorrelationResult", "phase_correlation", "unsupervised_wiener",
+    "PhaseCorrelationResult", "phase_correlation", "unsupervised_wiener", "hessian_matrix", "hessian_det",
+    "hessian_eigvals", "shape_index", "structure_tensor", "structure_tensor_eigvals", "frangi", "sato",
+    "meijering",
 ]
 
 
@@ -680,6 +682,111 @@ def fft_convolve_backward(x: torch.Tensor, psf: torch.Tensor, grad_out: torch.Te
     N.check(N.lib().lucem_fft_convolve_backward(ctx.handle, C.byref(ti), C.byref(tp), PadMode.CONSTANT,
                                                 _grid_arg(grid), C.byref(tg), tgx, tgp, ws.handle, _stream(x)))
     return gp, gx
+
+
+# ---------------------------------------------------------------------------
+# Gaussian-consumer operators (crates/lucem-ops/src/feature/structure.rs,
+# filter/ridge.rs): each scale's Hessian filters in one fused launch.
+
+
+def _empty_f32(x, n):
+    return [torch.empty(x.shape, dtype=torch.float32, device=x.device) for _ in range(n)]
+
+
+def _hessian_call(fn, x, sigma, mode, cval, outs, workspace):
+    ctx, ws = _ctx_ws(x, workspace)
+    ts = [_tensor(o, "output") for o in outs]
+    ti = _tensor(x, "input")
+    N.check(fn(ctx.handle, C.byref(ti), float(sigma), PadMode.parse(mode), float(cval), *[C.byref(t) for t in ts],
+               ws.handle, _stream(x)))
+    return outs
+
+
+@_dlpack_args
+def hessian_matrix(x: torch.Tensor, sigma: float, mode="reflect", cval: float = 0.0, *,
+                   workspace: Optional[Workspace] = None):
+    """hessian_matrix (crates/lucem-ops/src/feature/structure.rs:16-54): the
+    2-D Gaussian Hessian (H_rr, H_rc, H_cc) at scale sigma."""
+    return tuple(_hessian_call(N.lib().lucem_hessian_matrix, x, sigma, mode, cval, _empty_f32(x, 3), workspace))
+
+
+@_dlpack_args
+def hessian_det(x: torch.Tensor, sigma: float, mode="reflect", cval: float = 0.0, *,
+                workspace: Optional[Workspace] = None) -> torch.Tensor:
+    """hessian_det (feature/structure.rs:57-83): H_rr H_cc - H_rc^2."""
+    return _hessian_call(N.lib().lucem_hessian_det, x, sigma, mode, cval, _empty_f32(x, 1), workspace)[0]
+
+
+@_dlpack_args
+def hessian_eigvals(x: torch.Tensor, sigma: float, mode="reflect", cval: float = 0.0, *,
+                    workspace: Optional[Workspace] = None):
+    """hessian_eigvals (feature/structure.rs:86-97): (l1 >= l2)."""
+    return tuple(_hessian_call(N.lib().lucem_hessian_eigvals, x, sigma, mode, cval, _empty_f32(x, 2), workspace))
+
+
+@_dlpack_args
+def shape_index(x: torch.Tensor, sigma: float, mode="reflect", cval: float = 0.0, *,
+                workspace: Optional[Workspace] = None) -> torch.Tensor:
+    """shape_index (feature/structure.rs:164-191): Koenderink's shape index in
+    [-1, 1] from the Hessian eigenvalues."""
+    return _hessian_call(N.lib().lucem_shape_index, x, sigma, mode, cval, _empty_f32(x, 1), workspace)[0]
+
+
+@_dlpack_args
+def structure_tensor(x: torch.Tensor, sigma: float, mode="reflect", cval: float = 0.0, *,
+                     workspace: Optional[Workspace] = None):
+    """structure_tensor (feature/structure.rs:102-147): (A_rr, A_rc, A_cc),
+    the Gaussian-windowed outer products of the Sobel gradients."""
+    return tuple(_hessian_call(N.lib().lucem_structure_tensor, x, sigma, mode, cval, _empty_f32(x, 3), workspace))
+
+
+def structure_tensor_eigvals(arr, arc, acc):
+    """structure_tensor_eigvals (feature/structure.rs:150-161): (l1 >= l2)."""
+    arr, arc, acc = (from_dlpack(t) for t in (arr, arc, acc))
+    e1, e2 = _empty_f32(arr, 2)
+    ts = [_tensor(t, n) for t, n in ((arr, "arr"), (arc, "arc"), (acc, "acc"), (e1, "eig1"), (e2, "eig2"))]
+    N.check(N.lib().lucem_structure_tensor_eigvals(*[C.byref(t) for t in ts], _stream(arr)))
+    return e1, e2
+
+
+def _ridge(fn, x, sigmas, black_ridges, mode, cval, beta, gamma, out, workspace):
+    ctx, ws = _ctx_ws(x, workspace)
+    out = _out_like(x, out)
+    s = N.RidgeSettings()
+    N.lib().lucem_ridge_settings_default(C.byref(s))
+    if sigmas is not None:
+        arr, n = _doubles(sigmas)
+        s.sigmas, s.n_sigmas = C.cast(arr, C.POINTER(C.c_double)), n
+    s.black_ridges, s.mode, s.cval = int(bool(black_ridges)), PadMode.parse(mode), float(cval)
+    s.beta, s.gamma = float(beta), float(gamma)
+    ti, to = _tensor(x, "input"), _tensor(out, "output")
+    N.check(fn(ctx.handle, C.byref(ti), C.byref(s), C.byref(to), ws.handle, _stream(x)))
+    return out
+
+
+@_dlpack_args
+def frangi(x: torch.Tensor, sigmas=(1.0, 3.0, 5.0, 7.0, 9.0), *, black_ridges: bool = True, mode="reflect",
+           cval: float = 0.0, beta: float = 0.5, gamma: float = 15.0, out: Optional[torch.Tensor] = None,
+           workspace: Optional[Workspace] = None) -> torch.Tensor:
+    """frangi (crates/lucem-ops/src/filter/ridge.rs:87-145): multi-scale
+    vesselness, the maximum over the scales."""
+    return _ridge(N.lib().lucem_frangi, x, sigmas, black_ridges, mode, cval, beta, gamma, out, workspace)
+
+
+@_dlpack_args
+def sato(x: torch.Tensor, sigmas=(1.0, 3.0, 5.0, 7.0, 9.0), *, black_ridges: bool = True, mode="reflect",
+         cval: float = 0.0, out: Optional[torch.Tensor] = None,
+         workspace: Optional[Workspace] = None) -> torch.Tensor:
+    """sato (filter/ridge.rs:148-196): multi-scale tubeness."""
+    return _ridge(N.lib().lucem_sato, x, sigmas, black_ridges, mode, cval, 0.5, 15.0, out, workspace)
+
+
+@_dlpack_args
+def meijering(x: torch.Tensor, sigmas=(1.0, 3.0, 5.0, 7.0, 9.0), *, black_ridges: bool = True, mode="reflect",
+              cval: float = 0.0, out: Optional[torch.Tensor] = None,
+              workspace: Optional[Workspace] = None) -> torch.Tensor:
+    """meijering (filter/ridge.rs:199-245): multi-scale neuriteness."""
+    return _ridge(N.lib().lucem_meijering, x, sigmas, black_ridges, mode, cval, 0.5, 15.0, out, workspace)
 
 
 # ---------------------------------------------------------------------------

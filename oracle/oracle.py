@@ -644,3 +644,104 @@ def unsupervised_wiener(img, psf, num_iter=30, burnin=10, clip=True, seed=0):
     m32 = mean.real.astype(np.float32).astype(np.float64) + 1j * mean.imag.astype(np.float32).astype(np.float64)
     out = np.fft.ifftn(m32).real
     return (np.clip(out, -1.0, 1.0) if clip else out), chain
+
+
+# ---------------------------------------------------------------------------
+# Gaussian-consumer operators (feature/structure.rs, filter/ridge.rs): the
+# f32 restatement of the filters above, then the per-pixel kernels in f32
+# with every operation rounded as the reference's CubeCL kernels.
+
+_F = np.float32
+
+
+def hessian_matrix(x, sigma, mode="reflect", cval=0.0):
+    """feature/structure.rs:16-54: Gaussian derivatives of orders (2,0),
+    (1,1), (0,2)."""
+    x = np.asarray(x, _F)
+    return tuple(gaussian_blur(x, [sigma, sigma], orders=o, mode=mode, cval=cval).astype(_F)
+                 for o in ((2, 0), (1, 1), (0, 2)))
+
+
+def eigvals_2x2(a, b, c):
+    """core/kernels/eigen.rs:13-33."""
+    a, b, c = (np.asarray(v, _F) for v in (a, b, c))
+    mean = (a + c) * _F(0.5)
+    diff = (a - c) * _F(0.5)
+    r = np.sqrt(diff * diff + b * b).astype(_F)
+    return mean + r, mean - r
+
+
+def hessian_det(x, sigma, mode="reflect", cval=0.0):
+    """feature/structure.rs:57-83 with hessian_det_2d_kernel."""
+    a, b, c = hessian_matrix(x, sigma, mode, cval)
+    return a * c - b * b
+
+
+def shape_index_of(l1, l2):
+    """shape_index_2d_kernel (feature/kernels/structure.rs:40-80), f32."""
+    l1, l2 = np.asarray(l1, _F), np.asarray(l2, _F)
+    diff, s = l1 - l2, l1 + l2
+    scale = np.abs(l1) + np.abs(l2)
+    flat = (np.abs(diff) <= _F(1e-6) * scale) | (scale <= _F(1e-20))
+    lim = np.where((s < 0) & (scale > _F(1e-20)), _F(1), np.where((s > 0) & (scale > _F(1e-20)), _F(-1), _F(0)))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        ratio = (-s) / np.where(flat, _F(1), diff)
+        ax = np.abs(ratio)
+        inv = ax > 1
+        z = np.where(inv, _F(1) / np.where(ax == 0, _F(1), ax), ax).astype(_F)
+    z2 = z * z
+    poly = _F(-0.085133) + z2 * _F(0.0208351)
+    poly = _F(0.180141) + z2 * poly
+    poly = _F(-0.3302995) + z2 * poly
+    poly = _F(0.999866) + z2 * poly
+    at = z * poly
+    ang = np.where(inv, _F(1.5707964) - at, at)
+    out = np.where(ratio < 0, -ang, ang) * _F(0.63661975)
+    return np.where(flat, lim, out).astype(_F)
+
+
+def shape_index(x, sigma, mode="reflect", cval=0.0):
+    """feature/structure.rs:164-191."""
+    return shape_index_of(*eigvals_2x2(*hessian_matrix(x, sigma, mode, cval)))
+
+
+def structure_tensor(x, sigma, mode="reflect", cval=0.0):
+    """feature/structure.rs:102-147: Sobel gradients by two correlate_1d
+    passes each (filter/gradient.rs:71-107), outer products, Gaussian window."""
+    x = np.asarray(x, _F)
+    d, sm = [-1.0, 0.0, 1.0], [1.0, 2.0, 1.0]
+    gy = correlate_1d(correlate_1d(x, d, 0, mode, cval), sm, 1, mode, cval).astype(_F)
+    gx = correlate_1d(correlate_1d(x, sm, 0, mode, cval), d, 1, mode, cval).astype(_F)
+    return tuple(gaussian_blur(p, [sigma, sigma], mode=mode, cval=cval).astype(_F)
+                 for p in (gy * gy, gy * gx, gx * gx))
+
+
+def ridge_filter(x, kind, sigmas=(1.0, 3.0, 5.0, 7.0, 9.0), black_ridges=True, mode="reflect", cval=0.0,
+                 beta=0.5, gamma=15.0):
+    """frangi_into / sato_into / meijering_into (filter/ridge.rs:87-245) with
+    the scale kernels of filter/kernels/ridge.rs:11-98, f32."""
+    out = np.zeros(np.shape(x), _F)
+    ib = _F(1.0 / (2.0 * max(beta * beta, 1e-12)))
+    ic = _F(1.0 / (2.0 * max(gamma * gamma, 1e-12)))
+    for sg in sigmas:
+        e1, e2 = eigvals_2x2(*hessian_matrix(x, sg, mode, cval))
+        if kind == "frangi":
+            le = np.abs(e1) <= np.abs(e2)
+            l1, l2 = np.where(le, e1, e2), np.where(le, e2, e1)
+            valid = l2 > 0 if black_ridges else l2 < 0
+            al2 = np.maximum(np.abs(l2), _F(1e-10))
+            rb = l1 / al2
+            s2 = l1 * l1 + l2 * l2
+            resp = (np.exp(_F(0) - rb * rb * ib) * (_F(1) - np.exp(_F(0) - s2 * ic))).astype(_F)
+            out = np.where(valid, np.maximum(out, resp), out)
+        elif kind == "sato":
+            ss = _F(sg * sg)
+            s1, s2 = e1 * ss, e2 * ss
+            l2 = np.where(np.abs(s1) <= np.abs(s2), s2, s1)
+            out = np.maximum(out, np.maximum(l2, _F(0)) if black_ridges else np.maximum(_F(0) - l2, _F(0)))
+        else:
+            third = _F(-1.0 / 3.0)
+            m1, m2 = e1 + third * e2, e2 + third * e1
+            dom = np.where(np.abs(m1) >= np.abs(m2), m1, m2)
+            out = np.maximum(out, np.maximum(dom, _F(0)) if black_ridges else np.maximum(_F(0) - dom, _F(0)))
+    return out.astype(_F)

@@ -292,3 +292,28 @@ def test_unsupervised_wiener_oracle_reference_case(oracle):
     assert all(1e-6 <= b <= 1e3 for b in chain)
     _, other = oracle.unsupervised_wiener(blurred, box, 12, 4, True, 8)
     assert other != chain
+
+
+def test_shape_index_oracle_distinguishes_dome_and_cup(oracle):
+    """crates/lucem-ops/src/feature/structure.rs:193-214: on 17x17 paraboloids,
+    sigma 1.5, nearest padding, the centre's shape index is +1 for a dome and
+    -1 for a cup within 2e-2."""
+    y, x = np.mgrid[0:17, 0:17]
+    r2 = ((y - 8.0) ** 2 + (x - 8.0) ** 2).astype(np.float32)
+    assert abs(oracle.shape_index(-r2, 1.5, "nearest")[8, 8] - 1.0) < 2e-2
+    assert abs(oracle.shape_index(r2, 1.5, "nearest")[8, 8] + 1.0) < 2e-2
+
+
+def test_structure_and_ridge_oracle_properties(oracle):
+    """The structure tensor of a linear ramp is constant away from the borders
+    (gradient outer products of a constant gradient); the ridge filters of a
+    constant image are zero (a zero Hessian)."""
+    y, x = np.mgrid[0:24, 0:24].astype(np.float32)
+    arr, arc, acc = oracle.structure_tensor(2.0 * y + 3.0 * x, 1.0, "nearest")
+    # Sobel of 2y + 3x: g_r = 2 * 2 * 4 = 16, g_c = 3 * 2 * 4 = 24 inside.
+    np.testing.assert_allclose(arr[8:16, 8:16], 256.0, rtol=1e-6)
+    np.testing.assert_allclose(arc[8:16, 8:16], 384.0, rtol=1e-6)
+    np.testing.assert_allclose(acc[8:16, 8:16], 576.0, rtol=1e-6)
+    const = np.full((16, 16), 3.0, np.float32)
+    for kind in ("frangi", "sato", "meijering"):
+        assert np.abs(oracle.ridge_filter(const, kind, [1.0, 2.0])).max() < 1e-6
