@@ -508,6 +508,144 @@ def psf_fit_secondary(dev, steps=2):
             "grad_check": "FP64 central differences on 64 taps: tests/test_autograd_gpu.py"}
 
 
+def _timed_calls(dev, fn, reps, flush=True):
+    """Mean device ms of fn() over reps calls (CUDA events on the current
+    stream), after one warm-up call; L2 flushed before each call."""
+    import torch
+
+    s = torch.cuda.current_stream(dev)
+    buf = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev) if flush else None
+    fn()
+    tot = 0.0
+    for _ in range(reps):
+        if buf is not None:
+            buf.fill_(1.0)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        fn()
+        b.record(s)
+        torch.cuda.synchronize(dev)
+        tot += a.elapsed_time(b)
+    return tot / reps
+
+
+def spectral_ops_secondary(dev, reps=10):
+    """The frequency-domain operators on the FFT (the reference runs them on
+    its O(N^2) DFT with host loops): Butterworth and phase correlation of
+    2048 x 2048 f32 images (integer and 1/20-pixel), unsupervised Wiener of a
+    1024 x 1024 image (30 iterations, burn-in 10).  Device ms per call, L2
+    flushed; the CPU figures time the oracle's FP64 numpy restatements of the
+    same calls (numpy's FFT, the reference's loops vectorised) on the host."""
+    import torch
+
+    import lucem_b200 as lb
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(lb.synth.SEED_BASE + 12)
+    img = torch.rand((2048, 2048), generator=gen, device=dev)
+    mov = torch.roll(img, (37, -21), (0, 1)).contiguous()
+    small = img[:1024, :1024].contiguous()
+    psf = torch.from_numpy(lb.synth.gaussian_psf((15, 15), (2.0, 2.0)).astype(np.float32)).to(dev)
+    ws = lb.Workspace(dev.index)
+    res = {}
+    res["ms_butterworth_2048"] = _timed_calls(dev, lambda: lb.butterworth(img, 0.1, False, 2.0, workspace=ws), reps)
+    res["ms_phase_correlation_2048"] = _timed_calls(dev, lambda: lb.phase_correlation(img, mov, workspace=ws), reps)
+    res["ms_phase_correlation_2048_up20"] = _timed_calls(
+        dev, lambda: lb.phase_correlation(img, mov, upsample_factor=20, workspace=ws), 3)
+    res["ms_unsupervised_wiener_1024"] = _timed_calls(
+        dev, lambda: lb.unsupervised_wiener(small, psf, num_iter=30, burnin=10, workspace=ws), 3)
+    h_img, h_mov = img.cpu().numpy(), mov.cpu().numpy()
+    t0 = time.perf_counter()
+    O.butterworth(h_img, 0.1)
+    res["cpu_ms_butterworth_2048"] = 1e3 * (time.perf_counter() - t0)
+    t0 = time.perf_counter()
+    O.phase_correlation(h_img[:512, :512], h_mov[:512, :512], 20)
+    res["cpu_ms_phase_correlation_512_up20"] = 1e3 * (time.perf_counter() - t0)
+    t0 = time.perf_counter()
+    O.unsupervised_wiener(small.cpu().numpy(), psf.cpu().numpy(), 30, 10)
+    res["cpu_ms_unsupervised_wiener_1024"] = 1e3 * (time.perf_counter() - t0)
+    res["metric"] = ("spectral operators: butterworth / phase_correlation (2048^2, upsample 1 and 20) / "
+                     "unsupervised_wiener (1024^2, 30 iterations), ms per call")
+    res["cpu"] = "oracle FP64 numpy restatements, one call each (phase correlation at 512^2)"
+    return res
+
+
+def structure_secondary(dev, peak, reps=10):
+    """Gaussian-consumer operators on a 2048 x 2048 f32 blob image: Frangi
+    with the default scales (1, 3, 5, 7, 9: four fused launches and the
+    per-axis path for sigma 9), the Hessian eigenvalues and the structure
+    tensor at sigma 2, against the same results built from separate calls
+    (three Gaussian-derivative blurs, then the per-pixel math), as the
+    reference composes them.  Device ms per call, L2 flushed."""
+    import torch
+
+    import lucem_b200 as lb
+
+    x = torch.from_numpy(lb.synth.blob_image().astype(np.float32)).to(dev)
+    ws = lb.Workspace(dev.index)
+    px = x.numel()
+    ms_frangi = _timed_calls(dev, lambda: lb.frangi(x, workspace=ws), reps)
+    ms_eig = _timed_calls(dev, lambda: lb.hessian_eigvals(x, 2.0, workspace=ws), reps)
+    ms_st = _timed_calls(dev, lambda: lb.structure_tensor(x, 2.0, workspace=ws), reps)
+
+    def eig_separate():
+        a = lb.gaussian_blur(x, 2.0, orders=[2, 0], workspace=ws)
+        b = lb.gaussian_blur(x, 2.0, orders=[1, 1], workspace=ws)
+        c = lb.gaussian_blur(x, 2.0, orders=[0, 2], workspace=ws)
+        lb.structure_tensor_eigvals(a, b, c)
+
+    ms_eig_sep = _timed_calls(dev, eig_separate, reps)
+    # One fused Hessian launch: reads the image (4 B/px), writes two f32
+    # eigenvalue planes (8 B/px).
+    achieved = px * 12 / (ms_eig * 1e-3) / 1e9
+    return {"metric": "Gaussian-consumer operators (2048x2048 f32 blob image): frangi (default 5 scales), "
+                      "hessian_eigvals and structure_tensor at sigma 2, ms per call",
+            "value": px / (ms_eig * 1e-3) / 1e9, "unit": "GPix/s (hessian_eigvals, one fused launch)",
+            "ms_frangi_5_scales": ms_frangi, "ms_hessian_eigvals": ms_eig, "ms_structure_tensor": ms_st,
+            "ms_hessian_eigvals_separate_calls": ms_eig_sep, "fused_vs_separate": ms_eig_sep / ms_eig,
+            "l2": "flushed between calls",
+            "roofline": {"bound": "hbm", "kernel": "family_planes_kernel (three Hessian filters, eigenvalue "
+                                                   "epilogue)", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "algorithmic_bytes": px * 12, "traffic": None}}
+
+
+def pipeline_u16_secondary(dev, reps=5):
+    """The raw u16 tile upload on the pipeline path: a 4096 x 4096 u16 host
+    tile through run_op (Gaussian blur, sigma 2, input scale 1/65535), end to
+    end (host -> device copy, the kernel, device -> host copy), with the raw
+    u16 sent (2 B/px, the cast and scale fused into the kernel's load)
+    against the host decoding to f32 first (4 B/px sent), as the reference's
+    Pyramid::read_block path does.  Wall ms per tile (both synchronous)."""
+    import torch
+
+    import lucem_b200 as lb
+    from lucem_b200 import pipeline as P
+
+    rng = np.random.default_rng(lb.synth.SEED_BASE + 13)
+    tile = rng.integers(0, 65535, (4096, 4096), dtype=np.uint16)
+    spec = '{"op": "gaussian_blur", "sigma": 2.0}'
+    scale = 1.0 / 65535.0
+
+    def wall(fn):
+        fn()
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            fn()
+        torch.cuda.synchronize(dev)
+        return 1e3 * (time.perf_counter() - t0) / reps
+
+    ms_raw = wall(lambda: P.run_op(spec, [tile], input_scale=scale))
+    ms_f32 = wall(lambda: P.run_op(spec, [tile.astype(np.float32) * np.float32(scale)]))
+    return {"metric": "pipeline run_op e2e, 4096^2 u16 host tile, Gaussian sigma 2 (ms per tile)",
+            "ms_raw_u16_upload": ms_raw, "ms_host_decode_f32_upload": ms_f32, "speedup": ms_f32 / ms_raw,
+            "h2d_bytes_raw": int(tile.nbytes), "h2d_bytes_f32": int(tile.nbytes * 2),
+            "d2h_bytes": int(tile.size * 4)}
+
+
 def gaussian_batch_secondary(dev, peak, reps=5):
     """512 separate u16 images, sides ~ U[64, 1024] (independent), sigma from
     {1, 2, 4} per image, reflect, f32 out: lucem_gaussian_batch (one launch
@@ -809,6 +947,10 @@ def run_ours(args, rank, world, local_rank):
         line["secondary"]["rl_batch"] = rl_batch_secondary(dev, peak)
     if args.gauss_batch:
         line["secondary"]["gaussian_batch"] = gaussian_batch_secondary(dev, peak)
+    if args.consumers:
+        line["secondary"]["spectral_ops"] = spectral_ops_secondary(dev)
+        line["secondary"]["structure"] = structure_secondary(dev, peak)
+        line["secondary"]["pipeline_u16"] = pipeline_u16_secondary(dev)
     print(json.dumps(line), flush=True)
 
 
@@ -826,6 +968,9 @@ def main():
     ap.add_argument("--psf-fit", type=int, default=1, help="also measure the differentiable blind PSF fit")
     ap.add_argument("--rl-batch", type=int, default=1, help="also measure the batched uneven 2-D RL")
     ap.add_argument("--gauss-batch", type=int, default=1, help="also measure the batch of separate images")
+    ap.add_argument("--consumers", type=int, default=1,
+                    help="also measure the spectral operators, the Gaussian-consumer operators and the u16 "
+                         "pipeline upload")
     args = ap.parse_args()
     ITERS = args.iters
     world = int(os.environ.get("WORLD_SIZE", "1"))
