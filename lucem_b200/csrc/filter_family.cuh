@@ -250,7 +250,9 @@ __device__ __forceinline__ void tensor_epilogue(const FamParams &p, const TileGe
 // One 64 x 64 output tile: stage tile + halo (cast fused), then per filter
 // the axis-0 pass into IT and the axis-1 pass into registers, folded into
 // every response that uses the filter; responses written once at the end.
-template <typename T, int NOUT, int RF = -1, bool STAGED = false>
+// TENSOR: the tensor epilogue (FamParams::tensor) is compiled in; kernels
+// that never take it (the tile walk, the batch) leave it out.
+template <typename T, int NOUT, int RF = -1, bool STAGED = false, bool TENSOR = false>
 __device__ void family_tile(const FamParams &p, const TileGeom &g, float *A, float *IT) {
     const int tid = threadIdx.x;
     // RF >= 0: one filter whose two kernel radii are both RF, known at compile
@@ -407,11 +409,9 @@ __device__ void family_tile(const FamParams &p, const TileGeom &g, float *A, flo
         __syncthreads();  // IT is rewritten by the next filter
     }
 
-    if constexpr (NOUT >= 3) {
-        if (p.tensor != kTensorNone) {
-            tensor_epilogue<NOUT>(p, g, acc, yp, xc);
-            return;
-        }
+    if constexpr (TENSOR && NOUT >= 3) {
+        tensor_epilogue<NOUT>(p, g, acc, yp, xc);
+        return;
     }
     // Epilogue: bias / sqrt, then two 32-byte row segments per thread.
 #pragma unroll
@@ -446,7 +446,7 @@ __device__ void family_tile(const FamParams &p, const TileGeom &g, float *A, flo
 }
 
 // Planes launch: B planes of [H, W], each its own read and owned box.
-template <typename T, int NOUT, int RF = -1>
+template <typename T, int NOUT, int RF = -1, bool TENSOR = false>
 __global__ void __launch_bounds__(kThreads, RF >= 0 ? 3 : 2)
 family_planes_kernel(const __grid_constant__ FamParams p, int tiles_y, int tiles_x) {
     extern __shared__ float4 smem4[];
@@ -462,7 +462,7 @@ family_planes_kernel(const __grid_constant__ FamParams p, int tiles_y, int tiles
         g.rb_y = 0; g.rb_x = 0; g.rb_h = p.H; g.rb_w = p.W;
         g.oy = ty * kTH; g.ox = tx * kTW;
         g.th = min(kTH, p.H - g.oy); g.tw = min(kTW, p.W - g.ox);
-        family_tile<T, NOUT, RF>(p, g, A, IT);
+        family_tile<T, NOUT, RF, false, TENSOR>(p, g, A, IT);
         __syncthreads();
     }
 }
@@ -775,10 +775,11 @@ int dispatch_planes_tma(const FamParams &p, const CUtensorMap &map, int total, i
     return (int)cudaGetLastError();
 }
 
-template <typename T, int NOUT, int RF = -1>
+template <typename T, int NOUT, int RF = -1, bool TENSOR = false>
 int dispatch_planes(const FamParams &p, size_t smem, int grid, int ty, int tx, cudaStream_t s) {
-    cudaFuncSetAttribute(family_planes_kernel<T, NOUT, RF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    family_planes_kernel<T, NOUT, RF><<<grid, kThreads, smem, s>>>(p, ty, tx);
+    cudaFuncSetAttribute(family_planes_kernel<T, NOUT, RF, TENSOR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+    family_planes_kernel<T, NOUT, RF, TENSOR><<<grid, kThreads, smem, s>>>(p, ty, tx);
     return (int)cudaGetLastError();
 }
 
@@ -808,6 +809,7 @@ int dispatch_planes_n(const FamParams &p, size_t smem, int grid, int ty, int tx,
         default: break;
         }
     }
+    if (p.tensor != kTensorNone) return dispatch_planes<T, kFamMaxOutputs, -1, true>(p, smem, grid, ty, tx, s);
     return p.n_outputs == 1 ? dispatch_planes<T, 1>(p, smem, grid, ty, tx, s)
                             : dispatch_planes<T, kFamMaxOutputs>(p, smem, grid, ty, tx, s);
 }
