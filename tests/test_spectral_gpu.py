@@ -150,3 +150,21 @@ def test_dlpack_producers_in_and_out(oracle):
     w = host(lb.wiener_deconvolve(_Producer(dev(x)), _Producer(dev(psf)), balance=0.1, clip=False))
     oracle.assert_close(w, oracle.wiener_deconvolve(x, psf, balance=0.1, clip=False, fft=oracle.numpy_fft), 1e-4,
                         "wiener via dlpack")
+
+
+@pytest.mark.parametrize("shape", [(2048, 2048), (64, 128, 96), (3000, 7), (16384,)])
+def test_fft_nd_against_cufft(shape):
+    """Cross-check of the library's own transforms against cuFFT (torch.fft in
+    float64 on the device), at sizes the host DFT oracle is too slow for;
+    cuFFT is only this cross-check, never on the library's path."""
+    g = torch.Generator(device="cuda")
+    g.manual_seed(int(np.prod(shape)))
+    re = torch.rand(shape, generator=g, device="cuda") - 0.5
+    im = torch.rand(shape, generator=g, device="cuda") - 0.5
+    z = torch.complex(re.double(), im.double())
+    for inverse in (False, True):
+        gr, gi = lb.fft_nd(re, im, inverse=inverse)
+        w = torch.fft.ifftn(z) if inverse else torch.fft.fftn(z)
+        scale = float(w.abs().max())
+        err = max(float((gr.double() - w.real).abs().max()), float((gi.double() - w.imag).abs().max()))
+        assert err <= 1e-5 * scale, (shape, inverse, err / scale)
