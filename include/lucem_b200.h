@@ -543,6 +543,66 @@ lucem_status lucem_sato(lucem_ctx *ctx, const lucem_tensor *in, const lucem_ridg
 lucem_status lucem_meijering(lucem_ctx *ctx, const lucem_tensor *in, const lucem_ridge_settings *settings,
                              lucem_tensor *out, lucem_workspace *ws, void *stream);
 
+/* crates/lucem-ops/src/transform/pyramid.rs:98-133 Pyramid. */
+typedef struct lucem_pyramid_settings {
+    double downscale;      /* 2; > 1 */
+    double sigma;          /* < 0: the default 2 downscale / 6 */
+    int32_t order;         /* 1: bilinear; 0: nearest (orders 2..5, the spline prefilter, are refused) */
+    int32_t mode;          /* lucem_pad_mode (reflect) */
+    double cval;
+} lucem_pyramid_settings;
+void lucem_pyramid_settings_default(lucem_pyramid_settings *s);
+/* crates/lucem-ops/src/transform/pyramid.rs:135-168 pyramid_reduce: 2-D f32
+ * (or u8/u16) input [H, W] -> f32 out [ceil(H / downscale), ceil(W /
+ * downscale)]: the Gaussian blur (one fused launch, into the workspace),
+ * then the resize's resampling (transform/warp.rs:207-251, orders 0 and 1). */
+lucem_status lucem_pyramid_reduce(lucem_ctx *ctx, const lucem_tensor *in, const lucem_pyramid_settings *settings,
+                                  lucem_tensor *out, lucem_workspace *ws, void *stream);
+/* crates/lucem-ops/src/transform/pyramid.rs:171-208 pyramid_expand: the
+ * resampling up to out's shape, then the Gaussian blur.  The reference's
+ * default shape is ceil(H * downscale) x ceil(W * downscale). */
+lucem_status lucem_pyramid_expand(lucem_ctx *ctx, const lucem_tensor *in, const lucem_pyramid_settings *settings,
+                                  lucem_tensor *out, lucem_workspace *ws, void *stream);
+/* One band of crates/lucem-ops/src/transform/pyramid.rs:239-266
+ * laplacian_pyramid: out = fine - pyramid_expand(coarse, fine's shape). */
+lucem_status lucem_laplacian_band(lucem_ctx *ctx, const lucem_tensor *fine, const lucem_tensor *coarse,
+                                  const lucem_pyramid_settings *settings, lucem_tensor *out, lucem_workspace *ws,
+                                  void *stream);
+
+/* crates/lucem-ops/src/feature/blobs.rs:33-112 BlobDetector. */
+typedef struct lucem_blob_settings {
+    double min_sigma;        /* 1 */
+    double max_sigma;        /* 30 */
+    int64_t num_sigma;       /* 10 (LoG, DoH) */
+    double sigma_ratio;      /* 1.6 (DoG) */
+    double threshold;        /* 0.1, absolute */
+    double overlap;          /* 0.5, in [0, 1] */
+    int32_t log_scale;       /* 0: linear scale spacing (LoG, DoH) */
+    int64_t exclude_border;  /* 1 */
+} lucem_blob_settings;
+void lucem_blob_settings_default(lucem_blob_settings *s);
+/* crates/lucem-ops/src/feature/blobs.rs:16-30 Blob. */
+typedef struct lucem_blob {
+    int64_t y, x;
+    double sigma;
+    double response;
+} lucem_blob;
+/* crates/lucem-ops/src/feature/blobs.rs:204-236 blobs_log, :238-287
+ * blobs_dog, :289-345 blobs_doh: 2-D input.  Each scale's response
+ * (-sigma^2 LoG, DoG / (ratio - 1), sigma^4 det H) is one fused family
+ * launch into a scale stack kept on the device; one kernel marks the
+ * 3 x 3 x 3 maxima above the threshold (the reference's tie rule and
+ * border); the host sorts them (response descending, then y, x) and drops
+ * those overlapping a stronger blob by more than `overlap`.  Writes up to
+ * `cap` blobs to `out` and their total number to *n_out (call again with a
+ * larger `out` when *n_out > cap).  Synchronises on `stream`. */
+lucem_status lucem_blobs_log(lucem_ctx *ctx, const lucem_tensor *in, const lucem_blob_settings *settings,
+                             lucem_blob *out, int64_t cap, int64_t *n_out, lucem_workspace *ws, void *stream);
+lucem_status lucem_blobs_dog(lucem_ctx *ctx, const lucem_tensor *in, const lucem_blob_settings *settings,
+                             lucem_blob *out, int64_t cap, int64_t *n_out, lucem_workspace *ws, void *stream);
+lucem_status lucem_blobs_doh(lucem_ctx *ctx, const lucem_tensor *in, const lucem_blob_settings *settings,
+                             lucem_blob *out, int64_t cap, int64_t *n_out, lucem_workspace *ws, void *stream);
+
 /* The grid lucem_richardson_lucy uses (host only), before any autotuning of
  * the context: per axis the requested length, or the cheapest m * 2^k
  * (m in {1,3,5,7,9,15,21,25,27}) at least the padding's need, by length

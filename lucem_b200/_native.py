@@ -79,6 +79,21 @@ class RidgeSettings(C.Structure):
                 ("mode", C.c_int32), ("cval", C.c_double), ("beta", C.c_double), ("gamma", C.c_double)]
 
 
+class PyramidSettings(C.Structure):
+    _fields_ = [("downscale", C.c_double), ("sigma", C.c_double), ("order", C.c_int32), ("mode", C.c_int32),
+                ("cval", C.c_double)]
+
+
+class BlobSettings(C.Structure):
+    _fields_ = [("min_sigma", C.c_double), ("max_sigma", C.c_double), ("num_sigma", C.c_int64),
+                ("sigma_ratio", C.c_double), ("threshold", C.c_double), ("overlap", C.c_double),
+                ("log_scale", C.c_int32), ("exclude_border", C.c_int64)]
+
+
+class BlobC(C.Structure):
+    _fields_ = [("y", C.c_int64), ("x", C.c_int64), ("sigma", C.c_double), ("response", C.c_double)]
+
+
 class UnsupervisedWienerSettings(C.Structure):
     _fields_ = [("num_iter", C.c_int64), ("burnin", C.c_int64), ("clip", C.c_int32), ("seed", C.c_uint64)]
 
@@ -124,6 +139,14 @@ SIGNATURES = {
     "lucem_frangi": (I32, [P, TP, C.POINTER(RidgeSettings), TP, P, P]),
     "lucem_sato": (I32, [P, TP, C.POINTER(RidgeSettings), TP, P, P]),
     "lucem_meijering": (I32, [P, TP, C.POINTER(RidgeSettings), TP, P, P]),
+    "lucem_pyramid_settings_default": (None, [C.POINTER(PyramidSettings)]),
+    "lucem_pyramid_reduce": (I32, [P, TP, C.POINTER(PyramidSettings), TP, P, P]),
+    "lucem_pyramid_expand": (I32, [P, TP, C.POINTER(PyramidSettings), TP, P, P]),
+    "lucem_laplacian_band": (I32, [P, TP, TP, C.POINTER(PyramidSettings), TP, P, P]),
+    "lucem_blob_settings_default": (None, [C.POINTER(BlobSettings)]),
+    "lucem_blobs_log": (I32, [P, TP, C.POINTER(BlobSettings), C.POINTER(BlobC), I64, I64P, P, P]),
+    "lucem_blobs_dog": (I32, [P, TP, C.POINTER(BlobSettings), C.POINTER(BlobC), I64, I64P, P, P]),
+    "lucem_blobs_doh": (I32, [P, TP, C.POINTER(BlobSettings), C.POINTER(BlobC), I64, I64P, P, P]),
     "lucem_unsupervised_wiener_settings_default": (None, [C.POINTER(UnsupervisedWienerSettings)]),
     "lucem_unsupervised_wiener": (I32, [P, TP, TP, C.POINTER(UnsupervisedWienerSettings), TP, DP, P, P]),
     "lucem_workspace_wait_status": (I32, [P, P, I64P]),

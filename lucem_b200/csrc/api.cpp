@@ -3530,24 +3530,37 @@ lucem_status check_sigma(double sigma) {
     return ok();
 }
 
-// The three Hessian filters of one scale, orders (2,0), (1,1), (0,2) at
-// sigma (structure.rs:26-51): written as (a, b, c) into outs when tensor is
-// kTensorNone, else through the epilogue `tensor` into outs.
-lucem_status hessian_scale(lucem_ctx *ctx, const lucem_tensor *in, double sigma, int mode, double cval, int tensor,
-                           float p0, float p1, int black, int first, const TensorOuts &outs, lucem_workspace *ws,
-                           void *stream) {
+// One filter of a fused tensor launch: Gaussian of `sigma` (truncate 4) with
+// derivative orders (order0 along rows, order1 along columns).
+struct TensorFilter {
+    double sigma;
+    uint32_t order0, order1;
+};
+
+// Up to three 2-D Gaussian-derivative filters of `in` written as (a, b, c)
+// into outs when tensor is kTensorNone, else combined per pixel through the
+// epilogue `tensor` into outs: one fused family launch when every radius fits
+// the fused kernel, else the per-axis passes into workspace arrays and the
+// same epilogue elementwise.
+lucem_status filters_tensor(lucem_ctx *ctx, const lucem_tensor *in, const TensorFilter *flt, int nf, int mode,
+                            double cval, int tensor, float p0, float p1, int black, int first, const TensorOuts &outs,
+                            lucem_workspace *ws, void *stream) {
     const int64_t n = numel(in), H = in->dims[0], W = in->dims[1];
     if (n == 0) return ok();
-    const int64_t r = sigma > 0.0 ? (int64_t)radius_of(4.0, sigma) : 0;
-    const uint32_t ords[3][2] = {{2, 0}, {1, 1}, {0, 2}};
-    if (r <= kFamMaxRadius && H < (1 << 30) && W < (1 << 30)) {
+    int64_t r[3] = {0, 0, 0}, rmax = 0;
+    for (int f = 0; f < nf; ++f) {
+        r[f] = flt[f].sigma > 0.0 ? (int64_t)radius_of(4.0, flt[f].sigma) : 0;
+        rmax = std::max(rmax, r[f]);
+    }
+    if (rmax <= kFamMaxRadius && H < (1 << 30) && W < (1 << 30)) {
         FamParams fp;
         init_fam(&fp, in, mode, cval, 1.0);
-        fp.n_filters = 3;
-        for (int f = 0; f < 3; ++f) {
-            Pass a{0, sigma, ords[f][0], r}, b{1, sigma, ords[f][1], r};
+        fp.n_filters = nf;
+        for (int f = 0; f < nf; ++f) {
+            Pass a{0, flt[f].sigma, flt[f].order0, r[f]}, b{1, flt[f].sigma, flt[f].order1, r[f]};
             // sigma 0: the reference drops the axis (a copy, orders ignored).
-            fill_filter_taps(&fp, f, sigma > 0.0 ? &a : nullptr, sigma > 0.0 ? &b : nullptr);
+            const bool on = flt[f].sigma > 0.0;
+            fill_filter_taps(&fp, f, on ? &a : nullptr, on ? &b : nullptr);
             fp.rmax0 = std::max(fp.rmax0, fp.r0[f]);
             fp.rmax1 = std::max(fp.rmax1, fp.r1[f]);
         }
@@ -3558,7 +3571,7 @@ lucem_status hessian_scale(lucem_ctx *ctx, const lucem_tensor *in, double sigma,
             o.plane_stride = H * W;
             o.row_pitch = W;
             o.combine = (int)Combine::kLinear;
-            o.fa = k;
+            o.fa = k < nf ? k : -1;
             o.fb = -1;
             o.alpha = 1.0f;
         }
@@ -3569,29 +3582,40 @@ lucem_status hessian_scale(lucem_ctx *ctx, const lucem_tensor *in, double sigma,
         fp.tensor_p1 = p1;
         if (lucem_status st = fam_waits(ws, &fp, stream)) return st;
         int e = timed(kPassFamily, stream, [&] { return launch_family_planes(fp, in->dtype, stream); });
-        return e ? cuda_fail(e, "hessian family launch") : ok();
+        return e ? cuda_fail(e, "fused filter launch") : ok();
     }
     // Wider filters: the components by the per-axis passes, then the epilogue.
     float *comp[3] = {outs.o[0], outs.o[1], outs.o[2]};
     if (tensor != kTensorNone) {
         if (!ws) return fail(LUCEM_ERR_INVALID_HANDLE, "a workspace is required");
-        const char *names[3] = {"hessian_a", "hessian_b", "hessian_c"};
-        for (int k = 0; k < 3; ++k) {
+        const char *names[3] = {"tensor_a", "tensor_b", "tensor_c"};
+        for (int k = 0; k < nf; ++k) {
             void *p = nullptr;
             if (lucem_status st = ws->get(names[k], (size_t)n * sizeof(float), &p)) return st;
             comp[k] = static_cast<float *>(p);
         }
     }
-    for (int f = 0; f < 3; ++f) {
-        std::vector<Pass> passes = {Pass{0, sigma, ords[f][0], r}, Pass{1, sigma, ords[f][1], r}};
+    for (int f = 0; f < nf; ++f) {
+        std::vector<Pass> passes = {Pass{0, flt[f].sigma, flt[f].order0, r[f]},
+                                    Pass{1, flt[f].sigma, flt[f].order1, r[f]}};
+        if (flt[f].sigma <= 0.0) passes.clear();
         if (lucem_status st = run_passes(ctx, in, passes, mode, cval, 1.0, comp[f], ws, stream)) return st;
     }
     if (tensor == kTensorNone) return ok();
     int e = timed(kPassElementwise, stream, [&] {
-        return launch_tensor_elementwise(comp[0], comp[1], comp[2], outs.o[0], outs.o[1], outs.o[2], n, tensor, p0, p1,
-                                         black, first, stream);
+        return launch_tensor_elementwise(comp[0], comp[1], nf > 2 ? comp[2] : nullptr, outs.o[0], outs.o[1],
+                                         outs.o[2], n, tensor, p0, p1, black, first, stream);
     });
     return e ? cuda_fail(e, "tensor epilogue launch") : ok();
+}
+
+// The three Hessian filters of one scale, orders (2,0), (1,1), (0,2) at
+// sigma (structure.rs:26-51), through filters_tensor.
+lucem_status hessian_scale(lucem_ctx *ctx, const lucem_tensor *in, double sigma, int mode, double cval, int tensor,
+                           float p0, float p1, int black, int first, const TensorOuts &outs, lucem_workspace *ws,
+                           void *stream) {
+    const TensorFilter h[3] = {{sigma, 2, 0}, {sigma, 1, 1}, {sigma, 0, 2}};
+    return filters_tensor(ctx, in, h, 3, mode, cval, tensor, p0, p1, black, first, outs, ws, stream);
 }
 
 // Checks of the single-scale Hessian operators: 2-D input, f32 outputs of
@@ -3830,6 +3854,338 @@ lucem_status lucem_sato(lucem_ctx *ctx, const lucem_tensor *in, const lucem_ridg
 lucem_status lucem_meijering(lucem_ctx *ctx, const lucem_tensor *in, const lucem_ridge_settings *settings,
                              lucem_tensor *out, lucem_workspace *ws, void *stream) {
     return ridge_filter(ctx, "meijering", kTensorMeijering, in, settings, out, ws, stream);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Blob detectors (crates/lucem-ops/src/feature/blobs.rs): the scale stack on
+// the device (one fused launch per scale), its maxima by one kernel
+// (features.cu), sorting and overlap pruning on the host.
+
+namespace {
+
+enum class BlobKind { kLog, kDog, kDoh };
+
+// BlobDetector::validate (blobs.rs:68-94).
+lucem_status blob_validate(const lucem_blob_settings *s) {
+    if (!std::isfinite(s->min_sigma) || s->min_sigma <= 0.0)
+        return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `min_sigma`: min_sigma must be positive, got %g",
+                    s->min_sigma);
+    if (!std::isfinite(s->max_sigma) || s->max_sigma < s->min_sigma)
+        return fail(LUCEM_ERR_INVALID_PARAMETER,
+                    "invalid parameter `max_sigma`: max_sigma (%g) must be >= min_sigma (%g)", s->max_sigma,
+                    s->min_sigma);
+    if (s->num_sigma <= 0)
+        return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `num_sigma`: num_sigma must be at least 1");
+    if (!(s->overlap >= 0.0 && s->overlap <= 1.0))
+        return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `overlap`: overlap must be in 0.0..=1.0, got %g",
+                    s->overlap);
+    return ok();
+}
+
+// BlobDetector::sigmas (blobs.rs:96-111).
+std::vector<double> blob_sigmas(const lucem_blob_settings *s) {
+    if (s->num_sigma == 1 || std::fabs(s->max_sigma - s->min_sigma) <= DBL_EPSILON) return {s->min_sigma};
+    std::vector<double> v((size_t)s->num_sigma);
+    for (int64_t i = 0; i < s->num_sigma; ++i) {
+        const double t = (double)i / (double)(s->num_sigma - 1);
+        v[(size_t)i] = s->log_scale ? s->min_sigma * std::pow(s->max_sigma / s->min_sigma, t)
+                                    : s->min_sigma + t * (s->max_sigma - s->min_sigma);
+    }
+    return v;
+}
+
+// circle_overlap_fraction (blobs.rs:114-136): the lens area of two circles of
+// radius sqrt(2) sigma over the smaller circle's area.
+double blob_overlap(const lucem_blob &a, const lucem_blob &b) {
+    const double r1 = M_SQRT2 * a.sigma, r2 = M_SQRT2 * b.sigma;
+    const double dy = (double)a.y - (double)b.y, dx = (double)a.x - (double)b.x;
+    const double d = std::sqrt(dy * dy + dx * dx);
+    if (d >= r1 + r2) return 0.0;
+    if (d <= std::fabs(r1 - r2)) return 1.0;
+    const double rmin = std::min(r1, r2);
+    if (rmin <= 0.0) return 0.0;
+    const double c1 = std::min(std::max((d * d + r1 * r1 - r2 * r2) / (2.0 * d * r1), -1.0), 1.0);
+    const double c2 = std::min(std::max((d * d + r2 * r2 - r1 * r1) / (2.0 * d * r2), -1.0), 1.0);
+    const double t1 = r1 * r1 * std::acos(c1), t2 = r2 * r2 * std::acos(c2);
+    const double sq = (-d + r1 + r2) * (d + r1 - r2) * (d - r1 + r2) * (d + r1 + r2);
+    const double area = t1 + t2 - 0.5 * std::sqrt(std::max(sq, 0.0));
+    return area / (M_PI * rmin * rmin);
+}
+
+lucem_status blobs_run(lucem_ctx *ctx, BlobKind kind, const lucem_tensor *in, const lucem_blob_settings *settings,
+                       lucem_blob *out, int64_t cap, int64_t *n_out, lucem_workspace *ws, void *stream) {
+    TimerScope timer_scope(ws);
+    if (!ctx) return fail(LUCEM_ERR_INVALID_HANDLE, "null context");
+    if (!ws) return fail(LUCEM_ERR_INVALID_HANDLE, "a workspace is required");
+    if (!n_out || (cap > 0 && !out)) return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `out`: null");
+    *n_out = 0;
+    lucem_blob_settings def;
+    lucem_blob_settings_default(&def);
+    const lucem_blob_settings *s = settings ? settings : &def;
+    const char *op = kind == BlobKind::kLog ? "blobs_log" : kind == BlobKind::kDog ? "blobs_dog" : "blobs_doh";
+    lucem_status st;
+    if ((st = check_tensor("image", in)) || (st = check_2d(op, in)) || (st = blob_validate(s))) return st;
+    std::vector<double> sig;
+    if (kind == BlobKind::kDog) {
+        // blobs.rs:244-263: sigma, sigma * ratio, ... up to max_sigma.
+        if (!std::isfinite(s->sigma_ratio) || s->sigma_ratio <= 1.0)
+            return fail(LUCEM_ERR_INVALID_PARAMETER,
+                        "invalid parameter `sigma_ratio`: sigma_ratio must be > 1.0, got %g", s->sigma_ratio);
+        for (double v = s->min_sigma; v <= s->max_sigma * (1.0 + 1e-9); v *= s->sigma_ratio) sig.push_back(v);
+        if (sig.empty()) sig.push_back(s->min_sigma);
+    } else {
+        sig = blob_sigmas(s);
+    }
+    const int64_t n = numel(in), H = in->dims[0], W = in->dims[1];
+    if (n == 0) return ok();
+    const int ns = (int)sig.size();
+    const int64_t border = std::max<int64_t>(s->exclude_border, 1);
+    if (H <= 2 * border || W <= 2 * border) return ok();
+    void *pc = nullptr, *pl = nullptr, *pn = nullptr;
+    const int64_t bound = blob_candidate_bound(ns, H, W);
+    if ((st = ws->get("blob_stack", (size_t)ns * (size_t)n * sizeof(float), &pc)) ||
+        (st = ws->get("blob_candidates", (size_t)bound * sizeof(BlobCandidate), &pl)) ||
+        (st = ws->get("blob_count", sizeof(unsigned long long), &pn)))
+        return st;
+    float *cube = static_cast<float *>(pc);
+    // The scale stack: one fused launch per scale, the reference's scaling in
+    // the epilogue.
+    for (int i = 0; i < ns; ++i) {
+        const double sg = sig[(size_t)i];
+        TensorOuts o;
+        o.o[0] = cube + (size_t)i * (size_t)n;
+        if (kind == BlobKind::kLog) {
+            // -sigma^2 (d2/dy2 + d2/dx2) G * I (blobs.rs:219-232).
+            const TensorFilter f[2] = {{sg, 2, 0}, {sg, 0, 2}};
+            st = filters_tensor(ctx, in, f, 2, LUCEM_PAD_REFLECT, 0.0, kTensorScaledSum, (float)(-(sg * sg)), 1.0f, 0,
+                                1, o, ws, stream);
+        } else if (kind == BlobKind::kDog) {
+            // (G(sigma) - G(ratio sigma)) * I / (ratio - 1) (blobs.rs:265-283).
+            const TensorFilter f[2] = {{sg, 0, 0}, {sg * s->sigma_ratio, 0, 0}};
+            st = filters_tensor(ctx, in, f, 2, LUCEM_PAD_REFLECT, 0.0, kTensorScaledSum,
+                                (float)(1.0 / (s->sigma_ratio - 1.0)), -1.0f, 0, 1, o, ws, stream);
+        } else {
+            // sigma^4 det H (blobs.rs:313-339).
+            const TensorFilter f[3] = {{sg, 2, 0}, {sg, 1, 1}, {sg, 0, 2}};
+            st = filters_tensor(ctx, in, f, 3, LUCEM_PAD_REFLECT, 0.0, kTensorScaledDet, (float)std::pow(sg, 4.0),
+                                0.0f, 0, 1, o, ws, stream);
+        }
+        if (st) return st;
+    }
+    cudaStream_t cs = static_cast<cudaStream_t>(stream);
+    unsigned long long *cnt = static_cast<unsigned long long *>(pn);
+    CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof *cnt, cs), "count reset");
+    int e = timed(kPassElementwise, stream, [&] {
+        return launch_blob_candidates(cube, ns, (int)H, (int)W, (int)border, s->threshold,
+                                      static_cast<BlobCandidate *>(pl), bound, cnt, stream);
+    });
+    if (e) return cuda_fail(e, "blob maxima launch");
+    unsigned long long count = 0;
+    CUDA_TRY(cudaMemcpyAsync(&count, cnt, sizeof count, cudaMemcpyDeviceToHost, cs), "count download");
+    CUDA_TRY(cudaStreamSynchronize(cs), "synchronise");
+    const size_t nc = (size_t)std::min<unsigned long long>(count, (unsigned long long)bound);
+    std::vector<BlobCandidate> cand(nc);
+    if (nc) {
+        CUDA_TRY(cudaMemcpyAsync(cand.data(), pl, nc * sizeof(BlobCandidate), cudaMemcpyDeviceToHost, cs),
+                 "candidate download");
+        CUDA_TRY(cudaStreamSynchronize(cs), "synchronise");
+    }
+    // blobs.rs:183-200: response descending, then y, x (the reference's stable
+    // sort keeps scale order on full ties); then the greedy overlap pruning.
+    std::sort(cand.begin(), cand.end(), [](const BlobCandidate &a, const BlobCandidate &b) {
+        if (a.response != b.response) return a.response > b.response;
+        if (a.y != b.y) return a.y < b.y;
+        if (a.x != b.x) return a.x < b.x;
+        return a.s < b.s;
+    });
+    std::vector<lucem_blob> kept;
+    for (const BlobCandidate &c : cand) {
+        const lucem_blob b{c.y, c.x, sig[(size_t)c.s], (double)c.response};
+        bool drop = false;
+        for (const lucem_blob &k : kept)
+            if (blob_overlap(b, k) > s->overlap) {
+                drop = true;
+                break;
+            }
+        if (!drop) kept.push_back(b);
+    }
+    *n_out = (int64_t)kept.size();
+    for (int64_t i = 0; i < std::min<int64_t>(cap, (int64_t)kept.size()); ++i) out[i] = kept[(size_t)i];
+    return ok();
+}
+
+}  // namespace
+
+extern "C" {
+
+void lucem_blob_settings_default(lucem_blob_settings *s) {
+    s->min_sigma = 1.0;
+    s->max_sigma = 30.0;
+    s->num_sigma = 10;
+    s->sigma_ratio = 1.6;
+    s->threshold = 0.1;
+    s->overlap = 0.5;
+    s->log_scale = 0;
+    s->exclude_border = 1;
+}
+
+lucem_status lucem_blobs_log(lucem_ctx *ctx, const lucem_tensor *in, const lucem_blob_settings *settings,
+                             lucem_blob *out, int64_t cap, int64_t *n_out, lucem_workspace *ws, void *stream) {
+    return blobs_run(ctx, BlobKind::kLog, in, settings, out, cap, n_out, ws, stream);
+}
+
+lucem_status lucem_blobs_dog(lucem_ctx *ctx, const lucem_tensor *in, const lucem_blob_settings *settings,
+                             lucem_blob *out, int64_t cap, int64_t *n_out, lucem_workspace *ws, void *stream) {
+    return blobs_run(ctx, BlobKind::kDog, in, settings, out, cap, n_out, ws, stream);
+}
+
+lucem_status lucem_blobs_doh(lucem_ctx *ctx, const lucem_tensor *in, const lucem_blob_settings *settings,
+                             lucem_blob *out, int64_t cap, int64_t *n_out, lucem_workspace *ws, void *stream) {
+    return blobs_run(ctx, BlobKind::kDoh, in, settings, out, cap, n_out, ws, stream);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Pyramids (crates/lucem-ops/src/transform/pyramid.rs): the Gaussian blur of
+// the fused family path and the resize's resampling (features.cu).
+
+namespace {
+
+// Pyramid::resolved_sigma (pyramid.rs:115-132) and the orders built here.
+lucem_status pyramid_sigma(const lucem_pyramid_settings *s, double *sigma) {
+    if (!std::isfinite(s->downscale) || s->downscale <= 1.0)
+        return fail(LUCEM_ERR_INVALID_PARAMETER,
+                    "invalid parameter `downscale`: pyramid scale factor must be > 1.0, got %g", s->downscale);
+    const double sg = s->sigma < 0.0 ? 2.0 * s->downscale / 6.0 : s->sigma;
+    if (!std::isfinite(sg))
+        return fail(LUCEM_ERR_INVALID_PARAMETER,
+                    "invalid parameter `sigma`: sigma must be non-negative and finite, got %g", sg);
+    if (s->order < 0 || s->order > 5)
+        return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `order`: spline order must be in 0..=5, got %d",
+                    s->order);
+    if (s->order > 1)
+        return fail(LUCEM_ERR_INVALID_PARAMETER,
+                    "invalid parameter `order`: orders 2..=5 (B-spline prefiltered) are not built; use 0 or 1");
+    *sigma = sg;
+    return check_mode(s->mode);
+}
+
+// gaussian_blur_into with the pyramid's sigma, mode and cval, into out (f32).
+lucem_status pyramid_blur(lucem_ctx *ctx, const lucem_tensor *in, double sigma, const lucem_pyramid_settings *s,
+                          float *out, lucem_workspace *ws, void *stream) {
+    std::vector<Pass> passes;
+    if (sigma > 0.0) {
+        const int64_t r = (int64_t)radius_of(4.0, sigma);
+        passes = {Pass{0, sigma, 0, r}, Pass{1, sigma, 0, r}};
+    }
+    return run_passes(ctx, in, passes, s->mode, s->cval, 1.0, out, ws, stream);
+}
+
+// resize (warp.rs:207-251) without anti-aliasing: the inverse map
+// y = (H / OH) oy + (H / OH - 1) / 2, likewise x, in f32.
+lucem_status pyramid_resample(const float *in, int64_t H, int64_t W, float *out, int64_t OH, int64_t OW,
+                              const lucem_pyramid_settings *s, void *stream) {
+    const double sy = (double)H / (double)OH, sx = (double)W / (double)OW;
+    int e = timed(kPassElementwise, stream, [&] {
+        return launch_resample(in, (int)H, (int)W, out, (int)OH, (int)OW, (float)sy, (float)(0.5 * (sy - 1.0)),
+                               (float)sx, (float)(0.5 * (sx - 1.0)), s->order, s->mode, (float)s->cval, stream);
+    });
+    return e ? cuda_fail(e, "resample launch") : ok();
+}
+
+lucem_status pyramid_io(const char *op, const lucem_tensor *in, const lucem_tensor *out) {
+    lucem_status st;
+    if ((st = check_tensor("image", in)) || (st = check_tensor("output", out))) return st;
+    if ((st = check_2d(op, in)) || (st = check_2d(op, out)) || (st = require_f32_out(out)) ||
+        (st = not_aliased(in, out)))
+        return st;
+    return ok();
+}
+
+}  // namespace
+
+extern "C" {
+
+void lucem_pyramid_settings_default(lucem_pyramid_settings *s) {
+    s->downscale = 2.0;
+    s->sigma = -1.0;
+    s->order = 1;
+    s->mode = LUCEM_PAD_REFLECT;
+    s->cval = 0.0;
+}
+
+// pyramid.rs:135-168.
+lucem_status lucem_pyramid_reduce(lucem_ctx *ctx, const lucem_tensor *in, const lucem_pyramid_settings *settings,
+                                  lucem_tensor *out, lucem_workspace *ws, void *stream) {
+    TimerScope timer_scope(ws);
+    if (!ctx) return fail(LUCEM_ERR_INVALID_HANDLE, "null context");
+    if (!ws) return fail(LUCEM_ERR_INVALID_HANDLE, "a workspace is required");
+    lucem_pyramid_settings def;
+    lucem_pyramid_settings_default(&def);
+    const lucem_pyramid_settings *s = settings ? settings : &def;
+    lucem_status st;
+    if ((st = pyramid_io("pyramid_reduce", in, out))) return st;
+    double sigma;
+    if ((st = pyramid_sigma(s, &sigma))) return st;
+    const int64_t H = in->dims[0], W = in->dims[1];
+    const int64_t OH = std::max<int64_t>(1, (int64_t)std::ceil((double)H / s->downscale));
+    const int64_t OW = std::max<int64_t>(1, (int64_t)std::ceil((double)W / s->downscale));
+    if (out->dims[0] != OH || out->dims[1] != OW)
+        return fail(LUCEM_ERR_SHAPE_MISMATCH, "output shape %s does not match the reduced shape [%lld, %lld]",
+                    dims_str(out).c_str(), (long long)OH, (long long)OW);
+    if (H == 0 || W == 0) return ok();
+    void *pb = nullptr;
+    if ((st = ws->get("pyramid_blur", (size_t)(H * W) * sizeof(float), &pb))) return st;
+    if ((st = pyramid_blur(ctx, in, sigma, s, static_cast<float *>(pb), ws, stream))) return st;
+    return pyramid_resample(static_cast<const float *>(pb), H, W, static_cast<float *>(out->data), OH, OW, s, stream);
+}
+
+// pyramid.rs:171-208 (the output shape given by `out`).
+lucem_status lucem_pyramid_expand(lucem_ctx *ctx, const lucem_tensor *in, const lucem_pyramid_settings *settings,
+                                  lucem_tensor *out, lucem_workspace *ws, void *stream) {
+    TimerScope timer_scope(ws);
+    if (!ctx) return fail(LUCEM_ERR_INVALID_HANDLE, "null context");
+    if (!ws) return fail(LUCEM_ERR_INVALID_HANDLE, "a workspace is required");
+    lucem_pyramid_settings def;
+    lucem_pyramid_settings_default(&def);
+    const lucem_pyramid_settings *s = settings ? settings : &def;
+    lucem_status st;
+    if ((st = pyramid_io("pyramid_expand", in, out))) return st;
+    if (in->dtype != LUCEM_F32) return fail(LUCEM_ERR_UNSUPPORTED_DTYPE, "pyramid_expand takes an f32 image");
+    double sigma;
+    if ((st = pyramid_sigma(s, &sigma))) return st;
+    const int64_t H = in->dims[0], W = in->dims[1], OH = out->dims[0], OW = out->dims[1];
+    if (OH == 0 || OW == 0)
+        return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `output_shape`: output_shape dimensions must be >= 1");
+    if (H == 0 || W == 0) return ok();
+    void *pu = nullptr;
+    if ((st = ws->get("pyramid_up", (size_t)(OH * OW) * sizeof(float), &pu))) return st;
+    if ((st = pyramid_resample(static_cast<const float *>(in->data), H, W, static_cast<float *>(pu), OH, OW, s,
+                               stream)))
+        return st;
+    lucem_tensor up = *out;
+    up.data = pu;
+    return pyramid_blur(ctx, &up, sigma, s, static_cast<float *>(out->data), ws, stream);
+}
+
+// pyramid.rs:247-262: one band L = fine - expand(coarse).
+lucem_status lucem_laplacian_band(lucem_ctx *ctx, const lucem_tensor *fine, const lucem_tensor *coarse,
+                                  const lucem_pyramid_settings *settings, lucem_tensor *out, lucem_workspace *ws,
+                                  void *stream) {
+    lucem_status st;
+    if ((st = check_tensor("fine", fine)) || (st = check_tensor("output", out))) return st;
+    if ((st = same_shape("fine", fine, "output", out)) || (st = not_aliased(fine, out))) return st;
+    if (fine->dtype != LUCEM_F32) return fail(LUCEM_ERR_UNSUPPORTED_DTYPE, "laplacian bands take f32 levels");
+    if ((st = lucem_pyramid_expand(ctx, coarse, settings, out, ws, stream))) return st;
+    // elementwise::linear_combination_into(fine, expanded, 1, -1, 0).
+    int e = timed(kPassElementwise, stream, [&] {
+        return launch_linear_comb(static_cast<const float *>(fine->data), static_cast<const float *>(out->data),
+                                  static_cast<float *>(out->data), numel(fine), 1.0f, -1.0f, 0.0f, stream);
+    });
+    return e ? cuda_fail(e, "band combine launch") : ok();
 }
 
 }  // extern "C"

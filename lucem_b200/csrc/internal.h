@@ -57,6 +57,8 @@ enum TensorMode : int32_t {
     kTensorSato = 5,       // out0 = max(out0, sato(l1 sigma^2, l2 sigma^2)); p0 = sigma^2
     kTensorMeijering = 6,  // out0 = max(out0, meijering(l1, l2))
     kTensorOuter = 7,      // (a, b) = (g_r, g_c): out0 = a a, out1 = a b, out2 = b b
+    kTensorScaledSum = 8,  // out0 = p0 (a + p1 b), each step rounded (LoG / DoG responses)
+    kTensorScaledDet = 9,  // out0 = p0 (a c - b^2) (determinant-of-Hessian response)
 };
 
 // One launch of the fused 2-D family kernel over B planes of [H, W] (or over
@@ -150,6 +152,22 @@ int launch_fill(float *out, int64_t n, float v, void *stream);
 // running maximum starts at 0 instead of o0.
 int launch_tensor_elementwise(const float *a, const float *b, const float *c, float *o0, float *o1, float *o2,
                               int64_t n, int mode, float p0, float p1, int black, int first, void *stream);
+
+// features.cu: resampling on the resize grid (order 0 nearest, 1 bilinear;
+// the input sampled at (m0 oy + m2, m4 ox + m5), pad map outside).
+int launch_resample(const float *in, int H, int W, float *out, int OH, int OW, float m0, float m2, float m4,
+                    float m5, int order, int mode, float cval, void *stream);
+// features.cu: scale-space maxima of the blob detectors.
+struct BlobCandidate {
+    float response;
+    int32_t s, y, x;
+};
+// Upper bound of the maxima of an ns x H x W stack (no two are neighbours).
+int64_t blob_candidate_bound(int ns, int64_t H, int64_t W);
+// Appends the strict 3x3x3 maxima above `threshold` outside the border to
+// out (at most cap written) and counts them in *count (to be zeroed first).
+int launch_blob_candidates(const float *cube, int ns, int H, int W, int border, double threshold,
+                           BlobCandidate *out, int64_t cap, unsigned long long *count, void *stream);
 
 // ---- Gaussian planning shared by the entry points (api.cpp) ---------------
 

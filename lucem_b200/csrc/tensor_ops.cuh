@@ -11,6 +11,9 @@
 //   - Frangi, Sato, Meijering: filter/kernels/ridge.rs:11-98 (one scale,
 //                 folded into the running maximum)
 //   - outer products: outer_product_2d_kernel, feature/kernels/structure.rs:22-38
+//   - blob responses: the scaled LoG / DoG (scale_offset_into after the sum
+//                 or difference, core/elementwise.rs:50-75) and doh_scale_kernel
+//                 (feature/kernels/blobs.rs:8-21)
 #pragma once
 
 #include <cuda_runtime.h>
@@ -99,6 +102,15 @@ __device__ __forceinline__ int apply(int mode, float a, float b, float c, float 
         *o0 = shape_index(l1, l2);
         return 1;
     }
+    case kTensorScaledSum:
+        // scale_offset_into of the reference applied to the sum
+        // (gaussian_laplace_into) or difference (difference_of_gaussians_into).
+        *o0 = __fmul_rn(p0, __fadd_rn(a, __fmul_rn(p1, b)));
+        return 1;
+    case kTensorScaledDet:
+        // doh_scale_kernel, crates/lucem-ops/src/feature/kernels/blobs.rs:8-21.
+        *o0 = __fmul_rn(p0, __fsub_rn(__fmul_rn(a, c), __fmul_rn(b, b)));
+        return 1;
     case kTensorOuter:
         *o0 = __fmul_rn(a, a);
         *o1 = __fmul_rn(a, b);

@@ -12,6 +12,7 @@ kernels' load); outputs are float32.
 from __future__ import annotations
 
 import ctypes as C
+import math
 import threading
 from dataclasses import dataclass
 from typing import Optional, Sequence
@@ -33,7 +34,8 @@ __all__ = [
     "wiener_deconvolve", "from_dlpack", "fourier_gaussian", "fourier_box", "fourier_shift", "butterworth",
     "PhaseCorrelationResult", "phase_correlation", "unsupervised_wiener", "hessian_matrix", "hessian_det",
     "hessian_eigvals", "shape_index", "structure_tensor", "structure_tensor_eigvals", "frangi", "sato",
-    "meijering",
+    "meijering", "Blob", "blobs_log", "blobs_dog", "blobs_doh", "pyramid_reduce", "pyramid_expand",
+    "gaussian_pyramid", "laplacian_pyramid",
 ]
 
 
@@ -787,6 +789,150 @@ def meijering(x: torch.Tensor, sigmas=(1.0, 3.0, 5.0, 7.0, 9.0), *, black_ridges
               workspace: Optional[Workspace] = None) -> torch.Tensor:
     """meijering (filter/ridge.rs:199-245): multi-scale neuriteness."""
     return _ridge(N.lib().lucem_meijering, x, sigmas, black_ridges, mode, cval, 0.5, 15.0, out, workspace)
+
+
+def _pyramid_settings(downscale, sigma, order, mode, cval):
+    s = N.PyramidSettings()
+    N.lib().lucem_pyramid_settings_default(C.byref(s))
+    s.downscale = float(downscale)
+    s.sigma = -1.0 if sigma is None else float(sigma)
+    s.order, s.mode, s.cval = int(order), PadMode.parse(mode), float(cval)
+    return s
+
+
+def pyramid_reduce(x, *, downscale=2.0, sigma=None, order=1, mode="reflect", cval=0.0,
+                   workspace: Optional[Workspace] = None) -> torch.Tensor:
+    """pyramid_reduce (crates/lucem-ops/src/transform/pyramid.rs:135-168): the
+    Gaussian blur (sigma default 2 downscale / 6), then the resize to
+    ceil(H / downscale) x ceil(W / downscale) (orders 0 and 1)."""
+    x = from_dlpack(x)
+    ctx, ws = _ctx_ws(x, workspace)
+    if x.dim() != 2:
+        raise LucemError(3, f"pyramid_reduce expects 2-D array, got {x.dim()}-D")
+    oh = max(1, math.ceil(x.shape[0] / float(downscale))) if downscale > 1 else 1
+    ow = max(1, math.ceil(x.shape[1] / float(downscale))) if downscale > 1 else 1
+    out = torch.empty((oh, ow), dtype=torch.float32, device=x.device)
+    s = _pyramid_settings(downscale, sigma, order, mode, cval)
+    ti, to = _tensor(x, "image"), _tensor(out, "output")
+    N.check(N.lib().lucem_pyramid_reduce(ctx.handle, C.byref(ti), C.byref(s), C.byref(to), ws.handle, _stream(x)))
+    return out
+
+
+def pyramid_expand(x, output_shape=None, *, downscale=2.0, sigma=None, order=1, mode="reflect", cval=0.0,
+                   workspace: Optional[Workspace] = None) -> torch.Tensor:
+    """pyramid_expand (transform/pyramid.rs:171-208): the resize up (to
+    output_shape, default ceil(H downscale) x ceil(W downscale)), then the
+    Gaussian blur."""
+    x = from_dlpack(x)
+    ctx, ws = _ctx_ws(x, workspace)
+    if output_shape is None:
+        output_shape = (max(1, math.ceil(x.shape[0] * float(downscale))),
+                        max(1, math.ceil(x.shape[1] * float(downscale))))
+    out = torch.empty(tuple(output_shape), dtype=torch.float32, device=x.device)
+    s = _pyramid_settings(downscale, sigma, order, mode, cval)
+    ti, to = _tensor(x, "image"), _tensor(out, "output")
+    N.check(N.lib().lucem_pyramid_expand(ctx.handle, C.byref(ti), C.byref(s), C.byref(to), ws.handle, _stream(x)))
+    return out
+
+
+def gaussian_pyramid(x, max_layer: int, *, downscale=2.0, sigma=None, order=1, mode="reflect", cval=0.0,
+                     workspace: Optional[Workspace] = None):
+    """gaussian_pyramid (transform/pyramid.rs:211-236): [level_0 (a copy),
+    level_1, ...], at most max_layer reductions, stopping when a level is
+    1 x 1 or stops shrinking."""
+    x = from_dlpack(x)
+    if x.dim() != 2:
+        raise LucemError(3, f"gaussian_pyramid expects 2-D array, got {x.dim()}-D")
+    _pyramid_settings(downscale, sigma, order, mode, cval)
+    if not (math.isfinite(downscale) and downscale > 1.0):
+        raise LucemError(7, f"invalid parameter `downscale`: pyramid scale factor must be > 1.0, got {downscale}")
+    levels = [gaussian_blur(x, [0.0, 0.0], workspace=workspace)]
+    for _ in range(int(max_layer)):
+        cur = levels[-1]
+        if cur.shape[0] <= 1 and cur.shape[1] <= 1:
+            break
+        nxt = pyramid_reduce(cur, downscale=downscale, sigma=sigma, order=order, mode=mode, cval=cval,
+                             workspace=workspace)
+        done = tuple(nxt.shape) == tuple(cur.shape)
+        levels.append(nxt)
+        if done:
+            break
+    return levels
+
+
+def laplacian_pyramid(x, max_layer: int, *, downscale=2.0, sigma=None, order=1, mode="reflect", cval=0.0,
+                      workspace: Optional[Workspace] = None):
+    """laplacian_pyramid (transform/pyramid.rs:239-266): [L_0, ..., L_{N-1},
+    G_N], L_k = G_k - expand(G_{k+1}) to G_k's shape."""
+    g = gaussian_pyramid(x, max_layer, downscale=downscale, sigma=sigma, order=order, mode=mode, cval=cval,
+                         workspace=workspace)
+    if len(g) <= 1:
+        return g
+    ctx, ws = _ctx_ws(g[0], workspace)
+    s = _pyramid_settings(downscale, sigma, order, mode, cval)
+    bands = []
+    for fine, coarse in zip(g[:-1], g[1:]):
+        out = torch.empty_like(fine)
+        tf, tc, to = _tensor(fine, "fine"), _tensor(coarse, "coarse"), _tensor(out, "output")
+        N.check(N.lib().lucem_laplacian_band(ctx.handle, C.byref(tf), C.byref(tc), C.byref(s), C.byref(to),
+                                             ws.handle, _stream(fine)))
+        bands.append(out)
+    return bands + [g[-1]]
+
+
+@dataclass
+class Blob:
+    """crates/lucem-ops/src/feature/blobs.rs:16-30."""
+
+    y: int
+    x: int
+    sigma: float
+    response: float
+
+    def radius(self) -> float:
+        return math.sqrt(2.0) * self.sigma
+
+
+def _blobs(fn, x, min_sigma, max_sigma, num_sigma, sigma_ratio, threshold, overlap, log_scale, exclude_border,
+           workspace):
+    x = from_dlpack(x)
+    ctx, ws = _ctx_ws(x, workspace)
+    s = N.BlobSettings()
+    N.lib().lucem_blob_settings_default(C.byref(s))
+    s.min_sigma, s.max_sigma, s.num_sigma = float(min_sigma), float(max_sigma), int(num_sigma)
+    s.sigma_ratio, s.threshold, s.overlap = float(sigma_ratio), float(threshold), float(overlap)
+    s.log_scale, s.exclude_border = int(bool(log_scale)), int(exclude_border)
+    ti = _tensor(x, "image")
+    cap = 4096
+    while True:
+        buf = (N.BlobC * cap)()
+        n = C.c_int64()
+        N.check(fn(ctx.handle, C.byref(ti), C.byref(s), buf, cap, C.byref(n), ws.handle, _stream(x)))
+        if n.value <= cap:
+            return [Blob(int(b.y), int(b.x), float(b.sigma), float(b.response)) for b in buf[: n.value]]
+        cap = n.value
+
+
+def blobs_log(x, *, min_sigma=1.0, max_sigma=30.0, num_sigma=10, threshold=0.1, overlap=0.5, log_scale=False,
+              exclude_border=1, workspace: Optional[Workspace] = None):
+    """blobs_log (crates/lucem-ops/src/feature/blobs.rs:204-236): scale-normalised
+    LoG blobs, strongest first."""
+    return _blobs(N.lib().lucem_blobs_log, x, min_sigma, max_sigma, num_sigma, 1.6, threshold, overlap, log_scale,
+                  exclude_border, workspace)
+
+
+def blobs_dog(x, *, min_sigma=1.0, max_sigma=30.0, sigma_ratio=1.6, threshold=0.1, overlap=0.5, exclude_border=1,
+              workspace: Optional[Workspace] = None):
+    """blobs_dog (feature/blobs.rs:238-287): difference-of-Gaussians blobs."""
+    return _blobs(N.lib().lucem_blobs_dog, x, min_sigma, max_sigma, 10, sigma_ratio, threshold, overlap, False,
+                  exclude_border, workspace)
+
+
+def blobs_doh(x, *, min_sigma=1.0, max_sigma=30.0, num_sigma=10, threshold=0.1, overlap=0.5, log_scale=False,
+              exclude_border=1, workspace: Optional[Workspace] = None):
+    """blobs_doh (feature/blobs.rs:289-345): determinant-of-Hessian blobs."""
+    return _blobs(N.lib().lucem_blobs_doh, x, min_sigma, max_sigma, num_sigma, 1.6, threshold, overlap, log_scale,
+                  exclude_border, workspace)
 
 
 # ---------------------------------------------------------------------------

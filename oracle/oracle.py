@@ -745,3 +745,204 @@ def ridge_filter(x, kind, sigmas=(1.0, 3.0, 5.0, 7.0, 9.0), black_ridges=True, m
             dom = np.where(np.abs(m1) >= np.abs(m2), m1, m2)
             out = np.maximum(out, np.maximum(dom, _F(0)) if black_ridges else np.maximum(_F(0) - dom, _F(0)))
     return out.astype(_F)
+
+
+# ---------------------------------------------------------------------------
+# Blob detectors (feature/blobs.rs): the f32 scale stack from the restated
+# filters, then the reference's maxima, sort and overlap pruning.
+
+
+def blob_sigmas(min_sigma, max_sigma, num_sigma, log_scale):
+    """BlobDetector::sigmas (blobs.rs:96-111)."""
+    if num_sigma == 1 or abs(max_sigma - min_sigma) <= np.finfo(np.float64).eps:
+        return [min_sigma]
+    out = []
+    for i in range(num_sigma):
+        t = i / (num_sigma - 1)
+        out.append(min_sigma * (max_sigma / min_sigma) ** t if log_scale else min_sigma + t * (max_sigma - min_sigma))
+    return out
+
+
+def dog_sigmas(min_sigma, max_sigma, ratio):
+    """blobs.rs:256-263."""
+    out, s = [], min_sigma
+    while s <= max_sigma * (1.0 + 1e-9):
+        out.append(s)
+        s *= ratio
+    return out or [min_sigma]
+
+
+def blob_stack(x, kind, sigmas, ratio=1.6):
+    """The scale responses of blobs_log / blobs_dog / blobs_doh (blobs.rs:
+    219-232, 265-283, 313-339), f32, reflect padding."""
+    x = np.asarray(x, _F)
+    out = []
+    for sg in sigmas:
+        if kind == "log":
+            a = gaussian_blur(x, [sg, sg], orders=(2, 0)).astype(_F)
+            b = gaussian_blur(x, [sg, sg], orders=(0, 2)).astype(_F)
+            out.append(((a + b) * _F(-(sg * sg))).astype(_F))
+        elif kind == "dog":
+            a = gaussian_blur(x, [sg, sg]).astype(_F)
+            b = gaussian_blur(x, [sg * ratio, sg * ratio]).astype(_F)
+            out.append(((a - b) * _F(1.0 / (ratio - 1.0))).astype(_F))
+        else:
+            a, b, c = hessian_matrix(x, sg)
+            out.append((_F(sg ** 4) * (a * c - b * b)).astype(_F))
+    return np.stack(out)
+
+
+def blob_overlap(a, b):
+    """circle_overlap_fraction (blobs.rs:114-136); a, b: (y, x, sigma)."""
+    r1, r2 = np.sqrt(2.0) * a[2], np.sqrt(2.0) * b[2]
+    d = np.sqrt((a[0] - b[0]) ** 2 + (a[1] - b[1]) ** 2)
+    if d >= r1 + r2:
+        return 0.0
+    if d <= abs(r1 - r2):
+        return 1.0
+    rmin = min(r1, r2)
+    if rmin <= 0.0:
+        return 0.0
+    c1 = min(max((d * d + r1 * r1 - r2 * r2) / (2.0 * d * r1), -1.0), 1.0)
+    c2 = min(max((d * d + r2 * r2 - r1 * r1) / (2.0 * d * r2), -1.0), 1.0)
+    s = (-d + r1 + r2) * (d + r1 - r2) * (d - r1 + r2) * (d + r1 + r2)
+    area = r1 * r1 * np.arccos(c1) + r2 * r2 * np.arccos(c2) - 0.5 * np.sqrt(max(s, 0.0))
+    return area / (np.pi * rmin * rmin)
+
+
+def extract_blobs(cube, sigmas, threshold, overlap, exclude_border=1):
+    """extract_scale_space_blobs (blobs.rs:139-201): strict 3x3x3 maxima with
+    the reference's tie rule (an equal neighbour earlier in (scale, y, x) order
+    wins), threshold and border; sorted by response (descending), y, x; greedy
+    overlap pruning.  Returns [(y, x, sigma, response)]."""
+    cube = np.asarray(cube, _F)
+    ns, H, W = cube.shape
+    b = max(exclude_border, 1)
+    if H <= 2 * b or W <= 2 * b:
+        return []
+    raw = []
+    for s in range(ns):
+        val = cube[s, b:H - b, b:W - b]
+        is_max = val.astype(np.float64) > threshold
+        for ds in (-1, 0, 1):
+            t = s + ds
+            if t < 0 or t >= ns:
+                continue
+            for dy in (-1, 0, 1):
+                for dx in (-1, 0, 1):
+                    if ds == 0 and dy == 0 and dx == 0:
+                        continue
+                    nv = cube[t, b + dy:H - b + dy, b + dx:W - b + dx]
+                    before = ds < 0 or (ds == 0 and (dy < 0 or (dy == 0 and dx < 0)))
+                    is_max &= ~((nv > val) | ((nv == val) & before))
+        for y, x in zip(*np.nonzero(is_max)):
+            raw.append((int(y) + b, int(x) + b, sigmas[s], float(val[y, x]), s))
+    raw.sort(key=lambda r: (-r[3], r[0], r[1], r[4]))
+    kept = []
+    for r in raw:
+        if all(blob_overlap(r, k) <= overlap for k in kept):
+            kept.append(r)
+    return [k[:4] for k in kept]
+
+
+# ---------------------------------------------------------------------------
+# Pyramids (transform/pyramid.rs) with resize's order 0 / 1 resampling
+# (transform/warp.rs:207-251, core/kernels/spline.rs:90-139), f32.
+
+
+def pad_map(p, n, mode):
+    """core/kernels/pad.rs:11-34 on an integer array; -1: the constant."""
+    m = parse_mode(mode) if isinstance(mode, str) else mode
+    p = np.asarray(p, np.int64)
+    inside = (p >= 0) & (p < n)
+    if m == 1:  # constant
+        out = np.full(p.shape, -1, np.int64)
+    elif m == 2:  # nearest
+        out = np.clip(p, 0, n - 1)
+    elif m == 4:  # wrap
+        out = np.mod(p, n)
+    elif m == 0:  # reflect
+        r = np.mod(p, 2 * n)
+        out = np.where(r < n, r, 2 * n - 1 - r)
+    else:  # mirror
+        per = max(2 * n - 2, 1)
+        r = np.mod(p, per)
+        out = np.where(r < n, r, per - r)
+    return np.where(inside, p, out)
+
+
+def resize(x, oh, ow, order=1, mode="reflect", cval=0.0):
+    """resize without anti-aliasing: output (oy, ox) samples the input at
+    (sy oy + (sy - 1)/2, sx ox + (sx - 1)/2), f32, nearest or bilinear."""
+    x = np.asarray(x, _F)
+    H, W = x.shape
+    sy, sx = H / oh, W / ow
+    oy = np.arange(oh, dtype=_F)[:, None]
+    ox = np.arange(ow, dtype=_F)[None, :]
+    y = (_F(sy) * oy + _F(0.5 * (sy - 1.0))).astype(_F)
+    xx = (_F(sx) * ox + _F(0.5 * (sx - 1.0))).astype(_F)
+    y, xx = np.broadcast_to(y, (oh, ow)), np.broadcast_to(xx, (oh, ow))
+
+    def sample(py, px):
+        ok = (py >= 0) & (px >= 0)
+        return np.where(ok, x[np.maximum(py, 0), np.maximum(px, 0)], _F(cval)).astype(_F)
+
+    if order == 0:
+        return sample(pad_map(np.floor(y + _F(0.5)), H, mode), pad_map(np.floor(xx + _F(0.5)), W, mode))
+    y0, x0 = np.floor(y), np.floor(xx)
+    fy, fx = (y - y0).astype(_F), (xx - x0).astype(_F)
+    acc = np.zeros((oh, ow), _F)
+    for dy in (0, 1):
+        wy = (_F(1) - fy) if dy == 0 else fy
+        py = pad_map(y0.astype(np.int64) + dy, H, mode)
+        for dx in (0, 1):
+            wx = (_F(1) - fx) if dx == 0 else fx
+            px = pad_map(x0.astype(np.int64) + dx, W, mode)
+            acc = (acc + (wy * wx).astype(_F) * sample(py, px)).astype(_F)
+    return acc
+
+
+def _pyr_sigma(downscale, sigma):
+    return 2.0 * downscale / 6.0 if sigma is None else sigma
+
+
+def pyramid_reduce(x, downscale=2.0, sigma=None, order=1, mode="reflect", cval=0.0):
+    """pyramid.rs:135-168."""
+    x = np.asarray(x, _F)
+    sg = _pyr_sigma(downscale, sigma)
+    sm = gaussian_blur(x, [sg, sg], mode=mode, cval=cval).astype(_F) if sg > 0 else x
+    oh = max(1, int(np.ceil(x.shape[0] / downscale)))
+    ow = max(1, int(np.ceil(x.shape[1] / downscale)))
+    return resize(sm, oh, ow, order, mode, cval)
+
+
+def pyramid_expand(x, shape=None, downscale=2.0, sigma=None, order=1, mode="reflect", cval=0.0):
+    """pyramid.rs:171-208."""
+    x = np.asarray(x, _F)
+    if shape is None:
+        shape = (max(1, int(np.ceil(x.shape[0] * downscale))), max(1, int(np.ceil(x.shape[1] * downscale))))
+    up = resize(x, shape[0], shape[1], order, mode, cval)
+    sg = _pyr_sigma(downscale, sigma)
+    return gaussian_blur(up, [sg, sg], mode=mode, cval=cval).astype(_F) if sg > 0 else up
+
+
+def gaussian_pyramid(x, max_layer, **kw):
+    """pyramid.rs:211-236."""
+    levels = [np.asarray(x, _F).copy()]
+    for _ in range(max_layer):
+        cur = levels[-1]
+        if cur.shape[0] <= 1 and cur.shape[1] <= 1:
+            break
+        nxt = pyramid_reduce(cur, **kw)
+        levels.append(nxt)
+        if nxt.shape == cur.shape:
+            break
+    return levels
+
+
+def laplacian_pyramid(x, max_layer, **kw):
+    """pyramid.rs:239-266."""
+    g = gaussian_pyramid(x, max_layer, **kw)
+    if len(g) <= 1:
+        return g
+    return [(f - pyramid_expand(c, f.shape, **kw)).astype(_F) for f, c in zip(g[:-1], g[1:])] + [g[-1]]

@@ -317,3 +317,30 @@ def test_structure_and_ridge_oracle_properties(oracle):
     const = np.full((16, 16), 3.0, np.float32)
     for kind in ("frangi", "sato", "meijering"):
         assert np.abs(oracle.ridge_filter(const, kind, [1.0, 2.0])).max() < 1e-6
+
+
+def test_blob_oracle_reference_case(oracle):
+    """crates/lucem-ops/src/feature/blobs.rs:350-392: a 25x25 Gaussian blob
+    (sigma 2.5) at (12, 12); LoG, DoG and DoH each report it first."""
+    y, x = np.mgrid[0:25, 0:25]
+    img = np.exp(-((y - 12.0) ** 2 + (x - 12.0) ** 2) / (2 * 2.5 ** 2)).astype(np.float32)
+    sig = oracle.blob_sigmas(1.5, 4.0, 6, False)
+    for kind, thr, sigmas in (("log", 0.05, sig), ("dog", 0.05, oracle.dog_sigmas(1.5, 4.0, 1.3)),
+                              ("doh", 0.01, sig)):
+        blobs = oracle.extract_blobs(oracle.blob_stack(img, kind, sigmas, 1.3), sigmas, thr, 0.5, 2)
+        assert blobs and blobs[0][:2] == (12, 12), (kind, blobs[:2])
+
+
+def test_pyramid_oracle_reference_case(oracle):
+    """crates/lucem-ops/src/transform/pyramid.rs:271-292: a 4x4 ramp; the
+    Gaussian pyramid of 2 layers has shapes 4x4, 2x2, 1x1 and the Laplacian
+    one three levels starting at 4x4; bilinear resize of a constant is the
+    constant, and resizing by 1 is the identity."""
+    img = np.arange(1, 17, dtype=np.float32).reshape(4, 4)
+    g = oracle.gaussian_pyramid(img, 2)
+    assert [a.shape for a in g] == [(4, 4), (2, 2), (1, 1)]
+    lap = oracle.laplacian_pyramid(img, 2)
+    assert len(lap) == 3 and lap[0].shape == (4, 4)
+    c = np.full((7, 9), 3.0, np.float32)
+    np.testing.assert_allclose(oracle.resize(c, 4, 5), 3.0, rtol=1e-6)
+    np.testing.assert_array_equal(oracle.resize(img, 4, 4, order=1), img)
