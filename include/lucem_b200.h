@@ -59,7 +59,9 @@ typedef enum lucem_status {
     LUCEM_ERR_INVALID_HANDLE = 16       /* NULL / foreign context or workspace */
 } lucem_status;
 
-typedef enum lucem_dtype { LUCEM_U8 = 1, LUCEM_U16 = 2, LUCEM_F32 = 3 } lucem_dtype;
+/* LUCEM_U32: label and edge maps only (lucem_canny's output); every other
+ * entry point refuses it as an unsupported element type. */
+typedef enum lucem_dtype { LUCEM_U8 = 1, LUCEM_U16 = 2, LUCEM_F32 = 3, LUCEM_U32 = 4 } lucem_dtype;
 
 /* crates/lucem-ops/src/core/pad.rs:84-88 (same ids). */
 typedef enum lucem_pad_mode {
@@ -542,6 +544,31 @@ lucem_status lucem_sato(lucem_ctx *ctx, const lucem_tensor *in, const lucem_ridg
 /* crates/lucem-ops/src/filter/ridge.rs:199-235 meijering_into. */
 lucem_status lucem_meijering(lucem_ctx *ctx, const lucem_tensor *in, const lucem_ridge_settings *settings,
                              lucem_tensor *out, lucem_workspace *ws, void *stream);
+
+/* crates/lucem-ops/src/feature/canny.rs:17-45 Canny. */
+typedef struct lucem_canny_settings {
+    double sigma;               /* 1; Gaussian pre-smoothing, >= 0 */
+    int32_t has_low;            /* 0: low threshold 0.1 max |grad| */
+    double low_threshold;
+    int32_t has_high;           /* 0: high threshold 0.2 max |grad| */
+    double high_threshold;
+    int32_t use_quantiles;      /* 1: thresholds are fractions of max |grad| */
+    int32_t mode;               /* lucem_pad_mode (reflect) */
+    double cval;
+} lucem_canny_settings;
+void lucem_canny_settings_default(lucem_canny_settings *s);
+/* crates/lucem-ops/src/feature/canny.rs:47-165 canny: 2-D input -> u32 edge
+ * map (1 on edges).  The Gaussian blur and the Sobel gradients are fused
+ * family launches (the magnitude and the quantised direction in the second
+ * one's epilogue); one kernel does the non-maximum suppression and the
+ * maximum magnitude; the hysteresis, done by the reference as a host BFS
+ * from the strong pixels, is 8-connected component labelling of the pixels
+ * at or above the low threshold on the device (union-find), keeping the
+ * components that hold a pixel at or above the high threshold: the same
+ * edge set.  Synchronises once to read the maximum, unless both thresholds
+ * are given as values. */
+lucem_status lucem_canny(lucem_ctx *ctx, const lucem_tensor *in, const lucem_canny_settings *settings,
+                         lucem_tensor *out, lucem_workspace *ws, void *stream);
 
 /* crates/lucem-ops/src/transform/pyramid.rs:98-133 Pyramid. */
 typedef struct lucem_pyramid_settings {

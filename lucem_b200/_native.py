@@ -21,7 +21,7 @@ STATUS_NAMES = {
     9: "AXIS_OUT_OF_BOUNDS", 10: "REPEATED_AXIS", 11: "TOO_MANY_ELEMENTS", 12: "OUT_OF_DEVICE_MEMORY",
     13: "UNSUPPORTED_DTYPE", 14: "CUDA", 15: "DEVICE_TIMEOUT", 16: "INVALID_HANDLE",
 }
-U8, U16, F32 = 1, 2, 3
+U8, U16, F32, U32 = 1, 2, 3, 4
 PAD_REFLECT, PAD_CONSTANT, PAD_NEAREST, PAD_MIRROR, PAD_WRAP = 0, 1, 2, 3, 4
 RESP_GAUSSIAN, RESP_DOG, RESP_LAPLACE, RESP_GRAD_MAG, RESP_UNSHARP = 0, 1, 2, 3, 4
 
@@ -90,6 +90,12 @@ class BlobSettings(C.Structure):
                 ("log_scale", C.c_int32), ("exclude_border", C.c_int64)]
 
 
+class CannySettings(C.Structure):
+    _fields_ = [("sigma", C.c_double), ("has_low", C.c_int32), ("low_threshold", C.c_double),
+                ("has_high", C.c_int32), ("high_threshold", C.c_double), ("use_quantiles", C.c_int32),
+                ("mode", C.c_int32), ("cval", C.c_double)]
+
+
 class BlobC(C.Structure):
     _fields_ = [("y", C.c_int64), ("x", C.c_int64), ("sigma", C.c_double), ("response", C.c_double)]
 
@@ -143,6 +149,8 @@ SIGNATURES = {
     "lucem_pyramid_reduce": (I32, [P, TP, C.POINTER(PyramidSettings), TP, P, P]),
     "lucem_pyramid_expand": (I32, [P, TP, C.POINTER(PyramidSettings), TP, P, P]),
     "lucem_laplacian_band": (I32, [P, TP, TP, C.POINTER(PyramidSettings), TP, P, P]),
+    "lucem_canny_settings_default": (None, [C.POINTER(CannySettings)]),
+    "lucem_canny": (I32, [P, TP, C.POINTER(CannySettings), TP, P, P]),
     "lucem_blob_settings_default": (None, [C.POINTER(BlobSettings)]),
     "lucem_blobs_log": (I32, [P, TP, C.POINTER(BlobSettings), C.POINTER(BlobC), I64, I64P, P, P]),
     "lucem_blobs_dog": (I32, [P, TP, C.POINTER(BlobSettings), C.POINTER(BlobC), I64, I64P, P, P]),

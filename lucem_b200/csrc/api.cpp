@@ -4189,3 +4189,193 @@ lucem_status lucem_laplacian_band(lucem_ctx *ctx, const lucem_tensor *fine, cons
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Canny (crates/lucem-ops/src/feature/canny.rs:47-165).  One fused family
+// launch gives the Sobel gradients of the smoothed image with the magnitude
+// and the direction sector in its epilogue; one kernel suppresses the
+// non-maxima and reduces the maximum magnitude; four launches do the
+// hysteresis (features.cu).
+
+namespace {
+
+// Correlating with a then with b is correlating with their full convolution
+// (offsets add): the Gaussian's 2 r + 1 taps and a 3-tap Sobel stencil make
+// 2 r + 3 taps.
+std::vector<double> compose3(const std::vector<double> &g, const double (&s)[3]) {
+    std::vector<double> c(g.size() + 2, 0.0);
+    for (size_t k = 0; k < g.size(); ++k)
+        for (int j = 0; j < 3; ++j) c[k + (size_t)j] += g[k] * s[j];
+    return c;
+}
+
+// The gradient launch over `src`: filter 0 differentiates along rows (the
+// reference's gy), filter 1 along columns (gx), each axis' taps given with
+// radius `R`; the epilogue writes |g| and the sector.
+lucem_status canny_gradient_launch(const lucem_tensor *src, int mode, double cval, const std::vector<double> &ty0,
+                                   const std::vector<double> &ty1, const std::vector<double> &tx0,
+                                   const std::vector<double> &tx1, int R, float *mag, float *sector,
+                                   lucem_workspace *ws, void *stream) {
+    FamParams fp;
+    init_fam(&fp, src, mode, cval, 1.0);
+    fp.n_filters = 2;
+    const int kr = fam_kernel_radius(R);
+    const std::vector<double> *t[2][2] = {{&ty0, &ty1}, {&tx0, &tx1}};
+    for (int f = 0; f < 2; ++f) {
+        std::memset(fp.taps0[f], 0, sizeof fp.taps0[f]);
+        std::memset(fp.taps1[f], 0, sizeof fp.taps1[f]);
+        for (size_t i = 0; i < t[f][0]->size(); ++i) {
+            const float a = (float)(*t[f][0])[i], b = (float)(*t[f][1])[i];
+            fp.taps0[f][i + (size_t)(kr - R)] = float2_{a, a};
+            fp.taps1[f][i + (size_t)(kr - R)] = float2_{b, b};
+        }
+        fp.r0[f] = fp.r1[f] = kr;
+    }
+    fp.rmax0 = fp.rmax1 = kr;
+    fp.n_outputs = 3;
+    float *outs[3] = {mag, sector, nullptr};
+    const int64_t n = (int64_t)fp.H * fp.W;
+    for (int k = 0; k < 3; ++k) {
+        FamOutput &o = fp.outs[k];
+        o.out = outs[k];
+        o.plane_stride = n;
+        o.row_pitch = fp.W;
+        o.combine = (int)Combine::kLinear;
+        o.fa = k < 2 ? k : -1;
+        o.fb = -1;
+        o.alpha = 1.0f;
+    }
+    fp.tensor = kTensorCannyGrad;
+    if (lucem_status st = fam_waits(ws, &fp, stream)) return st;
+    int e = timed(kPassFamily, stream, [&] { return launch_family_planes(fp, src->dtype, stream); });
+    return e ? cuda_fail(e, "canny gradient launch") : ok();
+}
+
+}  // namespace
+
+extern "C" {
+
+void lucem_canny_settings_default(lucem_canny_settings *s) {
+    s->sigma = 1.0;
+    s->has_low = 0;
+    s->low_threshold = 0.0;
+    s->has_high = 0;
+    s->high_threshold = 0.0;
+    s->use_quantiles = 0;
+    s->mode = LUCEM_PAD_REFLECT;
+    s->cval = 0.0;
+}
+
+lucem_status lucem_canny(lucem_ctx *ctx, const lucem_tensor *in, const lucem_canny_settings *settings,
+                         lucem_tensor *out, lucem_workspace *ws, void *stream) {
+    TimerScope timer_scope(ws);
+    if (!ctx) return fail(LUCEM_ERR_INVALID_HANDLE, "null context");
+    if (!ws) return fail(LUCEM_ERR_INVALID_HANDLE, "a workspace is required");
+    lucem_canny_settings def;
+    lucem_canny_settings_default(&def);
+    const lucem_canny_settings *s = settings ? settings : &def;
+    lucem_status st;
+    if ((st = check_tensor("image", in)) || (st = check_2d("canny", in))) return st;
+    if (!std::isfinite(s->sigma) || s->sigma < 0.0)
+        return fail(LUCEM_ERR_INVALID_PARAMETER,
+                    "invalid parameter `sigma`: sigma must be non-negative and finite, got %g", s->sigma);
+    if ((st = check_mode(s->mode))) return st;
+    // The output: a u32 edge map of the image's shape.
+    if (!out) return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `output`: null tensor");
+    if (out->dtype != LUCEM_U32)
+        return fail(LUCEM_ERR_UNSUPPORTED_DTYPE, "canny writes a u32 edge map, got element type %d", out->dtype);
+    if ((st = same_shape("image", in, "output", out))) return st;
+    const int64_t n = numel(in), H = in->dims[0], W = in->dims[1];
+    if (n == 0) return ok();
+    if (!out->data) return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `output`: null data pointer");
+    {
+        const uintptr_t a0 = reinterpret_cast<uintptr_t>(in->data), a1 = a0 + (uintptr_t)n * dtype_size(in->dtype);
+        const uintptr_t b0 = reinterpret_cast<uintptr_t>(out->data), b1 = b0 + (uintptr_t)n * 4u;
+        if (a0 < b1 && b0 < a1)
+            return fail(LUCEM_ERR_ALIASED_BUFFERS, "input and output arrays must not share the same device buffer");
+    }
+    if (H >= (1 << 30) || W >= (1 << 30))
+        return fail(LUCEM_ERR_TOO_MANY_ELEMENTS, "canny: a side of 2^30 or more");
+    void *pm = nullptr, *ps = nullptr, *pn = nullptr, *px = nullptr;
+    if ((st = ws->get("canny_mag", (size_t)n * sizeof(float), &pm)) ||
+        (st = ws->get("canny_sector", (size_t)n * sizeof(float), &ps)) ||
+        (st = ws->get("canny_nms", (size_t)n * sizeof(float), &pn)) || (st = ws->get("canny_max", 64, &px)))
+        return st;
+    float *mag = static_cast<float *>(pm), *sector = static_cast<float *>(ps), *nms = static_cast<float *>(pn);
+    cudaStream_t cs = static_cast<cudaStream_t>(stream);
+
+    // Gaussian pre-smoothing (truncate 4; sigma 0 leaves the image as it is),
+    // then the Sobel stencils (gradient.rs:71-107).
+    const double deriv[3] = {-1.0, 0.0, 1.0}, smooth[3] = {1.0, 2.0, 1.0};
+    const int64_t r = s->sigma > 0.0 ? (int64_t)radius_of(4.0, s->sigma) : 0;
+    std::vector<double> g((size_t)(2 * r + 1), 1.0);
+    if (s->sigma > 0.0) gaussian_taps(s->sigma, 0, r, g.data());
+    // For the reflect, mirror and wrap extensions, the smoothed image's
+    // extension is the smoothing of the input's (a symmetric kernel on a
+    // symmetric or periodic signal), so the stencils compose with the
+    // Gaussian into one filter over the input.  The constant and nearest
+    // extensions do not commute with the blur: those smooth first, as the
+    // reference does.
+    const bool compose = (s->mode == LUCEM_PAD_REFLECT || s->mode == LUCEM_PAD_MIRROR || s->mode == LUCEM_PAD_WRAP) &&
+                         r + 1 <= kFamMaxRadius;
+    if (compose) {
+        const std::vector<double> gd = compose3(g, deriv), gs = compose3(g, smooth);
+        st = canny_gradient_launch(in, s->mode, s->cval, gd, gs, gs, gd, (int)r + 1, mag, sector, ws, stream);
+    } else {
+        // The smoothed image goes through the nms slot (free until the
+        // suppression writes it).
+        std::vector<Pass> passes;
+        if (s->sigma > 0.0) passes = {Pass{0, s->sigma, 0, r}, Pass{1, s->sigma, 0, r}};
+        if ((st = run_passes(ctx, in, passes, s->mode, s->cval, 1.0, nms, ws, stream))) return st;
+        lucem_tensor view = *in;
+        view.data = nms;
+        view.dtype = LUCEM_F32;
+        const std::vector<double> d(deriv, deriv + 3), sm(smooth, smooth + 3);
+        st = canny_gradient_launch(&view, s->mode, s->cval, d, sm, sm, d, 1, mag, sector, ws, stream);
+    }
+    if (st) return st;
+
+    unsigned int *max_bits = static_cast<unsigned int *>(px);
+    CUDA_TRY(cudaMemsetAsync(max_bits, 0, sizeof *max_bits, cs), "maximum reset");
+    int e = timed(kPassElementwise, stream,
+                  [&] { return launch_canny_nms(mag, sector, nms, (int)H, (int)W, max_bits, stream); });
+    if (e) return cuda_fail(e, "non-maximum suppression launch");
+
+    // Thresholds (canny.rs:108-121); the maximum is needed unless both
+    // thresholds are given as values.
+    double max_mag = 0.0;
+    if (!(s->has_low && s->has_high && !s->use_quantiles)) {
+        unsigned int bits = 0;
+        CUDA_TRY(cudaMemcpyAsync(&bits, max_bits, sizeof bits, cudaMemcpyDeviceToHost, cs), "maximum download");
+        CUDA_TRY(cudaStreamSynchronize(cs), "synchronise");
+        float m;
+        std::memcpy(&m, &bits, sizeof m);
+        max_mag = std::max((double)m, 0.0);
+    }
+    double low = s->has_low ? s->low_threshold : 0.1 * max_mag;
+    double high = s->has_high ? s->high_threshold : 0.2 * max_mag;
+    if (s->use_quantiles) {
+        low *= max_mag;
+        high *= max_mag;
+    }
+    if (high < low)
+        return fail(LUCEM_ERR_INVALID_PARAMETER,
+                    "invalid parameter `high_threshold`: high_threshold (%g) must be >= low_threshold (%g)", high,
+                    low);
+    uint32_t *edges = static_cast<uint32_t *>(out->data);
+    // No strong pixel can exist unless high > 0; with low <= 0 nothing grows
+    // from them, so the mask is the strong pixels themselves.
+    if (!(high > 0.0)) {
+        CUDA_TRY(cudaMemsetAsync(edges, 0, (size_t)n * sizeof(uint32_t), cs), "edge map reset");
+        return ok();
+    }
+    const double mask_low = low > 0.0 ? low : high;
+    // The sector slot is free after the suppression: it holds the labels.
+    e = timed(kPassElementwise, stream, [&] {
+        return launch_canny_hysteresis(nms, (int)H, (int)W, mask_low, high, reinterpret_cast<uint32_t *>(sector),
+                                       edges, stream);
+    });
+    return e ? cuda_fail(e, "hysteresis launch") : ok();
+}
+
+}  // extern "C"

@@ -1,5 +1,5 @@
-// features.cu -- the resampling of the pyramids, and the scale-space maxima
-// of the blob detectors.
+// features.cu -- the resampling of the pyramids, the scale-space maxima of
+// the blob detectors, and Canny's suppression and hysteresis.
 //
 // Resampling (resize, crates/lucem-ops/src/transform/warp.rs:207-251, through
 // affine_coords_2d_kernel, transform/kernels/warp.rs:10-33, and the order 0
@@ -21,6 +21,17 @@
 // No two survivors are neighbours (each would have to beat the other), so at
 // most one survives per 2 x 2 x 2 block: ceil(ns/2) ceil(H/2) ceil(W/2)
 // bounds the list (blob_candidate_bound).
+//
+// Canny (crates/lucem-ops/src/feature/canny.rs:47-165): the non-maximum
+// suppression of canny_nms_kernel (feature/kernels/canny.rs:44-86), with the
+// maximum gradient magnitude reduced in the same pass, and the hysteresis.
+// The reference's hysteresis is a host BFS from the strong pixels (nms >=
+// high) through the weak ones (nms >= low), 8-connected.  The pixels it
+// reaches are exactly the 8-connected components of the weak mask that hold
+// a strong pixel, so here it is connected-component labelling on the device:
+// union-find over the mask where a label only ever moves to a smaller pixel
+// index (atomicMin), roots flagged by their strong pixels, then every masked
+// pixel takes its root's flag.  Four launches, no host round trip.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -116,7 +127,150 @@ __global__ void resample_kernel(const float *__restrict__ in, int H, int W, floa
     }
 }
 
+__global__ void __launch_bounds__(256) canny_nms_kernel(const float *__restrict__ mag,
+                                                        const float *__restrict__ sector, float *__restrict__ nms,
+                                                        int H, int W, unsigned int *__restrict__ max_bits) {
+    const int64_t total = (int64_t)H * W;
+    float local = 0.0f;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        const int y = (int)(i / W), x = (int)(i - (int64_t)y * W);
+        const float m = mag[i];
+        if (m > local) local = m;  // NaN and -0 never raise it
+        float v = 0.0f;
+        if (y > 0 && x > 0 && y + 1 < H && x + 1 < W) {
+            const int s = (int)sector[i];
+            // Sector 0 compares along the row, 2 along the column, 1 on the
+            // main diagonal, 3 on the anti-diagonal.
+            const int64_t d = s == 0 ? 1 : (s == 2 ? W : (s == 1 ? (int64_t)W + 1 : (int64_t)W - 1));
+            const float n1 = mag[i - d], n2 = mag[i + d];
+            v = (m >= n1 && m >= n2) ? m : 0.0f;
+        }
+        nms[i] = v;
+    }
+    // Block maximum, then one atomic per block: non-negative floats order as
+    // their bit patterns do.
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) local = fmaxf(local, __shfl_xor_sync(0xffffffffu, local, o));
+    __shared__ float warp_max[8];
+    if ((threadIdx.x & 31) == 0) warp_max[threadIdx.x >> 5] = local;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float b = warp_max[0];
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) b = fmaxf(b, warp_max[w]);
+        atomicMax(max_bits, __float_as_uint(b));
+    }
+}
+
+constexpr uint32_t kNoLabel = 0xffffffffu;
+
+// Root of x: labels point to smaller indices until a root points to itself,
+// so the walk ends within x steps.  Loads bypass L1 (other SMs relink).
+__device__ __forceinline__ uint32_t find_root(const uint32_t *labels, uint32_t x) {
+    uint32_t p = __ldcg(labels + x);
+    while (p != x) {
+        x = p;
+        p = __ldcg(labels + x);
+    }
+    return x;
+}
+
+// Joins the trees of a and b by hanging the larger root under the smaller.
+// When the atomic finds the larger root already relinked, the retry starts
+// from the value it found, which is smaller: every retry lowers a + b, so
+// the loop ends within 2 n rounds (the bound below is never reached).
+__device__ __forceinline__ void unite(uint32_t *labels, uint32_t a, uint32_t b, int64_t bound) {
+    for (int64_t it = 0; it < bound; ++it) {
+        a = find_root(labels, a);
+        b = find_root(labels, b);
+        if (a == b) return;
+        if (a < b) {
+            const uint32_t t = a;
+            a = b;
+            b = t;
+        }
+        const uint32_t old = atomicMin(labels + a, b);
+        if (old == a) return;
+        a = old;
+    }
+}
+
+__global__ void canny_label_init_kernel(const float *__restrict__ nms, int64_t total, double low,
+                                        uint32_t *__restrict__ labels, uint32_t *__restrict__ edges) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        labels[i] = (double)nms[i] >= low ? (uint32_t)i : kNoLabel;
+        edges[i] = 0u;
+    }
+}
+
+// Unions with the four neighbours that come before the pixel in raster
+// order (left, and the three above); the other four do the same towards it.
+__global__ void canny_label_merge_kernel(int H, int W, uint32_t *__restrict__ labels) {
+    const int64_t total = (int64_t)H * W, bound = 2 * total + 2;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        if (__ldcg(labels + i) == kNoLabel) continue;
+        const int y = (int)(i / W), x = (int)(i - (int64_t)y * W);
+        if (x > 0 && __ldcg(labels + i - 1) != kNoLabel) unite(labels, (uint32_t)i, (uint32_t)(i - 1), bound);
+        if (y > 0) {
+            for (int dx = -1; dx <= 1; ++dx) {
+                const int nx = x + dx;
+                if (nx < 0 || nx >= W) continue;
+                const int64_t j = i - W + dx;
+                if (__ldcg(labels + j) != kNoLabel) unite(labels, (uint32_t)i, (uint32_t)j, bound);
+            }
+        }
+    }
+}
+
+// Every masked pixel's label becomes its root; a strong pixel flags its root.
+__global__ void canny_label_root_kernel(const float *__restrict__ nms, int64_t total, double high,
+                                        uint32_t *__restrict__ labels, uint32_t *__restrict__ edges) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        if (__ldcg(labels + i) == kNoLabel) continue;
+        const uint32_t r = find_root(labels, (uint32_t)i);
+        labels[i] = r;
+        if ((double)nms[i] >= high) edges[r] = 2u;
+    }
+}
+
+// Edges: the masked pixels whose root was flagged.  A root rewrites its own
+// flag 2 -> 1 while others read it; both are non-zero.
+__global__ void canny_label_final_kernel(int64_t total, const uint32_t *__restrict__ labels,
+                                         uint32_t *__restrict__ edges) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t r = labels[i];
+        edges[i] = (r != kNoLabel && __ldcg(edges + r) != 0u) ? 1u : 0u;
+    }
+}
+
+unsigned grid_for(int64_t total, int threads) {
+    int64_t blocks = (total + threads - 1) / threads;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    return (unsigned)(blocks < 1 ? 1 : blocks);
+}
+
 }  // namespace
+
+int launch_canny_nms(const float *mag, const float *sector, float *nms, int H, int W, unsigned int *max_bits,
+                     void *stream) {
+    const int64_t total = (int64_t)H * W;
+    if (total <= 0) return 0;
+    canny_nms_kernel<<<grid_for(total, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(mag, sector, nms, H, W,
+                                                                                          max_bits);
+    return (int)cudaGetLastError();
+}
+
+int launch_canny_hysteresis(const float *nms, int H, int W, double low, double high, uint32_t *labels,
+                            uint32_t *edges, void *stream) {
+    const int64_t total = (int64_t)H * W;
+    if (total <= 0) return 0;
+    cudaStream_t cs = static_cast<cudaStream_t>(stream);
+    const unsigned g = grid_for(total, 256);
+    canny_label_init_kernel<<<g, 256, 0, cs>>>(nms, total, low, labels, edges);
+    canny_label_merge_kernel<<<g, 256, 0, cs>>>(H, W, labels);
+    canny_label_root_kernel<<<g, 256, 0, cs>>>(nms, total, high, labels, edges);
+    canny_label_final_kernel<<<g, 256, 0, cs>>>(total, labels, edges);
+    return (int)cudaGetLastError();
+}
 
 int launch_resample(const float *in, int H, int W, float *out, int OH, int OW, float m0, float m2, float m4,
                     float m5, int order, int mode, float cval, void *stream) {

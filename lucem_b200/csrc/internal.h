@@ -59,6 +59,7 @@ enum TensorMode : int32_t {
     kTensorOuter = 7,      // (a, b) = (g_r, g_c): out0 = a a, out1 = a b, out2 = b b
     kTensorScaledSum = 8,  // out0 = p0 (a + p1 b), each step rounded (LoG / DoG responses)
     kTensorScaledDet = 9,  // out0 = p0 (a c - b^2) (determinant-of-Hessian response)
+    kTensorCannyGrad = 10, // (a, b) = (g_r, g_c): out0 = |g|, out1 = the direction sector 0..3 (as f32)
 };
 
 // One launch of the fused 2-D family kernel over B planes of [H, W] (or over
@@ -157,6 +158,14 @@ int launch_tensor_elementwise(const float *a, const float *b, const float *c, fl
 // the input sampled at (m0 oy + m2, m4 ox + m5), pad map outside).
 int launch_resample(const float *in, int H, int W, float *out, int OH, int OW, float m0, float m2, float m4,
                     float m5, int order, int mode, float cval, void *stream);
+// features.cu: Canny's non-maximum suppression (nms, and the maximum of mag
+// as non-negative float bits in *max_bits, to be zeroed first) and its
+// hysteresis by connected components: edges = 1 on the components of
+// (nms >= low) that hold a pixel with nms >= high (labels: H W scratch).
+int launch_canny_nms(const float *mag, const float *sector, float *nms, int H, int W, unsigned int *max_bits,
+                     void *stream);
+int launch_canny_hysteresis(const float *nms, int H, int W, double low, double high, uint32_t *labels,
+                            uint32_t *edges, void *stream);
 // features.cu: scale-space maxima of the blob detectors.
 struct BlobCandidate {
     float response;

@@ -111,6 +111,13 @@ __device__ __forceinline__ int apply(int mode, float a, float b, float c, float 
         // doh_scale_kernel, crates/lucem-ops/src/feature/kernels/blobs.rs:8-21.
         *o0 = __fmul_rn(p0, __fsub_rn(__fmul_rn(a, c), __fmul_rn(b, b)));
         return 1;
+    case kTensorCannyGrad: {
+        // canny_grad_dir_kernel, crates/lucem-ops/src/feature/kernels/canny.rs:13-41.
+        *o0 = __fsqrt_rn(__fadd_rn(__fmul_rn(a, a), __fmul_rn(b, b)));
+        const float ay = fabsf(a), ax = fabsf(b), t = 0.41421357f;
+        *o1 = ay <= __fmul_rn(ax, t) ? 0.0f : (ax <= __fmul_rn(ay, t) ? 2.0f : (__fmul_rn(a, b) >= 0.0f ? 1.0f : 3.0f));
+        return 2;
+    }
     case kTensorOuter:
         *o0 = __fmul_rn(a, a);
         *o1 = __fmul_rn(a, b);

@@ -35,7 +35,7 @@ __all__ = [
     "PhaseCorrelationResult", "phase_correlation", "unsupervised_wiener", "hessian_matrix", "hessian_det",
     "hessian_eigvals", "shape_index", "structure_tensor", "structure_tensor_eigvals", "frangi", "sato",
     "meijering", "Blob", "blobs_log", "blobs_dog", "blobs_doh", "pyramid_reduce", "pyramid_expand",
-    "gaussian_pyramid", "laplacian_pyramid",
+    "gaussian_pyramid", "laplacian_pyramid", "canny",
 ]
 
 
@@ -53,7 +53,7 @@ class PadMode:
         return out.value
 
 
-_DTYPES = {torch.float32: N.F32, torch.uint8: N.U8, torch.uint16: N.U16}
+_DTYPES = {torch.float32: N.F32, torch.uint8: N.U8, torch.uint16: N.U16, torch.uint32: N.U32}
 
 # ---------------------------------------------------------------------------
 # Context / workspace
@@ -933,6 +933,32 @@ def blobs_doh(x, *, min_sigma=1.0, max_sigma=30.0, num_sigma=10, threshold=0.1, 
     """blobs_doh (feature/blobs.rs:289-345): determinant-of-Hessian blobs."""
     return _blobs(N.lib().lucem_blobs_doh, x, min_sigma, max_sigma, num_sigma, 1.6, threshold, overlap, log_scale,
                   exclude_border, workspace)
+
+
+@_dlpack_args
+def canny(x: torch.Tensor, sigma: float = 1.0, low_threshold: Optional[float] = None,
+          high_threshold: Optional[float] = None, use_quantiles: bool = False, mode="reflect", cval: float = 0.0, *,
+          out: Optional[torch.Tensor] = None, workspace: Optional[Workspace] = None) -> torch.Tensor:
+    """canny (crates/lucem-ops/src/feature/canny.rs:47-165): Gaussian
+    smoothing, Sobel gradients, non-maximum suppression along the quantised
+    direction and 8-connected hysteresis; a u32 edge map (1 on edges).
+    Thresholds default to 0.1 / 0.2 of the maximum gradient magnitude; with
+    use_quantiles they are fractions of it."""
+    ctx, ws = _ctx_ws(x, workspace)
+    if out is None:
+        out = torch.empty(x.shape, dtype=torch.uint32, device=x.device)
+    s = N.CannySettings()
+    N.lib().lucem_canny_settings_default(C.byref(s))
+    s.sigma = float(sigma)
+    if low_threshold is not None:
+        s.has_low, s.low_threshold = 1, float(low_threshold)
+    if high_threshold is not None:
+        s.has_high, s.high_threshold = 1, float(high_threshold)
+    s.use_quantiles = int(bool(use_quantiles))
+    s.mode, s.cval = PadMode.parse(mode), float(cval)
+    ti, to = _tensor(x, "image"), _tensor(out, "output")
+    N.check(N.lib().lucem_canny(ctx.handle, C.byref(ti), C.byref(s), C.byref(to), ws.handle, _stream(x)))
+    return out
 
 
 # ---------------------------------------------------------------------------

@@ -946,3 +946,90 @@ def laplacian_pyramid(x, max_layer, **kw):
     if len(g) <= 1:
         return g
     return [(f - pyramid_expand(c, f.shape, **kw)).astype(_F) for f, c in zip(g[:-1], g[1:])] + [g[-1]]
+
+
+def canny_gradients(x, sigma=1.0, mode="reflect", cval=0.0):
+    """canny.rs:64-106 with canny_grad_dir_kernel (feature/kernels/canny.rs:
+    13-41): the Gaussian pre-smoothing, the Sobel stencils as two correlate
+    passes each (filter/gradient.rs:71-107), then in f32 the magnitude and the
+    direction sector (0 along rows, 2 along columns, 1 / 3 the diagonals)."""
+    x = np.asarray(x, _F)
+    sm = gaussian_blur(x, [sigma, sigma], mode=mode, cval=cval).astype(_F)
+    d, s = [-1.0, 0.0, 1.0], [1.0, 2.0, 1.0]
+    gy = correlate_1d(correlate_1d(sm, d, 0, mode, cval), s, 1, mode, cval).astype(_F)
+    gx = correlate_1d(correlate_1d(sm, s, 0, mode, cval), d, 1, mode, cval).astype(_F)
+    mag = np.sqrt(gy * gy + gx * gx).astype(_F)
+    ay, ax, t = np.abs(gy), np.abs(gx), _F(0.41421357)
+    sector = np.where(ay <= ax * t, 0, np.where(ax <= ay * t, 2, np.where(gy * gx >= 0, 1, 3)))
+    return mag, sector.astype(np.int32)
+
+
+def canny_nms(mag, sector):
+    """canny_nms_kernel (feature/kernels/canny.rs:44-86): border pixels 0; an
+    interior pixel keeps its magnitude when it is >= both neighbours along its
+    sector's direction."""
+    mag = np.asarray(mag, _F)
+    H, W = mag.shape
+    nms = np.zeros_like(mag)
+    if H < 3 or W < 3:
+        return nms
+    c, s = mag[1:-1, 1:-1], sector[1:-1, 1:-1]
+
+    def at(dy, dx):
+        return mag[1 + dy:H - 1 + dy, 1 + dx:W - 1 + dx]
+
+    conds = [s == 0, s == 2, s == 1]
+    n1 = np.select(conds, [at(0, -1), at(-1, 0), at(-1, -1)], at(-1, 1))
+    n2 = np.select(conds, [at(0, 1), at(1, 0), at(1, 1)], at(1, -1))
+    nms[1:-1, 1:-1] = np.where((c >= n1) & (c >= n2), c, _F(0))
+    return nms
+
+
+def canny_thresholds(max_mag, low=None, high=None, use_quantiles=False):
+    """canny.rs:108-121."""
+    lo = 0.1 * max_mag if low is None else float(low)
+    hi = 0.2 * max_mag if high is None else float(high)
+    if use_quantiles:
+        lo, hi = lo * max_mag, hi * max_mag
+    if hi < lo:
+        raise ValueError(f"high_threshold ({hi}) must be >= low_threshold ({lo})")
+    return lo, hi
+
+
+def canny_hysteresis(nms, low, high):
+    """canny.rs:123-162: breadth-first from every pixel with nms >= high
+    (when high > 0) through the 8-neighbours with nms >= low (when low > 0)."""
+    from collections import deque
+    v = np.asarray(nms, np.float64)
+    H, W = v.shape
+    edges = ((v >= high) & (high > 0)).ravel()
+    weak = ((v >= low) & (low > 0)).ravel()
+    q = deque(np.flatnonzero(edges).tolist())
+    while q:
+        i = q.popleft()
+        y, x = divmod(i, W)
+        for dy in (-1, 0, 1):
+            for dx in (-1, 0, 1):
+                ny, nx = y + dy, x + dx
+                if (dy or dx) and 0 <= ny < H and 0 <= nx < W:
+                    j = ny * W + nx
+                    if not edges[j] and weak[j]:
+                        edges[j] = True
+                        q.append(j)
+    return edges.reshape(H, W).astype(np.uint32)
+
+
+def canny(x, sigma=1.0, low_threshold=None, high_threshold=None, use_quantiles=False, mode="reflect", cval=0.0):
+    """canny (feature/canny.rs:47-165): u32 edge map."""
+    x = np.asarray(x, _F)
+    if x.ndim != 2:
+        raise ValueError("canny expects a 2-D array")
+    if not np.isfinite(sigma) or sigma < 0:
+        raise ValueError(f"sigma must be non-negative and finite, got {sigma}")
+    if x.size == 0:
+        return np.zeros(x.shape, np.uint32)
+    mag, sector = canny_gradients(x, sigma, mode, cval)
+    nms = canny_nms(mag, sector)
+    max_mag = max(float(np.max(mag)), 0.0)
+    lo, hi = canny_thresholds(max_mag, low_threshold, high_threshold, use_quantiles)
+    return canny_hysteresis(nms, lo, hi)

@@ -344,3 +344,24 @@ def test_pyramid_oracle_reference_case(oracle):
     c = np.full((7, 9), 3.0, np.float32)
     np.testing.assert_allclose(oracle.resize(c, 4, 5), 3.0, rtol=1e-6)
     np.testing.assert_array_equal(oracle.resize(img, 4, 4, order=1), img)
+
+
+def test_canny_oracle_reference_case(oracle):
+    """crates/lucem-ops/src/feature/canny.rs:172-189: a 10x10 square of ones
+    in a 20x20 image, sigma 1: 28..60 edge pixels, none inside or at the
+    corner.  Then the hysteresis rules on a hand-made suppression map: weak
+    pixels join only through 8-connected chains to a strong one, and a low
+    threshold of 0 grows nothing."""
+    data = np.zeros((20, 20), np.float32)
+    data[5:15, 5:15] = 1.0
+    e = oracle.canny(data, 1.0)
+    assert e.dtype == np.uint32 and 28 <= int(e.sum()) <= 60
+    assert e[10, 10] == 0 and e[0, 0] == 0
+    nms = np.zeros((6, 7), np.float32)
+    nms[1, 1], nms[2, 2], nms[3, 3] = 5.0, 2.0, 2.0   # strong, then a diagonal chain of weak pixels
+    nms[1, 5], nms[2, 5] = 2.0, 2.0                     # weak, not connected
+    np.testing.assert_array_equal(np.argwhere(oracle.canny_hysteresis(nms, 1.0, 4.0)), [[1, 1], [2, 2], [3, 3]])
+    np.testing.assert_array_equal(np.argwhere(oracle.canny_hysteresis(nms, 0.0, 4.0)), [[1, 1]])
+    assert oracle.canny_hysteresis(nms, 1.0, 0.0).sum() == 0
+    with pytest.raises(ValueError):
+        oracle.canny_thresholds(10.0, 0.5, 0.4)
