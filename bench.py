@@ -612,6 +612,54 @@ def structure_secondary(dev, peak, reps=10):
                          "frac": achieved / peak, "algorithmic_bytes": px * 12, "traffic": None}}
 
 
+def features_secondary(dev, reps=5):
+    """The remaining Gaussian consumers on the blob image scaled to [0, 1]
+    (2048 x 2048 f32): Canny at sigma 2 (default thresholds: one host read of
+    the maximum), LoG / DoH blob detection with scales 1..10 (10 scales; the
+    per-axis path above sigma 7.9) and DoG (ratio 1.6), threshold 0.1; the
+    Gaussian and Laplacian pyramids (5 layers) of a 4096 x 4096 f32 image.
+    Device ms per call, L2 flushed.  The CPU figures time the oracle's
+    restatements (its C filters, numpy per-pixel steps, Python hysteresis
+    and pruning) on the host: Canny and the pyramid at the same sizes, LoG
+    blobs at 1024 x 1024."""
+    import torch
+
+    import lucem_b200 as lb
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    h = lb.synth.blob_image().astype(np.float32)
+    h /= h.max()
+    x = torch.from_numpy(h).to(dev)
+    big = torch.from_numpy(np.tile(h, (2, 2))).to(dev)
+    ws = lb.Workspace(dev.index)
+    kw = dict(min_sigma=1.0, max_sigma=10.0, threshold=0.1, workspace=ws)
+    res = {"ms_canny_2048_sigma2": _timed_calls(dev, lambda: lb.canny(x, 2.0, workspace=ws), reps),
+           "ms_blobs_log_2048": _timed_calls(dev, lambda: lb.blobs_log(x, num_sigma=10, **kw), reps),
+           "ms_blobs_doh_2048": _timed_calls(dev, lambda: lb.blobs_doh(x, num_sigma=10, **kw), reps),
+           "ms_blobs_dog_2048": _timed_calls(dev, lambda: lb.blobs_dog(x, sigma_ratio=1.6, **kw), reps),
+           "ms_gaussian_pyramid_4096_5": _timed_calls(dev, lambda: lb.gaussian_pyramid(big, 5, workspace=ws), reps),
+           "ms_laplacian_pyramid_4096_5": _timed_calls(dev, lambda: lb.laplacian_pyramid(big, 5, workspace=ws),
+                                                       reps)}
+    res["n_blobs_log_2048"] = len(lb.blobs_log(x, num_sigma=10, **kw))
+    res["canny_gpix_s"] = x.numel() / (res["ms_canny_2048_sigma2"] * 1e-3) / 1e9
+    t0 = time.perf_counter()
+    O.canny(h, 2.0)
+    res["cpu_ms_canny_2048_sigma2"] = 1e3 * (time.perf_counter() - t0)
+    t0 = time.perf_counter()
+    sig = O.blob_sigmas(1.0, 10.0, 10, False)
+    O.extract_blobs(O.blob_stack(h[:1024, :1024].copy(), "log", sig), sig, 0.1, 0.5, 1)
+    res["cpu_ms_blobs_log_1024"] = 1e3 * (time.perf_counter() - t0)
+    t0 = time.perf_counter()
+    O.gaussian_pyramid(np.tile(h, (2, 2)), 5)
+    res["cpu_ms_gaussian_pyramid_4096_5"] = 1e3 * (time.perf_counter() - t0)
+    res["metric"] = ("canny (2048^2, sigma 2), blobs_log / doh / dog (2048^2, sigma 1..10), gaussian / laplacian "
+                     "pyramid (4096^2, 5 layers), ms per call")
+    res["cpu"] = "oracle restatements, one call each, on the host (LoG blobs at 1024^2)"
+    return res
+
+
 def pipeline_u16_secondary(dev, reps=5):
     """The raw u16 tile upload on the pipeline path: a 4096 x 4096 u16 host
     tile through run_op (Gaussian blur, sigma 2, input scale 1/65535), end to
@@ -950,6 +998,7 @@ def run_ours(args, rank, world, local_rank):
     if args.consumers:
         line["secondary"]["spectral_ops"] = spectral_ops_secondary(dev)
         line["secondary"]["structure"] = structure_secondary(dev, peak)
+        line["secondary"]["features"] = features_secondary(dev)
         line["secondary"]["pipeline_u16"] = pipeline_u16_secondary(dev)
     print(json.dumps(line), flush=True)
 
@@ -969,8 +1018,8 @@ def main():
     ap.add_argument("--rl-batch", type=int, default=1, help="also measure the batched uneven 2-D RL")
     ap.add_argument("--gauss-batch", type=int, default=1, help="also measure the batch of separate images")
     ap.add_argument("--consumers", type=int, default=1,
-                    help="also measure the spectral operators, the Gaussian-consumer operators and the u16 "
-                         "pipeline upload")
+                    help="also measure the spectral operators, the Gaussian-consumer operators (Hessian, "
+                         "ridge, structure tensor, Canny, blobs, pyramids) and the u16 pipeline upload")
     args = ap.parse_args()
     ITERS = args.iters
     world = int(os.environ.get("WORLD_SIZE", "1"))
