@@ -253,7 +253,7 @@ __device__ __forceinline__ void tensor_epilogue(const FamParams &p, const TileGe
 // TENSOR: the tensor epilogue (FamParams::tensor) is compiled in; kernels
 // that never take it (the tile walk, the batch) leave it out.
 template <typename T, int NOUT, int RF = -1, bool STAGED = false, bool TENSOR = false>
-__device__ void family_tile(const FamParams &p, const TileGeom &g, float *A, float *IT) {
+__device__ void family_tile(const FamParams &p, const TileGeom &g, float *A, float *IT, bool preloaded = false) {
     const int tid = threadIdx.x;
     // RF >= 0: one filter whose two kernel radii are both RF, known at compile
     // time (strides and tap loops become constants).
@@ -268,7 +268,8 @@ __device__ void family_tile(const FamParams &p, const TileGeom &g, float *A, flo
     // ...; each lane covers columns lane, lane + 32, ... of a row (no index
     // division), and every lane issues the loads of 4 rows before storing
     // any of them, so many global loads are in flight per warp.
-    if constexpr (!STAGED) {
+    // preloaded: A already holds the window (copied ahead by the caller).
+    if (!STAGED && !preloaded) {
         const int wy0 = g.oy - g.rb_y - R0, wx0 = g.ox - g.rb_x - R1;  // window origin in the read box
         const T *wbase = in + (int64_t)g.rb_y * ipitch + g.rb_x;
         const bool interior = wy0 >= 0 && wx0 >= 0 && wy0 + AH <= g.rb_h && wx0 + AWP <= g.rb_w;
@@ -467,46 +468,144 @@ family_planes_kernel(const __grid_constant__ FamParams p, int tiles_y, int tiles
     }
 }
 
-// Work-list launch: tiles of uneven blocks of a [C, H, W] slide.  With a
-// counter the CTAs are persistent and take tiles from it; without one each
-// CTA walks tiles blockIdx.x, +gridDim.x, ...
-template <typename T, int NOUT>
-__global__ void __launch_bounds__(kThreads, 2)
-family_work_kernel(const __grid_constant__ FamParams p, const FamWork *__restrict__ work, int n_work,
-                   int n_tiles, int tile_base, int *counter) {
-    extern __shared__ float4 smem4[];
-    float *A = reinterpret_cast<float *>(smem4);
-    float *IT = A + (kTH + 2 * p.rmax0) * (kTW + 2 * p.rmax1);
-    __shared__ int next_tile;
-    int t = counter ? -1 : (int)blockIdx.x;
-    while (true) {
-        if (counter) {
-            if (threadIdx.x == 0) next_tile = atomicAdd(counter, 1);
-            __syncthreads();
-            t = next_tile;
-            __syncthreads();
+// Asynchronous global -> shared copies (cp.async, completion waited for by
+// the issuing thread, then a block barrier makes them visible).
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void *dst, const void *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Tile tg of a work list (global index): the item owning it, then its place
+// in the item's own box.  The item is searched from *hint (the previous
+// tile's item: tiles are taken in increasing order, so it is that item or one
+// a few entries on), by a short forward scan, else by binary search.
+__device__ __forceinline__ TileGeom work_geom(const FamWork *__restrict__ work, int n_work, int tg, int *hint) {
+    int lo = *hint;
+    bool found = false;
+    if (lo >= 0 && lo < n_work && work[lo].tile_begin <= tg) {
+        for (int k = 0; k < 8; ++k) {
+            if (lo + 1 >= n_work || work[lo + 1].tile_begin > tg) {
+                found = true;
+                break;
+            }
+            ++lo;
         }
-        if (t >= n_tiles) break;
-        // Binary search for the work item owning tile t (global index tg).
-        const int tg = t + tile_base;
-        int lo = 0, hi = n_work - 1;
+    } else {
+        lo = 0;
+    }
+    if (!found) {
+        int hi = n_work - 1;
         while (lo < hi) {
             int mid = (lo + hi + 1) >> 1;
             if (work[mid].tile_begin <= tg) lo = mid; else hi = mid - 1;
         }
-        const FamWork w = work[lo];
-        int local = tg - w.tile_begin;
-        int tiles_x = (w.own_w + kTW - 1) / kTW;
-        int ty = local / tiles_x, tx = local - ty * tiles_x;
-        TileGeom g{};
-        g.plane = w.channel;
-        g.rb_y = w.read_y; g.rb_x = w.read_x; g.rb_h = w.read_h; g.rb_w = w.read_w;
-        g.oy = w.own_y + ty * kTH; g.ox = w.own_x + tx * kTW;
-        g.th = min(kTH, w.own_y + w.own_h - g.oy); g.tw = min(kTW, w.own_x + w.own_w - g.ox);
-        family_tile<T, NOUT>(p, g, A, IT);
-        __syncthreads();
-        if (!counter) t += gridDim.x;
     }
+    *hint = lo;
+    const FamWork w = work[lo];
+    const int local = tg - w.tile_begin;
+    const int tiles_x = (w.own_w + kTW - 1) / kTW;
+    const int ty = local / tiles_x, tx = local - ty * tiles_x;
+    TileGeom g{};
+    g.plane = w.channel;
+    g.rb_y = w.read_y; g.rb_x = w.read_x; g.rb_h = w.read_h; g.rb_w = w.read_w;
+    g.oy = w.own_y + ty * kTH; g.ox = w.own_x + tx * kTW;
+    g.th = min(kTH, w.own_y + w.own_h - g.oy); g.tw = min(kTW, w.own_x + w.own_w - g.ox);
+    return g;
+}
+
+// Starts the copy of tile g's raw window (tile + halo, inside its read box)
+// into `raw` (pitch AWP elements) when no pad map is needed and the window's
+// rows are 16- or 4-byte aligned; returns false (nothing issued) otherwise.
+// The answer is the same in every thread.
+template <typename T>
+__device__ __forceinline__ bool prefetch_window(const FamParams &p, const TileGeom &g, T *raw) {
+    const int R0 = p.rmax0, R1 = p.rmax1, AWP = kTW + 2 * R1, AH = kTH + 2 * R0;
+    const int wy0 = g.oy - g.rb_y - R0, wx0 = g.ox - g.rb_x - R1;
+    if (wy0 < 0 || wx0 < 0 || wy0 + AH > g.rb_h || wx0 + AWP > g.rb_w) return false;
+    const T *w0 = static_cast<const T *>(p.in) + (int64_t)g.plane * p.in_plane_stride +
+                  (int64_t)(g.rb_y + wy0) * p.in_row_pitch + (g.rb_x + wx0);
+    const size_t row_bytes = (size_t)AWP * sizeof(T), pitch_bytes = (size_t)p.in_row_pitch * sizeof(T);
+    const uintptr_t a = reinterpret_cast<uintptr_t>(w0);
+    const char *src = reinterpret_cast<const char *>(w0);
+    char *dst = reinterpret_cast<char *>(raw);
+    if (a % 16 == 0 && pitch_bytes % 16 == 0 && row_bytes % 16 == 0) {
+        const int per_row = (int)(row_bytes / 16), n = AH * per_row;
+        for (int i = threadIdx.x; i < n; i += kThreads) {
+            const int r = i / per_row, c = i - r * per_row;
+            cp_async16(dst + (size_t)r * row_bytes + 16 * c, src + (size_t)r * pitch_bytes + 16 * c);
+        }
+        return true;
+    }
+    if (a % 4 == 0 && pitch_bytes % 4 == 0 && row_bytes % 4 == 0) {
+        const int per_row = (int)(row_bytes / 4), n = AH * per_row;
+        for (int i = threadIdx.x; i < n; i += kThreads) {
+            const int r = i / per_row, c = i - r * per_row;
+            cp_async4(dst + (size_t)r * row_bytes + 4 * c, src + (size_t)r * pitch_bytes + 4 * c);
+        }
+        return true;
+    }
+    return false;
+}
+
+// Work-list launch: tiles of uneven blocks of a [C, H, W] slide.  With a
+// counter the CTAs are persistent and take tiles from it; without one each
+// CTA walks tiles blockIdx.x, +gridDim.x, ...  With `raw` room (prefetch),
+// a CTA starts the copy of its next tile's window before computing the
+// current one, so the loads of one tile overlap the filters of the previous
+// (its first tile, and tiles that need the pad map, load as they go).
+template <typename T, int NOUT>
+__global__ void __launch_bounds__(kThreads, 2)
+family_work_kernel(const __grid_constant__ FamParams p, const FamWork *__restrict__ work, int n_work,
+                   int n_tiles, int tile_base, int *counter, int prefetch) {
+    extern __shared__ float4 smem4[];
+    const int AWP = kTW + 2 * p.rmax1, AH = kTH + 2 * p.rmax0;
+    float *A = reinterpret_cast<float *>(smem4);
+    float *IT = A + AH * AWP;
+    T *raw = reinterpret_cast<T *>(reinterpret_cast<uintptr_t>(IT + AWP * kITP + 15) & ~(uintptr_t)15);
+    // Thread 0 takes the next tile and writes its geometry here; the block
+    // reads it after the barrier (callers make sure every thread has read
+    // the previous one first).
+    __shared__ int next_tile;
+    __shared__ TileGeom next_geom;
+    int hint = 0;  // thread 0's item search start
+    auto fetch = [&](int cur) {
+        if (threadIdx.x == 0) {
+            const int tn = counter ? atomicAdd(counter, 1) : (cur < 0 ? (int)blockIdx.x : cur + (int)gridDim.x);
+            next_tile = tn;
+            if (tn < n_tiles) next_geom = work_geom(work, n_work, tn + tile_base, &hint);
+        }
+        __syncthreads();
+        return next_tile;
+    };
+    int t = fetch(-1);
+    TileGeom g = next_geom;
+    bool staged = false;  // tile t's window is in raw (copies issued)
+    while (t < n_tiles) {
+        if (staged) {
+            cp_async_wait_all();
+            __syncthreads();
+            using V2 = typename Pair<T>::type;
+            const V2 *r2 = reinterpret_cast<const V2 *>(raw);
+            float2 *a2 = reinterpret_cast<float2 *>(A);
+            for (int i = threadIdx.x; i < AWP * AH / 2; i += kThreads) {
+                const V2 v = r2[i];
+                a2[i] = make_float2(to_f32_scaled(v.x, p.in_scale), to_f32_scaled(v.y, p.in_scale));
+            }
+        }
+        __syncthreads();  // raw converted; every thread holds g
+        const int tn = fetch(t);
+        const bool next_staged = prefetch && tn < n_tiles && prefetch_window<T>(p, next_geom, raw);
+        family_tile<T, NOUT>(p, g, A, IT, staged);
+        __syncthreads();
+        t = tn;
+        g = next_geom;
+        staged = next_staged;
+    }
+    cp_async_wait_all();
 }
 
 
@@ -783,11 +882,23 @@ int dispatch_planes(const FamParams &p, size_t smem, int grid, int ty, int tx, c
     return (int)cudaGetLastError();
 }
 
+// Persistent walks (a counter) get the raw-window buffer for the next
+// tile's copies when two CTAs per SM still fit with it; the grid is then the
+// resident CTAs, at most `grid`.
 template <typename T, int NOUT>
 int dispatch_work(const FamParams &p, size_t smem, int grid, const FamWork *work, int n_work,
                   int n_tiles, int tile_base, int *counter, cudaStream_t s) {
+    const size_t raw = ((size_t)(kTW + 2 * p.rmax1) * (kTH + 2 * p.rmax0) * sizeof(T) + 15) & ~(size_t)15;
+    const int prefetch = counter && 2 * (smem + raw + 16 + 1024) <= 227 * 1024 ? 1 : 0;
+    if (prefetch) smem += raw + 16;
     cudaFuncSetAttribute(family_work_kernel<T, NOUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    family_work_kernel<T, NOUT><<<grid, kThreads, smem, s>>>(p, work, n_work, n_tiles, tile_base, counter);
+    if (counter) {
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, family_work_kernel<T, NOUT>, kThreads, smem);
+        if (per_sm < 1) per_sm = 1;
+        if (grid > sm_count() * per_sm) grid = sm_count() * per_sm;
+    }
+    family_work_kernel<T, NOUT><<<grid, kThreads, smem, s>>>(p, work, n_work, n_tiles, tile_base, counter, prefetch);
     return (int)cudaGetLastError();
 }
 

@@ -191,6 +191,32 @@ def test_tiled_walk_matches_per_block_filtering(oracle, persistent):
             assert np.abs(got[1] - whole).max() < 1e-3
 
 
+@pytest.mark.parametrize("dtype,W", [(np.uint16, 1536), (np.uint16, 1030), (np.uint8, 1024), (np.float32, 1000)])
+def test_persistent_walk_with_prefetch_equals_per_block(oracle, dtype, W):
+    """The persistent walk copies each CTA's next tile window ahead
+    (16-byte chunks when rows allow, else 4-byte); with ~4 tiles per CTA most
+    tiles take that path.  Its responses must equal the per-block launches
+    (no copies ahead) bit for bit, and the oracle on a block."""
+    rng = np.random.default_rng(W)
+    C, H = 3, 1000
+    x = rng.integers(0, 250 if dtype == np.uint8 else 5000, (C, H, W)).astype(dtype)
+    xt = torch.from_numpy(x.astype(np.int32)).cuda().to(getattr(torch, np.dtype(dtype).name))
+    resp = [("gaussian", 1.0), ("gaussian", 2.0), ("gaussian", 4.0), ("dog", 1.0, 3.0)]
+    for halo in (32, 3):
+        blocks = lb.schedule((1, H, W), (1, 256, 256), (0, halo, halo))
+        a = [host(o) for o in lb.gaussian_family_tiles(xt, blocks, resp, persistent=True)]
+        b = [host(o) for o in lb.gaussian_family_tiles(xt, blocks, resp, persistent=False)]
+        for k in range(4):
+            assert np.array_equal(a[k], b[k]), (halo, k)
+        blk = blocks[len(blocks) // 2]
+        ry, rx, rh, rw = blk.read_origin[1], blk.read_origin[2], blk.read_size[1], blk.read_size[2]
+        part = np.ascontiguousarray(x[1, ry:ry + rh, rx:rx + rw].astype(np.float32))
+        w = oracle.gaussian_blur(part, [4.0])[blk.origin[1] - ry:blk.origin[1] - ry + blk.size[1],
+                                              blk.origin[2] - rx:blk.origin[2] - rx + blk.size[2]]
+        got = a[2][1, blk.origin[1]:blk.origin[1] + blk.size[1], blk.origin[2]:blk.origin[2] + blk.size[2]]
+        oracle.assert_close(got, w.astype(np.float64), RTOL, f"halo {halo} prefetch block")
+
+
 def test_errors_mirror_the_reference():
     x = torch.zeros((4, 5), device="cuda")
     with pytest.raises(lb.LucemError) as e:
