@@ -369,6 +369,24 @@ lucem_status lucem_autotune_fft(lucem_ctx *ctx, const int64_t *lengths, int32_t 
                                 void *stream);
 lucem_status lucem_autotune_query(lucem_ctx *ctx, int32_t kind, int64_t length, double *ns_per_element);
 lucem_status lucem_autotune_save(lucem_ctx *ctx, const char *path);
+/* Launch settings of the Gaussian family kernels, as the reference tunes its
+ * CubeCL launches (crates/lucem-core/src/compute/tune.rs:1-27: candidates
+ * benchmarked once per device and problem-size key, the fastest reused).
+ * While enabled, the first plain 2-D blur or persistent tile walk of each
+ * key -- kernel kind, SM count, element type, filter count, largest radius,
+ * power-of-two class of the tile count -- times its candidate settings on
+ * the call's own data (copying the next tile's window ahead by tensor copy
+ * or cp.async or not; one or as many persistent CTAs per SM as fit; every
+ * candidate computes the same result), keeps the fastest and launches with
+ * it; later calls of the key reuse it.  Tuning synchronises the stream and
+ * is skipped during stream capture.  Disabled (the default), cached plans
+ * are still used and other keys take the built-in heuristics.  Plans are
+ * saved and loaded with the FFT costs ("plan <key> <code>" lines). */
+lucem_status lucem_autotune_enable(lucem_ctx *ctx, int32_t enable);
+/* The cached plans: keys as NUL-terminated strings of at most 63 chars in a
+ * [cap][64] array, codes in plans (1 + bits: 1 copy ahead, 2 one CTA per
+ * SM); *n_out = the number cached. */
+lucem_status lucem_autotune_plans(lucem_ctx *ctx, char *keys, int32_t *plans, int32_t cap, int32_t *n_out);
 lucem_status lucem_autotune_load(lucem_ctx *ctx, const char *path);
 
 /* ---- CUDA graphs of launch-only calls ------------------------------------

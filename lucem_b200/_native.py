@@ -194,6 +194,8 @@ SIGNATURES = {
     "lucem_autotune_query": (I32, [P, I32, I64, C.POINTER(C.c_double)]),
     "lucem_autotune_save": (I32, [P, C.c_char_p]),
     "lucem_autotune_load": (I32, [P, C.c_char_p]),
+    "lucem_autotune_enable": (I32, [P, I32]),
+    "lucem_autotune_plans": (I32, [P, C.c_char_p, C.POINTER(I32), I32, C.POINTER(I32)]),
     "lucem_graph_begin": (I32, [P]),
     "lucem_graph_end": (I32, [P, C.POINTER(P)]),
     "lucem_graph_launch": (I32, [P, P]),

@@ -229,6 +229,9 @@ struct lucem_ctx {
     std::map<std::string, void *> cache;
     // Autotuned FFT pass costs: (kind 0 column / 1 row, length) -> ns per element.
     std::map<std::pair<int, int64_t>, double> tune;
+    // Autotuned launch settings of the family kernels: key -> FamParams::plan.
+    std::map<std::string, int> plans;
+    bool tune_on = false;
     void *get_or_upload(const std::string &key, const void *host, size_t bytes, int *err) {
         std::lock_guard<std::mutex> lk(mu);
         auto it = cache.find(key);
@@ -715,6 +718,86 @@ lucem_status fam_waits(lucem_workspace *ws, FamParams *fp, void *stream) {
     return ok();
 }
 
+// Launch-settings key of a family launch: kernel kind, SM count, element
+// type, filter count, largest radius and the power-of-two class of its tile
+// count (the reference keys CubeCL's tuning by device id and size class,
+// crates/lucem-core/src/compute/tune.rs:12-27).
+std::string plan_key(const lucem_ctx *ctx, const char *kind, int dtype, const FamParams &fp, int64_t tiles) {
+    int64_t cls = 1;
+    while (cls < tiles) cls <<= 1;
+    char b[96];
+    snprintf(b, sizeof b, "%s-sm%d-t%d-f%d-r%d-n%lld", kind, ctx->sms, dtype, fp.n_filters,
+             std::max(fp.rmax0, fp.rmax1), (long long)cls);
+    return b;
+}
+
+int64_t plane_tiles(const FamParams &fp) {
+    return (int64_t)((fp.H + kFamTile - 1) / kFamTile) * ((fp.W + kFamTile - 1) / kFamTile) * fp.B;
+}
+
+// Runs launch() with the key's cached plan; while tuning is on and the key
+// is new (and the stream is not being captured), first times every
+// candidate plan on this call's data (one warm-up and two timed runs each;
+// every candidate computes the same result), caches the fastest and runs it
+// last.
+template <class F>
+int tuned_launch(lucem_ctx *ctx, const std::string &key, const std::vector<int> &cands, FamParams *fp,
+                 void *stream, F &&launch) {
+    bool tune = false;
+    {
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        auto it = ctx->plans.find(key);
+        if (it != ctx->plans.end()) fp->plan = it->second;
+        else tune = ctx->tune_on && cands.size() > 1;
+    }
+    cudaStream_t cs = static_cast<cudaStream_t>(stream);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (tune && cudaStreamIsCapturing(cs, &cap) == cudaSuccess && cap == cudaStreamCaptureStatusNone) {
+        cudaEvent_t a = nullptr, b = nullptr;
+        int e = (int)cudaEventCreate(&a);
+        if (!e) e = (int)cudaEventCreate(&b);
+        int best_plan = 0;
+        float best = 0.f;
+        for (size_t i = 0; i < cands.size() && !e; ++i) {
+            fp->plan = cands[i];
+            float tmin = -1.f;
+            for (int rep = 0; rep < 3 && !e; ++rep) {
+                e = (int)cudaEventRecord(a, cs);
+                if (!e) e = launch();
+                if (!e) e = (int)cudaEventRecord(b, cs);
+                if (!e) e = (int)cudaEventSynchronize(b);
+                float ms = 0.f;
+                if (!e) e = (int)cudaEventElapsedTime(&ms, a, b);
+                if (!e && rep > 0 && (tmin < 0.f || ms < tmin)) tmin = ms;
+            }
+            if (!e && (best_plan == 0 || tmin < best)) {
+                best = tmin;
+                best_plan = cands[i];
+            }
+        }
+        if (a) cudaEventDestroy(a);
+        if (b) cudaEventDestroy(b);
+        if (e) return e;
+        fp->plan = best_plan;
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        ctx->plans[key] = best_plan;
+    }
+    return launch();
+}
+
+// Candidate plans: the plain 2-D blur (loads or tensor copies ahead), the
+// persistent walk (copies ahead or not, one or as many CTAs per SM as fit).
+std::vector<int> blur_candidates(const FamParams &fp) {
+    const int r = fp.r0[0];
+    const bool rf = fp.n_filters == 1 && fp.r1[0] == r && fp.rmax0 == r && fp.rmax1 == r && r >= 2 && r <= 16 &&
+                    (r <= 12 || r == 16);
+    if (!rf) return {};
+    return {1, 1 + kPlanAhead};
+}
+std::vector<int> walk_candidates() {
+    return {1, 1 + kPlanAhead, 1 + kPlanOneCta, 1 + kPlanAhead + kPlanOneCta};
+}
+
 // Executes a pass list from `in` into `out` (f32): the reference's
 // separable::run (crates/lucem-ops/src/core/separable.rs:20-61), with the
 // last two passes fused into one launch when they are the two innermost axes
@@ -781,7 +864,11 @@ lucem_status run_passes(lucem_ctx *ctx, const lucem_tensor *in, const std::vecto
         o.beta = 0.0f;
         o.bias = 0.0f;
         if (lucem_status ws_st = fam_waits(ws, &fp, stream)) return ws_st;
-        int e = timed(kPassFamily, stream, [&] { return launch_family_planes(fp, src_dtype, stream); });
+        int e = tuned_launch(ctx, plan_key(ctx, "blur", src_dtype, fp, plane_tiles(fp)), blur_candidates(fp), &fp,
+                             stream, [&] {
+                                 return timed(kPassFamily, stream,
+                                              [&] { return launch_family_planes(fp, src_dtype, stream); });
+                             });
         if (e) return cuda_fail(e, "gaussian family launch");
     }
     return ok();
@@ -1535,11 +1622,16 @@ lucem_status lucem_gaussian_family_tiles(lucem_ctx *ctx, const lucem_tensor *sli
     const FamWork *wd = static_cast<const FamWork *>(wdev);
     int e = 0;
     if (persistent) {
-        CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(int32_t), static_cast<cudaStream_t>(stream)), "counter reset");
-        size_t smem = family_smem_bytes(fp.rmax0, fp.rmax1);
-        int per_sm = (int)std::max<size_t>(1, std::min<size_t>(4, (200 * 1024) / (smem + 2048)));
-        e = timed(kPassFamily, stream, [&] { return launch_family_work(fp, slide->dtype, wd, (int32_t)work.size(), (int32_t)tiles, 0,
-                               static_cast<int32_t *>(cnt), ctx->sms * per_sm, stream); });
+        // The launcher caps the grid at the CTAs that are resident at once.
+        e = tuned_launch(ctx, plan_key(ctx, "walk", slide->dtype, fp, (int64_t)tiles), walk_candidates(), &fp, stream,
+                         [&] {
+                             int r = (int)cudaMemsetAsync(cnt, 0, sizeof(int32_t), static_cast<cudaStream_t>(stream));
+                             if (r) return r;
+                             return timed(kPassFamily, stream, [&] {
+                                 return launch_family_work(fp, slide->dtype, wd, (int32_t)work.size(), (int32_t)tiles,
+                                                           0, static_cast<int32_t *>(cnt), ctx->sms * 4, stream);
+                             });
+                         });
     } else {
         for (size_t i = 0; i < work.size() && !e; ++i) {
             int32_t t0 = work[i].tile_begin;
@@ -1584,7 +1676,7 @@ lucem_status lucem_gaussian_batch(lucem_ctx *ctx, int32_t n, const lucem_tensor 
             return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `set_ids`: image %d has set %d of %d", i,
                         set_ids[i], n_sets);
     }
-    int th = 64, tw = 64;
+    int th = kFamTile, tw = kFamTile;
     family_tile_dims(&th, &tw);
     // Work list: images grouped by sigma set, each set's tiles numbered from 0.
     std::vector<FamImage> items;
@@ -2575,6 +2667,8 @@ lucem_status lucem_autotune_save(lucem_ctx *ctx, const char *path) {
     std::lock_guard<std::mutex> lk(ctx->mu);
     std::fprintf(f, "# lucem_b200 FFT pass costs: kind (0 column, 1 row) length ns_per_element\n");
     for (auto &kv : ctx->tune) std::fprintf(f, "%d %lld %.9g\n", kv.first.first, (long long)kv.first.second, kv.second);
+    std::fprintf(f, "# family launch settings: plan key code\n");
+    for (auto &kv : ctx->plans) std::fprintf(f, "plan %s %d\n", kv.first.c_str(), kv.second);
     std::fclose(f);
     return ok();
 }
@@ -2586,8 +2680,19 @@ lucem_status lucem_autotune_load(lucem_ctx *ctx, const char *path) {
     if (!f) return fail(LUCEM_ERR_INVALID_PARAMETER, "cannot read %s", path);
     char line[256];
     std::map<std::pair<int, int64_t>, double> got;
+    std::map<std::string, int> plans;
     while (std::fgets(line, sizeof line, f)) {
         if (line[0] == '#' || line[0] == '\n') continue;
+        if (std::strncmp(line, "plan ", 5) == 0) {
+            char key[96];
+            int code = 0;
+            if (std::sscanf(line + 5, "%95s %d", key, &code) != 2 || code < 1 || code > 4) {
+                std::fclose(f);
+                return fail(LUCEM_ERR_INVALID_PARAMETER, "malformed autotune line in %s: %s", path, line);
+            }
+            plans[key] = code;
+            continue;
+        }
         int kind;
         long long len;
         double v;
@@ -2601,6 +2706,31 @@ lucem_status lucem_autotune_load(lucem_ctx *ctx, const char *path) {
     std::fclose(f);
     std::lock_guard<std::mutex> lk(ctx->mu);
     for (auto &kv : got) ctx->tune[kv.first] = kv.second;
+    for (auto &kv : plans) ctx->plans[kv.first] = kv.second;
+    return ok();
+}
+
+lucem_status lucem_autotune_enable(lucem_ctx *ctx, int32_t enable) {
+    if (!ctx) return fail(LUCEM_ERR_INVALID_HANDLE, "null context");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->tune_on = enable != 0;
+    return ok();
+}
+
+lucem_status lucem_autotune_plans(lucem_ctx *ctx, char *keys, int32_t *plans, int32_t cap, int32_t *n_out) {
+    if (!ctx) return fail(LUCEM_ERR_INVALID_HANDLE, "null context");
+    if (!n_out || cap < 0 || (cap > 0 && (!keys || !plans)))
+        return fail(LUCEM_ERR_INVALID_PARAMETER, "invalid parameter `keys`");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    int32_t i = 0;
+    for (auto &kv : ctx->plans) {
+        if (i < cap) {
+            std::snprintf(keys + 64 * (size_t)i, 64, "%s", kv.first.c_str());
+            plans[i] = kv.second;
+        }
+        ++i;
+    }
+    *n_out = i;
     return ok();
 }
 

@@ -16,8 +16,8 @@
 namespace lucem {
 namespace famk {
 
-constexpr int kTH = 64;        // output tile rows
-constexpr int kTW = 64;        // output tile columns
+constexpr int kTH = kFamTile;  // output tile rows
+constexpr int kTW = kFamTile;  // output tile columns
 constexpr int kThreads = 256;
 constexpr int kITP = 66;       // pitch of the transposed intermediate (even: 8-byte pairs)
 
@@ -889,13 +889,16 @@ template <typename T, int NOUT>
 int dispatch_work(const FamParams &p, size_t smem, int grid, const FamWork *work, int n_work,
                   int n_tiles, int tile_base, int *counter, cudaStream_t s) {
     const size_t raw = ((size_t)(kTW + 2 * p.rmax1) * (kTH + 2 * p.rmax0) * sizeof(T) + 15) & ~(size_t)15;
-    const int prefetch = counter && 2 * (smem + raw + 16 + 1024) <= 227 * 1024 ? 1 : 0;
+    const int bits = p.plan ? p.plan - 1 : 0;
+    const bool fits = (p.plan ? 1 : 2) * (smem + raw + 16 + 1024) <= 227 * 1024;
+    const int prefetch = counter && (p.plan ? (bits & kPlanAhead) != 0 : true) && fits ? 1 : 0;
     if (prefetch) smem += raw + 16;
     cudaFuncSetAttribute(family_work_kernel<T, NOUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (counter) {
         int per_sm = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, family_work_kernel<T, NOUT>, kThreads, smem);
         if (per_sm < 1) per_sm = 1;
+        if (bits & kPlanOneCta) per_sm = 1;
         if (grid > sm_count() * per_sm) grid = sm_count() * per_sm;
     }
     family_work_kernel<T, NOUT><<<grid, kThreads, smem, s>>>(p, work, n_work, n_tiles, tile_base, counter, prefetch);
@@ -911,7 +914,9 @@ int dispatch_planes_n(const FamParams &p, size_t smem, int grid, int ty, int tx,
 #define RFCASE(r)                                                                          \
     case r: {                                                                              \
         CUtensorMap map;                                                                   \
-        if (ty * tx * p.B >= 12 * sm_count() && make_plane_map<T>(p, r, &map))             \
+        const bool ahead = p.plan ? ((p.plan - 1) & kPlanAhead) != 0                     \
+                                  : ty * tx * p.B >= 12 * sm_count();                      \
+        if (ahead && make_plane_map<T>(p, r, &map))                                        \
             return dispatch_planes_tma<T, r>(p, map, ty * tx * p.B, ty, tx, s);            \
         return dispatch_planes<T, 1, r>(p, smem, grid, ty, tx, s);                         \
     }

@@ -21,6 +21,7 @@ constexpr int64_t kMaxDeviceElements = 0xFFFFFFFFll;
 // 0, 2, ..., 16, 20, 24, 28, 32; a filter of another radius runs at the next
 // one up with zero taps at both ends (fam_kernel_radius).
 constexpr int kFamMaxRadius = 32;
+constexpr int kFamTile = 64;  // output tile side of the family kernels
 constexpr int kFamMaxTaps = 2 * kFamMaxRadius + 1;
 constexpr int kFamMaxFilters = 8;
 constexpr int kFamMaxOutputs = 4;
@@ -45,6 +46,10 @@ struct FamOutput {
     float alpha, beta, bias;
     // fa or fb == -2 names the input sample itself (unsharp).
 };
+
+// Launch-setting bits of FamParams::plan (plan = 1 + bits).
+constexpr int32_t kPlanAhead = 1;   // copy the next tile's window ahead (tensor copy / cp.async)
+constexpr int32_t kPlanOneCta = 2;  // one persistent CTA per SM (else as many as fit)
 
 // Epilogue modes of FamParams::tensor (tensor_ops.cuh); 0: none, the
 // linear outputs.
@@ -86,6 +91,9 @@ struct FamParams {
     // wait_ns nanoseconds (0: the default, one second; -1: at once, without
     // polling), count each give-up in *wait_status (may be null).
     int32_t *wait_status;
+    // Launch settings: 0 = the built-in heuristics; else 1 + kPlan* bits,
+    // chosen by the autotuner.
+    int32_t plan;
     int64_t wait_ns;
     // Tensor epilogue (tensor_ops.cuh TensorMode; 0: none): the first three
     // filters' responses (a, b, c) are combined per pixel into outs[0..2]

@@ -30,7 +30,8 @@ __all__ = [
     "gaussian_family", "schedule", "gaussian_family_tiles", "richardson_lucy", "rl_grid",
     "gaussian_halo", "op_halo", "gaussian_blur_adjoint", "richardson_lucy_backward", "fft_convolve",
     "fft_convolve_backward", "RlBatch", "richardson_lucy_batch", "autotune_fft", "autotune_query",
-    "autotune_save", "autotune_load", "Graph", "gaussian_batch", "fft_nd", "fft_1d", "complex_mul",
+    "autotune_save", "autotune_load", "autotune_enable", "autotune_plans", "Graph", "gaussian_batch", "fft_nd",
+    "fft_1d", "complex_mul",
     "wiener_deconvolve", "from_dlpack", "fourier_gaussian", "fourier_box", "fourier_shift", "butterworth",
     "PhaseCorrelationResult", "phase_correlation", "unsupervised_wiener", "hessian_matrix", "hessian_det",
     "hessian_eigvals", "shape_index", "structure_tensor", "structure_tensor_eigvals", "frangi", "sato",
@@ -1215,6 +1216,26 @@ def autotune_query(kind: int, length: int, device=None) -> float:
 
 def autotune_save(path: str, device=None):
     N.check(N.lib().lucem_autotune_save(context(_device_index(device)).handle, str(path).encode()))
+
+
+def autotune_enable(enable: bool = True, device=None):
+    """lucem_autotune_enable: while on, the first plain 2-D blur or persistent
+    tile walk of each size class times its launch candidates and caches the
+    fastest (saved / loaded with autotune_save / autotune_load)."""
+    N.check(N.lib().lucem_autotune_enable(context(_device_index(device)).handle, int(bool(enable))))
+
+
+def autotune_plans(device=None) -> dict:
+    """The cached launch plans: {key: code}, code = 1 + bits (1 copy ahead,
+    2 one CTA per SM)."""
+    h = context(_device_index(device)).handle
+    n = C.c_int32()
+    N.check(N.lib().lucem_autotune_plans(h, None, None, 0, C.byref(n)))
+    cap = max(1, n.value)
+    keys = C.create_string_buffer(64 * cap)
+    codes = (C.c_int32 * cap)()
+    N.check(N.lib().lucem_autotune_plans(h, keys, codes, cap, C.byref(n)))
+    return {keys.raw[64 * i:64 * (i + 1)].split(b"\0", 1)[0].decode(): int(codes[i]) for i in range(min(n.value, cap))}
 
 
 def autotune_load(path: str, device=None):
