@@ -372,13 +372,13 @@ lucem_status lucem_autotune_save(lucem_ctx *ctx, const char *path);
 /* Launch settings of the Gaussian family kernels, as the reference tunes its
  * CubeCL launches (crates/lucem-core/src/compute/tune.rs:1-27: candidates
  * benchmarked once per device and problem-size key, the fastest reused).
- * While enabled, the first plain 2-D blur or persistent tile walk of each
- * key -- kernel kind, SM count, element type, filter count, largest radius,
- * power-of-two class of the tile count -- times its candidate settings on
- * the call's own data (copying the next tile's window ahead by tensor copy
- * or cp.async or not; one or as many persistent CTAs per SM as fit; every
- * candidate computes the same result), keeps the fastest and launches with
- * it; later calls of the key reuse it.  Tuning synchronises the stream and
+ * While enabled, the first plain 2-D blur, persistent tile walk or image
+ * batch set of each key -- kernel kind, SM count, element type, filter
+ * count, largest radius, power-of-two class of the tile count -- times its
+ * candidate settings on the call's own data (copying the next tile's window
+ * ahead by tensor copy or cp.async or not; one or as many persistent CTAs
+ * per SM as fit; every candidate computes the same result), keeps the
+ * fastest and launches with it; later calls of the key reuse it.  Tuning synchronises the stream and
  * is skipped during stream capture.  Disabled (the default), cached plans
  * are still used and other keys take the built-in heuristics.  Plans are
  * saved and loaded with the FFT costs ("plan <key> <code>" lines). */

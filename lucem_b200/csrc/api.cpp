@@ -1739,9 +1739,13 @@ lucem_status lucem_gaussian_batch(lucem_ctx *ctx, int32_t n, const lucem_tensor 
             FamParams fp;
             lucem_tensor view = ins[0];
             gaussian_fused_params(&fp, &view, mode, cval, (float)input_scale, rows, cols, nullptr);
-            e = timed(kPassFamily, stream, [&] {
-                return launch_family_batch(fp, ins[0].dtype, idev + b, cnt, set_tiles[(size_t)s2], stream);
-            });
+            e = tuned_launch(ctx, plan_key(ctx, "batch", ins[0].dtype, fp, set_tiles[(size_t)s2]), {1, 1 + kPlanAhead},
+                             &fp, stream, [&] {
+                                 return timed(kPassFamily, stream, [&] {
+                                     return launch_family_batch(fp, ins[0].dtype, idev + b, cnt,
+                                                                set_tiles[(size_t)s2], stream);
+                                 });
+                             });
         }
         if (e) return cuda_fail(e, "gaussian_batch launch");
     }

@@ -526,9 +526,11 @@ __device__ __forceinline__ bool prefetch_window(const FamParams &p, const TileGe
     const int R0 = p.rmax0, R1 = p.rmax1, AWP = kTW + 2 * R1, AH = kTH + 2 * R0;
     const int wy0 = g.oy - g.rb_y - R0, wx0 = g.ox - g.rb_x - R1;
     if (wy0 < 0 || wx0 < 0 || wy0 + AH > g.rb_h || wx0 + AWP > g.rb_w) return false;
-    const T *w0 = static_cast<const T *>(p.in) + (int64_t)g.plane * p.in_plane_stride +
-                  (int64_t)(g.rb_y + wy0) * p.in_row_pitch + (g.rb_x + wx0);
-    const size_t row_bytes = (size_t)AWP * sizeof(T), pitch_bytes = (size_t)p.in_row_pitch * sizeof(T);
+    const int64_t ipitch = g.in ? g.in_pitch : p.in_row_pitch;
+    const T *base = g.in ? static_cast<const T *>(g.in)
+                         : static_cast<const T *>(p.in) + (int64_t)g.plane * p.in_plane_stride;
+    const T *w0 = base + (int64_t)(g.rb_y + wy0) * ipitch + (g.rb_x + wx0);
+    const size_t row_bytes = (size_t)AWP * sizeof(T), pitch_bytes = (size_t)ipitch * sizeof(T);
     const uintptr_t a = reinterpret_cast<uintptr_t>(w0);
     const char *src = reinterpret_cast<const char *>(w0);
     char *dst = reinterpret_cast<char *>(raw);
@@ -609,50 +611,112 @@ family_work_kernel(const __grid_constant__ FamParams p, const FamWork *__restric
 }
 
 
-// Batch of separate 2-D images sharing one filter set: tile t belongs to
-// the last item whose tile_begin <= t; each image is its own read box.
-// CTAs walk tiles blockIdx.x, +gridDim.x, ...
-template <typename T, int RF = -1>
-__global__ void __launch_bounds__(kThreads, RF >= 0 ? 3 : 2)
-family_batch_kernel(const __grid_constant__ FamParams p, const FamImage *__restrict__ items, int n_items,
-                    int n_tiles) {
-    extern __shared__ float4 smem4[];
-    float *A = reinterpret_cast<float *>(smem4);
-    float *IT = A + (kTH + 2 * p.rmax0) * (kTW + 2 * p.rmax1);
-    for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
-        int lo = 0, hi = n_items - 1;
+// Tile t of a batch: the image owning it (the last item whose tile_begin
+// <= t, searched from *hint as work_geom does), then its place in that
+// image, which is its own read box.
+__device__ __forceinline__ TileGeom batch_geom(const FamImage *__restrict__ items, int n_items, int t, int *hint) {
+    int lo = *hint;
+    bool found = false;
+    if (lo >= 0 && lo < n_items && items[lo].tile_begin <= t) {
+        for (int k = 0; k < 8; ++k) {
+            if (lo + 1 >= n_items || items[lo + 1].tile_begin > t) {
+                found = true;
+                break;
+            }
+            ++lo;
+        }
+    } else {
+        lo = 0;
+    }
+    if (!found) {
+        int hi = n_items - 1;
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
             if (items[mid].tile_begin <= t) lo = mid; else hi = mid - 1;
         }
-        const FamImage it = items[lo];
-        const int local = t - it.tile_begin;
-        const int tiles_x = (it.W + kTW - 1) / kTW;
-        const int ty = local / tiles_x, tx = local - ty * tiles_x;
-        TileGeom g{};
-        g.plane = 0;
-        g.rb_y = 0; g.rb_x = 0; g.rb_h = it.H; g.rb_w = it.W;
-        g.oy = ty * kTH; g.ox = tx * kTW;
-        g.th = min(kTH, it.H - g.oy); g.tw = min(kTW, it.W - g.ox);
-        g.in = it.in;
-        g.out = it.out;
-        g.in_pitch = it.in_pitch;
-        g.out_pitch = it.out_pitch;
-        family_tile<T, 1, RF>(p, g, A, IT);
-        __syncthreads();
     }
+    *hint = lo;
+    const FamImage it = items[lo];
+    const int local = t - it.tile_begin;
+    const int tiles_x = (it.W + kTW - 1) / kTW;
+    const int ty = local / tiles_x, tx = local - ty * tiles_x;
+    TileGeom g{};
+    g.plane = 0;
+    g.rb_y = 0; g.rb_x = 0; g.rb_h = it.H; g.rb_w = it.W;
+    g.oy = ty * kTH; g.ox = tx * kTW;
+    g.th = min(kTH, it.H - g.oy); g.tw = min(kTW, it.W - g.ox);
+    g.in = it.in;
+    g.out = it.out;
+    g.in_pitch = it.in_pitch;
+    g.out_pitch = it.out_pitch;
+    return g;
 }
 
+// Batch of separate 2-D images sharing one filter set.  CTAs walk tiles
+// blockIdx.x, +gridDim.x, ...; with `raw` room (prefetch) a CTA copies its
+// next tile's window ahead while filtering the current one, as the tile
+// walk does.
+template <typename T, int RF = -1>
+__global__ void __launch_bounds__(kThreads, RF >= 0 ? 3 : 2)
+family_batch_kernel(const __grid_constant__ FamParams p, const FamImage *__restrict__ items, int n_items,
+                    int n_tiles, int prefetch) {
+    extern __shared__ float4 smem4[];
+    const int AWP = kTW + 2 * p.rmax1, AH = kTH + 2 * p.rmax0;
+    float *A = reinterpret_cast<float *>(smem4);
+    float *IT = A + AH * AWP;
+    T *raw = reinterpret_cast<T *>(reinterpret_cast<uintptr_t>(IT + AWP * kITP + 15) & ~(uintptr_t)15);
+    __shared__ TileGeom next_geom;
+    int hint = 0;  // thread 0's item search start
+    int t = blockIdx.x;
+    if (t >= n_tiles) return;
+    if (threadIdx.x == 0) next_geom = batch_geom(items, n_items, t, &hint);
+    __syncthreads();
+    TileGeom g = next_geom;
+    bool staged = false;
+    while (true) {
+        if (staged) {
+            cp_async_wait_all();
+            __syncthreads();
+            using V2 = typename Pair<T>::type;
+            const V2 *r2 = reinterpret_cast<const V2 *>(raw);
+            float2 *a2 = reinterpret_cast<float2 *>(A);
+            for (int i = threadIdx.x; i < AWP * AH / 2; i += kThreads) {
+                const V2 v = r2[i];
+                a2[i] = make_float2(to_f32_scaled(v.x, p.in_scale), to_f32_scaled(v.y, p.in_scale));
+            }
+        }
+        __syncthreads();  // raw converted; every thread holds g
+        const int tn = t + (int)gridDim.x;
+        if (threadIdx.x == 0 && tn < n_tiles) next_geom = batch_geom(items, n_items, tn, &hint);
+        __syncthreads();
+        const bool next_staged = prefetch && tn < n_tiles && prefetch_window<T>(p, next_geom, raw);
+        family_tile<T, 1, RF>(p, g, A, IT, staged);
+        __syncthreads();
+        if (tn >= n_tiles) break;
+        t = tn;
+        g = next_geom;
+        staged = next_staged;
+    }
+    cp_async_wait_all();
+}
+
+// The window copies ahead (a raw buffer in shared memory) only when a plan
+// asks for them: on the 512-image batch (sides 64..1024, one filter) the
+// autotuner measured them slower for radii 4, 8 and 16.
 template <typename T, int RF = -1>
 int dispatch_batch(const FamParams &p, size_t smem, const FamImage *items, int n_items, int n_tiles,
                    cudaStream_t s) {
+    const size_t raw = ((size_t)(kTW + 2 * p.rmax1) * (kTH + 2 * p.rmax0) * sizeof(T) + 15) & ~(size_t)15;
+    const bool want = p.plan ? ((p.plan - 1) & kPlanAhead) != 0 : false;
+    const int prefetch = want && smem + raw + 16 + 1024 <= 227 * 1024 ? 1 : 0;
+    if (prefetch) smem += raw + 16;
     cudaFuncSetAttribute(family_batch_kernel<T, RF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, family_batch_kernel<T, RF>, kThreads, smem);
     if (per_sm < 1) per_sm = 1;
     const int slots = sm_count() * per_sm;
     const int grid = n_tiles < slots ? n_tiles : slots;
-    family_batch_kernel<T, RF><<<grid, kThreads, smem, s>>>(p, items, n_items, n_tiles);
+    family_batch_kernel<T, RF><<<grid, kThreads, smem, s>>>(p, items, n_items, n_tiles, prefetch);
     return (int)cudaGetLastError();
 }
 
