@@ -62,6 +62,25 @@ def test_tuned_launches_equal_the_untuned_and_are_cached(tmp_path):
         lb.autotune_load(str(bad))
 
 
+def test_tuned_image_batch_equals_the_untuned():
+    """The batch's candidates include the window copies ahead (off by
+    default): every candidate runs once while tuning, and the result equals
+    the untuned launch bit for bit."""
+    rng = np.random.default_rng(17)
+    imgs = [torch.from_numpy(rng.integers(0, 4000, (int(h), int(w))).astype(np.int32)).cuda().to(torch.uint16)
+            for h, w in rng.integers(64, 700, (40, 2))]
+    sig = list(rng.choice([1.0, 2.0, 4.0], len(imgs)))
+    want = [host(o) for o in lb.gaussian_batch(imgs, sig)]
+    lb.autotune_enable(True)
+    try:
+        got = [host(o) for o in lb.gaussian_batch(imgs, sig)]
+    finally:
+        lb.autotune_enable(False)
+    assert any(k.startswith("batch") for k in lb.autotune_plans())
+    for a, b in zip(want, got):
+        assert np.array_equal(a, b)
+
+
 def test_tuning_is_skipped_during_capture():
     img = torch.from_numpy(np.random.default_rng(9).random((333, 517)).astype(np.float32)).cuda()
     want = host(lb.gaussian_blur(img, 3.0))
