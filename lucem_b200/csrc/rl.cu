@@ -317,8 +317,7 @@ __global__ void otf_z_kernel(const double2 *__restrict__ B, int kz, int cz, int 
 // shapes of launch_col below).
 int col_tile_width(int n) {
     switch (n) {
-    case 128: return 8;
-    case 64: case 256: case 512: return 16;
+    case 64: case 128: case 256: case 512: return 16;
     case 1024: case 2048: return 8;
     default: break;
     }
