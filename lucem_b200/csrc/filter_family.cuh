@@ -104,8 +104,11 @@ __device__ __forceinline__ void vpass(const float *__restrict__ A, int AWP, int 
                                    const float2 *__restrict__ w, float *__restrict__ IT) {
     constexpr int NT = 2 * R + 1;
     const int npairs = ncols / 2;
+    // q / npairs for q < 8 npairs <= 512 as a multiply and shift, exact
+    // there (the rounding of the reciprocal adds less than 1 / npairs).
+    const uint32_t inv = (65536u + (uint32_t)npairs - 1u) / (uint32_t)npairs;
     for (int q = threadIdx.x; q < npairs * 8; q += kThreads) {
-        const int cp = q % npairs, yc = q / npairs;
+        const int yc = (int)(((uint32_t)q * inv) >> 16), cp = q - yc * npairs;
         const float *col = A + (yc * 8 + row0) * AWP + cstart + 2 * cp;
         float2 acc[8];
 #pragma unroll
