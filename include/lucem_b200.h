@@ -583,8 +583,10 @@ void lucem_canny_settings_default(lucem_canny_settings *s);
  * from the strong pixels, is 8-connected component labelling of the pixels
  * at or above the low threshold on the device (union-find), keeping the
  * components that hold a pixel at or above the high threshold: the same
- * edge set.  Synchronises once to read the maximum, unless both thresholds
- * are given as values. */
+ * edge set.  With both thresholds left to their defaults the call is
+ * asynchronous (the thresholds are computed on the device from the maximum);
+ * with one or both given it synchronises once to read the maximum, unless
+ * both are values (not quantiles). */
 lucem_status lucem_canny(lucem_ctx *ctx, const lucem_tensor *in, const lucem_canny_settings *settings,
                          lucem_tensor *out, lucem_workspace *ws, void *stream);
 

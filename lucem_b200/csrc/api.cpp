@@ -4475,6 +4475,20 @@ lucem_status lucem_canny(lucem_ctx *ctx, const lucem_tensor *in, const lucem_can
                   [&] { return launch_canny_nms(mag, sector, nms, (int)H, (int)W, max_bits, stream); });
     if (e) return cuda_fail(e, "non-maximum suppression launch");
 
+    uint32_t *edges = static_cast<uint32_t *>(out->data);
+    // The sector slot is free after the suppression: it holds the labels.
+    uint32_t *labels = reinterpret_cast<uint32_t *>(sector);
+    if (!s->has_low && !s->has_high) {
+        // Both thresholds by default (canny.rs:108-116): high >= low always,
+        // so they are computed on the device from the maximum, no host
+        // round trip (the call stays asynchronous and capturable).
+        double *thr = reinterpret_cast<double *>(static_cast<char *>(px) + 16);
+        e = timed(kPassElementwise, stream, [&] {
+            int r = launch_canny_thresholds(max_bits, s->use_quantiles ? 1 : 0, thr, stream);
+            return r ? r : launch_canny_hysteresis(nms, (int)H, (int)W, thr, 0.0, 0.0, labels, edges, stream);
+        });
+        return e ? cuda_fail(e, "hysteresis launch") : ok();
+    }
     // Thresholds (canny.rs:108-121); the maximum is needed unless both
     // thresholds are given as values.
     double max_mag = 0.0;
@@ -4496,18 +4510,11 @@ lucem_status lucem_canny(lucem_ctx *ctx, const lucem_tensor *in, const lucem_can
         return fail(LUCEM_ERR_INVALID_PARAMETER,
                     "invalid parameter `high_threshold`: high_threshold (%g) must be >= low_threshold (%g)", high,
                     low);
-    uint32_t *edges = static_cast<uint32_t *>(out->data);
     // No strong pixel can exist unless high > 0; with low <= 0 nothing grows
-    // from them, so the mask is the strong pixels themselves.
-    if (!(high > 0.0)) {
-        CUDA_TRY(cudaMemsetAsync(edges, 0, (size_t)n * sizeof(uint32_t), cs), "edge map reset");
-        return ok();
-    }
-    const double mask_low = low > 0.0 ? low : high;
-    // The sector slot is free after the suppression: it holds the labels.
+    // from them, so the mask is the strong pixels themselves (the kernels
+    // apply both rules).
     e = timed(kPassElementwise, stream, [&] {
-        return launch_canny_hysteresis(nms, (int)H, (int)W, mask_low, high, reinterpret_cast<uint32_t *>(sector),
-                                       edges, stream);
+        return launch_canny_hysteresis(nms, (int)H, (int)W, nullptr, low, high, labels, edges, stream);
     });
     return e ? cuda_fail(e, "hysteresis launch") : ok();
 }

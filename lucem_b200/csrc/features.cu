@@ -33,6 +33,7 @@
 // index (atomicMin), roots flagged by their strong pixels, then every masked
 // pixel takes its root's flag.  Four launches, no host round trip.
 #include <cuda_runtime.h>
+#include <math_constants.h>
 
 #include <cstdint>
 
@@ -194,10 +195,41 @@ __device__ __forceinline__ void unite(uint32_t *labels, uint32_t a, uint32_t b, 
     }
 }
 
-__global__ void canny_label_init_kernel(const float *__restrict__ nms, int64_t total, double low,
-                                        uint32_t *__restrict__ labels, uint32_t *__restrict__ edges) {
+// canny.rs:108-116 with both thresholds left to their defaults: 0.1 and 0.2
+// of max(max |g|, 0), times that maximum again with use_quantiles; written
+// to thr[0..1] on the device, so the call needs no host round trip.
+__global__ void canny_thresholds_kernel(const unsigned int *__restrict__ max_bits, int quantiles,
+                                        double *__restrict__ thr) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const double m = fmax((double)__uint_as_float(*max_bits), 0.0);
+    double lo = 0.1 * m, hi = 0.2 * m;
+    if (quantiles) {
+        lo *= m;
+        hi *= m;
+    }
+    thr[0] = lo;
+    thr[1] = hi;
+}
+
+// The thresholds: from thr (device) when given, else the arguments.  The
+// mask is nms >= low when low > 0, else the strong pixels themselves (no
+// growth without a positive low threshold); nothing when high <= 0.
+__device__ __forceinline__ void canny_thr(const double *thr, double low, double high, double *mask_low,
+                                          double *strong) {
+    if (thr) {
+        low = thr[0];
+        high = thr[1];
+    }
+    *strong = high;
+    *mask_low = high > 0.0 ? (low > 0.0 ? low : high) : CUDART_INF;
+}
+
+__global__ void canny_label_init_kernel(const float *__restrict__ nms, int64_t total, const double *thr, double low,
+                                        double high, uint32_t *__restrict__ labels, uint32_t *__restrict__ edges) {
+    double mask_low, strong;
+    canny_thr(thr, low, high, &mask_low, &strong);
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
-        labels[i] = (double)nms[i] >= low ? (uint32_t)i : kNoLabel;
+        labels[i] = (double)nms[i] >= mask_low ? (uint32_t)i : kNoLabel;
         edges[i] = 0u;
     }
 }
@@ -222,13 +254,15 @@ __global__ void canny_label_merge_kernel(int H, int W, uint32_t *__restrict__ la
 }
 
 // Every masked pixel's label becomes its root; a strong pixel flags its root.
-__global__ void canny_label_root_kernel(const float *__restrict__ nms, int64_t total, double high,
-                                        uint32_t *__restrict__ labels, uint32_t *__restrict__ edges) {
+__global__ void canny_label_root_kernel(const float *__restrict__ nms, int64_t total, const double *thr, double low,
+                                        double high, uint32_t *__restrict__ labels, uint32_t *__restrict__ edges) {
+    double mask_low, strong;
+    canny_thr(thr, low, high, &mask_low, &strong);
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
         if (__ldcg(labels + i) == kNoLabel) continue;
         const uint32_t r = find_root(labels, (uint32_t)i);
         labels[i] = r;
-        if ((double)nms[i] >= high) edges[r] = 2u;
+        if ((double)nms[i] >= strong) edges[r] = 2u;
     }
 }
 
@@ -259,15 +293,20 @@ int launch_canny_nms(const float *mag, const float *sector, float *nms, int H, i
     return (int)cudaGetLastError();
 }
 
-int launch_canny_hysteresis(const float *nms, int H, int W, double low, double high, uint32_t *labels,
-                            uint32_t *edges, void *stream) {
+int launch_canny_thresholds(const unsigned int *max_bits, int quantiles, double *thr, void *stream) {
+    canny_thresholds_kernel<<<1, 32, 0, static_cast<cudaStream_t>(stream)>>>(max_bits, quantiles, thr);
+    return (int)cudaGetLastError();
+}
+
+int launch_canny_hysteresis(const float *nms, int H, int W, const double *thr, double low, double high,
+                            uint32_t *labels, uint32_t *edges, void *stream) {
     const int64_t total = (int64_t)H * W;
     if (total <= 0) return 0;
     cudaStream_t cs = static_cast<cudaStream_t>(stream);
     const unsigned g = grid_for(total, 256);
-    canny_label_init_kernel<<<g, 256, 0, cs>>>(nms, total, low, labels, edges);
+    canny_label_init_kernel<<<g, 256, 0, cs>>>(nms, total, thr, low, high, labels, edges);
     canny_label_merge_kernel<<<g, 256, 0, cs>>>(H, W, labels);
-    canny_label_root_kernel<<<g, 256, 0, cs>>>(nms, total, high, labels, edges);
+    canny_label_root_kernel<<<g, 256, 0, cs>>>(nms, total, thr, low, high, labels, edges);
     canny_label_final_kernel<<<g, 256, 0, cs>>>(total, labels, edges);
     return (int)cudaGetLastError();
 }

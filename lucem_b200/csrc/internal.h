@@ -167,13 +167,16 @@ int launch_tensor_elementwise(const float *a, const float *b, const float *c, fl
 int launch_resample(const float *in, int H, int W, float *out, int OH, int OW, float m0, float m2, float m4,
                     float m5, int order, int mode, float cval, void *stream);
 // features.cu: Canny's non-maximum suppression (nms, and the maximum of mag
-// as non-negative float bits in *max_bits, to be zeroed first) and its
-// hysteresis by connected components: edges = 1 on the components of
-// (nms >= low) that hold a pixel with nms >= high (labels: H W scratch).
+// as non-negative float bits in *max_bits, to be zeroed first), its default
+// thresholds on the device (thr[0] low, thr[1] high), and its hysteresis by
+// connected components: edges = 1 on the components of (nms >= low) that
+// hold a pixel with nms >= high (labels: H W scratch); the thresholds from
+// thr when it is not null, else low / high.
 int launch_canny_nms(const float *mag, const float *sector, float *nms, int H, int W, unsigned int *max_bits,
                      void *stream);
-int launch_canny_hysteresis(const float *nms, int H, int W, double low, double high, uint32_t *labels,
-                            uint32_t *edges, void *stream);
+int launch_canny_thresholds(const unsigned int *max_bits, int quantiles, double *thr, void *stream);
+int launch_canny_hysteresis(const float *nms, int H, int W, const double *thr, double low, double high,
+                            uint32_t *labels, uint32_t *edges, void *stream);
 // features.cu: scale-space maxima of the blob detectors.
 struct BlobCandidate {
     float response;

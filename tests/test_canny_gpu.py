@@ -175,3 +175,23 @@ def test_canny_errors_and_empty():
     e = lb.canny(torch.empty((0, 8), device="cuda"))
     assert e.shape == (0, 8) and e.dtype == torch.uint32
     assert int(host(lb.canny(torch.zeros((32, 32), device="cuda"))).sum()) == 0
+
+
+def test_default_thresholds_run_in_a_cuda_graph(oracle):
+    """With both thresholds left to their defaults they are computed on the
+    device: the call captures into a CUDA graph, and a replay on new data in
+    the same buffers equals the restatement."""
+    a = integer_image((160, 200), 31)
+    b = integer_image((160, 200), 32)
+    x = dev(a)
+    out = torch.empty((160, 200), dtype=torch.uint32, device="cuda")
+    lb.canny(x, sigma=0.0, out=out)  # sizes the workspace before capture
+    g = lb.Graph()
+    with g:
+        lb.canny(x, sigma=0.0, out=out)
+    x.copy_(dev(b))
+    g.launch()
+    assert np.array_equal(host(out), oracle.canny(b, 0.0))
+    for q in (True, False):
+        assert np.array_equal(host(lb.canny(dev(a), sigma=0.0, use_quantiles=q)),
+                              oracle.canny(a, 0.0, use_quantiles=q))
