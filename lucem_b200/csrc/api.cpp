@@ -4134,16 +4134,32 @@ lucem_status blobs_run(lucem_ctx *ctx, BlobKind kind, const lucem_tensor *in, co
         if (a.x != b.x) return a.x < b.x;
         return a.s < b.s;
     });
+    // The greedy pass checks each candidate against the blobs kept so far.
+    // Two blobs overlap only closer than r1 + r2 <= 2 sqrt(2) max sigma, so
+    // the kept blobs are bucketed on a grid of that cell and a candidate
+    // meets only those of its 3 x 3 cells: the same decisions as checking
+    // every kept blob (a zero overlap never exceeds the threshold).
     std::vector<lucem_blob> kept;
+    const double cell = 2.0 * M_SQRT2 * *std::max_element(sig.begin(), sig.end());
+    const int64_t gx = std::max<int64_t>(1, (int64_t)std::ceil((double)W / cell));
+    const int64_t gy = std::max<int64_t>(1, (int64_t)std::ceil((double)H / cell));
+    std::vector<std::vector<int32_t>> grid((size_t)(gx * gy));
     for (const BlobCandidate &c : cand) {
         const lucem_blob b{c.y, c.x, sig[(size_t)c.s], (double)c.response};
+        const int64_t cy = std::min<int64_t>(gy - 1, (int64_t)((double)c.y / cell));
+        const int64_t cx = std::min<int64_t>(gx - 1, (int64_t)((double)c.x / cell));
         bool drop = false;
-        for (const lucem_blob &k : kept)
-            if (blob_overlap(b, k) > s->overlap) {
-                drop = true;
-                break;
-            }
-        if (!drop) kept.push_back(b);
+        for (int64_t yy = std::max<int64_t>(0, cy - 1); yy <= std::min<int64_t>(gy - 1, cy + 1) && !drop; ++yy)
+            for (int64_t xx = std::max<int64_t>(0, cx - 1); xx <= std::min<int64_t>(gx - 1, cx + 1) && !drop; ++xx)
+                for (int32_t k : grid[(size_t)(yy * gx + xx)])
+                    if (blob_overlap(b, kept[(size_t)k]) > s->overlap) {
+                        drop = true;
+                        break;
+                    }
+        if (!drop) {
+            grid[(size_t)(cy * gx + cx)].push_back((int32_t)kept.size());
+            kept.push_back(b);
+        }
     }
     *n_out = (int64_t)kept.size();
     for (int64_t i = 0; i < std::min<int64_t>(cap, (int64_t)kept.size()); ++i) out[i] = kept[(size_t)i];
