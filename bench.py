@@ -516,14 +516,17 @@ def psf_fit_secondary(dev, steps=2):
 
 
 def _timed_calls(dev, fn, reps, flush=True):
-    """Mean device ms of fn() over reps calls (CUDA events on the current
-    stream), after one warm-up call; L2 flushed before each call."""
+    """Median ms of fn() over reps calls (CUDA events on the current stream,
+    so host work inside a call that synchronises counts too), after one
+    warm-up call; L2 flushed before each call.  The median: in the full
+    bench process a single call of the blob detectors now and then took
+    several ms longer (measured alone, their calls vary by under 5%)."""
     import torch
 
     s = torch.cuda.current_stream(dev)
     buf = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev) if flush else None
     fn()
-    tot = 0.0
+    times = []
     for _ in range(reps):
         if buf is not None:
             buf.fill_(1.0)
@@ -532,8 +535,8 @@ def _timed_calls(dev, fn, reps, flush=True):
         fn()
         b.record(s)
         torch.cuda.synchronize(dev)
-        tot += a.elapsed_time(b)
-    return tot / reps
+        times.append(a.elapsed_time(b))
+    return float(np.median(times))
 
 
 def spectral_ops_secondary(dev, reps=10):
