@@ -4140,7 +4140,11 @@ lucem_status blobs_run(lucem_ctx *ctx, BlobKind kind, const lucem_tensor *in, co
     // meets only those of its 3 x 3 cells: the same decisions as checking
     // every kept blob (a zero overlap never exceeds the threshold).
     std::vector<lucem_blob> kept;
-    const double cell = 2.0 * M_SQRT2 * *std::max_element(sig.begin(), sig.end());
+    // Cells no smaller than the overlap reach; no more cells than about
+    // four per candidate (a large image with small sigmas stays bounded).
+    const double reach = 2.0 * M_SQRT2 * *std::max_element(sig.begin(), sig.end());
+    const double cell = std::max(reach, std::sqrt((double)H * (double)W /
+                                                  (double)std::max<size_t>(1024, 4 * cand.size())));
     const int64_t gx = std::max<int64_t>(1, (int64_t)std::ceil((double)W / cell));
     const int64_t gy = std::max<int64_t>(1, (int64_t)std::ceil((double)H / cell));
     std::vector<std::vector<int32_t>> grid((size_t)(gx * gy));
