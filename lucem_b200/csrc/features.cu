@@ -30,11 +30,14 @@
 // reaches are exactly the 8-connected components of the weak mask that hold
 // a strong pixel, so here it is connected-component labelling on the device:
 // union-find over the mask where a label only ever moves to a smaller pixel
-// index (atomicMin), roots flagged by their strong pixels, then every masked
-// pixel takes its root's flag.  Four launches, no host round trip.
+// index (atomicMin; per 32 x 32 tile in shared memory first, then across the
+// tile borders in global memory), roots flagged by their strong pixels, then
+// every masked pixel takes its root's flag.  Four launches, no host round
+// trip.
 #include <cuda_runtime.h>
 #include <math_constants.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "internal.h"
@@ -224,25 +227,111 @@ __device__ __forceinline__ void canny_thr(const double *thr, double low, double 
     *mask_low = high > 0.0 ? (low > 0.0 ? low : high) : CUDART_INF;
 }
 
-__global__ void canny_label_init_kernel(const float *__restrict__ nms, int64_t total, const double *thr, double low,
-                                        double high, uint32_t *__restrict__ labels, uint32_t *__restrict__ edges) {
-    double mask_low, strong;
-    canny_thr(thr, low, high, &mask_low, &strong);
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
-        labels[i] = (double)nms[i] >= mask_low ? (uint32_t)i : kNoLabel;
-        edges[i] = 0u;
+// The labelling runs per 32 x 32 tile in shared memory first: the unions
+// inside a tile use shared-memory atomics, and every masked pixel leaves
+// with the global index of its tile-local root (the smallest index of its
+// tile-local component: row-major order inside a tile is raster order).
+// Only the pairs that cross a tile border are then joined in global memory.
+constexpr int kLabelTile = 32;
+
+__device__ __forceinline__ uint32_t find_root_s(const volatile uint32_t *L, uint32_t x) {
+    uint32_t p = L[x];
+    while (p != x) {
+        x = p;
+        p = L[x];
+    }
+    return x;
+}
+
+// As unite(), on a tile's shared labels (every retry lowers a + b, so the
+// loop ends within 2 * 1024 rounds).
+__device__ __forceinline__ void unite_s(uint32_t *L, uint32_t a, uint32_t b) {
+    for (int it = 0; it < 2 * kLabelTile * kLabelTile + 2; ++it) {
+        a = find_root_s(L, a);
+        b = find_root_s(L, b);
+        if (a == b) return;
+        if (a < b) {
+            const uint32_t t = a;
+            a = b;
+            b = t;
+        }
+        const uint32_t old = atomicMin(L + a, b);
+        if (old == a) return;
+        a = old;
     }
 }
 
-// Unions with the four neighbours that come before the pixel in raster
-// order (left, and the three above); the other four do the same towards it.
-__global__ void canny_label_merge_kernel(int H, int W, uint32_t *__restrict__ labels) {
-    const int64_t total = (int64_t)H * W, bound = 2 * total + 2;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+__global__ void __launch_bounds__(256) canny_label_local_kernel(const float *__restrict__ nms, int H, int W,
+                                                                const double *thr, double low, double high,
+                                                                uint32_t *__restrict__ labels,
+                                                                uint32_t *__restrict__ edges) {
+    constexpr int T = kLabelTile, TT = T * T;
+    __shared__ uint32_t L[TT];
+    double mask_low, strong;
+    canny_thr(thr, low, high, &mask_low, &strong);
+    const int tiles_x = (W + T - 1) / T, tiles = tiles_x * ((H + T - 1) / T);
+    for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const int y0 = (tile / tiles_x) * T, x0 = (tile % tiles_x) * T;
+        for (int k = threadIdx.x; k < TT; k += blockDim.x) {
+            const int y = y0 + k / T, x = x0 + k % T;
+            bool m = false;
+            if (y < H && x < W) {
+                const int64_t i = (int64_t)y * W + x;
+                m = (double)nms[i] >= mask_low;
+                edges[i] = 0u;
+            }
+            L[k] = m ? (uint32_t)k : kNoLabel;
+        }
+        __syncthreads();
+        // Unions with the raster-earlier neighbours inside the tile.
+        for (int k = threadIdx.x; k < TT; k += blockDim.x) {
+            if (L[k] == kNoLabel) continue;
+            const int ly = k / T, lx = k % T;
+            if (lx > 0 && L[k - 1] != kNoLabel) unite_s(L, (uint32_t)k, (uint32_t)(k - 1));
+            if (ly > 0) {
+                for (int dx = -1; dx <= 1; ++dx) {
+                    const int nx = lx + dx;
+                    if (nx < 0 || nx >= T) continue;
+                    const int j = k - T + dx;
+                    if (L[j] != kNoLabel) unite_s(L, (uint32_t)k, (uint32_t)j);
+                }
+            }
+        }
+        __syncthreads();
+        for (int k = threadIdx.x; k < TT; k += blockDim.x) {
+            const int y = y0 + k / T, x = x0 + k % T;
+            if (y >= H || x >= W) continue;
+            uint32_t g = kNoLabel;
+            if (L[k] != kNoLabel) {
+                const uint32_t r = find_root_s(L, (uint32_t)k);
+                g = (uint32_t)((int64_t)(y0 + (int)r / T) * W + x0 + (int)r % T);
+            }
+            labels[(int64_t)y * W + x] = g;
+        }
+        __syncthreads();
+    }
+}
+
+// The pairs across tile borders: a pixel on a tile's top row joins its
+// three neighbours above, one on its left column its left and upper-left
+// neighbours, one on its right column its upper-right neighbour (all in
+// other tiles, all raster-earlier).  One thread per (tile, border slot).
+__global__ void canny_label_border_kernel(int H, int W, uint32_t *__restrict__ labels) {
+    constexpr int T = kLabelTile;
+    const int tiles_x = (W + T - 1) / T, tiles = tiles_x * ((H + T - 1) / T);
+    const int64_t total = (int64_t)tiles * 3 * T, bound = 2 * (int64_t)H * W + 2;
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < total; s += (int64_t)gridDim.x * blockDim.x) {
+        const int tile = (int)(s / (3 * T)), slot = (int)(s % (3 * T));
+        const int y0 = (tile / tiles_x) * T, x0 = (tile % tiles_x) * T;
+        int y, x;
+        if (slot < T) { y = y0; x = x0 + slot; }                    // top row
+        else if (slot < 2 * T) { y = y0 + slot - T; x = x0; }       // left column
+        else { y = y0 + slot - 2 * T; x = x0 + T - 1; }             // right column
+        if (y >= H || x >= W) continue;
+        const int64_t i = (int64_t)y * W + x;
         if (__ldcg(labels + i) == kNoLabel) continue;
-        const int y = (int)(i / W), x = (int)(i - (int64_t)y * W);
-        if (x > 0 && __ldcg(labels + i - 1) != kNoLabel) unite(labels, (uint32_t)i, (uint32_t)(i - 1), bound);
-        if (y > 0) {
+        const bool top = y == y0 && y > 0, left = x == x0 && x > 0, right = x == x0 + T - 1 && y > y0;
+        if (top) {
             for (int dx = -1; dx <= 1; ++dx) {
                 const int nx = x + dx;
                 if (nx < 0 || nx >= W) continue;
@@ -250,6 +339,13 @@ __global__ void canny_label_merge_kernel(int H, int W, uint32_t *__restrict__ la
                 if (__ldcg(labels + j) != kNoLabel) unite(labels, (uint32_t)i, (uint32_t)j, bound);
             }
         }
+        if (left) {
+            if (__ldcg(labels + i - 1) != kNoLabel) unite(labels, (uint32_t)i, (uint32_t)(i - 1), bound);
+            if (y > y0 && __ldcg(labels + i - W - 1) != kNoLabel)
+                unite(labels, (uint32_t)i, (uint32_t)(i - W - 1), bound);
+        }
+        if (right && x + 1 < W && __ldcg(labels + i - W + 1) != kNoLabel)
+            unite(labels, (uint32_t)i, (uint32_t)(i - W + 1), bound);
     }
 }
 
@@ -304,8 +400,10 @@ int launch_canny_hysteresis(const float *nms, int H, int W, const double *thr, d
     if (total <= 0) return 0;
     cudaStream_t cs = static_cast<cudaStream_t>(stream);
     const unsigned g = grid_for(total, 256);
-    canny_label_init_kernel<<<g, 256, 0, cs>>>(nms, total, thr, low, high, labels, edges);
-    canny_label_merge_kernel<<<g, 256, 0, cs>>>(H, W, labels);
+    const int64_t tiles = (int64_t)((W + kLabelTile - 1) / kLabelTile) * ((H + kLabelTile - 1) / kLabelTile);
+    canny_label_local_kernel<<<(unsigned)std::min<int64_t>(tiles, 148 * 8), 256, 0, cs>>>(nms, H, W, thr, low, high,
+                                                                                         labels, edges);
+    canny_label_border_kernel<<<grid_for(tiles * 3 * kLabelTile, 256), 256, 0, cs>>>(H, W, labels);
     canny_label_root_kernel<<<g, 256, 0, cs>>>(nms, total, thr, low, high, labels, edges);
     canny_label_final_kernel<<<g, 256, 0, cs>>>(total, labels, edges);
     return (int)cudaGetLastError();
