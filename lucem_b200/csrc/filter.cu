@@ -90,31 +90,62 @@ constexpr int kRowMaxHalo = 15360; // beyond this: direct kernel
 constexpr int kColI = 64, kColK = 32;
 constexpr int kColMaxHalo = 960;
 
+// Register blocking of both kernels: a thread computes several consecutive
+// outputs, taps in blocks of 8 held in registers, each staged sample loaded
+// once per block and used by every output it reaches.  Every output still
+// accumulates its taps in index order from 0 (the reference's order), so
+// the results are those of one fmaf chain per output.
+constexpr int kRowPer = 4;  // consecutive outputs per thread along a contiguous axis
+
+// Staged samples along a contiguous axis at index i + i / 32: four
+// consecutive outputs per lane read 32 distinct banks.
+__device__ __forceinline__ int row_slot(int i) { return i + (i >> 5); }
+
 template <typename T, int MODE>
 __global__ void __launch_bounds__(256)
 corr_row_kernel(const T *__restrict__ in, float scale, float *__restrict__ out, int64_t outer,
                 int len, const float *__restrict__ w, int size, int left, float cval) {
     extern __shared__ float4 smem4[];
     float *S = reinterpret_cast<float *>(smem4);
-    float *Wsm = S + kRowSeg + size - 1;
+    const int n_in = kRowSeg + size - 1;
+    float *Wsm = S + row_slot(n_in + 16);
     const int segs = (len + kRowSeg - 1) / kRowSeg;
     for (int t = threadIdx.x; t < size; t += blockDim.x) Wsm[t] = w[t];
     for (int64_t b = blockIdx.x; b < outer * segs; b += gridDim.x) {
         int64_t o = b / segs;
         int i0 = (int)(b - o * segs) * kRowSeg;
         const T *row = in + o * len;
-        int n_in = kRowSeg + size - 1;
         __syncthreads();
         for (int j = threadIdx.x; j < n_in; j += blockDim.x) {
             int q = pad_index<MODE>(i0 - left + j, len);
-            S[j] = q < 0 ? cval : static_cast<float>(row[q]) * scale;
+            S[row_slot(j)] = q < 0 ? cval : static_cast<float>(row[q]) * scale;
         }
         __syncthreads();
-        for (int j = threadIdx.x; j < kRowSeg; j += blockDim.x) {
-            if (i0 + j >= len) break;
-            float acc = 0.0f;
-            for (int t = 0; t < size; ++t) acc = fmaf(Wsm[t], S[j + t], acc);
-            out[o * len + i0 + j] = acc;
+        for (int jb = threadIdx.x; jb < kRowSeg / kRowPer; jb += blockDim.x) {
+            const int j0 = jb * kRowPer;
+            if (i0 + j0 >= len) break;
+            float acc[kRowPer];
+#pragma unroll
+            for (int j = 0; j < kRowPer; ++j) acc[j] = 0.0f;
+            for (int s0 = 0; s0 < size; s0 += 8) {
+                float wv[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) wv[u] = s0 + u < size ? Wsm[s0 + u] : 0.0f;
+                // Samples past the staged ones (at most 7, in the slack
+                // after S) meet only taps past the end: never accumulated.
+#pragma unroll
+                for (int m = 0; m < 8 + kRowPer - 1; ++m) {
+                    const float x = S[row_slot(j0 + s0 + m)];
+#pragma unroll
+                    for (int j = 0; j < kRowPer; ++j) {
+                        const int u = m - j;
+                        if (u >= 0 && u < 8 && s0 + u < size) acc[j] = fmaf(wv[u], x, acc[j]);
+                    }
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < kRowPer; ++j)
+                if (i0 + j0 + j < len) out[o * len + i0 + j0 + j] = acc[j];
         }
     }
 }
@@ -124,8 +155,8 @@ __global__ void __launch_bounds__(256)
 corr_col_kernel(const T *__restrict__ in, float scale, float *__restrict__ out, int64_t outer,
                 int len, int64_t inner, const float *__restrict__ w, int size, int left, float cval) {
     extern __shared__ float4 smem4[];
-    float *S = reinterpret_cast<float *>(smem4);  // [kColI + size - 1][kColK]
-    float *Wsm = S + (kColI + size - 1) * kColK;
+    float *S = reinterpret_cast<float *>(smem4);  // [kColI + size - 1 + 8 slack rows][kColK]
+    float *Wsm = S + (kColI + size - 1 + 8) * kColK;
     const int64_t ks = (inner + kColK - 1) / kColK;
     const int is = (len + kColI - 1) / kColI;
     const int64_t nblk = outer * is * ks;
@@ -153,14 +184,29 @@ corr_col_kernel(const T *__restrict__ in, float scale, float *__restrict__ out, 
         __syncthreads();
         int64_t k = k0 + kk;
         if (k < inner) {
+            const int ii0 = ig * 8;
+            float acc[8];
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                int ii = ig * 8 + j;
-                if (i0 + ii >= len) break;
-                float acc = 0.0f;
-                for (int t = 0; t < size; ++t) acc = fmaf(Wsm[t], S[(ii + t) * kColK + kk], acc);
-                out[(o * len + i0 + ii) * inner + k] = acc;
+            for (int j = 0; j < 8; ++j) acc[j] = 0.0f;
+            for (int s0 = 0; s0 < size; s0 += 8) {
+                float wv[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) wv[u] = s0 + u < size ? Wsm[s0 + u] : 0.0f;
+                // Rows past the staged ones (at most 7, in the slack rows
+                // after S) meet only taps past the end: never accumulated.
+#pragma unroll
+                for (int m = 0; m < 15; ++m) {
+                    const float x = S[(ii0 + s0 + m) * kColK + kk];
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        const int u = m - j;
+                        if (u >= 0 && u < 8 && s0 + u < size) acc[j] = fmaf(wv[u], x, acc[j]);
+                    }
+                }
             }
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+                if (i0 + ii0 + j < len) out[(o * len + i0 + ii0 + j) * inner + k] = acc[j];
         }
     }
 }
@@ -189,13 +235,13 @@ int corr_launch(const T *in, float scale, float *out, int64_t outer, int64_t len
                 const float *w, int size, int left, float cval, cudaStream_t s) {
     const int sms = sm_count();
     if (inner == 1 && size - 1 <= kRowMaxHalo) {
-        size_t smem = (size_t)(kRowSeg + 2 * size) * sizeof(float) + 16;
+        size_t smem = (size_t)((kRowSeg + size - 1 + 16) + (kRowSeg + size + 15) / 32 + 1 + size) * sizeof(float) + 16;
         int64_t nb = outer * ((len + kRowSeg - 1) / kRowSeg);
         int grid = (int)(nb < (int64_t)sms * 16 ? nb : (int64_t)sms * 16);
         cudaFuncSetAttribute(corr_row_kernel<T, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         corr_row_kernel<T, MODE><<<grid, 256, smem, s>>>(in, scale, out, outer, (int)len, w, size, left, cval);
     } else if (inner > 1 && size - 1 <= kColMaxHalo) {
-        size_t smem = (size_t)((kColI + size - 1) * kColK + size) * sizeof(float) + 16;
+        size_t smem = (size_t)((kColI + size - 1 + 8) * kColK + size) * sizeof(float) + 16;
         int64_t nb = outer * ((len + kColI - 1) / kColI) * ((inner + kColK - 1) / kColK);
         int grid = (int)(nb < (int64_t)sms * 16 ? nb : (int64_t)sms * 16);
         cudaFuncSetAttribute(corr_col_kernel<T, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
