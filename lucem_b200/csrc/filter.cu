@@ -87,7 +87,8 @@ namespace {
 
 constexpr int kRowSeg = 1024;      // outputs per CTA along a contiguous axis
 constexpr int kRowMaxHalo = 15360; // beyond this: direct kernel
-constexpr int kColI = 64, kColK = 32;
+constexpr int kColI = 128, kColK = 32;
+constexpr int kColPer = kColI / 8;  // consecutive outputs per thread along a strided axis (8 row groups)
 constexpr int kColMaxHalo = 960;
 
 // Register blocking of both kernels: a thread computes several consecutive
@@ -162,7 +163,7 @@ corr_col_kernel(const T *__restrict__ in, float scale, float *__restrict__ out, 
     const int64_t nblk = outer * is * ks;
     for (int t = threadIdx.x; t < size; t += blockDim.x) Wsm[t] = w[t];
     const int kk = threadIdx.x & (kColK - 1);
-    const int ig = threadIdx.x / kColK;  // 0..7, 8 outputs each
+    const int ig = threadIdx.x / kColK;  // 0..7, kColPer outputs each
     for (int64_t b = blockIdx.x; b < nblk; b += gridDim.x) {
         int64_t o = b / (is * ks);
         int64_t r = b - o * is * ks;
@@ -184,10 +185,10 @@ corr_col_kernel(const T *__restrict__ in, float scale, float *__restrict__ out, 
         __syncthreads();
         int64_t k = k0 + kk;
         if (k < inner) {
-            const int ii0 = ig * 8;
-            float acc[8];
+            const int ii0 = ig * kColPer;
+            float acc[kColPer];
 #pragma unroll
-            for (int j = 0; j < 8; ++j) acc[j] = 0.0f;
+            for (int j = 0; j < kColPer; ++j) acc[j] = 0.0f;
             for (int s0 = 0; s0 < size; s0 += 8) {
                 float wv[8];
 #pragma unroll
@@ -195,17 +196,17 @@ corr_col_kernel(const T *__restrict__ in, float scale, float *__restrict__ out, 
                 // Rows past the staged ones (at most 7, in the slack rows
                 // after S) meet only taps past the end: never accumulated.
 #pragma unroll
-                for (int m = 0; m < 15; ++m) {
+                for (int m = 0; m < 8 + kColPer - 1; ++m) {
                     const float x = S[(ii0 + s0 + m) * kColK + kk];
 #pragma unroll
-                    for (int j = 0; j < 8; ++j) {
+                    for (int j = 0; j < kColPer; ++j) {
                         const int u = m - j;
                         if (u >= 0 && u < 8 && s0 + u < size) acc[j] = fmaf(wv[u], x, acc[j]);
                     }
                 }
             }
 #pragma unroll
-            for (int j = 0; j < 8; ++j)
+            for (int j = 0; j < kColPer; ++j)
                 if (i0 + ii0 + j < len) out[(o * len + i0 + ii0 + j) * inner + k] = acc[j];
         }
     }
