@@ -365,3 +365,20 @@ def test_canny_oracle_reference_case(oracle):
     assert oracle.canny_hysteresis(nms, 1.0, 0.0).sum() == 0
     with pytest.raises(ValueError):
         oracle.canny_thresholds(10.0, 0.5, 0.4)
+
+
+def test_canny_oracle_sectors_and_suppression(oracle):
+    """feature/kernels/canny.rs:13-86: the sector of a gradient along x is 0,
+    along y 2, along the main diagonal 1 and the anti-diagonal 3 (Sobel of
+    integer ramps is exact); suppression keeps a pixel only when it is >= both
+    neighbours along its sector, and clears the one-pixel border."""
+    y, x = np.mgrid[0:9, 0:9].astype(np.float32)
+    for img, sec in ((x, 0), (y, 2), (x + y, 1), (x - y, 3)):
+        mag, sector = oracle.canny_gradients(img, 0.0, mode="nearest")
+        assert (sector[2:-2, 2:-2] == sec).all(), sec
+        assert np.allclose(mag[2:-2, 2:-2], mag[4, 4])
+    # A ridge of magnitudes along x with a peak row: sector 2 compares rows.
+    mag = np.tile(np.array([1, 2, 5, 2, 1], np.float32)[:, None], (1, 6))
+    nms = oracle.canny_nms(mag, np.full(mag.shape, 2))
+    assert (nms[2, 1:-1] == 5).all() and nms[[1, 3]].max() == 0
+    assert nms[0].max() == 0 and nms[:, 0].max() == 0 and nms[:, -1].max() == 0
