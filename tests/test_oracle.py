@@ -382,3 +382,19 @@ def test_canny_oracle_sectors_and_suppression(oracle):
     nms = oracle.canny_nms(mag, np.full(mag.shape, 2))
     assert (nms[2, 1:-1] == 5).all() and nms[[1, 3]].max() == 0
     assert nms[0].max() == 0 and nms[:, 0].max() == 0 and nms[:, -1].max() == 0
+
+
+def test_blob_oracle_scales_and_overlap(oracle):
+    """feature/blobs.rs:96-136, 256-263: linear and log-spaced scales, the DoG
+    ladder sigma * ratio^k up to max_sigma, and the circle-overlap fraction
+    (radius sqrt(2) sigma): 1 for a blob inside another, 0 when apart, the
+    lens area over the smaller disc in between (two equal discs at distance
+    r: 2 acos(1/2) - sqrt(3)/2 over pi = 0.391)."""
+    np.testing.assert_allclose(oracle.blob_sigmas(1.0, 3.0, 5, False), [1.0, 1.5, 2.0, 2.5, 3.0])
+    np.testing.assert_allclose(oracle.blob_sigmas(1.0, 4.0, 3, True), [1.0, 2.0, 4.0])
+    np.testing.assert_allclose(oracle.dog_sigmas(1.0, 10.0, 1.6), [1.0, 1.6, 2.56, 4.096, 6.5536])
+    assert oracle.blob_overlap((5, 5, 2.0), (5, 5, 1.0)) == 1.0
+    assert oracle.blob_overlap((0, 0, 1.0), (0, 10, 1.0)) == 0.0
+    r = np.sqrt(2.0) * 2.0
+    got = oracle.blob_overlap((0, 0, 2.0), (0, r, 2.0))
+    assert abs(got - (2 * np.arccos(0.5) - np.sqrt(3) / 2) / np.pi) < 1e-12
