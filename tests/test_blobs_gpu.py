@@ -79,3 +79,23 @@ def test_blob_errors_and_empty():
         lb.blobs_log(torch.ones((2, 8, 8), device="cuda"))
     assert lb.blobs_log(torch.empty((0, 8), device="cuda")) == []
     assert lb.blobs_log(torch.ones((2, 2), device="cuda")) == []  # inside the border
+
+
+@pytest.mark.parametrize("kind", ["log", "doh"])
+def test_crowded_field_pruning_equals_the_restatement(oracle, kind):
+    """Blobs close enough to overlap, so the greedy pruning (done on the
+    host over a grid of cells as wide as the overlap reach) drops many
+    candidates: the kept list must equal the oracle's all-pairs pass."""
+    rng = np.random.default_rng(41 if kind == "log" else 43)
+    blobs = [(rng.uniform(8, 152), rng.uniform(8, 172), rng.uniform(1.5, 4.0), rng.uniform(0.5, 1.5))
+             for _ in range(70)]
+    img = gaussian_field((160, 180), blobs, background=0.02)
+    x = torch.from_numpy(img).cuda()
+    thr = 0.002 if kind == "doh" else 0.02
+    fn = lb.blobs_log if kind == "log" else lb.blobs_doh
+    got = fn(x, min_sigma=1.5, max_sigma=5.0, num_sigma=6, threshold=thr, overlap=0.3)
+    sig = oracle.blob_sigmas(1.5, 5.0, 6, False)
+    want = oracle.extract_blobs(oracle.blob_stack(img, kind, sig, 1.6), sig, thr, 0.3, 1)
+    assert len(got) == len(want) > 20, (len(got), len(want))
+    for g, w in zip(got, want):
+        assert (g.y, g.x) == w[:2] and g.sigma == pytest.approx(w[2], rel=1e-12)
